@@ -1,0 +1,347 @@
+#!/usr/bin/env python
+"""Benchmark: DOF-stage updates/s of the fused RK4 stage kernel on the
+512 x 512, P = 4 perturbed-quad workload (19.7M DOF), FP64.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One timed step = one RK4 time step = 5 fused stage launches on the resident
+state.  K steps are timed with CUDA events on the launching stream, bracketed
+by barrier + synchronize; the maximum over ranks is reported.  Under torchrun
+(N > 1) each rank runs an independent replica of the workload (weak scaling;
+a single mesh is not partitioned).  Rank 0 prints one JSON line.
+
+--impl reference times the reference's own CPU code (oracle/_ref, compiled from
+its sources) on the same workload, rank 0 only, one thread.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DOF-stage updates/s & HBM %; WaveHoltz solves/s at 1e-6, learned vs plain"
+UNIT = "DOF-stage/s"
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0  # GB/s, used only when MEASURED_PEAKS.json is absent
+REF_TIME_BUDGET = 150.0  # seconds of reference CPU work in --impl reference
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=512, help="elements per direction")
+    ap.add_argument("--P", type=int, default=4, help="polynomial degree (n_colloc = P + 1)")
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the FP32 companion measurement")
+    ap.add_argument("--tile", type=int, default=0)
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------- workload
+def workload(n: int, P: int, seed: int = 2024):
+    """Config: n x n quads on [-1,1]^2, interior vertices perturbed by U(-0.2h, 0.2h), outflow
+    boundaries, initial p = sum of 8 Gaussian pulses (centres U[-0.8,0.8]^2, widths U[0.03,0.1],
+    amplitudes N(0,1)), u = v = 0; dt = 0.1 min_h / (P+1)^2."""
+    from wavedg_b200 import meshgen as mg
+
+    v, q = mg.perturbed_rect(n, 0.2, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    centers = rng.uniform(-0.8, 0.8, size=(8, 2))
+    sigmas = rng.uniform(0.03, 0.1, size=8)
+    amps = rng.standard_normal(8)
+    return v, q, centers, sigmas, amps
+
+
+def algorithmic_bytes_per_step(ndof: int, nel: int, real: int) -> int:
+    """Per RK4 step: stage 0 reads u, writes du and u'; stages 1-4 also read du.
+    Plus the 64-byte corner block of every element per stage."""
+    return ndof * real * (3 + 4 * 4) + 5 * 64 * nel
+
+
+def peak_hbm():
+    try:
+        with open(PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi sampling of the GPU's clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.file is None:
+            return None
+        try:
+            self.file.flush()
+            rows = [r.split(", ") for r in open(self.file.name).read().strip().splitlines()]
+            os.unlink(self.file.name)
+        except Exception:
+            return None
+        rows = [r for r in rows if len(r) >= 9 and (self.uuid is None or self.uuid in r[0])]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].strip().replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].strip().replace(".", "").isdigit())
+                if any(r[3].strip().replace(".", "").isdigit() for r in rows) else None}
+
+
+# ------------------------------------------------------------ our arm
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    import wavedg_b200 as W
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier(device_ids=[local_rank])
+        torch.cuda.synchronize()
+
+    v, q, centers, sigmas, amps = workload(args.n, args.P)
+    mesh = W.Mesh2D.from_vertices(v, q)
+    basis = W.QuadratureRule.quadrature_rule(args.P + 1, W.QuadratureRule.GaussLobatto)
+    bc = np.zeros(mesh.n_edges(1), dtype=np.int32)
+    dt = 0.1 * mesh.min_h() / (args.P + 1) ** 2
+    stream = torch.cuda.current_stream()
+
+    def measure(precision, steps, warmup, tile=0):
+        sys_ = W.WaveSystem(mesh, basis, bc, precision=precision, device=local_rank)
+        sys_.set_stream(stream)
+        if tile:
+            sys_.tile = tile
+        u0 = torch.zeros(sys_.ndof, dtype=torch.float64, device="cuda")
+        sys_.load_gaussians(centers, sigmas, amps, 1.0, 0, True, out=u0)
+        sys_.upload(u0)
+        t = sys_.step_state(dt, 0.0, warmup)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        t = sys_.step_state(dt, t, steps)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        sys_.sync()
+        energy = sys_.energy()
+        return sys_, ms, energy, t
+
+    dev_props = torch.cuda.get_device_properties(local_rank)
+    uuid = str(getattr(dev_props, "uuid", "")) or None
+    with ClockSampler(uuid) as clk:
+        sys_, ms, energy, t_end = measure(args.precision, args.steps, args.warmup, args.tile)
+    clocks = clk.summary()
+    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms = float(ms_t.item())
+    ndof, nel = sys_.ndof, mesh.n_elem()
+    real = 8 if args.precision == "fp64" else 4
+    ms_step = ms / args.steps
+    value = world * ndof * 5 * args.steps / (ms / 1e3)
+
+    # e2e: the reference-facing C-ABI call with pinned host buffers, one RK4 step per call
+    e2e_steps = max(1, min(args.e2e_steps, args.steps))
+    host = torch.empty(ndof, dtype=torch.float64, pin_memory=True)
+    host.copy_(torch.from_numpy(sys_.download()))
+    hn = host.numpy()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sys_.rk4_steps(hn, dt, 0.0, 1)  # warm the staging path
+    barrier()
+    e0.record(stream)
+    tt = 0.0
+    for _ in range(e2e_steps):
+        tt = sys_.rk4_steps(hn, dt, tt, 1)
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    e2e_t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_ms = float(e2e_t.item())
+    e2e_value = world * ndof * 5 * e2e_steps / (e2e_ms / 1e3)
+
+    # roofline of the stage kernel: algorithmic bytes per step / device time per step
+    peak, peak_kind = peak_hbm()
+    bytes_step = algorithmic_bytes_per_step(ndof, nel, real)
+    achieved = bytes_step / (ms_step / 1e3) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get(f"{args.precision}_bytes_per_step_512")
+        except Exception:
+            traffic = None
+
+    extra = {"energy_final": energy, "t_final": t_end, "dt": dt, "tile": sys_.tile, "peak_kind": peak_kind}
+    if not args.no_extras and args.precision == "fp64":
+        s32, ms32, _, _ = measure("fp32", args.steps, args.warmup)
+        b32 = algorithmic_bytes_per_step(ndof, nel, 4)
+        extra["fp32"] = {"value": world * ndof * 5 * args.steps / (ms32 / 1e3), "unit": UNIT,
+                         "ms_per_step": ms32 / args.steps,
+                         "hbm_gbs": b32 / (ms32 / args.steps / 1e3) / 1e9,
+                         "frac": b32 / (ms32 / args.steps / 1e3) / 1e9 / peak}
+        del s32
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(v, q, bc, args.P + 1, dt, sys_.download())
+
+    if dist is not None:
+        dist.barrier(device_ids=[local_rank])
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32",
+        "data": "synthetic: seeded perturbed quad mesh and 8-Gaussian initial pressure (no dataset)",
+        "config": {"workload": f"rk4_{args.precision}_{args.n}x{args.n}_P{args.P}_perturbed_outflow",
+                   "elements": nel, "ndof": ndof, "P": args.P, "step": "1 RK4 step = 5 fused stage launches",
+                   "l2": "inputs larger than L2 (three 157 MB state buffers rotate)",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "stage_kernel", "bytes_per_step": bytes_step},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": ndof * 8, "d2h_bytes_per_step": ndof * 8,
+                "steps": e2e_steps, "api": "wdg_rk4_steps(host pinned u, nsteps=1)"},
+        "gpu_launches": 5 * args.steps,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+        "extra": extra,
+    }
+    print(json.dumps(out), flush=True)
+
+
+# ----------------------------------------------------------- CPU side
+def _ref_lib():
+    from oracle import cpu
+
+    if cpu.available("reference"):
+        return "reference", cpu
+    return "port", cpu
+
+
+def cpu_baseline(v, q, bc, n, dt, u0, budget=30.0):
+    """Reference CPU code on the same workload, 1 thread: set-up excluded, then RK4 steps until
+    the time budget (at least one full step)."""
+    kind, cpu = _ref_lib()
+    libkind = "reference" if kind == "reference" else "oracle"
+    mesh = cpu.Mesh(v, q, libkind)
+    op = cpu.Op(mesh, n, bc)
+    u = np.ascontiguousarray(u0, dtype=np.float64)
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        u, _ = op.rk4(u, dt, 1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el > budget or steps >= 50:
+            break
+    value = op.ndof * 5 * steps / el
+    return {"value": value, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"{steps} RK4 step(s) of the same {mesh.n_elem} element P={n - 1} workload, "
+                      f"operator set-up excluded, single thread ({os.cpu_count()} host cores present)"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    kind, cpu = _ref_lib()
+    libkind = "reference" if kind == "reference" else "oracle"
+    v, q, centers, sigmas, amps = workload(args.n, args.P)
+    n = args.P + 1
+    mesh = cpu.Mesh(v, q, libkind)
+    bc = np.zeros(mesh.n_edges(1), dtype=np.int32)
+    t_setup = time.perf_counter()
+    op = cpu.Op(mesh, n, bc)
+    u = op.load_gaussians(centers, sigmas, amps, 1.0, 0, True)
+    t_setup = time.perf_counter() - t_setup
+    dt = 0.1 * mesh.min_h() / n ** 2
+    # warm-up (at most one step) also measures the cost of a step
+    t0 = time.perf_counter()
+    u, _ = op.rk4(u, dt, 1)
+    per_step = time.perf_counter() - t0
+    runs = max(1, min(args.steps, int(REF_TIME_BUDGET / max(per_step, 1e-9))))
+    t0 = time.perf_counter()
+    u, _ = op.rk4(u, dt, runs)
+    el = time.perf_counter() - t0
+    value = op.ndof * 5 * runs / el
+    sample = (f"{runs} of {args.steps} requested RK4 steps (after 1 warm-up step) on the full {args.n}x{args.n} "
+              f"P={args.P} mesh, single thread, set-up ({t_setup:.1f} s) excluded")
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / runs * 1e3, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (same workload as ours)",
+           "config": {"workload": f"rk4_fp64_{args.n}x{args.n}_P{args.P}_perturbed_outflow",
+                      "elements": mesh.n_elem, "ndof": op.ndof, "P": args.P, "step": "1 RK4 step",
+                      "parallelism": "1 host thread (the reference is serial; its MPI build is unavailable here)"},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,180 @@
+/* wdg_b200.h -- C ABI of the B200 (sm_100a) wave hot path.
+ *
+ * Every entry point replaces one operator of the reference waveDG library
+ * (arotem3/waveDG) on the 2D, Gauss-Lobatto, approximate-quadrature path; the
+ * reference interface each one stands in for is cited beside it
+ * (path:line within the reference project).  Layouts are the reference's,
+ * column-major with the first index fastest:
+ *
+ *   state / RHS   u(d, i, j, el)        d = (p, u_x, u_y), i, j < n    (docs/docs.md:55-61)
+ *   face traces   uf(i, d, side, edge)                                (wavedg/FaceProlongator.hpp:43)
+ *
+ * Conventions
+ *   - Every function returns 0 (WDG_OK) or a negative WDG_ERR_* code; the
+ *     message of the last failure on the calling thread is wdg_last_error().
+ *   - Array arguments may be host or device memory; the library asks the CUDA
+ *     runtime which.  Host arrays are staged through the handle's device
+ *     buffers and the call returns when the result is back on the host.
+ *     Device arrays are used in place and the call is asynchronous on the
+ *     handle's stream (wdg_wave_set_stream; default: the legacy default
+ *     stream); wdg_wave_sync() waits and reports device-side errors.
+ *   - Like the reference's operators, a handle is not re-entrant: calls on one
+ *     handle must not overlap.  Distinct handles are independent.
+ *   - Operator "action" entry points ACCUMULATE into their output, as the
+ *     reference's do (source/Div.cpp:174, source/FaceProlongator.cpp:667);
+ *     callers zero the output first, exactly as the reference examples do.
+ *
+ * Boundary codes, one per boundary edge in the mesh's boundary-edge order
+ * (the order of Mesh2D::edge(i, FaceType::BOUNDARY)):
+ *   0 absorbing / outflow   exterior u_e = t (t.u) + n (p + n.u)/2, p_e = n.u_e
+ *                           (the formula wavedg/WaveEquation.hpp:77-84 intends;
+ *                           the reference evaluates p_e before u_e)
+ *   1 reflecting            wavedg/WaveEquation.hpp:64-69
+ *   2 Dirichlet p = 0       mirror state p_e = -p, u_e = u (README.md:6 names
+ *                           it; the reference has no 2D implementation)
+ */
+#ifndef WDG_B200_H
+#define WDG_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WDG_OK 0
+#define WDG_ERR_ARG -1         /* invalid argument (sizes, codes, null pointers) */
+#define WDG_ERR_CUDA -2        /* a CUDA runtime call failed */
+#define WDG_ERR_ALLOC -3       /* device or host allocation failed */
+#define WDG_ERR_TIMEOUT -4     /* a bounded device-side wait expired */
+#define WDG_ERR_UNSUPPORTED -5 /* degree / precision / feature not built */
+#define WDG_ERR_NOT_CONVERGED -6
+
+#define WDG_INTERIOR 0 /* dg::FaceType::INTERIOR (wavedg/Edge.hpp:11-22) */
+#define WDG_BOUNDARY 1 /* dg::FaceType::BOUNDARY */
+
+#define WDG_FP64 0 /* state, stepping and reductions in double */
+#define WDG_FP32 1 /* state and stepping in float; WaveHoltz filter, residual, norms and energy in double */
+
+typedef struct wdg_mesh wdg_mesh;
+typedef struct wdg_wave wdg_wave;
+typedef struct wdg_waveholtz wdg_waveholtz;
+
+const char *wdg_last_error(void);
+int wdg_version(void);
+/* n_colloc values this build has kernels for: writes up to cap entries, returns the count */
+int wdg_supported_degrees(int *n_colloc, int cap);
+
+/* ------------------------------------------------------------------ mesh */
+/* dg::Mesh2D::from_vertices (source/Mesh2D.cpp:5-92): xy (2, n_vert), quads (4, n_elem)
+ * counter-clockwise corners.  Same edge numbering as the reference (edges in order of first
+ * appearance over elements and sides 0..3), with 64-bit vertex-pair keys. */
+int wdg_mesh_from_vertices(int n_vert, const double *xy, int n_elem, const int *quads, wdg_mesh **out);
+/* dg::Mesh2D::uniform_rect (source/Mesh2D.cpp:130-163) */
+int wdg_mesh_uniform_rect(int nx, double ax, double bx, int ny, double ay, double by, wdg_mesh **out);
+/* Adopt the tables of an existing dg::Mesh2D (what a C++ drop-in reads through the reference's
+ * public API): corners (2, 4, n_elem) = QuadElement::corner(c) (wavedg/Element.hpp:123-126);
+ * per edge (el0, s0, el1, s1, delta) = Edge::{elements, sides, delta} (wavedg/Edge.hpp:37-49),
+ * in Mesh2D::edge(i, type) order; boundary rows ignore el1, s1, delta. */
+int wdg_mesh_from_tables(int n_elem, const double *corners, int n_interior, const int *interior_edges,
+                         int n_boundary, const int *boundary_edges, wdg_mesh **out);
+void wdg_mesh_destroy(wdg_mesh *mesh);
+int wdg_mesh_n_elem(const wdg_mesh *mesh);
+int wdg_mesh_n_edges(const wdg_mesh *mesh, int face_type);               /* Mesh2D::n_edges(type) */
+int wdg_mesh_edges(const wdg_mesh *mesh, int face_type, int *out);        /* (el0, s0, el1, s1, delta) rows */
+int wdg_mesh_min_h(const wdg_mesh *mesh, double *h);                      /* Mesh2D::min_h (source/Mesh2D.cpp:751-767) */
+int wdg_mesh_boundary_midpoints(const wdg_mesh *mesh, double *xy);         /* edge_metrics(1-pt rule, BOUNDARY).physical_coordinates() */
+
+/* QuadratureRule::gauss_lobatto (source/QuadratureRule.cpp:32-97) and
+ * lagrange_basis_deriv at the nodes (source/lagrange_interpolation.cpp:33-50):
+ * D (n, n), D[l + n*j] = phi_j'(x_l).  D may be NULL. */
+int wdg_gauss_lobatto(int n, double *x, double *w, double *D);
+
+/* ----------------------------------------------------- discretisation */
+/* One GPU-resident discretisation of the wave system on `mesh` with n_colloc GLL nodes per
+ * direction: WaveEquation(mesh, basis, approx_quad=true) (source/WaveEquation.cpp:5-30),
+ * WaveBC(mesh, bc, basis, true) (:70-105) and MassMatrix<true>(mesh, basis)
+ * (source/MassMatrix.cpp:6-28).  bc: one code per boundary edge (NULL = all 0).
+ * device: CUDA ordinal (-1 = current device). */
+int wdg_wave_create(const wdg_mesh *mesh, int n_colloc, const int *bc, int precision, int device, wdg_wave **out);
+void wdg_wave_destroy(wdg_wave *wave);
+int wdg_wave_info(const wdg_wave *wave, int *n_colloc, int *n_elem, long long *ndof, int *precision);
+int wdg_wave_set_stream(wdg_wave *wave, void *cuda_stream);
+int wdg_wave_sync(wdg_wave *wave);
+/* elements per thread block of the fused kernels (a multiple of 4; 0 = built-in default) */
+int wdg_wave_set_tile(wdg_wave *wave, int elems_per_block);
+int wdg_wave_get_tile(const wdg_wave *wave, int *elems_per_block);
+/* Mesh2D::element_metrics(basis).physical_coordinates(): xy (2, n, n, n_elem) */
+int wdg_wave_node_coords(wdg_wave *wave, double *xy);
+
+/* ---- Operator::action drop-ins, FP64, accumulate (y += A x) ---- */
+int wdg_div_action(wdg_wave *wave, const double *u, double *du);   /* Div<true>::action (source/Div.cpp:131-196) */
+int wdg_wave_action(wdg_wave *wave, const double *u, double *du);  /* WaveEquation::action (source/WaveEquation.cpp:54-68) */
+int wdg_wavebc_action(wdg_wave *wave, const double *u, double *du); /* WaveBC::action (source/WaveEquation.cpp:190-215) */
+/* LobattoFaceProlongator::action, n_var = 3 (source/FaceProlongator.cpp:565-590, 628-648):
+ * uf (n, 3, 2, n_edges(face_type)) is overwritten (boundary: side 1 zeroed). */
+int wdg_face_prolong(wdg_wave *wave, int face_type, const double *u, double *uf);
+/* LobattoFaceProlongator::t (source/FaceProlongator.cpp:650-714): u += P^T uf */
+int wdg_face_prolong_t(wdg_wave *wave, int face_type, const double *uf, double *u);
+/* EdgeFlux<true>::action with the upwind defaults a = -1, b = -1/2 (source/EdgeFlux.cpp:289-373):
+ * fb side 0 <- flux, side 1 <- -flux; fb may equal ub. */
+int wdg_edge_flux(wdg_wave *wave, int face_type, const double *ub, double *fb);
+/* apply_bc_2d (source/WaveEquation.cpp:144-167): side 1 of boundary traces <- exterior state */
+int wdg_apply_bc(wdg_wave *wave, double *uB);
+/* MassMatrix<true>::action / ::inv (source/MassMatrix.cpp:55-82) */
+int wdg_mass_action(wdg_wave *wave, int n_var, const double *x, double *y);
+int wdg_mass_inv(wdg_wave *wave, int n_var, double *x);
+
+/* ---- fused hot path ---- */
+/* The examples' time derivative (examples/wave2d.cpp:164-177 without its forcing callback;
+ * source/WaveHoltz.cpp:57-68): dudt = M^{-1} (A u + B u + s F).  F may be NULL.  One kernel. */
+int wdg_rhs(wdg_wave *wave, const double *u, double *dudt, const double *F, double s);
+/* nsteps of ode::RungeKutta4::step (wavedg/ode.hpp:66-93) on dudt = M^{-1}(A + B) u, in place;
+ * t advances by dt per step.  One fused kernel per RK stage. */
+int wdg_rk4_steps(wdg_wave *wave, double *u, double dt, double *t, int nsteps);
+
+/* ---- resident state (stays on the GPU in the handle's precision) ---- */
+int wdg_state_upload(wdg_wave *wave, const double *u);
+int wdg_state_download(wdg_wave *wave, double *u);
+/* device pointer of the resident state (double* for WDG_FP64, float* for WDG_FP32) */
+int wdg_state_device_ptr(wdg_wave *wave, void **ptr);
+/* like wdg_rk4_steps on the resident state; asynchronous */
+int wdg_state_rk4_steps(wdg_wave *wave, double dt, double *t, int nsteps);
+/* discrete energy 1/2 sum_i m_i |q_i|^2 of the resident state, accumulated in FP64 */
+int wdg_state_energy(wdg_wave *wave, double *energy);
+
+/* ---- LinearFunctional2D (wavedg/LinearFunctional.hpp:61-74, 136-202) ---- */
+/* physical coordinates of the n-point Gauss-Legendre quadrature points: xy (2, n, n, n_elem) */
+int wdg_quad_points(wdg_wave *wave, double *xy);
+/* F = (f, phi) from f sampled at those points: fq (n_var, n, n, n_elem) -> F (n_var, n, n, n_elem) */
+int wdg_linear_functional(wdg_wave *wave, int n_var, const double *fq, double *F);
+/* (f, phi) for f = scale * sum_k amp_k exp(-|x - c_k|^2 / (2 sigma_k^2)) in component comp
+ * (others 0), evaluated on the GPU; mass_inv != 0 returns M^{-1} (f, phi). */
+int wdg_load_gaussians(wdg_wave *wave, int n_src, const double *cx, const double *cy, const double *sigma,
+                       const double *amp, double scale, int comp, int mass_inv, double *F);
+
+/* ---- norms (source/linalg.cpp:102-131), FP64 on the GPU ---- */
+int wdg_norm(wdg_wave *wave, const double *x, double *result);
+int wdg_error(wdg_wave *wave, const double *x, const double *y, double *result);
+
+/* ------------------------------------------------------------ WaveHoltz */
+/* dg::WaveHoltz(omega, mesh, basis, bc, approx_quad=true) (source/WaveHoltz.cpp:5-30) on a
+ * discretisation: T = 2 pi / omega, dt = 0.5 min_h / n^2, nt = ceil(T / dt), dt = T / nt. */
+int wdg_waveholtz_create(wdg_wave *wave, double omega, wdg_waveholtz **out);
+void wdg_waveholtz_destroy(wdg_waveholtz *wh);
+int wdg_waveholtz_params(const wdg_waveholtz *wh, double *T, double *dt, int *nt);
+/* WaveHoltz::pi0 (source/WaveHoltz.cpp:55-89): w = Pi(0) for load vector F */
+int wdg_waveholtz_pi0(wdg_waveholtz *wh, double *w, const double *F);
+/* WaveHoltz::S (source/WaveHoltz.cpp:91-121), in place */
+int wdg_waveholtz_S(wdg_waveholtz *wh, double *w);
+/* WaveHoltz::postprocess (source/WaveHoltz.cpp:123-145): H (2, n_points) */
+int wdg_waveholtz_postprocess(wdg_waveholtz *wh, double *H, const double *w);
+/* The fixed-point loop of examples/waveholtz2d.cpp:137-185: pi0 = Pi(0)(F); from the initial
+ * guess in W iterate W <- S W + pi0 until ||W - W_prev|| / ||pi0|| < tol or maxit.
+ * Returns WDG_OK or WDG_ERR_NOT_CONVERGED; *iters and *residual are always written. */
+int wdg_waveholtz_solve(wdg_waveholtz *wh, const double *F, double tol, int maxit, double *W, int *iters,
+                        double *residual);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WDG_B200_H */

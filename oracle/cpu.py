@@ -1,0 +1,257 @@
+"""CPU checkers for the tests -- TEST INFRASTRUCTURE ONLY.
+
+Loads one of two shared libraries with the same C entry points:
+
+* ``oracle``    -- ``oracle/_build/liboracle.so``, the plain C++ restatement of
+  the reference algorithm (``oracle/wdg_oracle.cpp``); always buildable with g++.
+* ``reference`` -- ``oracle/_ref/libwdgref.so``, the reference library itself
+  compiled from its sources plus ``oracle/ref_harness.cpp``; built only where
+  the reference sources are present, and shipped prebuilt otherwise.
+
+Only the tests, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg
+import this module.  The product path (``wavedg_b200``) never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBS = {
+    "oracle": (os.path.join(HERE, "_build", "liboracle.so"), "orc_"),
+    "reference": (os.path.join(HERE, "_ref", "libwdgref.so"), "ref_"),
+}
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_v, _i, _d = C.c_void_p, C.c_int, C.c_double
+
+_SIGS = {
+    "mesh_create": ([_i, _dp, _i, _ip], _v),
+    "mesh_destroy": ([_v], None),
+    "mesh_n_elem": ([_v], _i),
+    "mesh_n_edges": ([_v, _i], _i),
+    "mesh_min_h": ([_v], _d),
+    "mesh_edges": ([_v, _i, _ip], None),
+    "mesh_boundary_midpoints": ([_v, _dp], None),
+    "basis": ([_i, _dp, _dp, _dp], None),
+    "op_create": ([_v, _i, _ip], _v),
+    "op_destroy": ([_v], None),
+    "node_coords": ([_v, _dp], None),
+    "div": ([_v, _dp, _dp], None),
+    "wave_action": ([_v, _dp, _dp], None),
+    "bc_action": ([_v, _dp, _dp], None),
+    "prolong": ([_v, _i, _dp, _dp], None),
+    "prolong_t": ([_v, _i, _dp, _dp], None),
+    "flux": ([_v, _i, _dp, _dp], None),
+    "apply_bc": ([_v, _dp], None),
+    "mass_inv": ([_v, _i, _dp], None),
+    "mass_action": ([_v, _i, _dp, _dp], None),
+    "rhs": ([_v, _dp, _dp], None),
+    "rhs_forced": ([_v, _dp, _dp, _dp, _d], None),
+    "rk4": ([_v, _d, _i, C.POINTER(C.c_double), _dp], None),
+    "load_gaussians": ([_v, _i, _dp, _dp, _dp, _dp, _d, _i, _i, _dp], None),
+    "norm": ([_i, _dp], _d),
+    "error": ([_i, _dp, _dp], _d),
+    "wh_create": ([_v, _d], _v),
+    "wh_destroy": ([_v], None),
+    "wh_params": ([_v, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int)], None),
+    "wh_pi0": ([_v, _dp, _dp], None),
+    "wh_S": ([_v, _dp], None),
+    "wh_postprocess": ([_v, _dp, _dp], None),
+    "wh_solve": ([_v, _dp, _d, _i, _dp, C.POINTER(C.c_double)], _i),
+}
+
+_loaded: dict[str, C.CDLL] = {}
+
+
+def build_oracle() -> str:
+    """Compile the C++ restatement (g++ only, a couple of seconds)."""
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    return LIBS["oracle"][0]
+
+
+def available(kind: str) -> bool:
+    return os.path.exists(LIBS[kind][0])
+
+
+def lib(kind: str = "oracle"):
+    if kind in _loaded:
+        return _loaded[kind]
+    path, prefix = LIBS[kind]
+    if kind == "oracle" and not os.path.exists(path):
+        build_oracle()
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{kind} checker library not built: {path}")
+    L = C.CDLL(path)
+    ns = type("CPUChecker", (), {})()
+    for name, (args, res) in _SIGS.items():
+        fn = getattr(L, prefix + name)
+        fn.argtypes = args
+        fn.restype = res
+        setattr(ns, name, fn)
+    ns._cdll = L
+    _loaded[kind] = ns
+    return ns
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Mesh:
+    """Mesh2D::from_vertices on the CPU checker (vertices (nv,2), quads (nel,4))."""
+
+    def __init__(self, verts, quads, kind="oracle"):
+        self.L = lib(kind)
+        self.verts = _f64(verts).reshape(-1, 2)
+        self.quads = np.ascontiguousarray(quads, dtype=np.int32).reshape(-1, 4)
+        self.h = self.L.mesh_create(len(self.verts), self.verts.ravel(), len(self.quads), self.quads.ravel())
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.mesh_destroy(self.h)
+            self.h = None
+
+    @property
+    def n_elem(self):
+        return self.L.mesh_n_elem(self.h)
+
+    def n_edges(self, kind):
+        return self.L.mesh_n_edges(self.h, kind)
+
+    def edges(self, kind):
+        out = np.zeros((self.n_edges(kind), 5), dtype=np.int32)
+        self.L.mesh_edges(self.h, kind, out.ravel())
+        return out
+
+    def min_h(self):
+        return self.L.mesh_min_h(self.h)
+
+    def boundary_midpoints(self):
+        out = np.zeros((self.n_edges(1), 2))
+        self.L.mesh_boundary_midpoints(self.h, out.ravel())
+        return out
+
+
+def basis(n, kind="oracle"):
+    L = lib(kind)
+    x, w, D = np.zeros(n), np.zeros(n), np.zeros(n * n)
+    L.basis(n, x, w, D)
+    return x, w, D.reshape(n, n, order="F")
+
+
+class Op:
+    """WaveEquation + boundary operator + MassMatrix<true> on the CPU checker."""
+
+    def __init__(self, mesh: Mesh, n: int, bc):
+        self.L, self.mesh, self.n = mesh.L, mesh, n
+        self.bc = np.ascontiguousarray(bc, dtype=np.int32)
+        assert len(self.bc) == mesh.n_edges(1)
+        self.h = self.L.op_create(mesh.h, n, self.bc)
+        self.ndof = 3 * n * n * mesh.n_elem
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.op_destroy(self.h)
+            self.h = None
+
+    def zeros(self):
+        return np.zeros(self.ndof)
+
+    def node_coords(self):
+        out = np.zeros(2 * self.ndof // 3)
+        self.L.node_coords(self.h, out)
+        return out
+
+    def div(self, u, du):
+        self.L.div(self.h, _f64(u), du)
+
+    def wave_action(self, u, du):
+        self.L.wave_action(self.h, _f64(u), du)
+
+    def bc_action(self, u, du):
+        self.L.bc_action(self.h, _f64(u), du)
+
+    def prolong(self, kind, u):
+        uf = np.zeros(self.n * 3 * 2 * self.mesh.n_edges(kind))
+        self.L.prolong(self.h, kind, _f64(u), uf)
+        return uf
+
+    def prolong_t(self, kind, uf, u):
+        self.L.prolong_t(self.h, kind, _f64(uf), u)
+
+    def flux(self, kind, uf):
+        fb = np.zeros_like(uf)
+        self.L.flux(self.h, kind, _f64(uf), fb)
+        return fb
+
+    def apply_bc(self, uB):
+        self.L.apply_bc(self.h, uB)
+
+    def mass_inv(self, nv, x):
+        self.L.mass_inv(self.h, nv, x)
+
+    def mass_action(self, nv, x):
+        y = np.zeros_like(x)
+        self.L.mass_action(self.h, nv, _f64(x), y)
+        return y
+
+    def rhs(self, u, F=None, s=0.0):
+        du = self.zeros()
+        if F is None:
+            self.L.rhs(self.h, _f64(u), du)
+        else:
+            self.L.rhs_forced(self.h, _f64(u), du, _f64(F), s)
+        return du
+
+    def rk4(self, u, dt, nsteps, t=0.0):
+        u = _f64(u).copy()
+        tt = C.c_double(t)
+        self.L.rk4(self.h, dt, nsteps, C.byref(tt), u)
+        return u, tt.value
+
+    def load_gaussians(self, centers, sigmas, amps, scale=1.0, comp=0, mass_inv=False):
+        c = _f64(centers).reshape(-1, 2)
+        F = self.zeros()
+        self.L.load_gaussians(self.h, len(c), _f64(c[:, 0]), _f64(c[:, 1]), _f64(sigmas), _f64(amps),
+                              scale, comp, 1 if mass_inv else 0, F)
+        return F
+
+
+class WaveHoltz:
+    def __init__(self, op: Op, omega: float):
+        self.op, self.L = op, op.L
+        self.h = self.L.wh_create(op.h, omega)
+        T, dt, nt = C.c_double(), C.c_double(), C.c_int()
+        self.L.wh_params(self.h, C.byref(T), C.byref(dt), C.byref(nt))
+        self.T, self.dt, self.nt = T.value, dt.value, nt.value
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.wh_destroy(self.h)
+            self.h = None
+
+    def pi0(self, F):
+        u = self.op.zeros()
+        self.L.wh_pi0(self.h, u, _f64(F))
+        return u
+
+    def S(self, W):
+        W = _f64(W).copy()
+        self.L.wh_S(self.h, W)
+        return W
+
+    def postprocess(self, W):
+        H = np.zeros(2 * self.op.ndof // 3)
+        self.L.wh_postprocess(self.h, H, _f64(W))
+        return H
+
+    def solve(self, pi0, tol, maxit, W0=None):
+        W = self.op.zeros() if W0 is None else _f64(W0).copy()
+        err = C.c_double()
+        it = self.L.wh_solve(self.h, _f64(pi0), tol, maxit, W, C.byref(err))
+        return W, it, err.value

@@ -1,0 +1,149 @@
+"""Generate the golden fixtures in tests/golden/ from the reference library.
+
+    make -C oracle ref          # compiles the reference (needs its sources)
+    python tests/golden/make_golden.py
+
+Every output array is produced by the reference waveDG code compiled from its
+own sources (oracle/_ref/libwdgref.so, driven through oracle/ref_harness.cpp).
+Inputs are seeded (numpy PCG64) and stored beside the outputs, so the fixtures
+are self-contained: the GPU box and the CPU tests read only these files.
+
+The absorbing (code 0) and Dirichlet (code 2) boundary operators are the
+harness's compositions of reference parts (see oracle/ref_harness.cpp); code 1
+and all interior operators are the reference classes themselves.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import cpu  # noqa: E402
+from wavedg_b200 import meshgen as mg  # noqa: E402
+
+KIND = "reference"
+
+
+def meshes():
+    v, q = mg.uniform_rect(4, -1.0, 1.0, 3, 0.0, 2.0)
+    yield "rect4x3", v, q
+    v, q = mg.perturbed_rect(6, 0.2, seed=11)
+    v, q = mg.scrambled(v, q, seed=12)
+    yield "scrambled6", v, q
+    v, q = mg.l_shape(3)
+    v, q = mg.scrambled(v, q, seed=13)
+    yield "lshape3", v, q
+
+
+def mesh_fixture(name, v, q):
+    m = cpu.Mesh(v, q, KIND)
+    np.savez_compressed(os.path.join(HERE, f"mesh_{name}.npz"), verts=v, quads=q, edges_interior=m.edges(0),
+                        edges_boundary=m.edges(1), min_h=m.min_h(), midpoints=m.boundary_midpoints())
+    return m
+
+
+def op_fixture(name, v, q, m, n, seed):
+    rng = np.random.default_rng(seed)
+    bc = rng.integers(0, 3, size=m.n_edges(1)).astype(np.int32)
+    op = cpu.Op(m, n, bc)
+    u = rng.standard_normal(op.ndof)
+    out = dict(verts=v, quads=q, n=n, bc=bc, u=u)
+    for nm in ("div", "wave_action", "bc_action"):
+        r = rng.standard_normal(op.ndof)  # these accumulate: start from a nonzero du
+        out[f"{nm}_in"] = r.copy()
+        getattr(op, nm)(u, r)
+        out[nm] = r
+    out["rhs"] = op.rhs(u)
+    F = rng.standard_normal(op.ndof)
+    out["F"] = F
+    out["rhs_forced"] = op.rhs(u, F, 0.37)
+    for k in (0, 1):
+        out[f"prolong{k}"] = op.prolong(k, u)
+        uf = rng.standard_normal(out[f"prolong{k}"].size)
+        out[f"flux{k}_in"] = uf
+        out[f"flux{k}"] = op.flux(k, uf)
+        r = rng.standard_normal(op.ndof)
+        out[f"prolong_t{k}_in"] = r.copy()
+        op.prolong_t(k, uf, r)
+        out[f"prolong_t{k}"] = r
+    uB = rng.standard_normal(n * 3 * 2 * m.n_edges(1))
+    out["apply_bc_in"] = uB.copy()
+    op.apply_bc(uB)
+    out["apply_bc"] = uB
+    x = u.copy()
+    op.mass_inv(3, x)
+    out["mass_inv"] = x
+    out["mass_action"] = op.mass_action(3, u)
+    out["rk4_dt"] = 1e-3
+    out["rk4"], _ = op.rk4(u, 1e-3, 3)
+    out["node_coords"] = op.node_coords()
+    cen = np.array([[0.1, 0.2], [-0.3, 0.4]])
+    out["load"] = op.load_gaussians(cen, [0.3, 0.2], [1.0, -0.5], 2.0, 0, False)
+    out["load_minv"] = op.load_gaussians(cen, [0.3, 0.2], [1.0, -0.5], 2.0, 1, True)
+    np.savez_compressed(os.path.join(HERE, f"op_{name}_n{n}.npz"), **out)
+
+
+def config1():
+    """32 x 32 uniform mesh on [-1,1]^2, P = 3, Dirichlet p = 0 on every boundary edge,
+    p0 = exp(-(x^2 + y^2)/0.01) assembled as M^{-1}(f, phi), dt = 0.1 h / (P+1)^2, 200 RK4 steps."""
+    v, q = mg.uniform_rect(32, -1.0, 1.0, 32, -1.0, 1.0)
+    m = cpu.Mesh(v, q, KIND)
+    bc = np.full(m.n_edges(1), 2, dtype=np.int32)
+    op = cpu.Op(m, 4, bc)
+    u0 = op.load_gaussians([[0.0, 0.0]], [np.sqrt(0.005)], [1.0], 1.0, 0, True)
+    dt = 0.1 * m.min_h() / 16.0
+    u1, _ = op.rk4(u0, dt, 1)
+    u200, t = op.rk4(u0, dt, 200)
+    np.savez_compressed(os.path.join(HERE, "config1_32x32_P3.npz"), verts=v, quads=q, bc=bc, n=4, dt=dt, u0=u0,
+                        rhs0=op.rhs(u0), u1=u1, u200=u200, t200=t)
+
+
+def waveholtz():
+    """5 x 5 perturbed mesh, P = 3, omega = 2; reflecting left/bottom walls, absorbing elsewhere
+    (the split examples/waveholtz2d.cpp uses), Gaussian forcing on p."""
+    v, q = mg.perturbed_rect(5, 0.2, seed=21)
+    m = cpu.Mesh(v, q, KIND)
+    bc = mg.boundary_codes_by_wall(m.boundary_midpoints(), left=1, bottom=1, right=0, top=0)
+    op = cpu.Op(m, 4, bc)
+    F = op.load_gaussians([[0.1, 0.2]], [0.2], [1.0], 4.0, 0, False)
+    wh = cpu.WaveHoltz(op, 2.0)
+    pi0 = wh.pi0(F)
+    S = wh.S(pi0)
+    W, it, err = wh.solve(pi0, 1e-6, 200)
+    H = wh.postprocess(W)
+    np.savez_compressed(os.path.join(HERE, "waveholtz_5x5_P3.npz"), verts=v, quads=q, bc=bc, n=4, omega=2.0, F=F,
+                        T=wh.T, dt=wh.dt, nt=wh.nt, pi0=pi0, S_pi0=S, W=W, iters=it, err=err, H=H)
+    # all-reflecting walls: the reference's own WaveHoltz class (pi0 and S)
+    bc1 = np.ones(m.n_edges(1), dtype=np.int32)
+    op1 = cpu.Op(m, 4, bc1)
+    wh1 = cpu.WaveHoltz(op1, 2.0)
+    p1 = wh1.pi0(F)
+    np.savez_compressed(os.path.join(HERE, "waveholtz_reflect_5x5_P3.npz"), verts=v, quads=q, bc=bc1, n=4,
+                        omega=2.0, F=F, pi0=p1, S_pi0=wh1.S(p1))
+
+
+def main():
+    if not cpu.available("reference"):
+        raise SystemExit("build the reference first: make -C oracle ref")
+    x = {}
+    for n in range(2, 10):
+        xs, ws, D = cpu.basis(n, KIND)
+        x[f"x{n}"], x[f"w{n}"], x[f"D{n}"] = xs, ws, D
+    np.savez_compressed(os.path.join(HERE, "basis.npz"), **x)
+    cases = {"rect4x3": [6], "scrambled6": [3, 4, 5, 7], "lshape3": [5]}
+    for seed, (name, v, q) in enumerate(meshes()):
+        m = mesh_fixture(name, v, q)
+        for n in cases[name]:
+            op_fixture(name, v, q, m, n, 100 * seed + n)
+    config1()
+    waveholtz()
+    print("fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,114 @@
+"""The oracle (oracle/wdg_oracle.cpp) against the reference's golden vectors.
+
+Every fixture in tests/golden/ was produced by the reference library compiled
+from its own sources (tests/golden/make_golden.py).  The oracle restates the
+algorithm independently (64-bit edge keys, Newton-computed GLL nodes, Jacobi
+eigen-decomposition for the flux matrices), so agreement here pins it.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden, golden_files, rel
+from oracle import cpu
+
+TOL = 1e-13  # FP64 restatement vs reference: only rounding order differs
+
+
+def test_basis_matches_reference():
+    g = golden("basis.npz")
+    for n in range(2, 10):
+        x, w, D = cpu.basis(n, "oracle")
+        assert np.abs(x - g[f"x{n}"]).max() < 1e-15
+        assert np.abs(w - g[f"w{n}"]).max() < 1e-15
+        assert rel(D, g[f"D{n}"]) < 1e-14
+
+
+@pytest.mark.parametrize("fname", golden_files("mesh_"))
+def test_mesh_connectivity(fname):
+    g = golden(fname)
+    m = cpu.Mesh(g["verts"], g["quads"], "oracle")
+    np.testing.assert_array_equal(m.edges(0), g["edges_interior"])
+    np.testing.assert_array_equal(m.edges(1), g["edges_boundary"])
+    assert m.min_h() == g["min_h"]
+    np.testing.assert_array_equal(m.boundary_midpoints(), g["midpoints"])
+
+
+@pytest.mark.parametrize("fname", golden_files("op_"))
+def test_operators(fname):
+    g = golden(fname)
+    m = cpu.Mesh(g["verts"], g["quads"], "oracle")
+    op = cpu.Op(m, int(g["n"]), g["bc"])
+    u = g["u"]
+    for nm in ("div", "wave_action", "bc_action"):
+        r = g[f"{nm}_in"].copy()
+        getattr(op, nm)(u, r)
+        assert rel(r, g[nm]) < TOL, nm
+    assert rel(op.rhs(u), g["rhs"]) < TOL
+    assert rel(op.rhs(u, g["F"], 0.37), g["rhs_forced"]) < TOL
+    for k in (0, 1):
+        assert rel(op.prolong(k, u), g[f"prolong{k}"]) == 0.0
+        assert rel(op.flux(k, g[f"flux{k}_in"]), g[f"flux{k}"]) < TOL
+        r = g[f"prolong_t{k}_in"].copy()
+        op.prolong_t(k, g[f"flux{k}_in"], r)
+        assert rel(r, g[f"prolong_t{k}"]) < 1e-15
+    uB = g["apply_bc_in"].copy()
+    op.apply_bc(uB)
+    assert rel(uB, g["apply_bc"]) < TOL
+    x = u.copy()
+    op.mass_inv(3, x)
+    assert rel(x, g["mass_inv"]) < TOL
+    assert rel(op.mass_action(3, u), g["mass_action"]) < TOL
+    un, _ = op.rk4(u, float(g["rk4_dt"]), 3)
+    assert rel(un, g["rk4"]) < TOL
+    assert rel(op.node_coords(), g["node_coords"]) < 1e-15
+    cen = np.array([[0.1, 0.2], [-0.3, 0.4]])
+    assert rel(op.load_gaussians(cen, [0.3, 0.2], [1.0, -0.5], 2.0, 0, False), g["load"]) < 1e-13
+    assert rel(op.load_gaussians(cen, [0.3, 0.2], [1.0, -0.5], 2.0, 1, True), g["load_minv"]) < 1e-13
+
+
+def test_config1_trajectory():
+    g = golden("config1_32x32_P3.npz")
+    m = cpu.Mesh(g["verts"], g["quads"], "oracle")
+    op = cpu.Op(m, int(g["n"]), g["bc"])
+    u0 = op.load_gaussians([[0.0, 0.0]], [np.sqrt(0.005)], [1.0], 1.0, 0, True)
+    assert rel(u0, g["u0"]) < 1e-13
+    assert rel(op.rhs(g["u0"]), g["rhs0"]) < TOL
+    u1, _ = op.rk4(g["u0"], float(g["dt"]), 1)
+    assert rel(u1, g["u1"]) < TOL
+    u200, t = op.rk4(g["u0"], float(g["dt"]), 200)
+    assert rel(u200, g["u200"]) < 1e-12
+    assert t == g["t200"]
+
+
+def test_waveholtz():
+    g = golden("waveholtz_5x5_P3.npz")
+    m = cpu.Mesh(g["verts"], g["quads"], "oracle")
+    op = cpu.Op(m, int(g["n"]), g["bc"])
+    wh = cpu.WaveHoltz(op, float(g["omega"]))
+    assert (wh.T, wh.dt, wh.nt) == (g["T"], g["dt"], g["nt"])
+    pi0 = wh.pi0(g["F"])
+    assert rel(pi0, g["pi0"]) < 1e-13
+    assert rel(wh.S(g["pi0"]), g["S_pi0"]) < 1e-13
+    W, it, err = wh.solve(g["pi0"], 1e-6, 200)
+    assert it == g["iters"]
+    assert rel(W, g["W"]) < 1e-12
+    assert rel(wh.postprocess(g["W"]), g["H"]) < 1e-13
+
+
+def test_waveholtz_reflecting_uses_reference_class():
+    g = golden("waveholtz_reflect_5x5_P3.npz")
+    m = cpu.Mesh(g["verts"], g["quads"], "oracle")
+    op = cpu.Op(m, int(g["n"]), g["bc"])
+    wh = cpu.WaveHoltz(op, float(g["omega"]))
+    assert rel(wh.pi0(g["F"]), g["pi0"]) < 1e-13
+    assert rel(wh.S(g["pi0"]), g["S_pi0"]) < 1e-13
+
+
+def test_oracle_catches_planted_error():
+    """A mistake planted in the oracle's inputs must show up as a parity failure."""
+    g = golden("op_scrambled6_n5.npz")
+    m = cpu.Mesh(g["verts"], g["quads"], "oracle")
+    bc = g["bc"].copy()
+    bc[0] = (bc[0] + 1) % 3  # wrong boundary code on one edge
+    op = cpu.Op(m, int(g["n"]), bc)
+    assert rel(op.rhs(g["u"]), g["rhs"]) > 1e-6

@@ -1,0 +1,97 @@
+// Internal launch interface between the C-ABI layer (wave.cu, waveholtz.cu)
+// and the kernels (kernels.cu).  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace wdg
+{
+    // stage-kernel flags
+    enum : int
+    {
+        F_VOL = 1,        // volume term  (Div<true>)
+        F_INT = 2,        // interior-face flux (WaveEquation's EdgeFlux)
+        F_BND = 4,        // boundary-face flux (WaveBC)
+        F_MINV = 8,       // multiply by the inverse diagonal mass matrix
+        F_ACCUM = 16,     // out += result (operator mode)
+        F_FORCE = 32,     // + fscale * F before M^{-1}
+        F_READ_DU = 64,   // RK stage > 0: du = a du + dt r (stage 0 never reads du)
+        F_FILTER = 128,   // acc += acc_c * u_new  (FP64 WaveHoltz filter)
+        F_ALL = F_VOL | F_INT | F_BND | F_MINV,
+    };
+
+    template <typename Real>
+    struct StageArgs
+    {
+        const Real *u;        // state in
+        Real *out;            // operator mode: result; RK mode: u_new (never aliases u)
+        Real *du;             // RK register (RK mode)
+        const Real *F;        // forcing load vector (F_FORCE)
+        double *acc;          // filter accumulator (F_FILTER)
+        const double *corners;
+        const int4 *nbr;
+        const uint32_t *finfo;
+        int nel;
+        int flags;
+        int tile;             // elements per tile (multiple of 4)
+        int use_tma;          // 1: full tiles are staged with cp.async.bulk
+        Real rk_a, rk_b, dt, fscale;
+        double acc_c;
+        unsigned *err;        // device error word (bit 0: wait timeout, bit 1: bad neighbour index)
+    };
+
+    struct Geometry
+    {
+        int n = 0, nel = 0;
+        const double *corners = nullptr;   // (8, nel)
+        const int4 *nbr = nullptr;         // (nel)
+        const uint32_t *finfo = nullptr;   // (nel)
+        const int *face_edge = nullptr;    // (4, nel): 2*edge + side
+        const int *edgesI = nullptr;       // (5, nI)
+        const int *edgesB = nullptr;       // (5, nB)
+        int nI = 0, nB = 0;
+        const int *codesB = nullptr;       // (nB)
+    };
+
+    int upload_basis_tables(int device);   // once per device
+    bool degree_supported(int n);
+    int default_tile(int n, bool fp32);
+    int max_tile(int n);
+
+    // fused stage: RK = true for the time-stepping epilogue
+    template <typename Real>
+    cudaError_t launch_stage(int n, bool rk, const StageArgs<Real> &a, int grid_limit, cudaStream_t s);
+    template <typename Real>
+    size_t stage_smem_bytes(int n, int tile, int flags);
+
+    // reference-layout component kernels (FP64)
+    cudaError_t launch_prolong(const Geometry &g, int type, const double *u, double *uf, cudaStream_t s);
+    cudaError_t launch_prolong_t(const Geometry &g, int type, const double *uf, double *u, cudaStream_t s);
+    cudaError_t launch_edge_flux(const Geometry &g, int type, const double *ub, double *fb, cudaStream_t s);
+    cudaError_t launch_apply_bc(const Geometry &g, double *uB, cudaStream_t s);
+    cudaError_t launch_mass(const Geometry &g, int n_var, const double *x, double *y, bool inverse, cudaStream_t s);
+    cudaError_t launch_node_coords(const Geometry &g, bool gauss_legendre, double *xy, cudaStream_t s);
+    cudaError_t launch_linear_functional(const Geometry &g, int n_var, const double *fq, double *F, cudaStream_t s);
+    cudaError_t launch_load_gaussians(const Geometry &g, int nsrc, const double *src /*(4, nsrc) device*/,
+                                      double scale, int comp, double *F, cudaStream_t s);
+
+    // element-wise helpers
+    template <typename A, typename B>
+    cudaError_t launch_convert(const A *x, B *y, long long n, cudaStream_t s);
+    template <typename Real>
+    cudaError_t launch_scale_into(const double *x, Real *p, double *acc, double c, long long n, cudaStream_t s);
+    cudaError_t launch_wh_post(const double *W, const double *P, double omega, long long npts, double *H,
+                               cudaStream_t s);
+
+    // FP64 reductions: result written to *out (device); scratch holds >= reduce_scratch_doubles()
+    int reduce_scratch_doubles();
+    template <typename Real>
+    cudaError_t launch_sumsq(const Real *x, const Real *y, long long n, double *scratch, double *out, cudaStream_t s);
+    template <typename Real>
+    cudaError_t launch_energy(const Geometry &g, const Real *u, double *scratch, double *out, cudaStream_t s);
+    // WaveHoltz update: W_new = acc + pi0 (pi0 may be null); out = sum (W_new - W)^2; W <- W_new
+    cudaError_t launch_wh_update(double *W, const double *acc, const double *pi0, long long n, double *scratch,
+                                 double *out, cudaStream_t s);
+} // namespace wdg

@@ -1,0 +1,67 @@
+// Internal layout of the wdg_wave handle, shared by wave.cu and waveholtz.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "common.hpp"
+#include "launch.hpp"
+
+struct wdg_wave
+{
+    int device = 0;
+    cudaStream_t stream = 0;
+    int n = 0, nel = 0, precision = WDG_FP64, tile = 0;
+    long long ndof = 0;
+    int nI = 0, nB = 0;
+    double min_h = 0.0;
+
+    // geometry (device)
+    double *d_corners = nullptr;
+    int4 *d_nbr = nullptr;
+    uint32_t *d_finfo = nullptr;
+    int *d_face_edge = nullptr;
+    int *d_edgesI = nullptr, *d_edgesB = nullptr, *d_codes = nullptr;
+    wdg::Geometry geo;
+
+    // state buffers in the stepping precision: [0] resident state, [1], [2] rotation
+    void *d_state[3] = {nullptr, nullptr, nullptr};
+    void *d_du = nullptr;
+    // FP64 staging for host-pointer calls (lazily allocated)
+    double *d_stage[3] = {nullptr, nullptr, nullptr};
+    // reductions
+    double *d_scratch = nullptr;
+    double *d_result = nullptr; // 8 doubles
+    double *h_result = nullptr; // pinned, 8 doubles
+    unsigned *d_err = nullptr;
+    double *d_src = nullptr;    // gaussian source table
+    int src_cap = 0;
+
+    size_t real_size() const { return precision == WDG_FP32 ? sizeof(float) : sizeof(double); }
+};
+
+namespace wdg
+{
+    // which memory an argument lives in
+    int is_device_ptr(const wdg_wave *w, const void *p, bool &dev);
+    int ensure_stage(wdg_wave *w, int k);
+    int ensure_states(wdg_wave *w);
+    int check_device_error(wdg_wave *w);
+    int sync(wdg_wave *w);
+
+    // Low-storage RK4 (wavedg/ode.hpp:66-93) on buffer A (stepping precision),
+    // rotating A->B->C->B->C->A per step.  Optional forcing F * s(t_stage) with
+    // s(t) = -sin(omega t)/omega and FP64 filter acc += c_it * u after each step.
+    struct RKExtras
+    {
+        const void *F = nullptr;   // forcing in the stepping precision (nullable)
+        double omega = 0.0;        // s(t) = -sin(omega t)/omega when F != nullptr
+        double *acc = nullptr;     // FP64 filter (nullable)
+        const double *c_filter = nullptr; // per-step filter weights (host array, nsteps)
+    };
+    template <typename Real>
+    int rk4_run(wdg_wave *w, Real *A, double dt, double &t, int nsteps, const RKExtras &x);
+
+    extern const double rk4a[5], rk4b[5], rk4c[5];
+} // namespace wdg

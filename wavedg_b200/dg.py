@@ -1,0 +1,543 @@
+"""Python mirror of the reference's `dg::` interface over the C ABI.
+
+Class and method names, argument meaning and accumulate-into-output semantics
+follow waveDG (arotem3/waveDG):
+
+    Mesh2D.uniform_rect / from_vertices / from_file   source/Mesh2D.cpp:5-163
+    QuadratureRule.quadrature_rule                    wavedg/QuadratureRule.hpp:77
+    WaveEquation(mesh, basis, approx_quad).action     source/WaveEquation.cpp:5-68
+    WaveBC(mesh, bc, basis, approx_quad).action       source/WaveEquation.cpp:70-215
+    MassMatrix(mesh, basis).action / .inv             source/MassMatrix.cpp:6-82
+    Div, make_face_prolongator, EdgeFlux              source/Div.cpp, FaceProlongator.cpp, EdgeFlux.cpp
+    LinearFunctional2D(mesh, basis).action            wavedg/LinearFunctional.hpp:61-202
+    RungeKutta4(n).step(dt, f, t, u)                  wavedg/ode.hpp:46-94
+    WaveHoltz(omega, mesh, basis, bc, approx_quad)    source/WaveHoltz.cpp
+    norm / error                                      source/linalg.cpp:102-131
+
+Arrays are numpy float64 (host memory; results are back when the call
+returns) or CUDA float64 torch tensors (device memory; asynchronous on the
+handle's stream).  Errors raise WdgError, as the reference's wdg_error throws.
+Only the Gauss-Lobatto, approx_quad=True path is built for the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _lib
+from ._lib import WDG_FP32, WDG_FP64, WdgError, check, lib
+
+
+class FaceType:
+    INTERIOR = 0
+    BOUNDARY = 1
+
+
+def _precision(p) -> int:
+    if p in (WDG_FP64, "fp64", "float64", np.float64):
+        return WDG_FP64
+    if p in (WDG_FP32, "fp32", "float32", np.float32):
+        return WDG_FP32
+    raise ValueError(f"precision must be 'fp64' or 'fp32', not {p!r}")
+
+
+def _ptr(a, writable: bool = False, name: str = "array"):
+    """(c_void_p, keepalive) for a float64 numpy array or CUDA torch tensor."""
+    if a is None:
+        return None, None
+    mod = type(a).__module__
+    if mod.startswith("torch"):
+        if a.dtype.__repr__() != "torch.float64":
+            raise TypeError(f"{name}: torch tensors must be float64")
+        if not a.is_contiguous():
+            raise ValueError(f"{name}: tensor must be contiguous")
+        return C.c_void_p(a.data_ptr()), a
+    if not isinstance(a, np.ndarray):
+        raise TypeError(f"{name}: expected a numpy array or a CUDA torch tensor")
+    if a.dtype != np.float64 or not a.flags.c_contiguous:
+        if writable:
+            raise TypeError(f"{name}: output arrays must be C-contiguous float64")
+        a = np.ascontiguousarray(a, dtype=np.float64)
+    if writable and not a.flags.writeable:
+        raise ValueError(f"{name}: array is read-only")
+    return C.c_void_p(a.ctypes.data), a
+
+
+def _size(a) -> int:
+    return int(a.numel()) if type(a).__module__.startswith("torch") else int(np.asarray(a).size)
+
+
+# ------------------------------------------------------------------ quadrature
+class QuadratureRule:
+    """Quadrature rule on [-1, 1]; the GPU operators take Gauss-Lobatto rules."""
+
+    GaussLegendre = 0
+    GaussLobatto = 1
+    _cache: dict = {}
+
+    def __init__(self, n: int, type_: int):
+        self.n, self.type = int(n), type_
+        if type_ == self.GaussLobatto:
+            x, w = np.zeros(n), np.zeros(n)
+            check(lib().wdg_gauss_lobatto(n, C.c_void_p(x.ctypes.data), C.c_void_p(w.ctypes.data), None),
+                  "gauss_lobatto")
+        else:
+            x, w = np.polynomial.legendre.leggauss(n)
+        self.x, self.w = x, w
+
+    @classmethod
+    def quadrature_rule(cls, n: int, rule: int = GaussLegendre) -> "QuadratureRule":
+        key = (int(n), rule)
+        if key not in cls._cache:
+            cls._cache[key] = cls(n, rule)
+        return cls._cache[key]
+
+    def derivative_matrix(self) -> np.ndarray:
+        """D[l, j] = phi_j'(x_l) (lagrange_basis_deriv at the nodes)."""
+        if self.type != self.GaussLobatto:
+            raise WdgError(_lib.WDG_ERR_UNSUPPORTED, "derivative matrix only for Gauss-Lobatto rules")
+        x, w, D = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n * self.n)
+        check(lib().wdg_gauss_lobatto(self.n, C.c_void_p(x.ctypes.data), C.c_void_p(w.ctypes.data),
+                                      C.c_void_p(D.ctypes.data)))
+        return D.reshape(self.n, self.n, order="F")
+
+
+def _gll_n(basis) -> int:
+    if isinstance(basis, QuadratureRule):
+        if basis.type != QuadratureRule.GaussLobatto:
+            raise WdgError(_lib.WDG_ERR_UNSUPPORTED,
+                           "the GPU operators are built for Gauss-Lobatto bases (LobattoFaceProlongator path)")
+        return basis.n
+    return int(basis)
+
+
+# ------------------------------------------------------------------------ mesh
+class Mesh2D:
+    """Quad mesh; same element and edge numbering as dg::Mesh2D."""
+
+    def __init__(self, handle, verts=None, quads=None):
+        self._h = handle
+        self.verts, self.quads = verts, quads
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().wdg_mesh_destroy(h)
+            self._h = None
+
+    @staticmethod
+    def from_vertices(x, elems) -> "Mesh2D":
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 2)
+        q = np.ascontiguousarray(elems, dtype=np.int32).reshape(-1, 4)
+        h = C.c_void_p()
+        check(lib().wdg_mesh_from_vertices(len(x), C.c_void_p(x.ctypes.data), len(q), C.c_void_p(q.ctypes.data),
+                                           C.byref(h)), "Mesh2D.from_vertices")
+        return Mesh2D(h, x, q)
+
+    @staticmethod
+    def uniform_rect(nx: int, ax: float, bx: float, ny: int, ay: float, by: float) -> "Mesh2D":
+        from .meshgen import uniform_rect
+
+        v, q = uniform_rect(nx, ax, bx, ny, ay, by)
+        return Mesh2D.from_vertices(v, q)
+
+    @staticmethod
+    def from_file(directory: str) -> "Mesh2D":
+        """Mesh2D::from_file format: info.txt (n_pts n_elem), coordinates.txt, elements.txt."""
+        with open(os.path.join(directory, "info.txt")) as f:
+            n_pts, n_elem = (int(t) for t in f.read().split()[:2])
+        x = np.loadtxt(os.path.join(directory, "coordinates.txt"), dtype=np.float64).reshape(-1, 2)[:n_pts]
+        e = np.loadtxt(os.path.join(directory, "elements.txt"), dtype=np.int64).reshape(-1, 4)[:n_elem]
+        return Mesh2D.from_vertices(x, e.astype(np.int32))
+
+    @staticmethod
+    def from_tables(corners, interior_edges, boundary_edges) -> "Mesh2D":
+        c = np.ascontiguousarray(corners, dtype=np.float64).reshape(-1, 8)
+        ie = np.ascontiguousarray(interior_edges, dtype=np.int32).reshape(-1, 5)
+        be = np.ascontiguousarray(boundary_edges, dtype=np.int32).reshape(-1, 5)
+        h = C.c_void_p()
+        check(lib().wdg_mesh_from_tables(len(c), C.c_void_p(c.ctypes.data), len(ie), C.c_void_p(ie.ctypes.data),
+                                         len(be), C.c_void_p(be.ctypes.data), C.byref(h)), "Mesh2D.from_tables")
+        return Mesh2D(h)
+
+    def n_elem(self) -> int:
+        return check(lib().wdg_mesh_n_elem(self._h))
+
+    def n_edges(self, face_type: int) -> int:
+        return check(lib().wdg_mesh_n_edges(self._h, face_type))
+
+    def edges(self, face_type: int) -> np.ndarray:
+        out = np.zeros((self.n_edges(face_type), 5), dtype=np.int32)
+        check(lib().wdg_mesh_edges(self._h, face_type, C.c_void_p(out.ctypes.data)))
+        return out
+
+    def min_h(self) -> float:
+        h = C.c_double()
+        check(lib().wdg_mesh_min_h(self._h, C.byref(h)))
+        return h.value
+
+    def boundary_midpoints(self) -> np.ndarray:
+        out = np.zeros((self.n_edges(FaceType.BOUNDARY), 2))
+        check(lib().wdg_mesh_boundary_midpoints(self._h, C.c_void_p(out.ctypes.data)))
+        return out
+
+
+# ---------------------------------------------------------- discretisation
+class Discretisation:
+    """One wdg_wave handle: geometry of `mesh` on the GPU for n GLL nodes."""
+
+    def __init__(self, mesh: Mesh2D, n: int, bc=None, precision="fp64", device: int = -1):
+        self.mesh, self.n = mesh, int(n)
+        self.precision = _precision(precision)
+        codes = None
+        if bc is not None:
+            codes = np.ascontiguousarray(bc, dtype=np.int32)
+            if codes.size != mesh.n_edges(FaceType.BOUNDARY):
+                raise WdgError(_lib.WDG_ERR_ARG, "bc needs one code per boundary edge")
+        self._codes = codes
+        h = C.c_void_p()
+        check(lib().wdg_wave_create(mesh._h, self.n, None if codes is None else C.c_void_p(codes.ctypes.data),
+                                    self.precision, device, C.byref(h)), "wdg_wave_create")
+        self._h = h
+        nd = C.c_longlong()
+        check(lib().wdg_wave_info(h, None, None, C.byref(nd), None))
+        self.ndof = nd.value
+        self.n_elem = mesh.n_elem()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().wdg_wave_destroy(h)
+            self._h = None
+
+    def set_stream(self, stream) -> None:
+        """A torch.cuda.Stream, a raw cudaStream_t int, or None (legacy default stream)."""
+        raw = getattr(stream, "cuda_stream", stream)
+        check(lib().wdg_wave_set_stream(self._h, C.c_void_p(raw or 0)))
+
+    def sync(self) -> None:
+        check(lib().wdg_wave_sync(self._h))
+
+    @property
+    def tile(self) -> int:
+        t = C.c_int()
+        check(lib().wdg_wave_get_tile(self._h, C.byref(t)))
+        return t.value
+
+    @tile.setter
+    def tile(self, v: int) -> None:
+        check(lib().wdg_wave_set_tile(self._h, int(v)), "set_tile")
+
+    def zeros(self) -> np.ndarray:
+        return np.zeros(self.ndof)
+
+    def node_coordinates(self) -> np.ndarray:
+        """element_metrics(basis).physical_coordinates(): (2, n, n, n_elem) flattened."""
+        xy = np.zeros(2 * self.ndof // 3)
+        check(lib().wdg_wave_node_coords(self._h, C.c_void_p(xy.ctypes.data)))
+        return xy
+
+    def quad_points(self) -> np.ndarray:
+        xy = np.zeros(2 * self.ndof // 3)
+        check(lib().wdg_quad_points(self._h, C.c_void_p(xy.ctypes.data)))
+        return xy
+
+    def _call(self, fn, *arrays, what=""):
+        check(fn(self._h, *arrays), what)
+
+    # fused hot path ---------------------------------------------------------
+    def rhs(self, u, dudt, F=None, s: float = 0.0) -> None:
+        """dudt <- M^{-1}(A u + B u + s F), one fused kernel."""
+        pu, _ku = _ptr(u, name="u")
+        pd, _kd = _ptr(dudt, True, "dudt")
+        pF, _kF = _ptr(F, name="F")
+        check(lib().wdg_rhs(self._h, pu, pd, pF, float(s)), "rhs")
+
+    def rk4_steps(self, u, dt: float, t: float, nsteps: int) -> float:
+        """nsteps of low-storage RK4 in place; returns the new time."""
+        pu, _k = _ptr(u, True, "u")
+        tt = C.c_double(t)
+        check(lib().wdg_rk4_steps(self._h, pu, float(dt), C.byref(tt), int(nsteps)), "rk4_steps")
+        return tt.value
+
+    # resident state -----------------------------------------------------------
+    def upload(self, u) -> None:
+        p, _k = _ptr(u, name="u")
+        check(lib().wdg_state_upload(self._h, p), "state_upload")
+
+    def download(self, u=None):
+        if u is None:
+            u = np.zeros(self.ndof)
+        p, _k = _ptr(u, True, "u")
+        check(lib().wdg_state_download(self._h, p), "state_download")
+        return u
+
+    def state_ptr(self) -> int:
+        p = C.c_void_p()
+        check(lib().wdg_state_device_ptr(self._h, C.byref(p)))
+        return p.value
+
+    def step_state(self, dt: float, t: float, nsteps: int) -> float:
+        tt = C.c_double(t)
+        check(lib().wdg_state_rk4_steps(self._h, float(dt), C.byref(tt), int(nsteps)), "state_rk4_steps")
+        return tt.value
+
+    def energy(self) -> float:
+        e = C.c_double()
+        check(lib().wdg_state_energy(self._h, C.byref(e)), "state_energy")
+        return e.value
+
+    def load_gaussians(self, centers, sigmas, amps, scale=1.0, comp=0, mass_inv=False, out=None):
+        c = np.ascontiguousarray(centers, dtype=np.float64).reshape(-1, 2)
+        cx, cy = np.ascontiguousarray(c[:, 0]), np.ascontiguousarray(c[:, 1])
+        sg = np.ascontiguousarray(np.broadcast_to(np.asarray(sigmas, dtype=np.float64), (len(c),)))
+        am = np.ascontiguousarray(np.broadcast_to(np.asarray(amps, dtype=np.float64), (len(c),)))
+        F = np.zeros(self.ndof) if out is None else out
+        pF, _k = _ptr(F, True, "F")
+        check(lib().wdg_load_gaussians(self._h, len(c), C.c_void_p(cx.ctypes.data), C.c_void_p(cy.ctypes.data),
+                                       C.c_void_p(sg.ctypes.data), C.c_void_p(am.ctypes.data), float(scale),
+                                       int(comp), 1 if mass_inv else 0, pF), "load_gaussians")
+        return F
+
+    def norm(self, x) -> float:
+        r = C.c_double()
+        px, _k = _ptr(x, name="x")
+        check(lib().wdg_norm(self._h, px, C.byref(r)))
+        return r.value
+
+    def error(self, x, y) -> float:
+        r = C.c_double()
+        px, _kx = _ptr(x, name="x")
+        py, _ky = _ptr(y, name="y")
+        check(lib().wdg_error(self._h, px, py, C.byref(r)))
+        return r.value
+
+
+def _require_approx(approx_quad: bool) -> None:
+    if not approx_quad:
+        raise WdgError(_lib.WDG_ERR_UNSUPPORTED,
+                       "exact-quadrature operators (Div<false>, EdgeFlux<false>, MassMatrix<false>) are not built; "
+                       "use approx_quad=True")
+
+
+class Operator:
+    """dg::Operator: action(x, y) accumulates y += A x, like the reference's operators."""
+
+    def action(self, *args):  # pragma: no cover - interface
+        raise NotImplementedError
+
+
+class WaveEquation(Operator):
+    """du += Div(u) + P^T Flux(P u) over interior edges (source/WaveEquation.cpp:54-68)."""
+
+    def __init__(self, mesh: Mesh2D, basis, approx_quad: bool = False, quad=None, precision="fp64"):
+        _require_approx(approx_quad)
+        self.disc = Discretisation(mesh, _gll_n(basis), None, precision)
+
+    def action(self, *args) -> None:
+        u, du = args[-2], args[-1]  # action(u, du) or action(n_var, u, du); n_var is ignored
+        pu, _ku = _ptr(u, name="u")
+        pd, _kd = _ptr(du, True, "du")
+        check(lib().wdg_wave_action(self.disc._h, pu, pd), "WaveEquation.action")
+
+
+class WaveBC(Operator):
+    """du += boundary flux with exterior states from bc (source/WaveEquation.cpp:190-215)."""
+
+    def __init__(self, mesh: Mesh2D, bc, basis, approx_quad: bool = False, quad=None):
+        _require_approx(approx_quad)
+        self.disc = Discretisation(mesh, _gll_n(basis), bc)
+
+    def action(self, *args) -> None:
+        u, du = args[-2], args[-1]
+        pu, _ku = _ptr(u, name="u")
+        pd, _kd = _ptr(du, True, "du")
+        check(lib().wdg_wavebc_action(self.disc._h, pu, pd), "WaveBC.action")
+
+    def apply_bc(self, uB) -> None:
+        """apply_bc_2d on boundary traces (n, 3, 2, n_boundary): side 1 <- exterior state."""
+        p, _k = _ptr(uB, True, "uB")
+        check(lib().wdg_apply_bc(self.disc._h, p), "apply_bc")
+
+
+class Div(Operator):
+    """Div<true> of the wave system: du += (F(u), grad phi) (source/Div.cpp:131-196)."""
+
+    def __init__(self, mesh: Mesh2D, basis, approx_quad: bool = True):
+        _require_approx(approx_quad)
+        self.disc = Discretisation(mesh, _gll_n(basis))
+
+    def action(self, *args) -> None:
+        u, du = args[-2], args[-1]
+        pu, _ku = _ptr(u, name="u")
+        pd, _kd = _ptr(du, True, "du")
+        check(lib().wdg_div_action(self.disc._h, pu, pd), "Div.action")
+
+
+class FaceProlongator:
+    """LobattoFaceProlongator for n_var = 3 (source/FaceProlongator.cpp:497-714)."""
+
+    def __init__(self, mesh: Mesh2D, basis, face_type: int, bc=None):
+        self.disc = Discretisation(mesh, _gll_n(basis), bc)
+        self.face_type = face_type
+        self.n_faces = mesh.n_edges(face_type)
+
+    def size(self) -> int:
+        return self.disc.n * 3 * 2 * self.n_faces
+
+    def action(self, n_var: int, u, uf) -> None:
+        if n_var != 3:
+            raise WdgError(_lib.WDG_ERR_UNSUPPORTED, "the GPU prolongator is built for the wave system (n_var = 3)")
+        pu, _ku = _ptr(u, name="u")
+        pf, _kf = _ptr(uf, True, "uf")
+        check(lib().wdg_face_prolong(self.disc._h, self.face_type, pu, pf), "FaceProlongator.action")
+
+    def t(self, n_var: int, uf, u) -> None:
+        if n_var != 3:
+            raise WdgError(_lib.WDG_ERR_UNSUPPORTED, "the GPU prolongator is built for the wave system (n_var = 3)")
+        pf, _kf = _ptr(uf, name="uf")
+        pu, _ku = _ptr(u, True, "u")
+        check(lib().wdg_face_prolong_t(self.disc._h, self.face_type, pf, pu), "FaceProlongator.t")
+
+
+def make_face_prolongator(mesh: Mesh2D, basis, face_type: int) -> FaceProlongator:
+    return FaceProlongator(mesh, basis, face_type)
+
+
+class EdgeFlux(Operator):
+    """EdgeFlux<true> of the wave system with the upwind defaults a = -1, b = -1/2."""
+
+    def __init__(self, mesh: Mesh2D, face_type: int, basis, approx_quad: bool = True):
+        _require_approx(approx_quad)
+        self.disc = Discretisation(mesh, _gll_n(basis))
+        self.face_type = face_type
+
+    def action(self, *args) -> None:
+        ub, fb = args[-2], args[-1]
+        pu, _ku = _ptr(ub, name="ub")
+        pf, _kf = _ptr(fb, True, "fb")
+        check(lib().wdg_edge_flux(self.disc._h, self.face_type, pu, pf), "EdgeFlux.action")
+
+
+class MassMatrix:
+    """MassMatrix<true>: diagonal w_i w_j detJ (source/MassMatrix.cpp:6-82)."""
+
+    def __init__(self, mesh: Mesh2D, basis, quad=None, approx_quad: bool = True):
+        _require_approx(approx_quad)
+        self.disc = Discretisation(mesh, _gll_n(basis))
+
+    def action(self, *args) -> None:
+        n_var, x, y = (args if len(args) == 3 else (1, *args))
+        px, _kx = _ptr(x, name="x")
+        py, _ky = _ptr(y, True, "y")
+        check(lib().wdg_mass_action(self.disc._h, int(n_var), px, py), "MassMatrix.action")
+
+    def inv(self, *args) -> None:
+        n_var, x = (args if len(args) == 2 else (1, *args))
+        px, _kx = _ptr(x, True, "x")
+        check(lib().wdg_mass_inv(self.disc._h, int(n_var), px), "MassMatrix.inv")
+
+
+class WaveSystem(Discretisation):
+    """The examples' time derivative M^{-1}(A + B) u (+ s F) as one fused GPU operator."""
+
+    def __init__(self, mesh: Mesh2D, basis, bc=None, precision="fp64", device: int = -1):
+        super().__init__(mesh, _gll_n(basis), bc, precision, device)
+
+    def __call__(self, dudt, t, u) -> None:  # f(F, t, u) as ode::RungeKutta4 calls it
+        self.rhs(u, dudt)
+
+
+class LinearFunctional2D:
+    """(f, phi) with the n-point Gauss-Legendre rule (wavedg/LinearFunctional.hpp:136-202)."""
+
+    def __init__(self, mesh: Mesh2D, basis, quad=None):
+        if quad is not None and quad.n != _gll_n(basis):
+            raise WdgError(_lib.WDG_ERR_UNSUPPORTED, "only the default n-point quadrature is built")
+        self.disc = Discretisation(mesh, _gll_n(basis))
+
+    def action(self, n_var: int, f, F) -> None:
+        """f(x, y) -> array (n_var, npts) (vectorised over quadrature points)."""
+        xy = self.disc.quad_points().reshape(-1, 2)
+        vals = np.asarray(f(xy[:, 0], xy[:, 1]), dtype=np.float64).reshape(n_var, -1)
+        fq = np.ascontiguousarray(vals.T)
+        pF, _k = _ptr(F, True, "F")
+        check(lib().wdg_linear_functional(self.disc._h, int(n_var), C.c_void_p(fq.ctypes.data), pF),
+              "LinearFunctional2D.action")
+
+
+class RungeKutta4:
+    """ode::RungeKutta4 (wavedg/ode.hpp:46-94).  f must be a WaveSystem: the whole step
+    (five fused stages) runs on the GPU."""
+
+    def __init__(self, n: int):
+        self.n = int(n)
+
+    def step(self, dt: float, f: WaveSystem, t: float, u) -> float:
+        if not isinstance(f, WaveSystem):
+            raise WdgError(_lib.WDG_ERR_UNSUPPORTED, "RungeKutta4.step needs a WaveSystem (fused GPU RHS)")
+        if _size(u) != self.n or f.ndof != self.n:
+            raise WdgError(_lib.WDG_ERR_ARG, "state length does not match RungeKutta4(n)")
+        return f.rk4_steps(u, dt, t, 1)
+
+
+class WaveHoltz:
+    """dg::WaveHoltz on the GPU (source/WaveHoltz.cpp)."""
+
+    def __init__(self, omega: float, mesh: Mesh2D, basis, bc, approx_quad: bool = False, precision="fp64",
+                 device: int = -1, system: WaveSystem | None = None):
+        _require_approx(approx_quad)
+        self.omega = float(omega)
+        self.system = system if system is not None else WaveSystem(mesh, basis, bc, precision, device)
+        h = C.c_void_p()
+        check(lib().wdg_waveholtz_create(self.system._h, self.omega, C.byref(h)), "WaveHoltz")
+        self._h = h
+        T, dt, nt = C.c_double(), C.c_double(), C.c_int()
+        check(lib().wdg_waveholtz_params(h, C.byref(T), C.byref(dt), C.byref(nt)))
+        self.T, self.dt, self.nt = T.value, dt.value, nt.value
+        self.ndof = self.system.ndof
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().wdg_waveholtz_destroy(h)
+            self._h = None
+
+    def K(self, t: float) -> float:
+        return self.omega / np.pi * (np.cos(self.omega * t) - 0.25)
+
+    def pi0(self, w, F) -> None:
+        pw, _kw = _ptr(w, True, "w")
+        pF, _kF = _ptr(F, name="F")
+        check(lib().wdg_waveholtz_pi0(self._h, pw, pF), "WaveHoltz.pi0")
+
+    def S(self, w) -> None:
+        pw, _k = _ptr(w, True, "w")
+        check(lib().wdg_waveholtz_S(self._h, pw), "WaveHoltz.S")
+
+    def postprocess(self, H, w) -> None:
+        pH, _kH = _ptr(H, True, "H")
+        pw, _kw = _ptr(w, name="w")
+        check(lib().wdg_waveholtz_postprocess(self._h, pH, pw), "WaveHoltz.postprocess")
+
+    def solve(self, F, tol: float = 1e-6, maxit: int = 1000, W=None, raise_on_stall: bool = False):
+        """pi0, then W <- S W + pi0 until ||W - W_prev|| / ||pi0|| < tol.  Returns (W, iters, residual)."""
+        if W is None:
+            W = np.zeros(self.ndof)
+        pW, _kW = _ptr(W, True, "W")
+        pF, _kF = _ptr(F, name="F")
+        it, res = C.c_int(), C.c_double()
+        st = lib().wdg_waveholtz_solve(self._h, pF, float(tol), int(maxit), pW, C.byref(it), C.byref(res))
+        if st != _lib.WDG_ERR_NOT_CONVERGED or raise_on_stall:
+            check(st, "WaveHoltz.solve")
+        return W, it.value, res.value
+
+
+def norm(x, system: Discretisation) -> float:
+    return system.norm(x)
+
+
+def error(x, y, system: Discretisation) -> float:
+    return system.error(x, y)
