@@ -48,7 +48,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the FP32 companion measurement")
-    ap.add_argument("--tile", type=int, default=0)
+    ap.add_argument("--tile", type=int, default=0, help="elements per block (0: autotune)")
+    ap.add_argument("--stages", type=int, default=0, help="pipeline depth with --tile (0: default)")
     return ap.parse_args()
 
 
@@ -98,7 +99,11 @@ class ClockSampler:
         try:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+                                          "-lms", "100"], stdout=self.file, stderr=subprocess.DEVNULL)
+            # wait (at most 5 s) for the first sample so the timed region is covered
+            t0 = time.time()
+            while time.time() - t0 < 5 and os.path.getsize(self.file.name) == 0:
+                time.sleep(0.05)
         except Exception:
             self.proc = None
         return self
@@ -162,11 +167,15 @@ def run_ours(args, rank, world, local_rank):
     def measure(precision, steps, warmup, tile=0):
         sys_ = W.WaveSystem(mesh, basis, bc, precision=precision, device=local_rank)
         sys_.set_stream(stream)
-        if tile:
-            sys_.tile = tile
         u0 = torch.zeros(sys_.ndof, dtype=torch.float64, device="cuda")
         sys_.load_gaussians(centers, sigmas, amps, 1.0, 0, True, out=u0)
         sys_.upload(u0)
+        if tile:
+            if args.stages:
+                sys_.set_stages(args.stages)
+            sys_.tile = tile
+        else:
+            sys_.autotune(4)  # elements per block and pipeline depth, timed on this GPU
         t = sys_.step_state(dt, 0.0, warmup)
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -226,7 +235,7 @@ def run_ours(args, rank, world, local_rank):
         except Exception:
             traffic = None
 
-    extra = {"energy_final": energy, "t_final": t_end, "dt": dt, "tile": sys_.tile, "peak_kind": peak_kind}
+    extra = {"energy_final": energy, "t_final": t_end, "dt": dt, "launch": sys_.launch_config(), "peak_kind": peak_kind}
     if not args.no_extras and args.precision == "fp64":
         s32, ms32, _, _ = measure("fp32", args.steps, args.warmup)
         b32 = algorithmic_bytes_per_step(ndof, nel, 4)

@@ -102,6 +102,16 @@ int wdg_wave_sync(wdg_wave *wave);
 /* elements per thread block of the fused kernels (a multiple of 4; 0 = built-in default) */
 int wdg_wave_set_tile(wdg_wave *wave, int elems_per_block);
 int wdg_wave_get_tile(const wdg_wave *wave, int *elems_per_block);
+/* upper bound on the persistent CTAs of the fused kernels (0 = one full wave of resident CTAs);
+ * lowering it makes each CTA walk more tiles (used by the tuner and the pipeline tests) */
+int wdg_wave_set_max_ctas(wdg_wave *wave, int max_ctas);
+/* depth of the bulk-copy pipeline of the fused kernels: 2, 3 or 4 tiles staged (0 = default);
+ * the tile shrinks if needed to fit shared memory */
+int wdg_wave_set_stages(wdg_wave *wave, int stages);
+int wdg_wave_get_launch(const wdg_wave *wave, int *elems_per_block, int *stages, int *max_ctas);
+/* the project's autotuner: times `steps` RK4 steps (dt = 0, state unchanged) for every
+ * (elements per block, pipeline depth) that fits and keeps the fastest for this handle */
+int wdg_wave_autotune(wdg_wave *wave, int steps, float *best_ms_per_step);
 /* Mesh2D::element_metrics(basis).physical_coordinates(): xy (2, n, n, n_elem) */
 int wdg_wave_node_coords(wdg_wave *wave, double *xy);
 

@@ -37,6 +37,31 @@ def test_rhs_vs_oracle_full_size(gpu_lib, big):
     assert rel(du, ref) < 1e-12
 
 
+def test_rk4_step_vs_oracle_full_size(gpu_lib, big):
+    """One RK4 step (5 fused stages) at full size against the oracle."""
+    from oracle import cpu
+
+    W, v, q, mesh, basis, bc = big
+    sys = W.WaveSystem(mesh, basis, bc)
+    xy = sys.node_coordinates().reshape(-1, 2)
+    rng = np.random.default_rng(9)
+    u = rng.standard_normal(sys.ndof) * 0.1
+    u[0::3] += np.exp(-((xy[:, 0] - 0.3) ** 2 + xy[:, 1] ** 2) / (2 * 0.1**2))
+    dt = 0.1 * mesh.min_h() / 25.0
+    un = u.copy()
+    sys.rk4_steps(un, dt, 0.0, 1)
+    op = cpu.Op(cpu.Mesh(v, q, "oracle"), 5, bc)
+    ref, _ = op.rk4(u, dt, 1)
+    assert rel(un, ref) < 1e-12
+    # every supported tile size agrees at full size
+    for tile in (8, 12, 16):
+        sys.tile = tile
+        u2 = u.copy()
+        sys.rk4_steps(u2, dt, 0.0, 1)
+        assert rel(u2, ref) < 1e-12, tile
+    sys.tile = 0
+
+
 def test_linearity(gpu_lib, big):
     torch = pytest.importorskip("torch")
     W, v, q, mesh, basis, bc = big

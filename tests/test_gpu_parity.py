@@ -123,6 +123,52 @@ def test_tile_sizes_agree(gpu_lib, tile):
     assert rel(un, g["rk4"]) < TOL
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_many_tiles_per_cta(gpu_lib, precision):
+    """Few CTAs on a 48 x 48 scrambled mesh: every CTA walks dozens of tiles through the
+    double-buffered pipeline (tile sizes 4..24, stage 0 and stages 1-4, tail tiles)."""
+    from oracle import cpu
+    import wavedg_b200 as W
+    from wavedg_b200 import meshgen as mg
+
+    v, q = mg.perturbed_rect(48, 0.2, seed=5)
+    v, q = mg.scrambled(v, q, seed=6)
+    mesh = W.Mesh2D.from_vertices(v, q)
+    basis = W.QuadratureRule.quadrature_rule(5, W.QuadratureRule.GaussLobatto)
+    bc = np.random.default_rng(7).integers(0, 3, size=mesh.n_edges(1)).astype(np.int32)
+    op = cpu.Op(cpu.Mesh(v, q, "oracle"), 5, bc)
+    u = np.random.default_rng(8).standard_normal(op.ndof)
+    ref_rhs = op.rhs(u)
+    ref_rk, _ = op.rk4(u, 1e-3, 2)
+    sys = W.WaveSystem(mesh, basis, bc, precision=precision)
+    tol = TOL if precision == "fp64" else 2e-5
+    for stages in (2, 3, 4):
+      sys.set_stages(stages)
+      for tile in (4, 8, 12, 16, 20):
+        for ctas in (1, 3, 7):
+            try:
+                sys.tile = tile
+            except W.WdgError:
+                continue  # does not fit shared memory at this depth
+            sys.set_max_ctas(ctas)
+            un = u.copy()
+            sys.rk4_steps(un, 1e-3, 0.0, 2)
+            assert rel(un, ref_rk) < tol, (tile, ctas, rel(un, ref_rk))
+            if precision == "fp64":
+                du = np.zeros_like(u)
+                sys.rhs(u, du)
+                assert rel(du, ref_rhs) < TOL, (tile, ctas)
+    sys.set_max_ctas(0)
+    sys.set_stages(0)
+    sys.tile = 0
+    ms = sys.autotune(2)
+    cfg = sys.launch_config()
+    assert ms > 0 and cfg["stages"] in (2, 3, 4)
+    un = u.copy()
+    sys.rk4_steps(un, 1e-3, 0.0, 2)
+    assert rel(un, ref_rk) < tol
+
+
 def test_config1_trajectory(gpu_lib):
     """32 x 32, P = 3, Dirichlet p = 0, 200 RK4 steps: state vs the reference at steps 1 and 200."""
     g = golden("config1_32x32_P3.npz")

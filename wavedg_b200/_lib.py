@@ -59,6 +59,10 @@ SIGNATURES = {
     "wdg_wave_sync": ([_v], _i),
     "wdg_wave_set_tile": ([_v, _i], _i),
     "wdg_wave_get_tile": ([_v, _ip], _i),
+    "wdg_wave_set_max_ctas": ([_v, _i], _i),
+    "wdg_wave_set_stages": ([_v, _i], _i),
+    "wdg_wave_get_launch": ([_v, _ip, _ip, _ip], _i),
+    "wdg_wave_autotune": ([_v, _i, C.POINTER(C.c_float)], _i),
     "wdg_wave_node_coords": ([_v, _v], _i),
     "wdg_div_action": ([_v, _v, _v], _i),
     "wdg_wave_action": ([_v, _v, _v], _i),

@@ -72,4 +72,10 @@ namespace wdg
         std::vector<int> face_edge;      // (4, nel): edge index within its type list, or -1
     };
     int build_face_tables(const wdg_mesh &m, const int *bc, FaceTables &ft);
+
+    // What the stage kernel reads per element side: the DOF offset of the
+    // partner node that faces this side's face-node 0 (-1 on the boundary),
+    // and a byte: bits 0-1 stride code (partner offset for face-node k is
+    // base + k * {+3, -3, +3n, -3n}[code]), bits 3-4 boundary code, bit 7 boundary.
+    void build_partner_tables(const FaceTables &ft, int n, std::vector<int> &fbase, std::vector<uint32_t> &fcode);
 } // namespace wdg

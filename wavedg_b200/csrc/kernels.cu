@@ -53,11 +53,24 @@ namespace wdg
 
     bool degree_supported(int n) { return n == 2 || n == 3 || n == 4 || n == 5 || n == 6 || n == 7 || n == 8 || n == 9; }
 
-    int max_tile(int n) { return (512 / (n * n)) & ~3; }
-    int default_tile(int n, bool fp32)
+    int max_tile(int n) { return (384 / (n + 8)) & ~3; }
+
+    template <typename Real>
+    size_t stage_smem_bytes(int n, int tile, int flags, int stages);
+
+    // largest tile (multiple of 4, <= 512 threads) with which two CTAs of a
+    // `stages`-deep pipeline share an SM
+    int default_tile(int n, bool fp32, int stages)
     {
-        (void)fp32;
-        return max_tile(n);
+        const size_t budget = (227 * 1024) / 2 - 1024;
+        for (int e = max_tile(n); e >= 4; e -= 4)
+        {
+            const size_t b = fp32 ? stage_smem_bytes<float>(n, e, F_RK, stages)
+                                  : stage_smem_bytes<double>(n, e, F_RK, stages);
+            if (b <= budget)
+                return e;
+        }
+        return 4;
     }
 
     int upload_basis_tables(int device)
@@ -148,14 +161,41 @@ namespace wdg
             : "memory");
         return ok != 0;
     }
-    // bounded: try_wait itself suspends for a hardware time slice per poll
-    constexpr int kMaxPolls = 1 << 22;
+    // try_wait with a suspend-time hint: the thread sleeps until the phase
+    // completes or the hint (ns) runs out, instead of spinning on the issue port
+    __device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t *bar, uint32_t parity)
+    {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(smem_u32(bar)), "r"(parity), "r"(100000u)
+            : "memory");
+        return ok != 0;
+    }
+    __device__ __forceinline__ uint64_t globaltimer_ns()
+    {
+        uint64_t t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        return t;
+    }
+    // bounded wait: gives up after kWaitLimitNs of wall time (the copies it waits
+    // for take microseconds; the limit only guards against a lost completion)
+    constexpr uint64_t kWaitLimitNs = 2000000000ull;
     __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
     {
-        for (int it = 0; it < kMaxPolls; ++it)
-            if (mbar_try_wait(bar, parity))
+        if (mbar_try_wait(bar, parity))
+            return true;
+        const uint64_t t0 = globaltimer_ns();
+        for (;;)
+        {
+            if (mbar_try_wait_sleep(bar, parity))
                 return true;
-        return false;
+            if (globaltimer_ns() - t0 > kWaitLimitNs)
+                return false;
+        }
     }
 
     // ------------------------------------------------------------- geometry
@@ -232,320 +272,501 @@ namespace wdg
     }
 
     // ------------------------------------------------------- stage kernel
-    template <int N, typename Real, bool RK>
-    __global__ void __launch_bounds__(512) stage_kernel(const StageArgs<Real> a)
+    // per-thread asynchronous global -> shared copies (LDGSTS); used for the
+    // neighbour traces, which are scattered 8-byte pieces unsuited to TMA
+    template <int BYTES>
+    __device__ __forceinline__ void cp_async(void *dst, const void *src)
     {
-        constexpr int NN = N * N, ND = 3 * NN;
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src), "n"(BYTES)
+                     : "memory");
+    }
+    __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+    template <int PENDING>
+    __device__ __forceinline__ void cp_async_wait()
+    {
+        asm volatile("cp.async.wait_group %0;" ::"n"(PENDING) : "memory");
+    }
+
+    __device__ __forceinline__ void bulk_s2g(void *dst, const void *src, uint32_t bytes)
+    {
+        asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+                     "r"(bytes)
+                     : "memory");
+    }
+    __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+    __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+    __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+    __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+    template <int N>
+    __device__ __forceinline__ int partner_stride(uint32_t byte)
+    {
+        const uint32_t c = byte & 3u;
+        return (c == 0) ? 3 : (c == 1) ? -3 : (c == 2) ? 3 * N : -3 * N;
+    }
+
+    // Shared-memory layout of one CTA (E elements per tile, ND = 3 n^2 values per
+    // element, NF = 4 n face nodes per element):
+    //   [S <= 4 mbarriers][buffer 0 .. S-1][halo 0][halo 1][face flux][G][Rx][Ms][basis x, w]
+    //   buffer    = u tile | du tile (stages > 0) | corners (8 doubles) | partner bases (int4) | codes (u32)
+    //   halo      = (E, NF, 3) neighbour traces from outside the tile, filled by cp.async
+    //   face flux = (E, NF, 3) upwind flux contribution of every face node
+    //   G, Rx     = (E, 3, n^2) eta-fluxes and xi-derivatives
+    //   Ms        = (E, n^2) inverse diagonal mass
+    template <typename Real>
+    size_t stage_smem_bytes(int n, int tile, int flags, int stages)
+    {
+        const size_t nd = 3 * (size_t)n * n;
+        const bool du = (flags & F_RK) != 0; // RK launches stage du' in place, whether or not they read du
+        const size_t ub = (size_t)tile * nd * sizeof(Real);
+        const size_t bufb = ub * (du ? 2 : 1) + (size_t)tile * 84;
+        const size_t face = (size_t)tile * 12 * n * sizeof(Real);
+        const size_t minv = (size_t)tile * n * n * sizeof(Real);
+        const size_t basis = (2 * n * sizeof(Real) + 15) & ~size_t(15);
+        return 32 + (size_t)stages * bufb + 3 * face + 2 * ub + minv + basis;
+    }
+
+    // n line threads (one per row / column) and 8 face threads (two per side) per element
+    constexpr int kMaxThreads = 384;
+    int stage_threads(int n, int tile) { return (n + 8) * tile; }
+
+    template <int N, typename Real, bool RK>
+    __global__ void __launch_bounds__(kMaxThreads, 2) stage_kernel(const StageArgs<Real> a)
+    {
+        constexpr int NN = N * N, ND = 3 * NN, NF = 4 * N;
         const int E = a.tile;
         const int flags = a.flags;
         const bool has_du = RK && (flags & F_READ_DU);
         const int ntiles = (a.nel + E - 1) / E;
+        const int G = gridDim.x;
+        const int TL = N * E; // line threads; the next 8 E threads are face threads
 
         extern __shared__ __align__(128) unsigned char smem[];
-        const size_t ub = (size_t)E * ND * sizeof(Real);
-        const size_t bufb = ub * (has_du ? 2 : 1) + (size_t)E * (64 + 16 + 4);
+        const int ub = E * ND * (int)sizeof(Real);
+        // RK launches keep a du tile in every buffer: stage 0 does not read du but
+        // still stages du' there for the bulk store
+        const int bufb = ub * (RK ? 2 : 1) + E * 84;
+        const int gofs = ub * (RK ? 2 : 1); // geometry block within a buffer
+        const int S = a.stages;             // pipeline depth: tiles in flight + 1
         uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
-        unsigned char *buf0 = smem + 16;
-        Real *Fs = reinterpret_cast<Real *>(buf0 + 2 * bufb);
-        Real *Gs = Fs + (size_t)3 * NN * E;
-        Real *nrm = Gs + (size_t)3 * NN * E; // (3, 4, E): nx, ny, meas
+        unsigned char *buf0 = smem + 32;
+        Real *halo = reinterpret_cast<Real *>(buf0 + S * bufb); // 2 x (E, NF, 3)
+        Real *fc = halo + 2 * E * NF * 3;                       // (E, NF, 3)
+        Real *Gs = fc + E * NF * 3;                             // (E, 3, NN)
+        Real *Rx = Gs + 3 * NN * E;                             // (E, 3, NN)
+        Real *Ms = Rx + 3 * NN * E;                             // (E, NN)
+        Real *bx = Ms + NN * E;                                 // nodes (N), weights (N)
+        const Real *xs = bx, *ws = bx + N;
 
         const int t = threadIdx.x;
-        const int e = t / NN, node = t - e * NN;
-        const int i = node % N, j = node / N;
-
-        // faces through this node (corners lie on two)
-        int fA = -1, kA = 0, fB = -1, kB = 0;
-        {
-            int fs[2] = {-1, -1}, ks[2] = {0, 0}, c = 0;
-            if (j == 0) { fs[c] = 0; ks[c++] = i; }
-            if (i == N - 1) { fs[c] = 1; ks[c++] = j; }
-            if (j == N - 1 && c < 2) { fs[c] = 2; ks[c++] = i; }
-            if (i == 0 && c < 2) { fs[c] = 3; ks[c++] = j; }
-            fA = fs[0]; kA = ks[0]; fB = fs[1]; kB = ks[1];
-        }
+        // line role: t = e * N + m -> element e, row (phase 1) / column (phase 2) m, all 3 components
+        const bool line = t < TL;
+        const int le = t / N, lm = t - (t / N) * N;
+        // face role: t - TL = (fe * 4 + ff) * 2 + fh -> nodes fh, fh + 2, ... of side ff of element fe
+        const bool face = !line;
+        const int fe = (t - TL) >> 3, ff = ((t - TL) >> 1) & 3, fh = (t - TL) & 1;
 
         if (t == 0)
         {
-            mbar_init(&bars[0], 1);
-            mbar_init(&bars[1], 1);
+            for (int q = 0; q < S; ++q)
+                mbar_init(&bars[q], 1);
             fence_mbar_init();
         }
-        __syncthreads();
+        if (t < 2 * N)
+            bx[t] = (t < N) ? Tab<Real>::x(N, t) : Tab<Real>::w(N, t - N);
 
-        auto tile_full = [&](int k) { return (k + 1) * E <= a.nel; };
-        auto issue = [&](int k, int b)
+        auto tma_tile = [&](int k) { return a.use_tma && (k + 1) * E <= a.nel; };
+        auto issue_tma = [&](int k, int b)
         {
-            if (k >= ntiles || !a.use_tma || !tile_full(k))
+            if (k >= ntiles || !tma_tile(k))
                 return;
             const size_t el0 = (size_t)k * E;
             unsigned char *base = buf0 + b * bufb;
-            const uint32_t bytes = (uint32_t)(ub * (has_du ? 2 : 1) + (size_t)E * 84);
-            mbar_expect_tx(&bars[b], bytes);
+            mbar_expect_tx(&bars[b], (uint32_t)(ub * (has_du ? 2 : 1) + E * 84));
             bulk_g2s(base, a.u + el0 * ND, (uint32_t)ub, &bars[b]);
             if (has_du)
                 bulk_g2s(base + ub, a.du + el0 * ND, (uint32_t)ub, &bars[b]);
-            unsigned char *g = base + ub * (has_du ? 2 : 1);
+            unsigned char *g = base + gofs;
             bulk_g2s(g, a.corners + 8 * el0, (uint32_t)(64 * E), &bars[b]);
-            bulk_g2s(g + 64 * E, a.nbr + el0, (uint32_t)(16 * E), &bars[b]);
-            bulk_g2s(g + 80 * E, a.finfo + el0, (uint32_t)(4 * E), &bars[b]);
+            bulk_g2s(g + 64 * E, a.fbase + el0, (uint32_t)(16 * E), &bars[b]);
+            bulk_g2s(g + 80 * E, a.fcode + el0, (uint32_t)(4 * E), &bars[b]);
         };
-        if (t == 0)
+        // partner base of this face thread's side in tile k (-1: none), and its stride
+        auto load_partner = [&](int k, int &base, int &stride)
         {
-            issue(blockIdx.x, 0);
-            issue(blockIdx.x + gridDim.x, 1);
-        }
-
-        Real Di[N], Dj[N];
+            base = -1;
+            stride = 0;
+            const int el = k * E + fe;
+            if (!face || fe >= E || k >= ntiles || el >= a.nel || !(flags & F_INT))
+                return;
+            const uint32_t byte = (__ldg(a.fcode + el) >> (8 * ff)) & 0xffu;
+            if (byte & 0x80u)
+                return;
+            base = __ldg(reinterpret_cast<const int *>(a.fbase + el) + ff);
+            stride = partner_stride<N>(byte);
+        };
+        // start copying the side's exterior traces for tile k (those outside the tile) into halo slot hb
+        auto issue_halo = [&](int k, int hb, int base, int stride)
+        {
+            if (base < 0 || k >= ntiles)
+                return;
+            const int lo = k * E * ND, hi = min(k * E + E, a.nel) * ND;
+            Real *dst = halo + ((hb * E + fe) * NF + ff * N) * 3;
 #pragma unroll
-        for (int l = 0; l < N; ++l)
+            for (int kk = 0; kk < N; ++kk)
+            {
+                if ((kk & 1) != fh)
+                    continue;
+                const int off = base + kk * stride;
+                if (off >= lo && off < hi)
+                    continue; // read from the staged tile instead
+                if (off < 0 || off + 3 > a.nel * ND)
+                {
+                    atomicOr(a.err, 2u);
+                    continue;
+                }
+                cp_async<sizeof(Real)>(dst + 3 * kk, a.u + off);
+                cp_async<sizeof(Real)>(dst + 3 * kk + 1, a.u + off + 1);
+                cp_async<sizeof(Real)>(dst + 3 * kk + 2, a.u + off + 2);
+            }
+        };
+
+        int bad = 0;
+        if (t == 0)
+            for (int q = 0; q < S; ++q)
+                issue_tma(blockIdx.x + q * G, q);
+        int pbase, pstride;
+        load_partner(blockIdx.x, pbase, pstride);
+        issue_halo(blockIdx.x, 0, pbase, pstride);
+        cp_async_commit();
+        load_partner(blockIdx.x + G, pbase, pstride); // issued at the top of iteration 0
+        if (t == 0 && blockIdx.x < ntiles && tma_tile(blockIdx.x) && !mbar_wait(&bars[0], 0))
+            bad = 1;
+        if (__syncthreads_or(bad))
         {
-            Di[l] = Tab<Real>::D(N, l + N * i);
-            Dj[l] = Tab<Real>::D(N, l + N * j);
+            if (t == 0)
+                atomicOr(a.err, 1u);
+            cp_async_wait<0>();
+            return;
         }
-        const Real xi = Tab<Real>::x(N, i), eta = Tab<Real>::x(N, j);
-        const Real wi = Tab<Real>::w(N, i), wj = Tab<Real>::w(N, j);
-        const Real wA = (fA >= 0) ? Tab<Real>::w(N, kA) : Real(0);
-        const Real wB = (fB >= 0) ? Tab<Real>::w(N, kB) : Real(0);
 
         int it = 0;
-        for (int k = blockIdx.x; k < ntiles; k += gridDim.x, ++it)
+        for (int k = blockIdx.x; k < ntiles; k += G, ++it)
         {
-            const int b = it & 1;
-            const uint32_t par = (it >> 1) & 1;
+            const int b = it % S; // data buffer of this tile
+            const int h = it & 1; // halo slot of this tile
             const int el0 = k * E;
             const int ne = min(E, a.nel - el0);
-            unsigned char *base = buf0 + b * bufb;
-            Real *us = reinterpret_cast<Real *>(base);
-            Real *dus = reinterpret_cast<Real *>(base + ub);
-            double *cs = reinterpret_cast<double *>(base + ub * (has_du ? 2 : 1));
-            int4 *ns = reinterpret_cast<int4 *>(cs + 8 * E);
-            uint32_t *is = reinterpret_cast<uint32_t *>(ns + E);
+            Real *us = reinterpret_cast<Real *>(buf0 + b * bufb);
+            Real *dus = reinterpret_cast<Real *>(buf0 + b * bufb + ub);
+            const double *cs = reinterpret_cast<const double *>(buf0 + b * bufb + gofs);
+            const int *ps = reinterpret_cast<const int *>(cs + 8 * E);            // (4, E) partner bases
+            const uint32_t *is = reinterpret_cast<const uint32_t *>(ps + 4 * E); // (E) codes
+            const bool tin = tma_tile(k);
+            const bool tout = RK && a.tma_out && (k + 1) * E <= a.nel;
 
-            if (a.use_tma && tile_full(k))
-            {
-                const bool ok = mbar_wait(&bars[b], par);
-                if (__syncthreads_or(!ok))
-                {
-                    // give the other buffer's copies a bounded chance to land, then leave
-                    if (t == 0)
-                    {
-                        atomicOr(a.err, 1u);
-                        const int kn = k + gridDim.x;
-                        if (kn < ntiles && tile_full(kn))
-                            mbar_wait(&bars[b ^ 1], ((it + 1) >> 1) & 1);
-                    }
-                    __syncthreads();
-                    return;
-                }
-            }
-            else
+            if (!tin)
             {
                 for (int q = t; q < ne * ND; q += blockDim.x)
                     us[q] = a.u[(size_t)el0 * ND + q];
                 if (has_du)
                     for (int q = t; q < ne * ND; q += blockDim.x)
                         dus[q] = a.du[(size_t)el0 * ND + q];
+                double *cw = const_cast<double *>(cs);
                 for (int q = t; q < ne * 8; q += blockDim.x)
-                    cs[q] = a.corners[8 * (size_t)el0 + q];
+                    cw[q] = a.corners[8 * (size_t)el0 + q];
                 for (int q = t; q < ne; q += blockDim.x)
                 {
-                    ns[q] = a.nbr[el0 + q];
-                    is[q] = a.finfo[el0 + q];
+                    reinterpret_cast<int4 *>(const_cast<int *>(ps))[q] = a.fbase[el0 + q];
+                    const_cast<uint32_t *>(is)[q] = a.fcode[el0 + q];
                 }
                 __syncthreads();
             }
 
-            const bool act = e < ne;
-            const size_t g = ((size_t)(el0 + e) * NN + node) * 3;
-            const uint32_t info = act ? is[e] : 0u;
-            const int4 nb4 = act ? ns[e] : make_int4(-1, -1, -1, -1);
-
-            // neighbour traces that live outside the tile: issue the loads now
-            Real xA[3] = {0, 0, 0}, xB[3] = {0, 0, 0};
-            int srcA = 0, srcB = 0; // 0 none, 1 smem (index in nA/nB), 2 registers, 3 boundary
-            int nA = 0, nB = 0;
-            auto locate = [&](int f, int kk, int &src, int &sidx, Real x[3])
+            // ---------------- phase 1: xi-lines and face fluxes
+            if (line && le < ne)
             {
-                if (f < 0 || !act)
-                    return;
-                const uint32_t byte = (info >> (8 * f)) & 0xffu;
-                if (byte & 0x80u)
+                // row j = lm of element le.  Contravariant fluxes (source/Div.cpp:5-53 for the
+                // wave system): F = W (y_eta u - x_eta v, y_eta p, -x_eta p),
+                // G = W (-y_xi u + x_xi v, -y_xi p, x_xi p); x_xi, y_xi are constant along a
+                // row of the bilinear map, x_eta, y_eta vary linearly with xi.
+                const double *c = cs + 8 * le;
+                const Real eta = xs[lm], wj = ws[lm];
+                const Real Xxi = Real(0.25) * ((Real(1) - eta) * Real(c[2] - c[0]) + (Real(1) + eta) * Real(c[4] - c[6]));
+                const Real Yxi = Real(0.25) * ((Real(1) - eta) * Real(c[3] - c[1]) + (Real(1) + eta) * Real(c[5] - c[7]));
+                const Real ex0 = Real(c[6] - c[0]), ex1 = Real(c[4] - c[2]);
+                const Real ey0 = Real(c[7] - c[1]), ey1 = Real(c[5] - c[3]);
+                const Real *row = us + le * ND + 3 * N * lm;
+                Real *g0 = Gs + le * 3 * NN + N * lm;
+                Real *m0 = Ms + le * NN + N * lm;
+                Real Fp[N], Fu[N], Fv[N];
+#pragma unroll
+                for (int l = 0; l < N; ++l)
                 {
-                    src = (flags & F_BND) ? 3 : 0;
-                    return;
+                    const Real xl = xs[l];
+                    const Real Xeta = Real(0.25) * ((Real(1) - xl) * ex0 + (Real(1) + xl) * ex1);
+                    const Real Yeta = Real(0.25) * ((Real(1) - xl) * ey0 + (Real(1) + xl) * ey1);
+                    const Real W = ws[l] * wj;
+                    const Real p = row[3 * l], u = row[3 * l + 1], v = row[3 * l + 2];
+                    const Real WYe = Yeta * W, WXe = Xeta * W, WYx = Yxi * W, WXx = Xxi * W;
+                    Fp[l] = WYe * u - WXe * v;
+                    Fu[l] = WYe * p;
+                    Fv[l] = -WXe * p;
+                    g0[l] = -WYx * u + WXx * v;
+                    g0[NN + l] = -WYx * p;
+                    g0[2 * NN + l] = WXx * p;
+                    // MassMatrix<true>: w_i w_j detJ (source/MassMatrix.cpp:6-28)
+                    m0[l] = Real(1) / (W * (Xxi * Yeta - Yxi * Xeta));
                 }
-                if (!(flags & F_INT))
-                    return;
-                const int nb = (f == 0) ? nb4.x : (f == 1) ? nb4.y : (f == 2) ? nb4.z : nb4.w;
-                if (nb < 0 || nb >= a.nel)
+                // du(i, j) += sum_l D(l, i) F(l, j)   (div_2d_c, source/Div.cpp:131-179)
+                Real *r0 = Rx + le * 3 * NN + N * lm;
+#pragma unroll
+                for (int i = 0; i < N; ++i)
                 {
-                    atomicOr(a.err, 2u);
-                    return;
-                }
-                const int kn = (byte & 4u) ? (N - 1 - kk) : kk;
-                const int nn = face_node(N, (int)(byte & 3u), kn);
-                const int le = nb - el0;
-                if (le >= 0 && le < ne)
-                {
-                    src = 1;
-                    sidx = le * ND + 3 * nn;
-                }
-                else
-                {
-                    src = 2;
-                    const Real *p = a.u + ((size_t)nb * NN + nn) * 3;
-                    x[0] = __ldg(p);
-                    x[1] = __ldg(p + 1);
-                    x[2] = __ldg(p + 2);
-                }
-            };
-            locate(fA, kA, srcA, nA, xA);
-            locate(fB, kB, srcB, nB, xB);
-
-            // per-DOF side inputs that are not staged
-            Real Fv[3] = {0, 0, 0}, ov[3] = {0, 0, 0};
-            double accv[3] = {0, 0, 0};
-            if (act)
-            {
-                if (flags & F_FORCE)
-                    for (int d = 0; d < 3; ++d)
-                        Fv[d] = a.F[g + d];
-                if (!RK && (flags & F_ACCUM))
-                    for (int d = 0; d < 3; ++d)
-                        ov[d] = a.out[g + d];
-                if (RK && (flags & F_FILTER))
-                    for (int d = 0; d < 3; ++d)
-                        accv[d] = a.acc[g + d];
-            }
-
-            // phase A: contravariant fluxes and mass at this node; side normals
-            Real q[3] = {0, 0, 0}, minv = 0;
-            if (act)
-            {
-                q[0] = us[e * ND + 3 * node + 0];
-                q[1] = us[e * ND + 3 * node + 1];
-                q[2] = us[e * ND + 3 * node + 2];
-                Real J[4];
-                jacobian<Real>(cs + 8 * e, xi, eta, J);
-                const Real W = wi * wj;
-                const Real Yeta = J[3] * W, Xeta = J[2] * W, Yxi = J[1] * W, Xxi = J[0] * W;
-                Real *F0 = Fs + (size_t)e * 3 * NN, *G0 = Gs + (size_t)e * 3 * NN;
-                F0[node] = Yeta * q[1] - Xeta * q[2];
-                F0[NN + node] = Yeta * q[0];
-                F0[2 * NN + node] = -Xeta * q[0];
-                G0[node] = -Yxi * q[1] + Xxi * q[2];
-                G0[NN + node] = -Yxi * q[0];
-                G0[2 * NN + node] = Xxi * q[0];
-                minv = Real(1) / (wi * wj * (J[0] * J[3] - J[1] * J[2]));
-            }
-            if (t < 4 * ne)
-            {
-                const int ee = t >> 2, f = t & 3;
-                double nx, ny, ms;
-                side_normal(cs + 8 * ee, f, nx, ny, ms);
-                nrm[(ee * 4 + f) * 3 + 0] = (Real)nx;
-                nrm[(ee * 4 + f) * 3 + 1] = (Real)ny;
-                nrm[(ee * 4 + f) * 3 + 2] = (Real)ms;
-            }
-            __syncthreads();
-
-            // phase B: volume contraction + face fluxes
-            if (act)
-            {
-                Real r[3] = {0, 0, 0};
-                if (flags & F_VOL)
-                {
-                    const Real *F0 = Fs + (size_t)e * 3 * NN, *G0 = Gs + (size_t)e * 3 * NN;
+                    Real ap = 0, au = 0, av = 0;
 #pragma unroll
                     for (int l = 0; l < N; ++l)
                     {
-                        const int fl = l + N * j, gl = i + N * l;
-                        r[0] += Di[l] * F0[fl] + Dj[l] * G0[gl];
-                        r[1] += Di[l] * F0[NN + fl] + Dj[l] * G0[NN + gl];
-                        r[2] += Di[l] * F0[2 * NN + fl] + Dj[l] * G0[2 * NN + gl];
+                        const Real d = Tab<Real>::D(N, l + N * i);
+                        ap += d * Fp[l];
+                        au += d * Fu[l];
+                        av += d * Fv[l];
                     }
+                    r0[i] = ap;
+                    r0[NN + i] = au;
+                    r0[2 * NN + i] = av;
                 }
-                auto face = [&](int f, int src, int sidx, Real x[3], Real wk)
+            }
+            if (face)
+            {
+                // the next tile's traces start now; this tile's (started one iteration earlier) have landed
+                issue_halo(k + G, h ^ 1, pbase, pstride);
+                cp_async_commit();
+                cp_async_wait<1>();
+                load_partner(k + 2 * G, pbase, pstride);
+                if (fe < ne)
                 {
-                    if (src == 0)
-                        return;
-                    const Real *nv = nrm + (e * 4 + f) * 3;
-                    const Real nx = nv[0], ny = nv[1];
-                    if (src == 1)
+                    const uint32_t byte = (is[fe] >> (8 * ff)) & 0xffu;
+                    const bool bnd = (byte & 0x80u) != 0;
+                    Real *o = fc + (fe * NF + ff * N) * 3;
+                    if (bnd ? (flags & F_BND) : (flags & F_INT))
                     {
-                        x[0] = us[sidx];
-                        x[1] = us[sidx + 1];
-                        x[2] = us[sidx + 2];
+                        // outward normal and measure of the side (StraightEdge, wavedg/Edge.hpp:107-122)
+                        const double *c = cs + 8 * fe;
+                        const int p0 = c_from[ff], p1 = c_to[ff];
+                        const double dx = c[2 * p1] - c[2 * p0], dy = c[2 * p1 + 1] - c[2 * p0 + 1];
+                        const double s2 = dx * dx + dy * dy, rs = rsqrt(s2);
+                        const double sgn = (ff >= 2) ? -1.0 : 1.0;
+                        const Real nx = (Real)(sgn * dy * rs), ny = (Real)(-sgn * dx * rs);
+                        const Real hm = (Real)(0.25 * s2 * rs); // half the side measure
+                        const int code = (int)((byte >> 3) & 3u);
+                        const int base = ps[4 * fe + ff] - el0 * ND, stride = partner_stride<N>(byte);
+                        const Real *hb = halo + ((h * E + fe) * NF + ff * N) * 3;
+                        // own face node kk: (kk,0) (n-1,kk) (kk,n-1) (0,kk) for sides 0..3
+                        const int o0 = (ff == 1) ? 3 * (N - 1) : (ff == 2) ? 3 * N * (N - 1) : 0;
+                        const int os = (ff == 0 || ff == 2) ? 3 : 3 * N;
+                        const Real *own = us + fe * ND + o0;
+#pragma unroll
+                        for (int kk = 0; kk < N; ++kk)
+                        {
+                            if ((kk & 1) != fh)
+                                continue;
+                            const Real q[3] = {own[kk * os], own[kk * os + 1], own[kk * os + 2]};
+                            Real x[3];
+                            if (bnd)
+                                exterior<Real>(code, nx, ny, q, x);
+                            else
+                            {
+                                const int loc = base + kk * stride;
+                                const Real *src = (loc >= 0 && loc < ne * ND) ? us + loc : hb + 3 * kk;
+                                x[0] = src[0];
+                                x[1] = src[1];
+                                x[2] = src[2];
+                            }
+                            Real fl[3] = {0, 0, 0};
+                            upwind<Real>(nx, ny, Tab<Real>::w(N, kk) * hm, q, x, fl);
+                            o[3 * kk] = fl[0];
+                            o[3 * kk + 1] = fl[1];
+                            o[3 * kk + 2] = fl[2];
+                        }
                     }
-                    else if (src == 3)
+                    else
                     {
-                        const int code = (int)((info >> (8 * f + 3)) & 3u);
-                        exterior<Real>(code, nx, ny, q, x);
+#pragma unroll
+                        for (int kk = 0; kk < N; ++kk)
+                            if ((kk & 1) == fh)
+                            {
+                                o[3 * kk] = 0;
+                                o[3 * kk + 1] = 0;
+                                o[3 * kk + 2] = 0;
+                            }
                     }
-                    upwind<Real>(nx, ny, Real(0.5) * (wk * nv[2]), q, x, r);
-                };
-                face(fA, srcA, nA, xA, wA);
-                face(fB, srcB, nB, xB, wB);
-
-                if (flags & F_FORCE)
-                    for (int d = 0; d < 3; ++d)
-                        r[d] += Fv[d] * a.fscale;
-                if (flags & F_MINV)
-                    for (int d = 0; d < 3; ++d)
-                        r[d] *= minv;
-
-                if (RK)
-                {
-                    for (int d = 0; d < 3; ++d)
-                    {
-                        const Real dn = has_du ? a.rk_a * dus[e * ND + 3 * node + d] + a.dt * r[d] : a.dt * r[d];
-                        const Real un = q[d] + a.rk_b * dn;
-                        a.du[g + d] = dn;
-                        a.out[g + d] = un;
-                        if (flags & F_FILTER)
-                            a.acc[g + d] = accv[d] + a.acc_c * (double)un;
-                    }
-                }
-                else
-                {
-                    for (int d = 0; d < 3; ++d)
-                        a.out[g + d] = (flags & F_ACCUM) ? ov[d] + r[d] : r[d];
                 }
             }
             __syncthreads();
-            if (t == 0)
-                issue(k + 2 * gridDim.x, b);
-        }
-    }
 
-    template <typename Real>
-    size_t stage_smem_bytes(int n, int tile, int flags)
-    {
-        const size_t nd = 3 * (size_t)n * n;
-        const bool du = (flags & F_READ_DU) != 0;
-        const size_t ub = (size_t)tile * nd * sizeof(Real);
-        const size_t bufb = ub * (du ? 2 : 1) + (size_t)tile * 84;
-        return 16 + 2 * bufb + 2 * ub + (size_t)tile * 12 * sizeof(Real);
+            // ---------------- phase 2: eta-lines, face terms, M^{-1}, epilogue (in place)
+            if (line && le < ne)
+            {
+                // column i = lm of element le: du(i, j) += sum_l D(l, j) G(i, l)
+                const int i = lm;
+                const Real *gc = Gs + le * 3 * NN + i;
+                Real gp[N], gu[N], gv[N];
+#pragma unroll
+                for (int l = 0; l < N; ++l)
+                {
+                    gp[l] = gc[N * l];
+                    gu[l] = gc[NN + N * l];
+                    gv[l] = gc[2 * NN + N * l];
+                }
+                const Real *rc = Rx + le * 3 * NN + i;
+                const Real *fce = fc + le * NF * 3;
+                const Real *mc = Ms + le * NN + i;
+                Real *uc = us + le * ND + 3 * i;
+                Real *duc = dus + le * ND + 3 * i;
+                const size_t gb = (size_t)(el0 + le) * ND + 3 * i;
+#pragma unroll
+                for (int j = 0; j < N; ++j)
+                {
+                    Real r[3] = {0, 0, 0};
+                    if (flags & F_VOL)
+                    {
+                        r[0] = rc[N * j];
+                        r[1] = rc[NN + N * j];
+                        r[2] = rc[2 * NN + N * j];
+#pragma unroll
+                        for (int l = 0; l < N; ++l)
+                        {
+                            const Real d = Tab<Real>::D(N, l + N * j);
+                            r[0] += d * gp[l];
+                            r[1] += d * gu[l];
+                            r[2] += d * gv[l];
+                        }
+                    }
+                    // face-flux slots (side * N + face node) through node (i, j)
+                    int sl[2] = {-1, -1}, ns = 0;
+                    if (j == 0) sl[ns++] = 0 * N + i;
+                    if (j == N - 1) sl[ns++] = 2 * N + i;
+                    if (i == N - 1 && ns < 2) sl[ns++] = 1 * N + j;
+                    if (i == 0 && ns < 2) sl[ns++] = 3 * N + j;
+                    for (int q = 0; q < ns; ++q)
+                    {
+                        const Real *o = fce + 3 * sl[q];
+                        r[0] += o[0];
+                        r[1] += o[1];
+                        r[2] += o[2];
+                    }
+                    if (flags & F_FORCE)
+                        for (int d = 0; d < 3; ++d)
+                            r[d] += a.F[gb + 3 * N * j + d] * a.fscale;
+                    if (flags & F_MINV)
+                    {
+                        const Real m = mc[N * j];
+                        r[0] *= m;
+                        r[1] *= m;
+                        r[2] *= m;
+                    }
+                    Real *un = uc + 3 * N * j;
+                    if (RK)
+                    {
+                        Real *dn = duc + 3 * N * j;
+#pragma unroll
+                        for (int d = 0; d < 3; ++d)
+                        {
+                            const Real dv = has_du ? a.rk_a * dn[d] + a.dt * r[d] : a.dt * r[d];
+                            dn[d] = dv;
+                            un[d] = un[d] + a.rk_b * dv;
+                        }
+                    }
+                    else
+                    {
+                        un[0] = r[0];
+                        un[1] = r[1];
+                        un[2] = r[2];
+                    }
+                }
+                if (tout)
+                    fence_async_smem();
+            }
+
+            // ---------------- end of tile: write back, refill the buffer
+            const int kn = k + G;
+            if (t == 0 && kn < ntiles && tma_tile(kn) && !mbar_wait(&bars[(it + 1) % S], ((it + 1) / S) & 1))
+                bad = 1;
+            if (__syncthreads_or(bad))
+            {
+                // leave after bounded waits for the copies still in flight (tiles it+2 .. it+S-1)
+                if (t == 0)
+                {
+                    atomicOr(a.err, 1u);
+                    for (int q = 2; q < S; ++q)
+                    {
+                        const int kq = k + q * G;
+                        if (kq < ntiles && tma_tile(kq))
+                            mbar_wait(&bars[(it + q) % S], ((it + q) / S) & 1);
+                    }
+                    bulk_wait_all();
+                }
+                cp_async_wait<0>();
+                return;
+            }
+            const bool filter = RK && (flags & F_FILTER);
+            if (tout && t == 0)
+            {
+                bulk_s2g(a.out + (size_t)el0 * ND, us, (uint32_t)ub);
+                bulk_s2g(a.du + (size_t)el0 * ND, dus, (uint32_t)ub);
+                bulk_commit();
+            }
+            if (!tout || filter)
+            {
+                const size_t g0 = (size_t)el0 * ND;
+                for (int q = t; q < ne * ND; q += blockDim.x)
+                {
+                    const Real v = us[q];
+                    if (!tout)
+                    {
+                        if (RK)
+                        {
+                            a.out[g0 + q] = v;
+                            a.du[g0 + q] = dus[q];
+                        }
+                        else
+                            a.out[g0 + q] = (flags & F_ACCUM) ? a.out[g0 + q] + v : v;
+                    }
+                    if (filter)
+                        a.acc[g0 + q] += a.acc_c * (double)v;
+                }
+                __syncthreads();
+            }
+            if (t == 0)
+            {
+                if (tout)
+                    bulk_wait_read(); // the buffer is refilled next
+                issue_tma(k + S * G, b);
+            }
+        }
+        cp_async_wait<0>();
+        if (t == 0)
+            bulk_wait_all();
     }
 
     template <int N, typename Real, bool RK>
     static cudaError_t launch_stage_n(const StageArgs<Real> &a, int grid_limit, cudaStream_t s)
     {
         auto kern = stage_kernel<N, Real, RK>;
-        const size_t smem = stage_smem_bytes<Real>(N, a.tile, a.flags);
+        const size_t smem = stage_smem_bytes<Real>(N, a.tile, a.flags | (RK ? F_RK : 0), a.stages);
         // the largest footprint any flag set can ask for, set once
         static bool attr_set[64] = {};
         int dev = 0;
         cudaGetDevice(&dev);
         if (!attr_set[dev & 63])
         {
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
             if (e != cudaSuccess)
                 return e;
             attr_set[dev & 63] = true;
         }
-        const int threads = a.tile * N * N;
+        const int threads = stage_threads(N, a.tile);
         const int ntiles = (a.nel + a.tile - 1) / a.tile;
         // resident CTAs per device for this (threads, smem); cached, one entry per device
         static int c_dev[64], c_threads[64], c_grid[64];
@@ -598,8 +819,8 @@ namespace wdg
 
     template cudaError_t launch_stage<double>(int, bool, const StageArgs<double> &, int, cudaStream_t);
     template cudaError_t launch_stage<float>(int, bool, const StageArgs<float> &, int, cudaStream_t);
-    template size_t stage_smem_bytes<double>(int, int, int);
-    template size_t stage_smem_bytes<float>(int, int, int);
+    template size_t stage_smem_bytes<double>(int, int, int, int);
+    template size_t stage_smem_bytes<float>(int, int, int, int);
 
     // --------------------------------------------- reference-layout kernels
     static inline int blocks_for(long long n, int threads) { return (int)std::min<long long>((n + threads - 1) / threads, 1 << 30); }

@@ -19,6 +19,7 @@ namespace wdg
         F_FORCE = 32,     // + fscale * F before M^{-1}
         F_READ_DU = 64,   // RK stage > 0: du = a du + dt r (stage 0 never reads du)
         F_FILTER = 128,   // acc += acc_c * u_new  (FP64 WaveHoltz filter)
+        F_RK = 256,       // shared-memory sizing only: the launch uses the RK epilogue
         F_ALL = F_VOL | F_INT | F_BND | F_MINV,
     };
 
@@ -31,12 +32,14 @@ namespace wdg
         const Real *F;        // forcing load vector (F_FORCE)
         double *acc;          // filter accumulator (F_FILTER)
         const double *corners;
-        const int4 *nbr;
-        const uint32_t *finfo;
+        const int4 *fbase;    // per side: DOF offset of the partner of face-node 0, -1 on the boundary
+        const uint32_t *fcode;// per side: stride code | bc code << 3 | boundary << 7
         int nel;
         int flags;
         int tile;             // elements per tile (multiple of 4)
-        int use_tma;          // 1: full tiles are staged with cp.async.bulk
+        int use_tma;          // 1: full tiles are loaded with cp.async.bulk
+        int tma_out;          // 1: full tiles of u' and du' are stored with cp.async.bulk (RK mode)
+        int stages;           // pipeline depth (2..4): tiles whose bulk loads are in flight + 1
         Real rk_a, rk_b, dt, fscale;
         double acc_c;
         unsigned *err;        // device error word (bit 0: wait timeout, bit 1: bad neighbour index)
@@ -57,14 +60,15 @@ namespace wdg
 
     int upload_basis_tables(int device);   // once per device
     bool degree_supported(int n);
-    int default_tile(int n, bool fp32);
+    int default_tile(int n, bool fp32, int stages);
+    constexpr int kDefaultStages = 2;
     int max_tile(int n);
 
     // fused stage: RK = true for the time-stepping epilogue
     template <typename Real>
     cudaError_t launch_stage(int n, bool rk, const StageArgs<Real> &a, int grid_limit, cudaStream_t s);
     template <typename Real>
-    size_t stage_smem_bytes(int n, int tile, int flags);
+    size_t stage_smem_bytes(int n, int tile, int flags, int stages);
 
     // reference-layout component kernels (FP64)
     cudaError_t launch_prolong(const Geometry &g, int type, const double *u, double *uf, cudaStream_t s);

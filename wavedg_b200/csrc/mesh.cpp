@@ -201,6 +201,38 @@ namespace wdg
         return WDG_OK;
     }
 
+    static int face_node_host(int n, int f, int k)
+    {
+        const int i = (f == 0 || f == 2) ? k : (f == 1 ? n - 1 : 0);
+        const int j = (f == 1 || f == 3) ? k : (f == 2 ? n - 1 : 0);
+        return i + n * j;
+    }
+
+    void build_partner_tables(const FaceTables &ft, int n, std::vector<int> &fbase, std::vector<uint32_t> &fcode)
+    {
+        const size_t nel = ft.info.size();
+        fbase.assign(4 * nel, -1);
+        fcode.assign(nel, 0u);
+        for (size_t el = 0; el < nel; ++el)
+            for (int f = 0; f < 4; ++f)
+            {
+                const uint32_t byte = (ft.info[el] >> (8 * f)) & 0xffu;
+                if (byte & 0x80u)
+                {
+                    fcode[el] |= byte << (8 * f);
+                    continue;
+                }
+                const int nb = ft.nbr[4 * el + f], fs = (int)(byte & 3u);
+                const bool flip = (byte & 4u) != 0;
+                const int nn0 = face_node_host(n, fs, flip ? n - 1 : 0);
+                const int nn1 = face_node_host(n, fs, flip ? n - 2 : 1);
+                const int step = nn1 - nn0;
+                const uint32_t code = (step == 1) ? 0u : (step == -1) ? 1u : (step == n) ? 2u : 3u;
+                fbase[4 * el + f] = 3 * (nb * n * n + nn0);
+                fcode[el] |= code << (8 * f);
+            }
+    }
+
     static double edge_length(const double *c, int s)
     {
         const double dx = c[2 * kSideTo[s]] - c[2 * kSideFrom[s]];

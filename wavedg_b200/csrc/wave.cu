@@ -111,10 +111,11 @@ namespace wdg
     {
         StageArgs<Real> a{};
         a.corners = w->d_corners;
-        a.nbr = w->d_nbr;
-        a.finfo = w->d_finfo;
+        a.fbase = w->d_fbase;
+        a.fcode = w->d_fcode;
         a.nel = w->nel;
         a.tile = w->tile;
+        a.stages = w->stages;
         a.err = w->d_err;
         return a;
     }
@@ -143,6 +144,7 @@ namespace wdg
                 a.rk_a = (Real)rk4a[st];
                 a.rk_b = (Real)rk4b[st];
                 a.use_tma = aligned16(src) ? 1 : 0;
+                a.tma_out = aligned16(dst) ? 1 : 0;
                 if (x.F)
                 {
                     a.flags |= F_FORCE;
@@ -156,7 +158,7 @@ namespace wdg
                     a.acc = x.acc;
                     a.acc_c = x.c_filter[s];
                 }
-                cudaError_t e = launch_stage<Real>(w->n, true, a, 0, w->stream);
+                cudaError_t e = launch_stage<Real>(w->n, true, a, w->max_ctas, w->stream);
                 if (e != cudaSuccess)
                     return cuda_fail(e, "stage kernel launch");
                 src = dst;
@@ -188,6 +190,13 @@ namespace
         if (count)
             WDG_CUDA(cudaMemcpy(d, h, sizeof(T) * count, cudaMemcpyHostToDevice));
         return WDG_OK;
+    }
+
+    constexpr size_t kMaxSmem = 227 * 1024;
+    size_t smem_for(const wdg_wave *w, int tile, int stages)
+    {
+        return w->precision == WDG_FP32 ? stage_smem_bytes<float>(w->n, tile, F_RK, stages)
+                                        : stage_smem_bytes<double>(w->n, tile, F_RK, stages);
     }
 
     struct DeviceGuard
@@ -273,14 +282,16 @@ namespace
     {
         StageArgs<double> a = base_args<double>(w);
         // operator launches always run the FP64 kernel, whatever the stepping precision
-        a.tile = default_tile(w->n, false);
+        a.tile = default_tile(w->n, false, kDefaultStages);
+        a.stages = kDefaultStages;
         a.u = u;
         a.out = out;
         a.flags = flags;
         a.F = F;
         a.fscale = s;
         a.use_tma = ((uintptr_t)u & 15u) == 0;
-        cudaError_t e = launch_stage<double>(w->n, false, a, 0, w->stream);
+        a.tma_out = 0;
+        cudaError_t e = launch_stage<double>(w->n, false, a, w->max_ctas, w->stream);
         if (e != cudaSuccess)
             return cuda_fail(e, "stage kernel launch (operator mode)");
         return WDG_OK;
@@ -367,6 +378,8 @@ extern "C"
             return fail(WDG_ERR_UNSUPPORTED, "wdg_wave_create: no kernels for this n_colloc (built: 2..9)");
         if (precision != WDG_FP64 && precision != WDG_FP32)
             return fail(WDG_ERR_ARG, "wdg_wave_create: precision must be WDG_FP64 or WDG_FP32");
+        if (3LL * n_colloc * n_colloc * mesh->nel >= (1LL << 31))
+            return fail(WDG_ERR_UNSUPPORTED, "wdg_wave_create: more than 2^31 DOF on one GPU");
         int ndev = 0;
         WDG_CUDA(cudaGetDeviceCount(&ndev));
         if (device < 0)
@@ -388,7 +401,7 @@ extern "C"
         w->nI = (int)mesh->interior.size();
         w->nB = (int)mesh->boundary.size();
         w->min_h = mesh->min_h;
-        w->tile = default_tile(n_colloc, precision == WDG_FP32);
+        w->tile = default_tile(n_colloc, precision == WDG_FP32, w->stages);
 
         int s = WDG_OK;
         auto chk = [&](int r)
@@ -401,6 +414,8 @@ extern "C"
         chk(dalloc(&w->d_nbr, nel));
         chk(dalloc(&w->d_finfo, nel));
         chk(dalloc(&w->d_face_edge, 4 * nel));
+        chk(dalloc(&w->d_fbase, nel));
+        chk(dalloc(&w->d_fcode, nel));
         chk(dalloc(&w->d_edgesI, 5 * (size_t)w->nI));
         chk(dalloc(&w->d_edgesB, 5 * (size_t)w->nB));
         chk(dalloc(&w->d_codes, (size_t)w->nB));
@@ -436,6 +451,11 @@ extern "C"
             chk(upload(w->d_nbr, nb4.data(), nel));
             chk(upload(w->d_finfo, ft.info.data(), nel));
             chk(upload(w->d_face_edge, ft.face_edge.data(), 4 * nel));
+            std::vector<int> fbase;
+            std::vector<uint32_t> fcode;
+            build_partner_tables(ft, n_colloc, fbase, fcode);
+            chk(upload(reinterpret_cast<int *>(w->d_fbase), fbase.data(), 4 * nel));
+            chk(upload(w->d_fcode, fcode.data(), nel));
             chk(upload(w->d_edgesI, ei.data(), ei.size()));
             chk(upload(w->d_edgesB, eb.data(), eb.size()));
             chk(upload(w->d_codes, codes.data(), codes.size()));
@@ -474,7 +494,8 @@ extern "C"
             return;
         DeviceGuard g(w->device);
         cudaStreamSynchronize(w->stream);
-        void *ptrs[] = {w->d_corners, w->d_nbr, w->d_finfo, w->d_face_edge, w->d_edgesI, w->d_edgesB, w->d_codes,
+        void *ptrs[] = {w->d_corners, w->d_nbr, w->d_finfo, w->d_face_edge, w->d_fbase, w->d_fcode, w->d_edgesI,
+                        w->d_edgesB, w->d_codes,
                         w->d_state[0], w->d_state[1], w->d_state[2], w->d_du, w->d_stage[0], w->d_stage[1],
                         w->d_stage[2], w->d_scratch, w->d_result, w->d_err, w->d_src};
         for (void *p : ptrs)
@@ -517,12 +538,111 @@ extern "C"
         if (!w)
             return fail(WDG_ERR_ARG, "null discretisation");
         if (tile == 0)
-            tile = default_tile(w->n, w->precision == WDG_FP32);
+            tile = default_tile(w->n, w->precision == WDG_FP32, w->stages);
         if (tile < 4 || (tile & 3) || tile > max_tile(w->n))
-            return fail(WDG_ERR_ARG, "tile must be a positive multiple of 4 with tile * n^2 <= 512");
+            return fail(WDG_ERR_ARG, "tile must be a positive multiple of 4 with (3 n + 8) * tile <= 512 threads");
+        if (smem_for(w, tile, w->stages) > kMaxSmem)
+            return fail(WDG_ERR_ARG, "tile too large for shared memory at this pipeline depth");
         w->tile = tile;
         return WDG_OK;
     }
+    int wdg_wave_set_stages(wdg_wave *w, int stages)
+    {
+        if (!w || stages < 0 || stages == 1 || stages > 4)
+            return fail(WDG_ERR_ARG, "wdg_wave_set_stages: stages must be 2, 3 or 4 (0 = default)");
+        if (stages == 0)
+            stages = kDefaultStages;
+        int tile = w->tile;
+        while (tile > 4 && smem_for(w, tile, stages) > kMaxSmem)
+            tile -= 4;
+        if (smem_for(w, tile, stages) > kMaxSmem)
+            return fail(WDG_ERR_ARG, "wdg_wave_set_stages: no tile fits shared memory at this depth");
+        w->stages = stages;
+        w->tile = tile;
+        return WDG_OK;
+    }
+
+    int wdg_wave_get_launch(const wdg_wave *w, int *tile, int *stages, int *max_ctas)
+    {
+        if (!w)
+            return fail(WDG_ERR_ARG, "null discretisation");
+        if (tile) *tile = w->tile;
+        if (stages) *stages = w->stages;
+        if (max_ctas) *max_ctas = w->max_ctas;
+        return WDG_OK;
+    }
+
+    // Time `steps` RK4 steps of every (tile, stages) candidate on the resident
+    // state with dt = 0 (state unchanged, traffic identical) and keep the fastest.
+    int wdg_wave_autotune(wdg_wave *w, int steps, float *best_ms_per_step)
+    {
+        if (!w || steps < 1)
+            return fail(WDG_ERR_ARG, "wdg_wave_autotune: bad arguments");
+        DeviceGuard g(w->device);
+        WDG_TRY(ensure_states(w));
+        cudaEvent_t e0, e1;
+        WDG_CUDA(cudaEventCreate(&e0));
+        WDG_CUDA(cudaEventCreate(&e1));
+        const int save_tile = w->tile, save_stages = w->stages;
+        float best = 1e30f;
+        int bt = save_tile, bs = save_stages, s = WDG_OK;
+        RKExtras none;
+        for (int st = 2; st <= 4 && s == WDG_OK; ++st)
+            for (int tile = 4; tile <= max_tile(w->n) && s == WDG_OK; tile += 4)
+            {
+                if (smem_for(w, tile, st) > kMaxSmem)
+                    continue;
+                w->tile = tile;
+                w->stages = st;
+                double t = 0.0;
+                auto run = [&](int n) -> int
+                {
+                    return w->precision == WDG_FP64
+                               ? rk4_run<double>(w, static_cast<double *>(w->d_state[0]), 0.0, t, n, none)
+                               : rk4_run<float>(w, static_cast<float *>(w->d_state[0]), 0.0, t, n, none);
+                };
+                s = run(1);
+                if (s != WDG_OK)
+                    break;
+                if (cudaEventRecord(e0, w->stream) != cudaSuccess)
+                {
+                    s = cuda_fail(cudaGetLastError(), "cudaEventRecord");
+                    break;
+                }
+                s = run(steps);
+                if (s != WDG_OK)
+                    break;
+                cudaEventRecord(e1, w->stream);
+                cudaEventSynchronize(e1);
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                ms /= steps;
+                if (ms < best)
+                {
+                    best = ms;
+                    bt = tile;
+                    bs = st;
+                }
+            }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        w->tile = (s == WDG_OK) ? bt : save_tile;
+        w->stages = (s == WDG_OK) ? bs : save_stages;
+        if (s == WDG_OK)
+            s = sync(w);
+        if (best_ms_per_step)
+            *best_ms_per_step = best;
+        return s;
+    }
+
+    int wdg_wave_set_max_ctas(wdg_wave *w, int max_ctas)
+    {
+        if (!w || max_ctas < 0)
+            return fail(WDG_ERR_ARG, "wdg_wave_set_max_ctas: bad arguments");
+        w->max_ctas = max_ctas;
+        return WDG_OK;
+    }
+
     int wdg_wave_get_tile(const wdg_wave *w, int *tile)
     {
         if (!w || !tile)

@@ -12,7 +12,7 @@ struct wdg_wave
 {
     int device = 0;
     cudaStream_t stream = 0;
-    int n = 0, nel = 0, precision = WDG_FP64, tile = 0;
+    int n = 0, nel = 0, precision = WDG_FP64, tile = 0, max_ctas = 0, stages = wdg::kDefaultStages;
     long long ndof = 0;
     int nI = 0, nB = 0;
     double min_h = 0.0;
@@ -22,6 +22,8 @@ struct wdg_wave
     int4 *d_nbr = nullptr;
     uint32_t *d_finfo = nullptr;
     int *d_face_edge = nullptr;
+    int4 *d_fbase = nullptr;
+    uint32_t *d_fcode = nullptr;
     int *d_edgesI = nullptr, *d_edgesB = nullptr, *d_codes = nullptr;
     wdg::Geometry geo;
 

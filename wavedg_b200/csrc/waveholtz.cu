@@ -179,8 +179,9 @@ extern "C"
         int dev_prev = 0;
         cudaGetDevice(&dev_prev);
         cudaSetDevice(w->device);
-        int s = WDG_OK;
-        cudaError_t e = cudaStreamCreateWithFlags(&h->cs, cudaStreamNonBlocking);
+        // state buffers must exist before a period is captured into a graph
+        int s = ensure_states(w);
+        cudaError_t e = (s == WDG_OK) ? cudaStreamCreateWithFlags(&h->cs, cudaStreamNonBlocking) : cudaSuccess;
         if (e == cudaSuccess)
             e = cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming);
         if (e == cudaSuccess)
@@ -194,7 +195,7 @@ extern "C"
             e = cudaMalloc(&h->d_pi0, sizeof(double) * nd + 64);
         if (e == cudaSuccess)
             e = cudaMalloc(&h->d_F, w->real_size() * nd + 64);
-        if (e != cudaSuccess)
+        if (s == WDG_OK && e != cudaSuccess)
             s = cuda_fail(e, "wdg_waveholtz_create");
         cudaSetDevice(dev_prev);
         if (s != WDG_OK)
@@ -297,10 +298,11 @@ extern "C"
             a.u = h->d_W;
             a.out = h->d_acc;
             a.corners = w->d_corners;
-            a.nbr = w->d_nbr;
-            a.finfo = w->d_finfo;
+            a.fbase = w->d_fbase;
+            a.fcode = w->d_fcode;
             a.nel = w->nel;
-            a.tile = default_tile(w->n, false);
+            a.tile = default_tile(w->n, false, kDefaultStages);
+            a.stages = kDefaultStages;
             a.flags = F_ALL;
             a.use_tma = 1;
             a.err = w->d_err;

@@ -230,6 +230,25 @@ class Discretisation:
     def tile(self, v: int) -> None:
         check(lib().wdg_wave_set_tile(self._h, int(v)), "set_tile")
 
+    def set_stages(self, stages: int) -> None:
+        """Depth of the bulk-copy pipeline (2, 3 or 4; 0 = default)."""
+        check(lib().wdg_wave_set_stages(self._h, int(stages)), "set_stages")
+
+    def launch_config(self) -> dict:
+        t, st, mc = C.c_int(), C.c_int(), C.c_int()
+        check(lib().wdg_wave_get_launch(self._h, C.byref(t), C.byref(st), C.byref(mc)))
+        return {"tile": t.value, "stages": st.value, "max_ctas": mc.value}
+
+    def autotune(self, steps: int = 5) -> float:
+        """Pick elements-per-block and pipeline depth by timing; returns the best ms per RK4 step."""
+        ms = C.c_float()
+        check(lib().wdg_wave_autotune(self._h, int(steps), C.byref(ms)), "autotune")
+        return ms.value
+
+    def set_max_ctas(self, n: int) -> None:
+        """Cap the persistent CTAs of the fused kernels (0 = one full wave)."""
+        check(lib().wdg_wave_set_max_ctas(self._h, int(n)), "set_max_ctas")
+
     def zeros(self) -> np.ndarray:
         return np.zeros(self.ndof)
 
