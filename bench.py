@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip the FP32 companion measurement")
     ap.add_argument("--tile", type=int, default=0, help="elements per block (0: autotune)")
     ap.add_argument("--stages", type=int, default=0, help="pipeline depth with --tile (0: default)")
+    ap.add_argument("--kernel", choices=["auto", "warp", "tiled"], default="auto",
+                    help="fused-kernel family (auto: the autotuner picks)")
     return ap.parse_args()
 
 
@@ -170,12 +172,16 @@ def run_ours(args, rank, world, local_rank):
         u0 = torch.zeros(sys_.ndof, dtype=torch.float64, device="cuda")
         sys_.load_gaussians(centers, sigmas, amps, 1.0, 0, True, out=u0)
         sys_.upload(u0)
-        if tile:
+        if args.kernel == "warp":
+            sys_.set_kernel(0)
+        elif args.kernel == "tiled" or tile:
+            sys_.set_kernel(1)
             if args.stages:
                 sys_.set_stages(args.stages)
-            sys_.tile = tile
+            if tile:
+                sys_.tile = tile
         else:
-            sys_.autotune(4)  # elements per block and pipeline depth, timed on this GPU
+            sys_.autotune(4)  # kernel family, elements per block and pipeline depth, timed on this GPU
         t = sys_.step_state(dt, 0.0, warmup)
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -108,9 +108,13 @@ int wdg_wave_set_max_ctas(wdg_wave *wave, int max_ctas);
 /* depth of the bulk-copy pipeline of the fused kernels: 2, 3 or 4 tiles staged (0 = default);
  * the tile shrinks if needed to fit shared memory */
 int wdg_wave_set_stages(wdg_wave *wave, int stages);
-int wdg_wave_get_launch(const wdg_wave *wave, int *elems_per_block, int *stages, int *max_ctas);
-/* the project's autotuner: times `steps` RK4 steps (dt = 0, state unchanged) for every
- * (elements per block, pipeline depth) that fits and keeps the fastest for this handle */
+/* fused-kernel family: 0 warp per element (nodes on lanes; n^2 <= 32 keeps them in registers),
+ * 1 tiled (element tiles staged in shared memory by a TMA bulk-copy pipeline), -1 default */
+int wdg_wave_set_kernel(wdg_wave *wave, int family);
+int wdg_wave_get_launch(const wdg_wave *wave, int *family, int *elems_per_block, int *stages, int *max_ctas);
+/* the project's autotuner: times `steps` RK4 steps (dt = 0, state unchanged) for the warp
+ * kernel and every (elements per block, pipeline depth) of the tiled kernel that fits, and
+ * keeps the fastest for this handle */
 int wdg_wave_autotune(wdg_wave *wave, int steps, float *best_ms_per_step);
 /* Mesh2D::element_metrics(basis).physical_coordinates(): xy (2, n, n, n_elem) */
 int wdg_wave_node_coords(wdg_wave *wave, double *xy);

@@ -53,12 +53,15 @@ def test_rk4_step_vs_oracle_full_size(gpu_lib, big):
     op = cpu.Op(cpu.Mesh(v, q, "oracle"), 5, bc)
     ref, _ = op.rk4(u, dt, 1)
     assert rel(un, ref) < 1e-12
-    # every supported tile size agrees at full size
-    for tile in (8, 12, 16):
-        sys.tile = tile
+    # both kernel families and several tile sizes agree at full size
+    for family, tile in ((0, 0), (1, 8), (1, 12), (1, 16)):
+        sys.set_kernel(family)
+        if tile:
+            sys.tile = tile
         u2 = u.copy()
         sys.rk4_steps(u2, dt, 0.0, 1)
-        assert rel(u2, ref) < 1e-12, tile
+        assert rel(u2, ref) < 1e-12, (family, tile)
+    sys.set_kernel(-1)
     sys.tile = 0
 
 

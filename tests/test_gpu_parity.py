@@ -112,12 +112,16 @@ def test_operators_device_arrays(gpu_lib, fname):
     assert rel(du2.cpu().numpy(), g["rhs"]) < TOL
 
 
-@pytest.mark.parametrize("tile", [4, 8, 12, 16, 20])
+@pytest.mark.parametrize("tile", [0, 4, 8, 12, 16, 20])
 def test_tile_sizes_agree(gpu_lib, tile):
     g = golden("op_scrambled6_n5.npz")
     W, mesh, basis = _setup(g)
     sys = W.WaveSystem(mesh, basis, g["bc"])
-    sys.tile = tile
+    if tile == 0:
+        sys.set_kernel(0)
+    else:
+        sys.set_kernel(1)
+        sys.tile = tile
     un = g["u"].copy()
     sys.rk4_steps(un, float(g["rk4_dt"]), 0.0, 3)
     assert rel(un, g["rk4"]) < TOL
@@ -142,6 +146,15 @@ def test_many_tiles_per_cta(gpu_lib, precision):
     ref_rk, _ = op.rk4(u, 1e-3, 2)
     sys = W.WaveSystem(mesh, basis, bc, precision=precision)
     tol = TOL if precision == "fp64" else 2e-5
+    sys.set_kernel(0)  # warp per element
+    un = u.copy()
+    sys.rk4_steps(un, 1e-3, 0.0, 2)
+    assert rel(un, ref_rk) < tol, ("warp", rel(un, ref_rk))
+    if precision == "fp64":
+        du = np.zeros_like(u)
+        sys.rhs(u, du)
+        assert rel(du, ref_rhs) < TOL
+    sys.set_kernel(1)  # tiled pipeline
     for stages in (2, 3, 4):
       sys.set_stages(stages)
       for tile in (4, 8, 12, 16, 20):
@@ -161,6 +174,7 @@ def test_many_tiles_per_cta(gpu_lib, precision):
     sys.set_max_ctas(0)
     sys.set_stages(0)
     sys.tile = 0
+    sys.set_kernel(-1)
     ms = sys.autotune(2)
     cfg = sys.launch_config()
     assert ms > 0 and cfg["stages"] in (2, 3, 4)

@@ -11,7 +11,8 @@ import re
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-LIB_PATH = os.path.join(HERE, "libwdg_b200.so")
+# WDG_B200_LIB selects another build of the library (e.g. one compiled with different options)
+LIB_PATH = os.environ.get("WDG_B200_LIB") or os.path.join(HERE, "libwdg_b200.so")
 HEADER = os.path.join(ROOT, "include", "wdg_b200.h")
 
 WDG_OK = 0
@@ -61,7 +62,8 @@ SIGNATURES = {
     "wdg_wave_get_tile": ([_v, _ip], _i),
     "wdg_wave_set_max_ctas": ([_v, _i], _i),
     "wdg_wave_set_stages": ([_v, _i], _i),
-    "wdg_wave_get_launch": ([_v, _ip, _ip, _ip], _i),
+    "wdg_wave_set_kernel": ([_v, _i], _i),
+    "wdg_wave_get_launch": ([_v, _ip, _ip, _ip, _ip], _i),
     "wdg_wave_autotune": ([_v, _i, C.POINTER(C.c_float)], _i),
     "wdg_wave_node_coords": ([_v, _v], _i),
     "wdg_div_action": ([_v, _v, _v], _i),

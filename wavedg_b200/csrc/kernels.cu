@@ -51,9 +51,11 @@ namespace wdg
     };
     __constant__ BasisTab c_tab[kMaxN + 1];
 
+    constexpr int kMaxThreads = 320; // threads per CTA of the stage kernel (launch bound)
+
     bool degree_supported(int n) { return n == 2 || n == 3 || n == 4 || n == 5 || n == 6 || n == 7 || n == 8 || n == 9; }
 
-    int max_tile(int n) { return (384 / (n + 8)) & ~3; }
+    int max_tile(int n) { return (kMaxThreads / (n + 8)) & ~3; }
 
     template <typename Real>
     size_t stage_smem_bytes(int n, int tile, int flags, int stages);
@@ -295,6 +297,7 @@ namespace wdg
     }
     __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
     __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+    __device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
     __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
     __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
@@ -327,7 +330,6 @@ namespace wdg
     }
 
     // n line threads (one per row / column) and 8 face threads (two per side) per element
-    constexpr int kMaxThreads = 384;
     int stage_threads(int n, int tile) { return (n + 8) * tile; }
 
     template <int N, typename Real, bool RK>
@@ -431,24 +433,20 @@ namespace wdg
             }
         };
 
+        // Pipeline: tile T_m (the m-th tile of this CTA) lives in buffer m % S.  Its bulk
+        // load is issued at the end of iteration m - S + 1, into the buffer of tile
+        // m - S whose bulk store has had a full iteration to drain, so S - 2 tiles are
+        // in flight ahead of the one being computed.
         int bad = 0;
         if (t == 0)
-            for (int q = 0; q < S; ++q)
+            for (int q = 0; q < S - 1; ++q)
                 issue_tma(blockIdx.x + q * G, q);
         int pbase, pstride;
         load_partner(blockIdx.x, pbase, pstride);
         issue_halo(blockIdx.x, 0, pbase, pstride);
         cp_async_commit();
         load_partner(blockIdx.x + G, pbase, pstride); // issued at the top of iteration 0
-        if (t == 0 && blockIdx.x < ntiles && tma_tile(blockIdx.x) && !mbar_wait(&bars[0], 0))
-            bad = 1;
-        if (__syncthreads_or(bad))
-        {
-            if (t == 0)
-                atomicOr(a.err, 1u);
-            cp_async_wait<0>();
-            return;
-        }
+        __syncthreads(); // mbarrier initialisation and the basis table are visible
 
         int it = 0;
         for (int k = blockIdx.x; k < ntiles; k += G, ++it)
@@ -465,6 +463,9 @@ namespace wdg
             const bool tin = tma_tile(k);
             const bool tout = RK && a.tma_out && (k + 1) * E <= a.nel;
 
+            // every thread waits (sleeping) on this tile's bulk loads
+            if (tin && !mbar_wait(&bars[b], (it / S) & 1))
+                bad = 1;
             if (!tin)
             {
                 for (int q = t; q < ne * ND; q += blockDim.x)
@@ -499,7 +500,12 @@ namespace wdg
                 const Real *row = us + le * ND + 3 * N * lm;
                 Real *g0 = Gs + le * 3 * NN + N * lm;
                 Real *m0 = Ms + le * NN + N * lm;
-                Real Fp[N], Fu[N], Fv[N];
+                // xi-contraction du(i, j) += sum_l D(l, i) F(l, j) (div_2d_c, source/Div.cpp:131-179),
+                // accumulated l-outer so the 3 N sums are independent
+                Real ap[N], au[N], av[N];
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+                    ap[i] = au[i] = av[i] = 0;
 #pragma unroll
                 for (int l = 0; l < N; ++l)
                 {
@@ -509,32 +515,30 @@ namespace wdg
                     const Real W = ws[l] * wj;
                     const Real p = row[3 * l], u = row[3 * l + 1], v = row[3 * l + 2];
                     const Real WYe = Yeta * W, WXe = Xeta * W, WYx = Yxi * W, WXx = Xxi * W;
-                    Fp[l] = WYe * u - WXe * v;
-                    Fu[l] = WYe * p;
-                    Fv[l] = -WXe * p;
+                    const Real Fp = WYe * u - WXe * v;
+                    const Real Fu = WYe * p;
+                    const Real Fv = -WXe * p;
                     g0[l] = -WYx * u + WXx * v;
                     g0[NN + l] = -WYx * p;
                     g0[2 * NN + l] = WXx * p;
                     // MassMatrix<true>: w_i w_j detJ (source/MassMatrix.cpp:6-28)
                     m0[l] = Real(1) / (W * (Xxi * Yeta - Yxi * Xeta));
+#pragma unroll
+                    for (int i = 0; i < N; ++i)
+                    {
+                        const Real d = Tab<Real>::D(N, l + N * i);
+                        ap[i] += d * Fp;
+                        au[i] += d * Fu;
+                        av[i] += d * Fv;
+                    }
                 }
-                // du(i, j) += sum_l D(l, i) F(l, j)   (div_2d_c, source/Div.cpp:131-179)
                 Real *r0 = Rx + le * 3 * NN + N * lm;
 #pragma unroll
                 for (int i = 0; i < N; ++i)
                 {
-                    Real ap = 0, au = 0, av = 0;
-#pragma unroll
-                    for (int l = 0; l < N; ++l)
-                    {
-                        const Real d = Tab<Real>::D(N, l + N * i);
-                        ap += d * Fp[l];
-                        au += d * Fu[l];
-                        av += d * Fv[l];
-                    }
-                    r0[i] = ap;
-                    r0[NN + i] = au;
-                    r0[2 * NN + i] = av;
+                    r0[i] = ap[i];
+                    r0[NN + i] = au[i];
+                    r0[2 * NN + i] = av[i];
                 }
             }
             if (face)
@@ -603,7 +607,23 @@ namespace wdg
                     }
                 }
             }
-            __syncthreads();
+            if (__syncthreads_or(bad))
+            {
+                // leave after bounded waits for the copies still in flight
+                if (t == 0)
+                {
+                    atomicOr(a.err, 1u);
+                    for (int q = 1; q < S - 1; ++q)
+                    {
+                        const int kq = k + q * G;
+                        if (kq < ntiles && tma_tile(kq))
+                            mbar_wait(&bars[(it + q) % S], ((it + q) / S) & 1);
+                    }
+                    bulk_wait_all();
+                }
+                cp_async_wait<0>();
+                return;
+            }
 
             // ---------------- phase 2: eta-lines, face terms, M^{-1}, epilogue (in place)
             if (line && le < ne)
@@ -611,15 +631,32 @@ namespace wdg
                 // column i = lm of element le: du(i, j) += sum_l D(l, j) G(i, l)
                 const int i = lm;
                 const Real *gc = Gs + le * 3 * NN + i;
-                Real gp[N], gu[N], gv[N];
-#pragma unroll
-                for (int l = 0; l < N; ++l)
-                {
-                    gp[l] = gc[N * l];
-                    gu[l] = gc[NN + N * l];
-                    gv[l] = gc[2 * NN + N * l];
-                }
                 const Real *rc = Rx + le * 3 * NN + i;
+                // eta-contraction, l-outer: 3 N independent sums seeded with the xi part
+                Real sp[N], su[N], sv[N];
+#pragma unroll
+                for (int j = 0; j < N; ++j)
+                {
+                    sp[j] = (flags & F_VOL) ? rc[N * j] : Real(0);
+                    su[j] = (flags & F_VOL) ? rc[NN + N * j] : Real(0);
+                    sv[j] = (flags & F_VOL) ? rc[2 * NN + N * j] : Real(0);
+                }
+                if (flags & F_VOL)
+                {
+#pragma unroll
+                    for (int l = 0; l < N; ++l)
+                    {
+                        const Real gp = gc[N * l], gu = gc[NN + N * l], gv = gc[2 * NN + N * l];
+#pragma unroll
+                        for (int j = 0; j < N; ++j)
+                        {
+                            const Real d = Tab<Real>::D(N, l + N * j);
+                            sp[j] += d * gp;
+                            su[j] += d * gu;
+                            sv[j] += d * gv;
+                        }
+                    }
+                }
                 const Real *fce = fc + le * NF * 3;
                 const Real *mc = Ms + le * NN + i;
                 Real *uc = us + le * ND + 3 * i;
@@ -628,21 +665,7 @@ namespace wdg
 #pragma unroll
                 for (int j = 0; j < N; ++j)
                 {
-                    Real r[3] = {0, 0, 0};
-                    if (flags & F_VOL)
-                    {
-                        r[0] = rc[N * j];
-                        r[1] = rc[NN + N * j];
-                        r[2] = rc[2 * NN + N * j];
-#pragma unroll
-                        for (int l = 0; l < N; ++l)
-                        {
-                            const Real d = Tab<Real>::D(N, l + N * j);
-                            r[0] += d * gp[l];
-                            r[1] += d * gu[l];
-                            r[2] += d * gv[l];
-                        }
-                    }
+                    Real r[3] = {sp[j], su[j], sv[j]};
                     // face-flux slots (side * N + face node) through node (i, j)
                     int sl[2] = {-1, -1}, ns = 0;
                     if (j == 0) sl[ns++] = 0 * N + i;
@@ -689,27 +712,8 @@ namespace wdg
                     fence_async_smem();
             }
 
-            // ---------------- end of tile: write back, refill the buffer
-            const int kn = k + G;
-            if (t == 0 && kn < ntiles && tma_tile(kn) && !mbar_wait(&bars[(it + 1) % S], ((it + 1) / S) & 1))
-                bad = 1;
-            if (__syncthreads_or(bad))
-            {
-                // leave after bounded waits for the copies still in flight (tiles it+2 .. it+S-1)
-                if (t == 0)
-                {
-                    atomicOr(a.err, 1u);
-                    for (int q = 2; q < S; ++q)
-                    {
-                        const int kq = k + q * G;
-                        if (kq < ntiles && tma_tile(kq))
-                            mbar_wait(&bars[(it + q) % S], ((it + q) / S) & 1);
-                    }
-                    bulk_wait_all();
-                }
-                cp_async_wait<0>();
-                return;
-            }
+            // ---------------- end of tile: write back, refill the previous tile's buffer
+            __syncthreads();
             const bool filter = RK && (flags & F_FILTER);
             if (tout && t == 0)
             {
@@ -740,14 +744,273 @@ namespace wdg
             }
             if (t == 0)
             {
+                // the buffer refilled next held tile it+1-S+... i.e. tile it-1 (S >= 2): its
+                // store (committed one iteration ago) must have finished reading shared memory
                 if (tout)
-                    bulk_wait_read(); // the buffer is refilled next
-                issue_tma(k + S * G, b);
+                    bulk_wait_read1();
+                else
+                    bulk_wait_read();
+                issue_tma(k + (S - 1) * G, (it + S - 1) % S);
             }
         }
         cp_async_wait<0>();
         if (t == 0)
             bulk_wait_all();
+    }
+
+    // ------------------------------------------------ warp-per-element kernel
+    // A warp owns EPW = 32 / n^2 elements (n <= 5) or one element with NPL =
+    // ceil(n^2 / 32) nodes per lane (n >= 6); every lane holds whole nodes.
+    //   * the node's state, RK register, the element's 4 corners and its face
+    //     table come straight from global memory in coalesced loads; face lanes
+    //     issue the loads of their partner's trace (L2) before any arithmetic;
+    //   * metrics and the six contravariant fluxes are formed per node and
+    //     exchanged through a per-warp scratch in shared memory (__syncwarp, no
+    //     CTA barrier); the 1-D derivative columns of the lane sit in registers;
+    //   * the upwind flux, forcing, M^{-1} and the RK update finish in registers
+    //     and are stored coalesced.
+    // Warps never wait for one another, so memory latency is covered by the many
+    // warps resident per SM.
+    template <int N>
+    struct WarpShape
+    {
+        static constexpr int NN = N * N;
+        static constexpr int EPW = (NN <= 32) ? 32 / NN : 1;
+        static constexpr int NPL = (NN <= 32) ? 1 : (NN + 31) / 32;
+    };
+    constexpr int kWarpThreads = 256;
+
+    template <typename Real>
+    size_t warp_smem_bytes(int n)
+    {
+        const int nn = n * n, epw = (nn <= 32) ? 32 / nn : 1;
+        const size_t dtab = ((size_t)nn * sizeof(Real) + 15) & ~size_t(15);
+        return dtab + (size_t)(kWarpThreads / 32) * epw * nn * 6 * sizeof(Real);
+    }
+
+    template <int N, typename Real, bool RK>
+    __global__ void __launch_bounds__(kWarpThreads, 3) warp_stage_kernel(const StageArgs<Real> a)
+    {
+        constexpr int NN = N * N, EPW = WarpShape<N>::EPW, NPL = WarpShape<N>::NPL;
+        const int flags = a.flags;
+        const bool has_du = RK && (flags & F_READ_DU);
+        extern __shared__ __align__(16) unsigned char wsmem[];
+        Real *Dsm = reinterpret_cast<Real *>(wsmem);
+        Real *X = reinterpret_cast<Real *>(wsmem + ((NN * sizeof(Real) + 15) & ~size_t(15))) +
+                  (threadIdx.x >> 5) * (EPW * NN * 6); // this warp's scratch: [slot][6][NN]
+        if (NPL > 1)
+        {
+            for (int q = threadIdx.x; q < NN; q += blockDim.x)
+                Dsm[q] = Tab<Real>::D(N, q);
+            __syncthreads();
+        }
+        const int lane = threadIdx.x & 31;
+        const int el_base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * EPW;
+        if (el_base >= a.nel)
+            return;
+
+        int node[NPL], slot[NPL], el[NPL];
+        bool act[NPL];
+#pragma unroll
+        for (int p = 0; p < NPL; ++p)
+        {
+            node[p] = (NPL == 1) ? lane % NN : lane + 32 * p;
+            slot[p] = (NPL == 1) ? lane / NN : 0;
+            el[p] = el_base + slot[p];
+            act[p] = ((NPL == 1) ? (lane < EPW * NN) : (node[p] < NN)) && el[p] < a.nel;
+        }
+        // derivative columns D(., i), D(., j) of a single-node lane
+        Real Di[NPL == 1 ? N : 1], Dj[NPL == 1 ? N : 1];
+        if (NPL == 1)
+        {
+            const int i = node[0] % N, j = node[0] / N;
+#pragma unroll
+            for (int l = 0; l < (NPL == 1 ? N : 1); ++l)
+            {
+                Di[l] = Tab<Real>::D(N, l + N * i);
+                Dj[l] = Tab<Real>::D(N, l + N * j);
+            }
+        }
+
+        // ---- loads: node state, RK register, side inputs, partner traces
+        Real q[NPL][3], dv[NPL][3], xf[NPL][2][3], Fv[NPL][3], ov[NPL][3];
+        double accv[NPL][3];
+        int nfc[NPL], fcs[NPL][2], fck[NPL][2];
+        uint32_t fbyte[NPL][2];
+#pragma unroll
+        for (int p = 0; p < NPL; ++p)
+        {
+            nfc[p] = 0;
+            if (!act[p])
+                continue;
+            const size_t g = ((size_t)el[p] * NN + node[p]) * 3;
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+            {
+                q[p][c] = a.u[g + c];
+                dv[p][c] = has_du ? a.du[g + c] : Real(0);
+                Fv[p][c] = (flags & F_FORCE) ? a.F[g + c] : Real(0);
+                ov[p][c] = (!RK && (flags & F_ACCUM)) ? a.out[g + c] : Real(0);
+                accv[p][c] = (RK && (flags & F_FILTER)) ? a.acc[g + c] : 0.0;
+            }
+            const int i = node[p] % N, j = node[p] / N;
+            if (j == 0) { fcs[p][nfc[p]] = 0; fck[p][nfc[p]++] = i; }
+            if (i == N - 1) { fcs[p][nfc[p]] = 1; fck[p][nfc[p]++] = j; }
+            if (j == N - 1 && nfc[p] < 2) { fcs[p][nfc[p]] = 2; fck[p][nfc[p]++] = i; }
+            if (i == 0 && nfc[p] < 2) { fcs[p][nfc[p]] = 3; fck[p][nfc[p]++] = j; }
+            if (nfc[p] == 0)
+                continue;
+            const int4 fb = a.fbase[el[p]];
+            const uint32_t code = a.fcode[el[p]];
+#pragma unroll
+            for (int s = 0; s < 2; ++s)
+            {
+                if (s >= nfc[p])
+                    continue;
+                const int f = fcs[p][s];
+                const uint32_t byte = (code >> (8 * f)) & 0xffu;
+                fbyte[p][s] = byte;
+                if ((byte & 0x80u) || !(flags & F_INT))
+                    continue;
+                const int off = ((f == 0) ? fb.x : (f == 1) ? fb.y : (f == 2) ? fb.z : fb.w) +
+                                fck[p][s] * partner_stride<N>(byte);
+                if (off < 0 || off + 3 > a.nel * 3 * NN)
+                {
+                    atomicOr(a.err, 2u);
+                    fbyte[p][s] = 0x40u; // skip this face
+                    continue;
+                }
+                xf[p][s][0] = __ldg(a.u + off);
+                xf[p][s][1] = __ldg(a.u + off + 1);
+                xf[p][s][2] = __ldg(a.u + off + 2);
+            }
+        }
+
+        // ---- metrics and contravariant fluxes at the nodes (source/Div.cpp:5-53)
+        Real minv[NPL];
+#pragma unroll
+        for (int p = 0; p < NPL; ++p)
+        {
+            minv[p] = 0;
+            if (!act[p])
+                continue;
+            const int i = node[p] % N, j = node[p] / N;
+            const double2 *cp = reinterpret_cast<const double2 *>(a.corners + 8 * (size_t)el[p]);
+            double c[8];
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+            {
+                const double2 v = __ldg(cp + k);
+                c[2 * k] = v.x;
+                c[2 * k + 1] = v.y;
+            }
+            Real J[4];
+            jacobian<Real>(c, Tab<Real>::x(N, i), Tab<Real>::x(N, j), J);
+            const Real W = Tab<Real>::w(N, i) * Tab<Real>::w(N, j);
+            const Real Yeta = J[3] * W, Xeta = J[2] * W, Yxi = J[1] * W, Xxi = J[0] * W;
+            Real *x = X + slot[p] * (6 * NN) + node[p];
+            x[0 * NN] = Yeta * q[p][1] - Xeta * q[p][2];
+            x[1 * NN] = Yeta * q[p][0];
+            x[2 * NN] = -Xeta * q[p][0];
+            x[3 * NN] = -Yxi * q[p][1] + Xxi * q[p][2];
+            x[4 * NN] = -Yxi * q[p][0];
+            x[5 * NN] = Xxi * q[p][0];
+            minv[p] = Real(1) / (W * (J[0] * J[3] - J[1] * J[2]));
+        }
+        __syncwarp();
+
+        // ---- volume, faces, M^{-1}, epilogue
+#pragma unroll
+        for (int p = 0; p < NPL; ++p)
+        {
+            if (!act[p])
+                continue;
+            const int i = node[p] % N, j = node[p] / N;
+            Real r[3] = {0, 0, 0};
+            if (flags & F_VOL)
+            {
+                const Real *x = X + slot[p] * (6 * NN);
+#pragma unroll
+                for (int l = 0; l < N; ++l)
+                {
+                    const Real di = (NPL == 1) ? Di[l % (NPL == 1 ? N : 1)] : Dsm[l + N * i];
+                    const Real dj = (NPL == 1) ? Dj[l % (NPL == 1 ? N : 1)] : Dsm[l + N * j];
+                    const int fl = l + N * j, gl = i + N * l;
+                    r[0] += di * x[fl] + dj * x[3 * NN + gl];
+                    r[1] += di * x[NN + fl] + dj * x[4 * NN + gl];
+                    r[2] += di * x[2 * NN + fl] + dj * x[5 * NN + gl];
+                }
+            }
+            if (nfc[p] > 0)
+            {
+                const double *c = a.corners + 8 * (size_t)el[p];
+#pragma unroll
+                for (int s = 0; s < 2; ++s)
+                {
+                    if (s >= nfc[p])
+                        continue;
+                    const uint32_t byte = fbyte[p][s];
+                    const bool bnd = (byte & 0x80u) != 0;
+                    if ((byte == 0x40u) || (bnd ? !(flags & F_BND) : !(flags & F_INT)))
+                        continue;
+                    const int f = fcs[p][s];
+                    const double dx = __ldg(c + 2 * c_to[f]) - __ldg(c + 2 * c_from[f]);
+                    const double dy = __ldg(c + 2 * c_to[f] + 1) - __ldg(c + 2 * c_from[f] + 1);
+                    const double s2 = dx * dx + dy * dy, rs = rsqrt(s2);
+                    const double sgn = (f >= 2) ? -1.0 : 1.0;
+                    const Real nx = (Real)(sgn * dy * rs), ny = (Real)(-sgn * dx * rs);
+                    Real x[3];
+                    if (bnd)
+                        exterior<Real>((int)((byte >> 3) & 3u), nx, ny, q[p], x);
+                    else
+                    {
+                        x[0] = xf[p][s][0];
+                        x[1] = xf[p][s][1];
+                        x[2] = xf[p][s][2];
+                    }
+                    upwind<Real>(nx, ny, Tab<Real>::w(N, fck[p][s]) * (Real)(0.25 * s2 * rs), q[p], x, r);
+                }
+            }
+            if (flags & F_FORCE)
+                for (int c = 0; c < 3; ++c)
+                    r[c] += Fv[p][c] * a.fscale;
+            if (flags & F_MINV)
+                for (int c = 0; c < 3; ++c)
+                    r[c] *= minv[p];
+            const size_t g = ((size_t)el[p] * NN + node[p]) * 3;
+            if (RK)
+            {
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                {
+                    const Real dn = has_du ? a.rk_a * dv[p][c] + a.dt * r[c] : a.dt * r[c];
+                    const Real un = q[p][c] + a.rk_b * dn;
+                    a.du[g + c] = dn;
+                    a.out[g + c] = un;
+                    if (flags & F_FILTER)
+                        a.acc[g + c] = accv[p][c] + a.acc_c * (double)un;
+                }
+            }
+            else
+            {
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    a.out[g + c] = (flags & F_ACCUM) ? ov[p][c] + r[c] : r[c];
+            }
+        }
+    }
+
+    template <int N, typename Real, bool RK>
+    static cudaError_t launch_warp_n(const StageArgs<Real> &a, cudaStream_t s)
+    {
+        auto kern = warp_stage_kernel<N, Real, RK>;
+        const size_t smem = warp_smem_bytes<Real>(N);
+        constexpr int EPW = WarpShape<N>::EPW;
+        const long long warps = ((long long)a.nel + EPW - 1) / EPW;
+        const int wpb = kWarpThreads / 32;
+        const long long blocks = (warps + wpb - 1) / wpb;
+        kern<<<(unsigned)blocks, kWarpThreads, smem, s>>>(a);
+        return cudaGetLastError();
     }
 
     template <int N, typename Real, bool RK>
@@ -799,6 +1062,8 @@ namespace wdg
     {
 #define WDG_CASE(NV)                                                                       \
     case NV:                                                                               \
+        if (a.family == 0)                                                                 \
+            return rk ? launch_warp_n<NV, Real, true>(a, s) : launch_warp_n<NV, Real, false>(a, s); \
         return rk ? launch_stage_n<NV, Real, true>(a, grid_limit, s)                       \
                   : launch_stage_n<NV, Real, false>(a, grid_limit, s);
         switch (n)

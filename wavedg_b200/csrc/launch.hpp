@@ -40,6 +40,7 @@ namespace wdg
         int use_tma;          // 1: full tiles are loaded with cp.async.bulk
         int tma_out;          // 1: full tiles of u' and du' are stored with cp.async.bulk (RK mode)
         int stages;           // pipeline depth (2..4): tiles whose bulk loads are in flight + 1
+        int family;           // 0: warp-per-element kernel, 1: tiled TMA-pipeline kernel
         Real rk_a, rk_b, dt, fscale;
         double acc_c;
         unsigned *err;        // device error word (bit 0: wait timeout, bit 1: bad neighbour index)
@@ -61,7 +62,9 @@ namespace wdg
     int upload_basis_tables(int device);   // once per device
     bool degree_supported(int n);
     int default_tile(int n, bool fp32, int stages);
-    constexpr int kDefaultStages = 2;
+    // warp-per-element kernel while an element's nodes fit one warp, tiled kernel beyond
+    inline int default_family(int n) { return (n * n <= 32) ? 0 : 1; }
+    constexpr int kDefaultStages = 3;
     int max_tile(int n);
 
     // fused stage: RK = true for the time-stepping epilogue

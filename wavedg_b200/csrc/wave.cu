@@ -116,6 +116,7 @@ namespace wdg
         a.nel = w->nel;
         a.tile = w->tile;
         a.stages = w->stages;
+        a.family = w->family;
         a.err = w->d_err;
         return a;
     }
@@ -284,6 +285,7 @@ namespace
         // operator launches always run the FP64 kernel, whatever the stepping precision
         a.tile = default_tile(w->n, false, kDefaultStages);
         a.stages = kDefaultStages;
+        a.family = w->family;
         a.u = u;
         a.out = out;
         a.flags = flags;
@@ -402,6 +404,7 @@ extern "C"
         w->nB = (int)mesh->boundary.size();
         w->min_h = mesh->min_h;
         w->tile = default_tile(n_colloc, precision == WDG_FP32, w->stages);
+        w->family = default_family(n_colloc);
 
         int s = WDG_OK;
         auto chk = [&](int r)
@@ -562,10 +565,19 @@ extern "C"
         return WDG_OK;
     }
 
-    int wdg_wave_get_launch(const wdg_wave *w, int *tile, int *stages, int *max_ctas)
+    int wdg_wave_set_kernel(wdg_wave *w, int family)
+    {
+        if (!w || family < -1 || family > 1)
+            return fail(WDG_ERR_ARG, "wdg_wave_set_kernel: 0 (warp per element), 1 (tiled) or -1 (default)");
+        w->family = (family < 0) ? default_family(w->n) : family;
+        return WDG_OK;
+    }
+
+    int wdg_wave_get_launch(const wdg_wave *w, int *family, int *tile, int *stages, int *max_ctas)
     {
         if (!w)
             return fail(WDG_ERR_ARG, "null discretisation");
+        if (family) *family = w->family;
         if (tile) *tile = w->tile;
         if (stages) *stages = w->stages;
         if (max_ctas) *max_ctas = w->max_ctas;
@@ -583,17 +595,19 @@ extern "C"
         cudaEvent_t e0, e1;
         WDG_CUDA(cudaEventCreate(&e0));
         WDG_CUDA(cudaEventCreate(&e1));
-        const int save_tile = w->tile, save_stages = w->stages;
+        const int save_tile = w->tile, save_stages = w->stages, save_family = w->family;
         float best = 1e30f;
-        int bt = save_tile, bs = save_stages, s = WDG_OK;
+        int bt = save_tile, bs = save_stages, bf = save_family, s = WDG_OK;
         RKExtras none;
-        for (int st = 2; st <= 4 && s == WDG_OK; ++st)
-            for (int tile = 4; tile <= max_tile(w->n) && s == WDG_OK; tile += 4)
+        // candidate 0: the warp-per-element kernel; then every fitting tiled configuration
+        for (int st = 1; st <= 4 && s == WDG_OK; ++st)
+            for (int tile = (st == 1 ? 0 : 4); tile <= (st == 1 ? 0 : max_tile(w->n)) && s == WDG_OK; tile += 4)
             {
-                if (smem_for(w, tile, st) > kMaxSmem)
+                if (st > 1 && smem_for(w, tile, st) > kMaxSmem)
                     continue;
-                w->tile = tile;
-                w->stages = st;
+                w->family = (st == 1) ? 0 : 1;
+                w->tile = (st == 1) ? save_tile : tile;
+                w->stages = (st == 1) ? save_stages : st;
                 double t = 0.0;
                 auto run = [&](int n) -> int
                 {
@@ -620,14 +634,16 @@ extern "C"
                 if (ms < best)
                 {
                     best = ms;
-                    bt = tile;
-                    bs = st;
+                    bt = w->tile;
+                    bs = w->stages;
+                    bf = w->family;
                 }
             }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         w->tile = (s == WDG_OK) ? bt : save_tile;
         w->stages = (s == WDG_OK) ? bs : save_stages;
+        w->family = (s == WDG_OK) ? bf : save_family;
         if (s == WDG_OK)
             s = sync(w);
         if (best_ms_per_step)

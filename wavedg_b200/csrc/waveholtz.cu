@@ -303,6 +303,7 @@ extern "C"
             a.nel = w->nel;
             a.tile = default_tile(w->n, false, kDefaultStages);
             a.stages = kDefaultStages;
+            a.family = w->family;
             a.flags = F_ALL;
             a.use_tma = 1;
             a.err = w->d_err;

@@ -234,10 +234,14 @@ class Discretisation:
         """Depth of the bulk-copy pipeline (2, 3 or 4; 0 = default)."""
         check(lib().wdg_wave_set_stages(self._h, int(stages)), "set_stages")
 
+    def set_kernel(self, family: int) -> None:
+        """0: warp per element, 1: tiled TMA pipeline, -1: default for this degree."""
+        check(lib().wdg_wave_set_kernel(self._h, int(family)), "set_kernel")
+
     def launch_config(self) -> dict:
-        t, st, mc = C.c_int(), C.c_int(), C.c_int()
-        check(lib().wdg_wave_get_launch(self._h, C.byref(t), C.byref(st), C.byref(mc)))
-        return {"tile": t.value, "stages": st.value, "max_ctas": mc.value}
+        f, t, st, mc = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        check(lib().wdg_wave_get_launch(self._h, C.byref(f), C.byref(t), C.byref(st), C.byref(mc)))
+        return {"kernel": ("warp", "tiled")[f.value], "tile": t.value, "stages": st.value, "max_ctas": mc.value}
 
     def autotune(self, steps: int = 5) -> float:
         """Pick elements-per-block and pipeline depth by timing; returns the best ms per RK4 step."""
