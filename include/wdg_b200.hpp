@@ -1,0 +1,214 @@
+// wdg_b200.hpp -- drop-in C++ classes for the reference waveDG interface.
+//
+// Include after the reference's headers (its include directories and the
+// generated wdg_config.hpp on the include path).  Each class derives from the
+// reference's own dg::Operator / dg::InvertibleOperator and takes the same
+// constructor arguments as the reference class it replaces, so a driver only
+// changes type names (dg::WaveEquation -> dg::b200::WaveEquation, ...).  All work
+// happens on the GPU through the C ABI in wdg_b200.h; host arrays are staged,
+// device arrays are used in place.  Errors throw std::runtime_error, like the
+// reference's wdg_error (source/wdg_error.cpp:5-20).
+#ifndef WDG_B200_HPP
+#define WDG_B200_HPP
+
+#include <cmath>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "wdg_b200.h"
+
+namespace dg
+{
+namespace b200
+{
+    inline void check(int status)
+    {
+        if (status < 0)
+            throw std::runtime_error(std::string("wdg_b200: ") + wdg_last_error());
+    }
+
+    // A dg::Mesh2D adopted through its public API: corners from QuadElement::corner
+    // (wavedg/Element.hpp:123-126) and the edge tables in Mesh2D::edge(i, type) order.
+    class Mesh
+    {
+    public:
+        explicit Mesh(const dg::Mesh2D &m)
+        {
+            const int nel = m.n_elem();
+            std::vector<double> corners(8 * (size_t)nel);
+            for (int el = 0; el < nel; ++el)
+            {
+                const auto *q = dynamic_cast<const dg::QuadElement *>(m.element(el));
+                if (!q)
+                    throw std::runtime_error("wdg_b200: only QuadElement meshes are supported");
+                for (int c = 0; c < 4; ++c)
+                {
+                    corners[8 * (size_t)el + 2 * c] = q->corner(c)[0];
+                    corners[8 * (size_t)el + 2 * c + 1] = q->corner(c)[1];
+                }
+            }
+            auto table = [&](dg::FaceType t)
+            {
+                std::vector<int> out(5 * (size_t)m.n_edges(t));
+                for (int e = 0; e < m.n_edges(t); ++e)
+                {
+                    const dg::Edge *E = m.edge(e, t);
+                    out[5 * e] = E->elements[0];
+                    out[5 * e + 1] = E->sides[0];
+                    out[5 * e + 2] = (t == dg::FaceType::INTERIOR) ? E->elements[1] : -1;
+                    out[5 * e + 3] = (t == dg::FaceType::INTERIOR) ? E->sides[1] : -1;
+                    out[5 * e + 4] = (t == dg::FaceType::INTERIOR) ? E->delta : 1;
+                }
+                return out;
+            };
+            const std::vector<int> ie = table(dg::FaceType::INTERIOR), be = table(dg::FaceType::BOUNDARY);
+            wdg_mesh *h = nullptr;
+            check(wdg_mesh_from_tables(nel, corners.data(), (int)(ie.size() / 5), ie.data(), (int)(be.size() / 5),
+                                       be.data(), &h));
+            h_.reset(h, wdg_mesh_destroy);
+        }
+        wdg_mesh *get() const { return h_.get(); }
+        int n_boundary() const { return wdg_mesh_n_edges(h_.get(), WDG_BOUNDARY); }
+
+    private:
+        std::shared_ptr<wdg_mesh> h_;
+    };
+
+    // one GPU discretisation of the wave system (geometry on the device)
+    class Discretisation
+    {
+    public:
+        Discretisation(const dg::Mesh2D &mesh, const dg::QuadratureRule *basis, const int *bc, int precision = WDG_FP64,
+                       int device = -1)
+            : mesh_(mesh)
+        {
+            if (!basis || basis->type != dg::QuadratureRule::GaussLobatto)
+                throw std::runtime_error("wdg_b200: the GPU operators are built for Gauss-Lobatto bases");
+            wdg_wave *w = nullptr;
+            check(wdg_wave_create(mesh_.get(), basis->n, bc, precision, device, &w));
+            h_.reset(w, wdg_wave_destroy);
+            long long nd = 0;
+            check(wdg_wave_info(w, nullptr, nullptr, &nd, nullptr));
+            ndof_ = nd;
+        }
+        wdg_wave *get() const { return h_.get(); }
+        long long ndof() const { return ndof_; }
+
+    private:
+        Mesh mesh_;
+        std::shared_ptr<wdg_wave> h_;
+        long long ndof_ = 0;
+    };
+
+    inline void require_approx(bool approx_quad)
+    {
+        if (!approx_quad)
+            throw std::runtime_error("wdg_b200: exact-quadrature operators are not built; use approx_quad = true");
+    }
+
+    // dg::WaveEquation (source/WaveEquation.cpp:5-68): du += Div(u) + P^T Flux(P u)
+    class WaveEquation : public dg::Operator
+    {
+    public:
+        WaveEquation(const dg::Mesh2D &mesh, const dg::QuadratureRule *basis, bool approx_quad = false,
+                     const dg::QuadratureRule *quad = nullptr)
+            : d_((require_approx(approx_quad), mesh), basis, nullptr) {}
+        void action(const double *u, double *du) const override { check(wdg_wave_action(d_.get(), u, du)); }
+        void action(int, const double *u, double *du) const override { action(u, du); }
+
+    private:
+        Discretisation d_;
+    };
+
+    // dg::WaveBC (source/WaveEquation.cpp:70-215); codes 0 absorbing, 1 reflecting, 2 Dirichlet p = 0
+    class WaveBC : public dg::Operator
+    {
+    public:
+        WaveBC(const dg::Mesh2D &mesh, const int *bc, const dg::QuadratureRule *basis, bool approx_quad,
+               const dg::QuadratureRule *quad = nullptr)
+            : d_((require_approx(approx_quad), mesh), basis, bc) {}
+        void action(const double *u, double *du) const override { check(wdg_wavebc_action(d_.get(), u, du)); }
+        void action(int, const double *u, double *du) const override { action(u, du); }
+
+    private:
+        Discretisation d_;
+    };
+
+    // dg::MassMatrix<true> (source/MassMatrix.cpp:6-82)
+    class MassMatrix : public dg::InvertibleOperator
+    {
+    public:
+        MassMatrix(const dg::Mesh2D &mesh, const dg::QuadratureRule *basis, const dg::QuadratureRule *quad = nullptr)
+            : d_(mesh, basis, nullptr) {}
+        void action(const double *x, double *y) const override { action(1, x, y); }
+        void action(int n_var, const double *x, double *y) const override
+        {
+            check(wdg_mass_action(d_.get(), n_var, x, y));
+        }
+        void inv(double *x) const override { inv(1, x); }
+        void inv(int n_var, double *x) const override { check(wdg_mass_inv(d_.get(), n_var, x)); }
+
+    private:
+        Discretisation d_;
+    };
+
+    // The examples' time derivative M^{-1}(A + B) u as one fused operator, with the
+    // fused ode::RungeKutta4 (wavedg/ode.hpp:66-93) stepping on the GPU.
+    class WaveSystem : public dg::Operator
+    {
+    public:
+        WaveSystem(const dg::Mesh2D &mesh, const dg::QuadratureRule *basis, const int *bc, int precision = WDG_FP64)
+            : d_(mesh, basis, bc, precision) {}
+        // y <- M^{-1} (A + B) x  (overwrites y)
+        void action(const double *x, double *y) const override { check(wdg_rhs(d_.get(), x, y, nullptr, 0.0)); }
+        void action(int, const double *x, double *y) const override { action(x, y); }
+        // ode::RungeKutta4::step, `nsteps` times: t += nsteps * dt, u in place
+        void rk4_steps(double dt, double &t, double *u, int nsteps = 1) const
+        {
+            check(wdg_rk4_steps(d_.get(), u, dt, &t, nsteps));
+        }
+        void autotune(int steps = 5) const { check(wdg_wave_autotune(d_.get(), steps, nullptr)); }
+        wdg_wave *get() const { return d_.get(); }
+        long long ndof() const { return d_.ndof(); }
+
+    private:
+        Discretisation d_;
+    };
+
+    // dg::WaveHoltz (source/WaveHoltz.cpp)
+    class WaveHoltz
+    {
+    public:
+        WaveHoltz(double omega, const dg::Mesh2D &mesh, const dg::QuadratureRule *basis, const int *bc,
+                  bool approx_quad = false, int precision = WDG_FP64)
+            : omega_(omega), sys_((require_approx(approx_quad), mesh), basis, bc, precision)
+        {
+            wdg_waveholtz *h = nullptr;
+            check(wdg_waveholtz_create(sys_.get(), omega, &h));
+            h_.reset(h, wdg_waveholtz_destroy);
+        }
+        double K(double t) const { return omega_ / M_PI * (std::cos(omega_ * t) - 0.25); }
+        void pi0(double *w, const double *F) const { check(wdg_waveholtz_pi0(h_.get(), w, F)); }
+        void S(double *w) const { check(wdg_waveholtz_S(h_.get(), w)); }
+        void postprocess(double *H, const double *w) const { check(wdg_waveholtz_postprocess(h_.get(), H, w)); }
+        // the fixed-point loop of examples/waveholtz2d.cpp:137-185; returns the iterations taken
+        int solve(const double *F, double tol, int maxit, double *W, double *residual) const
+        {
+            int it = 0;
+            const int s = wdg_waveholtz_solve(h_.get(), F, tol, maxit, W, &it, residual);
+            if (s != WDG_ERR_NOT_CONVERGED)
+                check(s);
+            return it;
+        }
+
+    private:
+        double omega_;
+        WaveSystem sys_;
+        std::shared_ptr<wdg_waveholtz> h_;
+    };
+} // namespace b200
+} // namespace dg
+
+#endif

@@ -1,0 +1,153 @@
+// dropin_test.cpp -- TEST INFRASTRUCTURE ONLY.
+//
+// A reference-style driver: it builds the reference's own Mesh2D, QuadratureRule
+// and operators, and the dg::b200 drop-ins from include/wdg_b200.hpp with the
+// same constructor arguments, then checks that the drop-ins give the reference's
+// answers -- operator by operator, through the reference's own ode::RungeKutta4
+// driving the GPU operators with host arrays (the examples/wave2d.cpp pattern),
+// through the fused GPU stepper, and through WaveHoltz.  Exit status 0 = all
+// within tolerance.  Built by `make -C oracle ref` into oracle/_ref/.
+#include <cmath>
+#include <cstdio>
+#include <random>
+#include <vector>
+
+#include "wavedg.hpp"
+#include "wdg_b200.hpp"
+
+using namespace dg;
+
+static double rel(const std::vector<double> &a, const std::vector<double> &b)
+{
+    double num = 0, den = 0;
+    for (size_t i = 0; i < a.size(); ++i)
+    {
+        num += (a[i] - b[i]) * (a[i] - b[i]);
+        den += b[i] * b[i];
+    }
+    return std::sqrt(num / (den > 0 ? den : 1.0));
+}
+
+static int failures = 0;
+static void report(const char *what, double err, double tol)
+{
+    const bool ok = err <= tol;
+    std::printf("%-44s %.3e  (tol %.0e)  %s\n", what, err, tol, ok ? "ok" : "FAIL");
+    failures += ok ? 0 : 1;
+}
+
+static Mesh2D perturbed_mesh(int n, unsigned seed)
+{
+    const int nv = (n + 1) * (n + 1);
+    std::vector<double> xy(2 * nv);
+    std::vector<int> q(4 * n * n);
+    std::mt19937 gen(seed);
+    std::uniform_real_distribution<double> U(-0.2, 0.2);
+    const double h = 2.0 / n;
+    for (int j = 0; j <= n; ++j)
+        for (int i = 0; i <= n; ++i)
+        {
+            const bool inner = i > 0 && i < n && j > 0 && j < n;
+            xy[2 * (i + (n + 1) * j)] = -1.0 + h * i + (inner ? U(gen) * h : 0.0);
+            xy[2 * (i + (n + 1) * j) + 1] = -1.0 + h * j + (inner ? U(gen) * h : 0.0);
+        }
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i)
+        {
+            int *e = &q[4 * (i + n * j)];
+            e[0] = i + (n + 1) * j;
+            e[1] = i + 1 + (n + 1) * j;
+            e[2] = i + 1 + (n + 1) * (j + 1);
+            e[3] = i + (n + 1) * (j + 1);
+        }
+    return Mesh2D::from_vertices(nv, xy.data(), n * n, q.data());
+}
+
+int main()
+{
+    auto basis = QuadratureRule::quadrature_rule(5, QuadratureRule::GaussLobatto);
+    Mesh2D mesh = perturbed_mesh(12, 7);
+    const int ndof = 3 * 25 * mesh.n_elem();
+    std::vector<int> bc(mesh.n_edges(FaceType::BOUNDARY), 1); // reflecting: the reference's WaveBC verbatim
+
+    WaveEquation a(mesh, basis, true);
+    WaveBC b(mesh, bc.data(), basis, true);
+    MassMatrix<true> m(mesh, basis);
+    b200::WaveEquation ga(mesh, basis, true);
+    b200::WaveBC gb(mesh, bc.data(), basis, true);
+    b200::MassMatrix gm(mesh, basis);
+
+    std::mt19937 gen(11);
+    std::normal_distribution<double> N01;
+    std::vector<double> u(ndof);
+    for (double &x : u)
+        x = N01(gen);
+
+    std::vector<double> r1(ndof, 0.0), r2(ndof, 0.0);
+    a.action(u.data(), r1.data());
+    ga.action(u.data(), r2.data());
+    report("WaveEquation::action", rel(r2, r1), 1e-12);
+    b.action(u.data(), r1.data());
+    gb.action(u.data(), r2.data());
+    report("WaveEquation + WaveBC::action", rel(r2, r1), 1e-12);
+    m.inv(3, r1.data());
+    gm.inv(3, r2.data());
+    report("MassMatrix<true>::inv", rel(r2, r1), 1e-12);
+
+    // the reference's RK4 driving (a) the reference operators, (b) the drop-ins on host arrays
+    const double dt = 0.1 * mesh.min_h() / 25.0;
+    ode::RungeKutta4 rk(ndof);
+    auto f_ref = [&](double *dudt, const double, const double *v)
+    {
+        for (int i = 0; i < ndof; ++i)
+            dudt[i] = 0.0;
+        a.action(v, dudt);
+        b.action(v, dudt);
+        m.inv(3, dudt);
+    };
+    auto f_gpu = [&](double *dudt, const double, const double *v)
+    {
+        for (int i = 0; i < ndof; ++i)
+            dudt[i] = 0.0;
+        ga.action(v, dudt);
+        gb.action(v, dudt);
+        gm.inv(3, dudt);
+    };
+    std::vector<double> ur = u, ug = u, uf = u;
+    double tr = 0.0, tg = 0.0, tf = 0.0;
+    for (int s = 0; s < 10; ++s)
+    {
+        rk.step(dt, f_ref, tr, ur.data());
+        rk.step(dt, f_gpu, tg, ug.data());
+    }
+    report("ode::RungeKutta4 over the drop-ins, 10 steps", rel(ug, ur), 1e-11);
+    b200::WaveSystem sys(mesh, basis, bc.data());
+    sys.rk4_steps(dt, tf, uf.data(), 10);
+    report("fused GPU RK4, 10 steps", rel(uf, ur), 1e-11);
+    report("time after 10 steps", std::abs(tf - tr), 1e-15);
+
+    // WaveHoltz with reflecting walls (the reference class itself)
+    Mesh2D small = perturbed_mesh(5, 3);
+    std::vector<int> bc2(small.n_edges(FaceType::BOUNDARY), 1);
+    const int nd2 = 3 * 25 * small.n_elem();
+    LinearFunctional2D L(small, basis);
+    std::vector<double> F(nd2);
+    L.action(3, [](const double *x, double *o) { o[0] = 4.0 * std::exp(-((x[0] - 0.1) * (x[0] - 0.1) + (x[1] - 0.2) * (x[1] - 0.2)) / 0.08); o[1] = o[2] = 0.0; }, F.data());
+    WaveHoltz wh(2.0, small, basis, bc2.data(), true);
+    b200::WaveHoltz gwh(2.0, small, basis, bc2.data(), true);
+    std::vector<double> p1(nd2), p2(nd2);
+    wh.pi0(p1.data(), F.data());
+    gwh.pi0(p2.data(), F.data());
+    report("WaveHoltz::pi0", rel(p2, p1), 1e-12);
+    std::vector<double> s1 = p1, s2 = p1;
+    wh.S(s1.data());
+    gwh.S(s2.data());
+    report("WaveHoltz::S", rel(s2, s1), 1e-12);
+    std::vector<double> H1(2 * nd2 / 3), H2(2 * nd2 / 3);
+    wh.postprocess(H1.data(), s1.data());
+    gwh.postprocess(H2.data(), s1.data());
+    report("WaveHoltz::postprocess", rel(H2, H1), 1e-12);
+
+    std::printf("%s\n", failures ? "DROP-IN FAILED" : "drop-in ok");
+    return failures ? 1 : 0;
+}
