@@ -165,6 +165,20 @@ int wdg_linear_functional(wdg_wave *wave, int n_var, const double *fq, double *F
 int wdg_load_gaussians(wdg_wave *wave, int n_src, const double *cx, const double *cy, const double *sigma,
                        const double *amp, double scale, int comp, int mass_inv, double *F);
 
+/* wdg_load_gaussians for callers that cannot allocate device memory (no counterpart in the
+ * reference) -- code that issues its work while a CUDA graph is being captured, where cudaMalloc
+ * is not allowed; loops whose memory is fixed before they start; hosts whose own allocator owns
+ * the GPU's memory.  The same load vector, but the source table is staged in a fixed 32 KiB array that
+ * belongs to the library image (held on every GPU that loads the library until the process exits)
+ * instead of a buffer allocated on first use.  Nothing is allocated: at most 1024 sources per call
+ * (more return WDG_ERR_ARG), and F must be device memory.  The first call on a device looks up the
+ * array's device address; make it before any stream capture.  All calls share the one table, so
+ * calls that overlap on the GPU (different streams or threads) race.  Asynchronous on the handle's
+ * stream; cx..amp may be host or device arrays. */
+int wdg_load_gaussians_noalloc(wdg_wave *wave, int n_src, const double *cx, const double *cy,
+                               const double *sigma, const double *amp, double scale, int comp, int mass_inv,
+                               double *F);
+
 /* ---- norms (source/linalg.cpp:102-131), FP64 on the GPU ---- */
 int wdg_norm(wdg_wave *wave, const double *x, double *result);
 int wdg_error(wdg_wave *wave, const double *x, const double *y, double *result);

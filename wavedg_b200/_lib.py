@@ -85,6 +85,7 @@ SIGNATURES = {
     "wdg_quad_points": ([_v, _v], _i),
     "wdg_linear_functional": ([_v, _i, _v, _v], _i),
     "wdg_load_gaussians": ([_v, _i, _v, _v, _v, _v, _d, _i, _i, _v], _i),
+    "wdg_load_gaussians_noalloc": ([_v, _i, _v, _v, _v, _v, _d, _i, _i, _v], _i),
     "wdg_norm": ([_v, _v, _dp], _i),
     "wdg_error": ([_v, _v, _v, _dp], _i),
     "wdg_waveholtz_create": ([_v, _d, _vp], _i),
