@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip the FP32 companion measurement")
     ap.add_argument("--tile", type=int, default=0, help="elements per block (0: autotune)")
     ap.add_argument("--stages", type=int, default=0, help="pipeline depth with --tile (0: default)")
-    ap.add_argument("--kernel", choices=["auto", "warp", "tiled"], default="auto",
+    ap.add_argument("--kernel", choices=["auto", "warp", "tiled", "ws"], default="auto",
                     help="fused-kernel family (auto: the autotuner picks)")
     return ap.parse_args()
 
@@ -174,8 +174,8 @@ def run_ours(args, rank, world, local_rank):
         sys_.upload(u0)
         if args.kernel == "warp":
             sys_.set_kernel(0)
-        elif args.kernel == "tiled" or tile:
-            sys_.set_kernel(1)
+        elif args.kernel in ("tiled", "ws") or tile:
+            sys_.set_kernel(2 if args.kernel == "ws" else 1)
             if args.stages:
                 sys_.set_stages(args.stages)
             if tile:

@@ -177,7 +177,7 @@ def test_many_tiles_per_cta(gpu_lib, precision):
     sys.set_kernel(-1)
     ms = sys.autotune(2)
     cfg = sys.launch_config()
-    assert ms > 0 and cfg["stages"] in (2, 3, 4)
+    assert ms > 0 and cfg["stages"] in (2, 3, 4, 5, 6)
     un = u.copy()
     sys.rk4_steps(un, 1e-3, 0.0, 2)
     assert rel(un, ref_rk) < tol

@@ -1000,6 +1000,27 @@ namespace wdg
         }
     }
 
+} // namespace wdg
+
+#include "stage_ws.cuh"
+
+namespace wdg
+{
+    int ws_chunk_unit(int n) { return kWsConsumers * ws_epw(n); }
+    size_t ws_smem_bytes(int n, bool fp32, int chunk, int ring)
+    {
+        return fp32 ? (size_t)ws_layout<float>(n, chunk, ring).total : (size_t)ws_layout<double>(n, chunk, ring).total;
+    }
+    int ws_default_chunk(int n, bool fp32)
+    {
+        const size_t budget = (227 * 1024) / 3 - 1024;
+        const int unit = ws_chunk_unit(n);
+        for (int r = 4; r >= 1; --r)
+            if (ws_smem_bytes(n, fp32, r * unit, kWsDefaultRing) <= budget)
+                return r * unit;
+        return unit;
+    }
+
     template <int N, typename Real, bool RK>
     static cudaError_t launch_warp_n(const StageArgs<Real> &a, cudaStream_t s)
     {
@@ -1062,6 +1083,8 @@ namespace wdg
     {
 #define WDG_CASE(NV)                                                                       \
     case NV:                                                                               \
+        if (a.family == 2 && rk && a.use_tma && a.tma_out)                                 \
+            return launch_ws_n<NV, Real>(a, grid_limit, s);                                \
         if (a.family == 0)                                                                 \
             return rk ? launch_warp_n<NV, Real, true>(a, s) : launch_warp_n<NV, Real, false>(a, s); \
         return rk ? launch_stage_n<NV, Real, true>(a, grid_limit, s)                       \

@@ -40,7 +40,10 @@ namespace wdg
         int use_tma;          // 1: full tiles are loaded with cp.async.bulk
         int tma_out;          // 1: full tiles of u' and du' are stored with cp.async.bulk (RK mode)
         int stages;           // pipeline depth (2..4): tiles whose bulk loads are in flight + 1
-        int family;           // 0: warp-per-element kernel, 1: tiled TMA-pipeline kernel
+        int family;           // 0: warp-per-element kernel, 1: tiled TMA-pipeline kernel,
+                              // 2: warp-specialised kernel (RK launches on aligned arrays; else tiled)
+        int chunk;            // family 2: elements per chunk (a multiple of 8 x elements per warp-round)
+        int ring;             // family 2: chunk slots in the shared-memory ring (2..6)
         Real rk_a, rk_b, dt, fscale;
         double acc_c;
         unsigned *err;        // device error word (bit 0: wait timeout, bit 1: bad neighbour index)
@@ -62,10 +65,16 @@ namespace wdg
     int upload_basis_tables(int device);   // once per device
     bool degree_supported(int n);
     int default_tile(int n, bool fp32, int stages);
-    // warp-per-element kernel while an element's nodes fit one warp, tiled kernel beyond
-    inline int default_family(int n) { return (n * n <= 32) ? 0 : 1; }
+    // the warp-specialised kernel for RK launches (operator launches take the tiled one)
+    inline int default_family(int) { return 2; }
     constexpr int kDefaultStages = 3;
     int max_tile(int n);
+
+    // warp-specialised family: chunk = 8 consumer warps x elements per warp-round x rounds
+    int ws_chunk_unit(int n);                 // the smallest valid chunk
+    size_t ws_smem_bytes(int n, bool fp32, int chunk, int ring);
+    constexpr int kWsDefaultRing = 3;
+    int ws_default_chunk(int n, bool fp32);   // most rounds (<= 4) whose default ring fits 3 CTAs per SM
 
     // fused stage: RK = true for the time-stepping epilogue
     template <typename Real>

@@ -117,6 +117,8 @@ namespace wdg
         a.tile = w->tile;
         a.stages = w->stages;
         a.family = w->family;
+        a.chunk = w->ws_chunk;
+        a.ring = w->ws_ring;
         a.err = w->d_err;
         return a;
     }
@@ -405,6 +407,7 @@ extern "C"
         w->min_h = mesh->min_h;
         w->tile = default_tile(n_colloc, precision == WDG_FP32, w->stages);
         w->family = default_family(n_colloc);
+        w->ws_chunk = ws_default_chunk(n_colloc, precision == WDG_FP32);
 
         int s = WDG_OK;
         auto chk = [&](int r)
@@ -536,10 +539,31 @@ extern "C"
         return sync(w);
     }
 
+    static int ws_set(wdg_wave *w, int chunk, int ring)
+    {
+        const bool fp32 = w->precision == WDG_FP32;
+        if (chunk == 0)
+            chunk = ws_default_chunk(w->n, fp32);
+        if (ring == 0)
+            ring = kWsDefaultRing;
+        const int unit = ws_chunk_unit(w->n);
+        if (chunk < unit || chunk % unit || chunk > 64 * unit)
+            return fail(WDG_ERR_ARG, "warp-specialised kernel: the chunk must be a multiple of 8 x elements per warp");
+        if (ring < 2 || ring > 6)
+            return fail(WDG_ERR_ARG, "warp-specialised kernel: the ring holds 2 to 6 chunks");
+        if (ws_smem_bytes(w->n, fp32, chunk, ring) > kMaxSmem)
+            return fail(WDG_ERR_ARG, "warp-specialised kernel: chunk x ring too large for shared memory");
+        w->ws_chunk = chunk;
+        w->ws_ring = ring;
+        return WDG_OK;
+    }
+
     int wdg_wave_set_tile(wdg_wave *w, int tile)
     {
         if (!w)
             return fail(WDG_ERR_ARG, "null discretisation");
+        if (w->family == 2)
+            return ws_set(w, tile, w->ws_ring);
         if (tile == 0)
             tile = default_tile(w->n, w->precision == WDG_FP32, w->stages);
         if (tile < 4 || (tile & 3) || tile > max_tile(w->n))
@@ -551,6 +575,16 @@ extern "C"
     }
     int wdg_wave_set_stages(wdg_wave *w, int stages)
     {
+        if (w && w->family == 2)
+        {
+            if (stages < 0 || stages == 1 || stages > 6)
+                return fail(WDG_ERR_ARG, "wdg_wave_set_stages: the ring holds 2 to 6 chunks (0 = default)");
+            int chunk = w->ws_chunk;
+            const int unit = ws_chunk_unit(w->n), ring = stages ? stages : kWsDefaultRing;
+            while (chunk > unit && ws_smem_bytes(w->n, w->precision == WDG_FP32, chunk, ring) > kMaxSmem)
+                chunk -= unit;
+            return ws_set(w, chunk, ring);
+        }
         if (!w || stages < 0 || stages == 1 || stages > 4)
             return fail(WDG_ERR_ARG, "wdg_wave_set_stages: stages must be 2, 3 or 4 (0 = default)");
         if (stages == 0)
@@ -567,8 +601,9 @@ extern "C"
 
     int wdg_wave_set_kernel(wdg_wave *w, int family)
     {
-        if (!w || family < -1 || family > 1)
-            return fail(WDG_ERR_ARG, "wdg_wave_set_kernel: 0 (warp per element), 1 (tiled) or -1 (default)");
+        if (!w || family < -1 || family > 2)
+            return fail(WDG_ERR_ARG,
+                        "wdg_wave_set_kernel: 0 (warp per element), 1 (tiled), 2 (warp-specialised) or -1 (default)");
         w->family = (family < 0) ? default_family(w->n) : family;
         return WDG_OK;
     }
@@ -578,8 +613,8 @@ extern "C"
         if (!w)
             return fail(WDG_ERR_ARG, "null discretisation");
         if (family) *family = w->family;
-        if (tile) *tile = w->tile;
-        if (stages) *stages = w->stages;
+        if (tile) *tile = (w->family == 2) ? w->ws_chunk : w->tile;
+        if (stages) *stages = (w->family == 2) ? w->ws_ring : w->stages;
         if (max_ctas) *max_ctas = w->max_ctas;
         return WDG_OK;
     }
@@ -596,18 +631,34 @@ extern "C"
         WDG_CUDA(cudaEventCreate(&e0));
         WDG_CUDA(cudaEventCreate(&e1));
         const int save_tile = w->tile, save_stages = w->stages, save_family = w->family;
+        const int save_chunk = w->ws_chunk, save_ring = w->ws_ring;
         float best = 1e30f;
-        int bt = save_tile, bs = save_stages, bf = save_family, s = WDG_OK;
+        int bt = save_tile, bs = save_stages, bf = save_family, bc = save_chunk, br = save_ring, s = WDG_OK;
         RKExtras none;
-        // candidate 0: the warp-per-element kernel; then every fitting tiled configuration
-        for (int st = 1; st <= 4 && s == WDG_OK; ++st)
-            for (int tile = (st == 1 ? 0 : 4); tile <= (st == 1 ? 0 : max_tile(w->n)) && s == WDG_OK; tile += 4)
+        // candidates: the warp-per-element kernel; every fitting tiled (tile, depth); every
+        // warp-specialised (chunk of 1..4 rounds, ring of 2..6) that fits shared memory
+        struct Cand
+        {
+            int family, a, b;
+        };
+        std::vector<Cand> cands;
+        cands.push_back({0, save_tile, save_stages});
+        for (int st = 2; st <= 4; ++st)
+            for (int tile = 4; tile <= max_tile(w->n); tile += 4)
+                if (smem_for(w, tile, st) <= kMaxSmem)
+                    cands.push_back({1, tile, st});
+        for (int r = 1; r <= 4; ++r)
+            for (int ring = 2; ring <= 6; ++ring)
+                if (ws_smem_bytes(w->n, w->precision == WDG_FP32, r * ws_chunk_unit(w->n), ring) <= kMaxSmem)
+                    cands.push_back({2, r * ws_chunk_unit(w->n), ring});
+        for (size_t ci = 0; ci < cands.size() && s == WDG_OK; ++ci)
             {
-                if (st > 1 && smem_for(w, tile, st) > kMaxSmem)
-                    continue;
-                w->family = (st == 1) ? 0 : 1;
-                w->tile = (st == 1) ? save_tile : tile;
-                w->stages = (st == 1) ? save_stages : st;
+                const Cand &cd = cands[ci];
+                w->family = cd.family;
+                w->tile = (cd.family == 1) ? cd.a : save_tile;
+                w->stages = (cd.family == 1) ? cd.b : save_stages;
+                w->ws_chunk = (cd.family == 2) ? cd.a : save_chunk;
+                w->ws_ring = (cd.family == 2) ? cd.b : save_ring;
                 double t = 0.0;
                 auto run = [&](int n) -> int
                 {
@@ -637,6 +688,8 @@ extern "C"
                     bt = w->tile;
                     bs = w->stages;
                     bf = w->family;
+                    bc = w->ws_chunk;
+                    br = w->ws_ring;
                 }
             }
         cudaEventDestroy(e0);
@@ -644,6 +697,8 @@ extern "C"
         w->tile = (s == WDG_OK) ? bt : save_tile;
         w->stages = (s == WDG_OK) ? bs : save_stages;
         w->family = (s == WDG_OK) ? bf : save_family;
+        w->ws_chunk = (s == WDG_OK) ? bc : save_chunk;
+        w->ws_ring = (s == WDG_OK) ? br : save_ring;
         if (s == WDG_OK)
             s = sync(w);
         if (best_ms_per_step)
@@ -663,7 +718,7 @@ extern "C"
     {
         if (!w || !tile)
             return fail(WDG_ERR_ARG, "null argument");
-        *tile = w->tile;
+        *tile = (w->family == 2) ? w->ws_chunk : w->tile;
         return WDG_OK;
     }
 

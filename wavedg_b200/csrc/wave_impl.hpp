@@ -13,7 +13,8 @@ struct wdg_wave
     int device = 0;
     cudaStream_t stream = 0;
     int n = 0, nel = 0, precision = WDG_FP64, tile = 0, max_ctas = 0, stages = wdg::kDefaultStages;
-    int family = 0; // fused-kernel family: 0 warp-per-element, 1 tiled TMA pipeline
+    int family = 0; // fused-kernel family: 0 warp-per-element, 1 tiled TMA pipeline, 2 warp-specialised
+    int ws_chunk = 0, ws_ring = wdg::kWsDefaultRing; // family 2 launch shape
     long long ndof = 0;
     int nI = 0, nB = 0;
     double min_h = 0.0;

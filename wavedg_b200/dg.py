@@ -231,17 +231,19 @@ class Discretisation:
         check(lib().wdg_wave_set_tile(self._h, int(v)), "set_tile")
 
     def set_stages(self, stages: int) -> None:
-        """Depth of the bulk-copy pipeline (2, 3 or 4; 0 = default)."""
+        """Depth of the bulk-copy pipeline: 2-4 for the tiled kernel, 2-6 chunk slots for
+        the warp-specialised one; 0 = default."""
         check(lib().wdg_wave_set_stages(self._h, int(stages)), "set_stages")
 
     def set_kernel(self, family: int) -> None:
-        """0: warp per element, 1: tiled TMA pipeline, -1: default for this degree."""
+        """0: warp per element, 1: tiled TMA pipeline, 2: warp-specialised TMA ring,
+        -1: default for this degree."""
         check(lib().wdg_wave_set_kernel(self._h, int(family)), "set_kernel")
 
     def launch_config(self) -> dict:
         f, t, st, mc = C.c_int(), C.c_int(), C.c_int(), C.c_int()
         check(lib().wdg_wave_get_launch(self._h, C.byref(f), C.byref(t), C.byref(st), C.byref(mc)))
-        return {"kernel": ("warp", "tiled")[f.value], "tile": t.value, "stages": st.value, "max_ctas": mc.value}
+        return {"kernel": ("warp", "tiled", "ws")[f.value], "tile": t.value, "stages": st.value, "max_ctas": mc.value}
 
     def autotune(self, steps: int = 5) -> float:
         """Pick elements-per-block and pipeline depth by timing; returns the best ms per RK4 step."""
