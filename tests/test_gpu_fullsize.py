@@ -54,7 +54,7 @@ def test_rk4_step_vs_oracle_full_size(gpu_lib, big):
     ref, _ = op.rk4(u, dt, 1)
     assert rel(un, ref) < 1e-12
     # both kernel families and several tile sizes agree at full size
-    for family, tile in ((0, 0), (1, 8), (1, 12), (1, 16), (2, 8), (2, 16), (2, 24)):
+    for family, tile in ((0, 0), (1, 8), (1, 12), (1, 16), (2, 0)):
         sys.set_kernel(family)
         if tile:
             sys.tile = tile

@@ -64,7 +64,7 @@ namespace wdg
     // `stages`-deep pipeline share an SM
     int default_tile(int n, bool fp32, int stages)
     {
-        const size_t budget = (227 * 1024) / 2 - 1024;
+        const size_t budget = (227 * 1024) / 3 - 1024;
         for (int e = max_tile(n); e >= 4; e -= 4)
         {
             const size_t b = fp32 ? stage_smem_bytes<float>(n, e, F_RK, stages)

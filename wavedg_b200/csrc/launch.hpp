@@ -73,7 +73,7 @@ namespace wdg
     // warp-specialised family: chunk = 8 consumer warps x elements per warp-round x rounds
     int ws_chunk_unit(int n);                 // the smallest valid chunk
     size_t ws_smem_bytes(int n, bool fp32, int chunk, int ring);
-    constexpr int kWsDefaultRing = 3;
+    constexpr int kWsDefaultRing = 2;
     int ws_default_chunk(int n, bool fp32);   // most rounds (<= 4) whose default ring fits 3 CTAs per SM
 
     // fused stage: RK = true for the time-stepping epilogue

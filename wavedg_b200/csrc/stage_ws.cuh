@@ -6,23 +6,31 @@
 //
 //   producer   ring of S chunk slots in shared memory.  For each chunk it
 //              waits until the slot is free, loads u, du and the element
-//              geometry with cp.async.bulk on the slot's `full` mbarrier, and
-//              once every consumer warp has arrived on the slot's `done`
-//              mbarrier it stores u' and du' back with cp.async.bulk straight
-//              from the slot (the results are written in place).
-//   consumers  a warp owns whole elements (EPW of them when an element's n^2
-//              nodes fit a warp, else one element with several nodes per
-//              lane) and never waits for another warp: contravariant fluxes go
-//              to a per-warp scratch, a __syncwarp, then each node lane
-//              contracts along both directions; face lanes (one per face node)
-//              form the upwind flux into a per-warp face buffer; node lanes
-//              add it, apply M^{-1} and the RK update, and write u', du' into
-//              the slot.
+//              geometry with cp.async.bulk, and gathers every face node's
+//              neighbour trace from the stage's input array with cp.async
+//              (8- or 4-byte pieces; the mesh is unstructured), all on the
+//              slot's `full` mbarrier.  Once every consumer warp has arrived
+//              on the slot's `done` mbarrier it stores u' and du' back with
+//              cp.async.bulk straight from the slot (results are in place).
+//   consumers  a warp owns EW = floor(32 / n) whole elements per round, one
+//              lane per grid line of each, all three fields per lane:
+//                row pass     lane m holds row j = m: forms the xi-fluxes F of
+//                             the row in registers and contracts them with
+//                             D (compile-time constants) into 3 n sums; adds
+//                             the upwind flux of the row's two face nodes
+//                             (sides 3 and 1); writes the sums and the row's
+//                             inverse mass to a per-warp scratch.
+//                column pass  lane m holds column i = m: eta-fluxes G, the
+//                             eta contraction, the face nodes of sides 0 and
+//                             2, plus the row pass's sums, M^{-1} and the RK
+//                             update of the column's nodes, in place.
+//              Warps sync only with __syncwarp; a chunk is released when all
+//              consumer warps have arrived on its `done` barrier.
 //
-// Neighbour traces are read from the stage's input array in global memory
-// (L2) by the face lanes, issued before the volume work so their latency
-// overlaps it; the slot copy of u cannot serve them because other warps
-// overwrite their elements in place.
+// The neighbour traces are gathered from global memory even when the
+// neighbour sits in the same chunk: consumer warps overwrite their elements
+// in place, so the slot's copy of u cannot serve another warp.  The gather
+// runs on the producer's lanes ahead of time, so no consumer waits on L2.
 //
 // Used for RK launches whose arrays are 16-byte aligned; every other launch
 // takes the tiled kernel.
@@ -33,34 +41,35 @@ namespace wdg
     struct WsShape
     {
         static constexpr int NN = N * N, ND = 3 * NN, NF = 4 * N;
-        static constexpr int EPW = (NN <= 32) ? 32 / NN : 1;    // elements per warp-round
-        static constexpr int NODES = EPW * NN, NPL = (NODES + 31) / 32; // node slots per lane
-        static constexpr int FACES = EPW * NF, FPL = (FACES + 31) / 32; // face slots per lane
+        static constexpr int EW = 32 / N; // elements per warp-round, one lane per line
     };
-    constexpr int kWsConsumers = 8;
+    constexpr int kWsConsumers = 4;
     constexpr int kWsThreads = 32 * (kWsConsumers + 1);
 
-    int ws_epw(int n) { return (n * n <= 32) ? 32 / (n * n) : 1; }
+    int ws_epw(int n) { return 32 / n; }
 
     // shared-memory layout (bytes), identical on host and device:
-    //   [2 S mbarriers | pad to 128][D (n^2), w (n), x (n) | pad to 128][S slots][consumer scratch]
-    //   slot    = u (C, 3 n^2) | du (C, 3 n^2) | corners (C, 8 doubles) | fbase (C, int4) | fcode (C, u32)
-    //   scratch = per warp, per element of a round: fluxes [n^2][6], face fluxes [4 n][3]
+    //   [2 S mbarriers | pad to 128][x (n), w (n) | pad to 128][S slots][consumer scratch]
+    //   slot    = u (C, 3 n^2) | du (C, 3 n^2) | halo (C, 4 n, 3) | corners (C, 8 doubles) | fcode (C, u32)
+    //   scratch = per warp, per element of a round: row-pass sums [n^2][3], inverse mass [n^2]
     struct WsLayout
     {
-        int ub, slot, tab, slots, scratch, warp_scratch, total;
+        int ub, hb, cb, kb, slot, tab, slots, scratch, warp_scratch, total;
     };
     template <typename Real>
     __host__ __device__ inline WsLayout ws_layout(int n, int chunk, int stages)
     {
         WsLayout L;
-        const int nn = n * n, epw = (nn <= 32) ? 32 / nn : 1;
+        const int nn = n * n, ew = 32 / n;
         L.ub = chunk * 3 * nn * (int)sizeof(Real);
-        L.slot = 2 * L.ub + chunk * 84;
+        L.hb = 2 * L.ub;                                   // halo
+        L.cb = L.hb + chunk * 12 * n * (int)sizeof(Real);  // corners
+        L.kb = L.cb + chunk * 64;                          // side codes
+        L.slot = L.kb + chunk * 4;
         L.tab = 128;
-        L.slots = (L.tab + (nn + 2 * n) * (int)sizeof(Real) + 127) & ~127;
+        L.slots = (L.tab + 2 * n * (int)sizeof(Real) + 127) & ~127;
         L.scratch = L.slots + stages * L.slot;
-        L.warp_scratch = ((epw * (6 * nn + 12 * n) * (int)sizeof(Real)) + 15) & ~15;
+        L.warp_scratch = ((ew * 4 * nn * (int)sizeof(Real)) + 15) & ~15;
         L.total = L.scratch + kWsConsumers * L.warp_scratch;
         return L;
     }
@@ -69,27 +78,57 @@ namespace wdg
     {
         asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
     }
+    // arrive on `bar` once this thread's earlier cp.async copies have landed; counts as
+    // one of the barrier's expected arrivals
+    __device__ __forceinline__ void cp_async_mbar_arrive(uint64_t *bar)
+    {
+        asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+    }
 
-    template <typename Real>
-    struct Vec2;
-    template <>
-    struct Vec2<double>
+    // Upwind flux of face node k of side SIDE of one element (own trace `own`),
+    // subtracted into r: the closed form of EdgeFlux (source/EdgeFlux.cpp:7-139)
+    // with the side's outward normal and measure (StraightEdge, wavedg/Edge.hpp:107-122)
+    // and the exterior state of WaveBC for boundary sides.
+    template <int N, typename Real, int SIDE>
+    __device__ __forceinline__ void ws_face(uint32_t codes, int flags, const double2 c01, const double2 c23,
+                                            const double2 c45, const double2 c67, Real wk, int k,
+                                            const Real *own, const Real *halo_e, Real &r0, Real &r1, Real &r2)
     {
-        using T = double2;
-    };
-    template <>
-    struct Vec2<float>
-    {
-        using T = float2;
-    };
+        const uint32_t byte = (codes >> (8 * SIDE)) & 0xffu;
+        const bool bnd = (byte & 0x80u) != 0;
+        if (bnd ? !(flags & F_BND) : !(flags & F_INT))
+            return;
+        // side SIDE runs from corner p0 to p1: 0: 0->1, 1: 1->2, 2: 3->2, 3: 0->3
+        const double2 a0 = (SIDE == 0 || SIDE == 3) ? c01 : (SIDE == 1) ? c23 : c67;
+        const double2 a1 = (SIDE == 0) ? c23 : (SIDE == 3) ? c67 : c45;
+        const double dx = a1.x - a0.x, dy = a1.y - a0.y;
+        const double s2 = dx * dx + dy * dy, rs = rsqrt(s2);
+        const double sgn = (SIDE >= 2) ? -1.0 : 1.0;
+        const Real nx = (Real)(sgn * dy * rs), ny = (Real)(-sgn * dx * rs);
+        const Real h = wk * (Real)(0.25 * s2 * rs);
+        const Real q[3] = {own[0], own[1], own[2]};
+        Real x[3];
+        if (bnd)
+            exterior<Real>((int)((byte >> 3) & 3u), nx, ny, q, x);
+        else
+        {
+            const Real *hp = halo_e + 3 * (SIDE * N + k);
+            x[0] = hp[0];
+            x[1] = hp[1];
+            x[2] = hp[2];
+        }
+        Real r[3] = {r0, r1, r2};
+        upwind<Real>(nx, ny, h, q, x, r);
+        r0 = r[0];
+        r1 = r[1];
+        r2 = r[2];
+    }
 
     template <int N, typename Real, bool EXTRA>
-    __global__ void __launch_bounds__(kWsThreads, 3) ws_stage_kernel(const StageArgs<Real> a)
+    __global__ void __launch_bounds__(kWsThreads, 2) ws_stage_kernel(const StageArgs<Real> a)
     {
         using Sh = WsShape<N>;
-        using R2 = typename Vec2<Real>::T;
-        constexpr int NN = Sh::NN, ND = Sh::ND, NF = Sh::NF, EPW = Sh::EPW;
-        constexpr int NPL = Sh::NPL, FPL = Sh::FPL;
+        constexpr int NN = Sh::NN, ND = Sh::ND, NF = Sh::NF, EW = Sh::EW;
         const int C = a.chunk, S = a.ring, G = gridDim.x;
         const int flags = a.flags;
         const bool has_du = (flags & F_READ_DU) != 0;
@@ -99,8 +138,8 @@ namespace wdg
         extern __shared__ __align__(128) unsigned char smem[];
         uint64_t *full = reinterpret_cast<uint64_t *>(smem);
         uint64_t *done = full + S;
-        Real *Dt = reinterpret_cast<Real *>(smem + L.tab); // D[l + N i] = phi_i'(x_l)
-        Real *wt = Dt + NN, *xt = wt + N;
+        Real *xt = reinterpret_cast<Real *>(smem + L.tab); // GLL nodes, then weights
+        Real *wt = xt + N;
         unsigned char *slots = smem + L.slots;
 
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -108,13 +147,13 @@ namespace wdg
         {
             for (int q = 0; q < S; ++q)
             {
-                mbar_init(&full[q], 1);
+                mbar_init(&full[q], 1 + 32); // the bulk-copy arrive + one cp.async arrive per producer lane
                 mbar_init(&done[q], kWsConsumers);
             }
             fence_mbar_init();
         }
-        for (int q = threadIdx.x; q < NN + 2 * N; q += blockDim.x)
-            Dt[q] = (q < NN) ? Tab<Real>::D(N, q) : (q < NN + N) ? Tab<Real>::w(N, q - NN) : Tab<Real>::x(N, q - NN - N);
+        for (int q = threadIdx.x; q < 2 * N; q += blockDim.x)
+            xt[q] = (q < N) ? Tab<Real>::x(N, q) : Tab<Real>::w(N, q - N);
         __syncthreads();
 
         // this CTA's chunks: k_m = blockIdx.x + m G
@@ -132,14 +171,12 @@ namespace wdg
                 {
                     if (lane == 0)
                     {
-                        mbar_expect_tx(&full[q], (uint32_t)(L.ub * (has_du ? 2 : 1) + C * 84));
+                        mbar_expect_tx(&full[q], (uint32_t)(L.ub * (has_du ? 2 : 1) + C * 68));
                         bulk_g2s(base, a.u + (size_t)el0 * ND, (uint32_t)L.ub, &full[q]);
                         if (has_du)
                             bulk_g2s(base + L.ub, a.du + (size_t)el0 * ND, (uint32_t)L.ub, &full[q]);
-                        unsigned char *g = base + 2 * L.ub;
-                        bulk_g2s(g, a.corners + 8 * (size_t)el0, (uint32_t)(64 * C), &full[q]);
-                        bulk_g2s(g + 64 * C, a.fbase + el0, (uint32_t)(16 * C), &full[q]);
-                        bulk_g2s(g + 80 * C, a.fcode + el0, (uint32_t)(4 * C), &full[q]);
+                        bulk_g2s(base + L.cb, a.corners + 8 * (size_t)el0, (uint32_t)(64 * C), &full[q]);
+                        bulk_g2s(base + L.kb, a.fcode + el0, (uint32_t)(4 * C), &full[q]);
                     }
                 }
                 else
@@ -152,21 +189,67 @@ namespace wdg
                         if (has_du)
                             dus[i] = a.du[(size_t)el0 * ND + i];
                     }
-                    double *cw = reinterpret_cast<double *>(base + 2 * L.ub);
+                    double *cw = reinterpret_cast<double *>(base + L.cb);
                     for (int i = lane; i < ne * 8; i += 32)
                         cw[i] = a.corners[8 * (size_t)el0 + i];
-                    int4 *bw = reinterpret_cast<int4 *>(base + 2 * L.ub + 64 * C);
-                    uint32_t *kw = reinterpret_cast<uint32_t *>(base + 2 * L.ub + 80 * C);
+                    uint32_t *kw = reinterpret_cast<uint32_t *>(base + L.kb);
                     for (int i = lane; i < ne; i += 32)
-                    {
-                        bw[i] = a.fbase[el0 + i];
                         kw[i] = a.fcode[el0 + i];
-                    }
                     __threadfence_block();
                     __syncwarp();
                     if (lane == 0)
                         mbar_arrive(&full[q]);
                 }
+                // neighbour traces of every interior face node of the chunk: one lane per
+                // (element, side); the table reads of a batch go out together, so a chunk
+                // costs one L2 round trip per batch rather than one per face node
+                if (flags & F_INT)
+                {
+                    Real *halo = reinterpret_cast<Real *>(base + L.hb);
+                    const int limit = a.nel * ND;
+                    constexpr int B = 4; // (element, side) pairs per lane per batch
+                    for (int p0 = 0; p0 < ne * 4; p0 += 32 * B)
+                    {
+                        uint32_t code[B];
+                        int off[B];
+#pragma unroll
+                        for (int b = 0; b < B; ++b)
+                        {
+                            const int pr = p0 + 32 * b + lane, le = pr >> 2, s = pr & 3;
+                            code[b] = 0x80u;
+                            off[b] = -1;
+                            if (pr < ne * 4)
+                            {
+                                code[b] = (__ldg(a.fcode + el0 + le) >> (8 * s)) & 0xffu;
+                                off[b] = __ldg(reinterpret_cast<const int *>(a.fbase + el0 + le) + s);
+                            }
+                        }
+#pragma unroll
+                        for (int b = 0; b < B; ++b)
+                        {
+                            const int pr = p0 + 32 * b + lane, le = pr >> 2, s = pr & 3;
+                            if (code[b] & 0x80u)
+                                continue; // boundary side (or past the chunk): no neighbour
+                            const int stride = partner_stride<N>(code[b]);
+                            if (off[b] < 0 || off[b] + (N - 1) * stride < 0 || off[b] + 3 > limit ||
+                                off[b] + (N - 1) * stride + 3 > limit)
+                            {
+                                atomicOr(a.err, 2u);
+                                continue;
+                            }
+                            Real *dst = halo + 3 * (le * NF + s * N);
+#pragma unroll
+                            for (int k = 0; k < N; ++k)
+                            {
+                                const Real *src = a.u + off[b] + k * stride;
+                                cp_async<sizeof(Real)>(dst + 3 * k, src);
+                                cp_async<sizeof(Real)>(dst + 3 * k + 1, src + 1);
+                                cp_async<sizeof(Real)>(dst + 3 * k + 2, src + 2);
+                            }
+                        }
+                    }
+                }
+                cp_async_mbar_arrive(&full[q]);
             };
             for (int m = 0; m < min(S, M); ++m)
                 load(m);
@@ -221,9 +304,12 @@ namespace wdg
 
         // ---------------------------------------------------------------- consumers
         const int cw = warp;
-        const int R = C / (kWsConsumers * EPW); // warp-rounds per chunk
-        Real *X = reinterpret_cast<Real *>(smem + L.scratch + cw * L.warp_scratch); // [EPW][NN][6]
-        Real *Fb = X + EPW * NN * 6;                                                  // [EPW][NF][3]
+        const int R = C / (kWsConsumers * EW); // warp-rounds per chunk
+        Real *Rx = reinterpret_cast<Real *>(smem + L.scratch + cw * L.warp_scratch); // [EW][NN][3] row-pass sums
+        Real *Mi = Rx + EW * NN * 3;                                                  // [EW][NN] inverse mass
+        const int el_l = lane / N, ln = lane - el_l * N; // element of the round, grid line
+        const bool lane_on = lane < EW * N;
+        const Real xm = lane_on ? xt[ln] : Real(0), wm = lane_on ? wt[ln] : Real(0);
 
         for (int m = 0; m < M; ++m)
         {
@@ -237,225 +323,177 @@ namespace wdg
             unsigned char *base = slots + q * L.slot;
             Real *us = reinterpret_cast<Real *>(base);
             Real *dus = us + C * ND;
-            const double *cs = reinterpret_cast<const double *>(base + 2 * L.ub);
-            const int *fbs = reinterpret_cast<const int *>(base + 2 * L.ub + 64 * C);
-            const uint32_t *fks = reinterpret_cast<const uint32_t *>(base + 2 * L.ub + 80 * C);
+            const Real *halo = reinterpret_cast<const Real *>(base + L.hb);
+            const double *cs = reinterpret_cast<const double *>(base + L.cb);
+            const uint32_t *fks = reinterpret_cast<const uint32_t *>(base + L.kb);
 
             for (int r = 0; r < R; ++r)
             {
-                const int eb = (cw * R + r) * EPW; // first chunk-local element of this round
-
-                // ---- node lanes: metrics, contravariant fluxes (source/Div.cpp:5-53), M^{-1}
-                Real minv[NPL];
-                Real fv[NPL][3];
-                double av[NPL][3];
-#pragma unroll
-                for (int p = 0; p < NPL; ++p)
+                const int le = (cw * R + r) * EW + el_l; // chunk-local element of this lane
+                const bool act = lane_on && le < ne;
+                double2 c01, c23, c45, c67;
+                uint32_t codes = 0;
+                const Real *halo_e = halo + le * NF * 3;
+                Real *ue = us + le * ND;
+                if (act)
                 {
-                    const int v = lane + 32 * p;
-                    const int ei = v / NN, node = v - ei * NN, le = eb + ei;
-                    minv[p] = 0;
-                    if (v >= Sh::NODES || le >= ne)
-                        continue;
-                    const int i = node % N, j = node / N;
-                    const Real *qn = us + le * ND + 3 * node;
-                    const Real q0 = qn[0], q1 = qn[1], q2 = qn[2];
                     const double2 *c2 = reinterpret_cast<const double2 *>(cs + 8 * le);
-                    const double2 c01 = c2[0], c23 = c2[1], c45 = c2[2], c67 = c2[3];
-                    const Real xi = xt[i], eta = xt[j];
-                    // QuadElement::jacobian (source/Element.cpp:21-27)
+                    c01 = c2[0];
+                    c23 = c2[1];
+                    c45 = c2[2];
+                    c67 = c2[3];
+                    codes = fks[le];
+
+                    // ---- row pass: row j = ln.  Contravariant fluxes of the wave system
+                    // (source/Div.cpp:5-53): F = W (y_eta u - x_eta v, y_eta p, -x_eta p); along a
+                    // row x_xi, y_xi are constant and x_eta, y_eta vary linearly with xi.
+                    const Real eta = xm, wj = wm;
                     const Real Xxi = Real(0.25) * ((Real(1) - eta) * Real(c23.x - c01.x) + (Real(1) + eta) * Real(c45.x - c67.x));
                     const Real Yxi = Real(0.25) * ((Real(1) - eta) * Real(c23.y - c01.y) + (Real(1) + eta) * Real(c45.y - c67.y));
-                    const Real Xeta = Real(0.25) * ((Real(1) - xi) * Real(c67.x - c01.x) + (Real(1) + xi) * Real(c45.x - c23.x));
-                    const Real Yeta = Real(0.25) * ((Real(1) - xi) * Real(c67.y - c01.y) + (Real(1) + xi) * Real(c45.y - c23.y));
-                    const Real W = wt[i] * wt[j];
-                    const Real WYe = W * Yeta, WXe = W * Xeta, WYx = W * Yxi, WXx = W * Xxi;
-                    Real *x = X + (ei * NN + node) * 6;
-                    // [F_p F_u | F_v G_p | G_u G_v]
-                    reinterpret_cast<R2 *>(x)[0] = R2{WYe * q1 - WXe * q2, WYe * q0};
-                    reinterpret_cast<R2 *>(x)[1] = R2{-WXe * q0, -WYx * q1 + WXx * q2};
-                    reinterpret_cast<R2 *>(x)[2] = R2{-WYx * q0, WXx * q0};
-                    // MassMatrix<true>: w_i w_j det J (source/MassMatrix.cpp:6-28)
-                    minv[p] = Real(1) / (W * (Xxi * Yeta - Yxi * Xeta));
-                    if (EXTRA)
-                    {
-                        const size_t g = (size_t)(el0 + le) * ND + 3 * node;
+                    const Real ex0 = Real(c67.x - c01.x), ex1 = Real(c45.x - c23.x);
+                    const Real ey0 = Real(c67.y - c01.y), ey1 = Real(c45.y - c23.y);
+                    const Real *row = ue + 3 * N * ln;
+                    Real ap[N], au[N], av[N];
 #pragma unroll
-                        for (int c = 0; c < 3; ++c)
+                    for (int i = 0; i < N; ++i)
+                        ap[i] = au[i] = av[i] = 0;
+                    Real *mrow = Mi + el_l * NN + N * ln;
+                    if (flags & F_VOL)
+                    {
+#pragma unroll
+                        for (int l = 0; l < N; ++l)
                         {
-                            fv[p][c] = (flags & F_FORCE) ? a.F[g + c] : Real(0);
-                            av[p][c] = (flags & F_FILTER) ? a.acc[g + c] : 0.0;
+                            const Real xl = Tab<Real>::x(N, l);
+                            const Real Xeta = Real(0.25) * ((Real(1) - xl) * ex0 + (Real(1) + xl) * ex1);
+                            const Real Yeta = Real(0.25) * ((Real(1) - xl) * ey0 + (Real(1) + xl) * ey1);
+                            const Real W = Tab<Real>::w(N, l) * wj;
+                            const Real p = row[3 * l], u = row[3 * l + 1], v = row[3 * l + 2];
+                            const Real WYe = W * Yeta, WXe = W * Xeta;
+                            const Real Fp = WYe * u - WXe * v, Fu = WYe * p, Fv = -WXe * p;
+                            // MassMatrix<true>: w_i w_j det J (source/MassMatrix.cpp:6-28)
+                            mrow[l] = Real(1) / (W * (Xxi * Yeta - Yxi * Xeta));
+                            // du(i, j) += sum_l D(l, i) F(l, j)  (div_2d_c, source/Div.cpp:131-179)
+#pragma unroll
+                            for (int i = 0; i < N; ++i)
+                            {
+                                const Real d = Tab<Real>::D(N, l + N * i);
+                                ap[i] += d * Fp;
+                                au[i] += d * Fu;
+                                av[i] += d * Fv;
+                            }
+                        }
+                    }
+                    else
+                    {
+#pragma unroll
+                        for (int l = 0; l < N; ++l)
+                        {
+                            const Real xl = Tab<Real>::x(N, l);
+                            const Real Xeta = Real(0.25) * ((Real(1) - xl) * ex0 + (Real(1) + xl) * ex1);
+                            const Real Yeta = Real(0.25) * ((Real(1) - xl) * ey0 + (Real(1) + xl) * ey1);
+                            mrow[l] = Real(1) / (Tab<Real>::w(N, l) * wj * (Xxi * Yeta - Yxi * Xeta));
+                        }
+                    }
+                    // face nodes of the row: (0, j) on side 3, (n-1, j) on side 1, face-node index j
+                    ws_face<N, Real, 3>(codes, flags, c01, c23, c45, c67, wj, ln, row, halo_e, ap[0], au[0], av[0]);
+                    ws_face<N, Real, 1>(codes, flags, c01, c23, c45, c67, wj, ln, row + 3 * (N - 1), halo_e,
+                                        ap[N - 1], au[N - 1], av[N - 1]);
+                    Real *rx = Rx + (el_l * NN + N * ln) * 3;
+#pragma unroll
+                    for (int i = 0; i < N; ++i)
+                    {
+                        rx[3 * i] = ap[i];
+                        rx[3 * i + 1] = au[i];
+                        rx[3 * i + 2] = av[i];
+                    }
+                }
+                __syncwarp();
+                if (act)
+                {
+                    // ---- column pass: column i = ln.  G = W (-y_xi u + x_xi v, -y_xi p, x_xi p);
+                    // along a column x_eta, y_eta are constant and x_xi, y_xi vary with eta.
+                    const int i = ln;
+                    const Real wi = wm;
+                    const Real dx0 = Real(c23.x - c01.x), dx1 = Real(c45.x - c67.x);
+                    const Real dy0 = Real(c23.y - c01.y), dy1 = Real(c45.y - c67.y);
+                    Real sp[N], su[N], sv[N];
+#pragma unroll
+                    for (int j = 0; j < N; ++j)
+                        sp[j] = su[j] = sv[j] = 0;
+                    if (flags & F_VOL)
+                    {
+#pragma unroll
+                        for (int l = 0; l < N; ++l)
+                        {
+                            const Real el = Tab<Real>::x(N, l);
+                            const Real Xxi = Real(0.25) * ((Real(1) - el) * dx0 + (Real(1) + el) * dx1);
+                            const Real Yxi = Real(0.25) * ((Real(1) - el) * dy0 + (Real(1) + el) * dy1);
+                            const Real W = wi * Tab<Real>::w(N, l);
+                            const Real *nd = ue + 3 * (i + N * l);
+                            const Real p = nd[0], u = nd[1], v = nd[2];
+                            const Real WYx = W * Yxi, WXx = W * Xxi;
+                            const Real Gp = -WYx * u + WXx * v, Gu = -WYx * p, Gv = WXx * p;
+                            // du(i, j) += sum_l D(l, j) G(i, l)
+#pragma unroll
+                            for (int j = 0; j < N; ++j)
+                            {
+                                const Real d = Tab<Real>::D(N, l + N * j);
+                                sp[j] += d * Gp;
+                                su[j] += d * Gu;
+                                sv[j] += d * Gv;
+                            }
+                        }
+                    }
+                    // face nodes of the column: (i, 0) on side 0, (i, n-1) on side 2, face-node index i
+                    ws_face<N, Real, 0>(codes, flags, c01, c23, c45, c67, wi, i, ue + 3 * i, halo_e, sp[0], su[0], sv[0]);
+                    ws_face<N, Real, 2>(codes, flags, c01, c23, c45, c67, wi, i, ue + 3 * (i + N * (N - 1)), halo_e,
+                                        sp[N - 1], su[N - 1], sv[N - 1]);
+
+                    // ---- epilogue per node of the column: + row-pass sums, forcing, M^{-1}, RK
+                    // update in place (wavedg/ode.hpp:66-93)
+                    const Real *rx = Rx + el_l * NN * 3;
+                    const Real *mi = Mi + el_l * NN;
+                    Real *de = dus + le * ND;
+#pragma unroll
+                    for (int j = 0; j < N; ++j)
+                    {
+                        const int node = i + N * j;
+                        Real r0 = sp[j] + rx[3 * node], r1 = su[j] + rx[3 * node + 1], r2 = sv[j] + rx[3 * node + 2];
+                        const size_t g = (size_t)(el0 + le) * ND + 3 * node;
+                        if (EXTRA && (flags & F_FORCE))
+                        {
+                            r0 += a.fscale * a.F[g];
+                            r1 += a.fscale * a.F[g + 1];
+                            r2 += a.fscale * a.F[g + 2];
+                        }
+                        if (flags & F_MINV)
+                        {
+                            const Real mv = mi[node];
+                            r0 *= mv;
+                            r1 *= mv;
+                            r2 *= mv;
+                        }
+                        Real *un = ue + 3 * node;
+                        Real *dn = de + 3 * node;
+                        const Real d0 = has_du ? a.rk_a * dn[0] + a.dt * r0 : a.dt * r0;
+                        const Real d1 = has_du ? a.rk_a * dn[1] + a.dt * r1 : a.dt * r1;
+                        const Real d2 = has_du ? a.rk_a * dn[2] + a.dt * r2 : a.dt * r2;
+                        const Real u0 = un[0] + a.rk_b * d0, u1 = un[1] + a.rk_b * d1, u2 = un[2] + a.rk_b * d2;
+                        dn[0] = d0;
+                        dn[1] = d1;
+                        dn[2] = d2;
+                        un[0] = u0;
+                        un[1] = u1;
+                        un[2] = u2;
+                        if (EXTRA && (flags & F_FILTER))
+                        {
+                            a.acc[g] += a.acc_c * (double)u0;
+                            a.acc[g + 1] += a.acc_c * (double)u1;
+                            a.acc[g + 2] += a.acc_c * (double)u2;
                         }
                     }
                 }
-
-                // ---- face lanes: own trace, and the partner trace from L2 (issued now, used later)
-                Real fo[FPL][3], fx[FPL][3];
-                uint32_t fbyte[FPL];
-#pragma unroll
-                for (int p = 0; p < FPL; ++p)
-                {
-                    const int f = lane + 32 * p;
-                    const int ei = f / NF, fl = f - ei * NF, le = eb + ei;
-                    fbyte[p] = 0x40u; // inactive
-                    if (f >= Sh::FACES || le >= ne)
-                        continue;
-                    const int s = fl / N, k = fl - s * N;
-                    const uint32_t byte = (fks[le] >> (8 * s)) & 0xffu;
-                    const Real *own = us + le * ND + 3 * face_node(N, s, k);
-                    fo[p][0] = own[0];
-                    fo[p][1] = own[1];
-                    fo[p][2] = own[2];
-                    fbyte[p] = byte;
-                    if (byte & 0x80u)
-                    {
-                        if (!(flags & F_BND))
-                            fbyte[p] = 0x40u;
-                        continue;
-                    }
-                    if (!(flags & F_INT))
-                    {
-                        fbyte[p] = 0x40u;
-                        continue;
-                    }
-                    const int off = fbs[4 * le + s] + k * partner_stride<N>(byte);
-                    if (off < 0 || off + 3 > a.nel * ND)
-                    {
-                        atomicOr(a.err, 2u);
-                        fbyte[p] = 0x40u;
-                        continue;
-                    }
-                    fx[p][0] = __ldg(a.u + off);
-                    fx[p][1] = __ldg(a.u + off + 1);
-                    fx[p][2] = __ldg(a.u + off + 2);
-                }
-                __syncwarp();
-
-                // ---- volume: du(i,j) = sum_l D(l,i) F(l,j) + D(l,j) G(i,l)  (div_2d_c, source/Div.cpp:131-179)
-                Real rv[NPL][3];
-#pragma unroll
-                for (int p = 0; p < NPL; ++p)
-                {
-                    rv[p][0] = rv[p][1] = rv[p][2] = 0;
-                    const int v = lane + 32 * p;
-                    const int ei = v / NN, node = v - ei * NN, le = eb + ei;
-                    if (v >= Sh::NODES || le >= ne || !(flags & F_VOL))
-                        continue;
-                    const int i = node % N, j = node / N;
-                    const Real *xe = X + ei * NN * 6;
-#pragma unroll
-                    for (int l = 0; l < N; ++l)
-                    {
-                        const Real di = Dt[l + N * i], dj = Dt[l + N * j];
-                        const Real *xf = xe + (l + N * j) * 6; // F at (l, j)
-                        const Real *xg = xe + (i + N * l) * 6; // G at (i, l)
-                        const R2 f01 = reinterpret_cast<const R2 *>(xf)[0];
-                        const Real f2 = xf[2], g0 = xg[3];
-                        const R2 g12 = reinterpret_cast<const R2 *>(xg)[2];
-                        rv[p][0] += di * f01.x + dj * g0;
-                        rv[p][1] += di * f01.y + dj * g12.x;
-                        rv[p][2] += di * f2 + dj * g12.y;
-                    }
-                }
-
-                // ---- upwind face fluxes (EdgeFlux / WaveBC closed form) into the face buffer
-#pragma unroll
-                for (int p = 0; p < FPL; ++p)
-                {
-                    const int f = lane + 32 * p;
-                    const int ei = f / NF, fl = f - ei * NF, le = eb + ei;
-                    if (f >= Sh::FACES || le >= ne)
-                        continue;
-                    Real *o = Fb + (ei * NF + fl) * 3;
-                    const uint32_t byte = fbyte[p];
-                    if (byte == 0x40u)
-                    {
-                        o[0] = o[1] = o[2] = 0;
-                        continue;
-                    }
-                    const int s = fl / N, k = fl - s * N;
-                    const int p0 = (0x0310 >> (4 * s)) & 0xf, p1 = (0x3221 >> (4 * s)) & 0xf; // side s runs p0 -> p1
-                    const double *c = cs + 8 * le;
-                    const double dx = c[2 * p1] - c[2 * p0], dy = c[2 * p1 + 1] - c[2 * p0 + 1];
-                    const double s2 = dx * dx + dy * dy, rs = rsqrt(s2);
-                    const double sgn = (s >= 2) ? -1.0 : 1.0;
-                    const Real nx = (Real)(sgn * dy * rs), ny = (Real)(-sgn * dx * rs);
-                    const Real hm = (Real)(0.25 * s2 * rs);
-                    Real xq[3];
-                    if (byte & 0x80u)
-                        exterior<Real>((int)((byte >> 3) & 3u), nx, ny, fo[p], xq);
-                    else
-                    {
-                        xq[0] = fx[p][0];
-                        xq[1] = fx[p][1];
-                        xq[2] = fx[p][2];
-                    }
-                    Real fl3[3] = {0, 0, 0};
-                    upwind<Real>(nx, ny, wt[k] * hm, fo[p], xq, fl3);
-                    o[0] = fl3[0];
-                    o[1] = fl3[1];
-                    o[2] = fl3[2];
-                }
-                __syncwarp();
-
-                // ---- combine, M^{-1}, RK update in place (wavedg/ode.hpp:66-93)
-#pragma unroll
-                for (int p = 0; p < NPL; ++p)
-                {
-                    const int v = lane + 32 * p;
-                    const int ei = v / NN, node = v - ei * NN, le = eb + ei;
-                    if (v >= Sh::NODES || le >= ne)
-                        continue;
-                    const int i = node % N, j = node / N;
-                    const Real *fe = Fb + ei * NF * 3;
-                    Real r0 = rv[p][0], r1 = rv[p][1], r2 = rv[p][2];
-                    // face slots (side * N + face node) through node (i, j)
-                    const int sa = (j == 0) ? i : (j == N - 1) ? 2 * N + i : -1;
-                    const int sb = (i == N - 1) ? N + j : (i == 0) ? 3 * N + j : -1;
-                    if (sa >= 0)
-                    {
-                        r0 += fe[3 * sa];
-                        r1 += fe[3 * sa + 1];
-                        r2 += fe[3 * sa + 2];
-                    }
-                    if (sb >= 0)
-                    {
-                        r0 += fe[3 * sb];
-                        r1 += fe[3 * sb + 1];
-                        r2 += fe[3 * sb + 2];
-                    }
-                    if (EXTRA && (flags & F_FORCE))
-                    {
-                        r0 += a.fscale * fv[p][0];
-                        r1 += a.fscale * fv[p][1];
-                        r2 += a.fscale * fv[p][2];
-                    }
-                    if (flags & F_MINV)
-                    {
-                        r0 *= minv[p];
-                        r1 *= minv[p];
-                        r2 *= minv[p];
-                    }
-                    Real *un = us + le * ND + 3 * node;
-                    Real *dn = dus + le * ND + 3 * node;
-                    const Real d0 = has_du ? a.rk_a * dn[0] + a.dt * r0 : a.dt * r0;
-                    const Real d1 = has_du ? a.rk_a * dn[1] + a.dt * r1 : a.dt * r1;
-                    const Real d2 = has_du ? a.rk_a * dn[2] + a.dt * r2 : a.dt * r2;
-                    const Real u0 = un[0] + a.rk_b * d0, u1 = un[1] + a.rk_b * d1, u2 = un[2] + a.rk_b * d2;
-                    dn[0] = d0;
-                    dn[1] = d1;
-                    dn[2] = d2;
-                    un[0] = u0;
-                    un[1] = u1;
-                    un[2] = u2;
-                    if (EXTRA && (flags & F_FILTER))
-                    {
-                        const size_t g = (size_t)(el0 + le) * ND + 3 * node;
-                        a.acc[g] = av[p][0] + a.acc_c * (double)u0;
-                        a.acc[g + 1] = av[p][1] + a.acc_c * (double)u1;
-                        a.acc[g + 2] = av[p][2] + a.acc_c * (double)u2;
-                    }
-                }
+                __syncwarp(); // the scratch is reused by the next round
             }
             // results are in the slot: hand them to the async proxy, then release the slot
             fence_async_smem();

@@ -548,7 +548,7 @@ extern "C"
             ring = kWsDefaultRing;
         const int unit = ws_chunk_unit(w->n);
         if (chunk < unit || chunk % unit || chunk > 64 * unit)
-            return fail(WDG_ERR_ARG, "warp-specialised kernel: the chunk must be a multiple of 8 x elements per warp");
+            return fail(WDG_ERR_ARG, "warp-specialised kernel: the chunk must be a multiple of 8 warps x elements per warp");
         if (ring < 2 || ring > 6)
             return fail(WDG_ERR_ARG, "warp-specialised kernel: the ring holds 2 to 6 chunks");
         if (ws_smem_bytes(w->n, fp32, chunk, ring) > kMaxSmem)
