@@ -14,16 +14,18 @@
 //              cp.async.bulk straight from the slot (results are in place).
 //   consumers  a warp owns EW = floor(32 / n) whole elements per round, one
 //              lane per grid line of each, all three fields per lane:
-//                row pass     lane m holds row j = m: forms the xi-fluxes F of
-//                             the row in registers and contracts them with
-//                             D (compile-time constants) into 3 n sums; adds
-//                             the upwind flux of the row's two face nodes
-//                             (sides 3 and 1); writes the sums and the row's
-//                             inverse mass to a per-warp scratch.
-//                column pass  lane m holds column i = m: eta-fluxes G, the
-//                             eta contraction, the face nodes of sides 0 and
-//                             2, plus the row pass's sums, M^{-1} and the RK
-//                             update of the column's nodes, in place.
+//                column pass  lane m holds column i = m: forms the eta-fluxes G
+//                             of the column in registers and contracts them
+//                             with D (compile-time constants) into 3 n sums;
+//                             adds the upwind flux of the column's two face
+//                             nodes (sides 0 and 2); writes the sums to a
+//                             per-warp scratch.
+//                row pass     lane m holds row j = m: xi-fluxes F, the xi
+//                             contraction, the face nodes of sides 3 and 1,
+//                             then per node the column pass's sums, M^{-1}
+//                             and the RK update, in place.  The row pass works
+//                             on contiguous 3 n-value runs, so its shared
+//                             memory accesses are free of bank conflicts.
 //              Warps sync only with __syncwarp; a chunk is released when all
 //              consumer warps have arrived on its `done` barrier.
 //
@@ -51,7 +53,7 @@ namespace wdg
     // shared-memory layout (bytes), identical on host and device:
     //   [2 S mbarriers | pad to 128][x (n), w (n) | pad to 128][S slots][consumer scratch]
     //   slot    = u (C, 3 n^2) | du (C, 3 n^2) | halo (C, 4 n, 3) | corners (C, 8 doubles) | fcode (C, u32)
-    //   scratch = per warp, per element of a round: row-pass sums [n^2][3], inverse mass [n^2]
+    //   scratch = per warp, per element of a round: column-pass sums [n^2][3]
     struct WsLayout
     {
         int ub, hb, cb, kb, slot, tab, slots, scratch, warp_scratch, total;
@@ -69,7 +71,7 @@ namespace wdg
         L.tab = 128;
         L.slots = (L.tab + 2 * n * (int)sizeof(Real) + 127) & ~127;
         L.scratch = L.slots + stages * L.slot;
-        L.warp_scratch = ((ew * 4 * nn * (int)sizeof(Real)) + 15) & ~15;
+        L.warp_scratch = ((ew * 3 * nn * (int)sizeof(Real)) + 15) & ~15;
         L.total = L.scratch + kWsConsumers * L.warp_scratch;
         return L;
     }
@@ -305,8 +307,7 @@ namespace wdg
         // ---------------------------------------------------------------- consumers
         const int cw = warp;
         const int R = C / (kWsConsumers * EW); // warp-rounds per chunk
-        Real *Rx = reinterpret_cast<Real *>(smem + L.scratch + cw * L.warp_scratch); // [EW][NN][3] row-pass sums
-        Real *Mi = Rx + EW * NN * 3;                                                  // [EW][NN] inverse mass
+        Real *Rc = reinterpret_cast<Real *>(smem + L.scratch + cw * L.warp_scratch); // [EW][NN][3] column-pass sums
         const int el_l = lane / N, ln = lane - el_l * N; // element of the round, grid line
         const bool lane_on = lane < EW * N;
         const Real xm = lane_on ? xt[ln] : Real(0), wm = lane_on ? wt[ln] : Real(0);
@@ -335,6 +336,7 @@ namespace wdg
                 uint32_t codes = 0;
                 const Real *halo_e = halo + le * NF * 3;
                 Real *ue = us + le * ND;
+                Real *rc = Rc + el_l * NN * 3; // this element's column-pass sums, (node, field)
                 if (act)
                 {
                     const double2 *c2 = reinterpret_cast<const double2 *>(cs + 8 * le);
@@ -344,74 +346,9 @@ namespace wdg
                     c67 = c2[3];
                     codes = fks[le];
 
-                    // ---- row pass: row j = ln.  Contravariant fluxes of the wave system
-                    // (source/Div.cpp:5-53): F = W (y_eta u - x_eta v, y_eta p, -x_eta p); along a
-                    // row x_xi, y_xi are constant and x_eta, y_eta vary linearly with xi.
-                    const Real eta = xm, wj = wm;
-                    const Real Xxi = Real(0.25) * ((Real(1) - eta) * Real(c23.x - c01.x) + (Real(1) + eta) * Real(c45.x - c67.x));
-                    const Real Yxi = Real(0.25) * ((Real(1) - eta) * Real(c23.y - c01.y) + (Real(1) + eta) * Real(c45.y - c67.y));
-                    const Real ex0 = Real(c67.x - c01.x), ex1 = Real(c45.x - c23.x);
-                    const Real ey0 = Real(c67.y - c01.y), ey1 = Real(c45.y - c23.y);
-                    const Real *row = ue + 3 * N * ln;
-                    Real ap[N], au[N], av[N];
-#pragma unroll
-                    for (int i = 0; i < N; ++i)
-                        ap[i] = au[i] = av[i] = 0;
-                    Real *mrow = Mi + el_l * NN + N * ln;
-                    if (flags & F_VOL)
-                    {
-#pragma unroll
-                        for (int l = 0; l < N; ++l)
-                        {
-                            const Real xl = Tab<Real>::x(N, l);
-                            const Real Xeta = Real(0.25) * ((Real(1) - xl) * ex0 + (Real(1) + xl) * ex1);
-                            const Real Yeta = Real(0.25) * ((Real(1) - xl) * ey0 + (Real(1) + xl) * ey1);
-                            const Real W = Tab<Real>::w(N, l) * wj;
-                            const Real p = row[3 * l], u = row[3 * l + 1], v = row[3 * l + 2];
-                            const Real WYe = W * Yeta, WXe = W * Xeta;
-                            const Real Fp = WYe * u - WXe * v, Fu = WYe * p, Fv = -WXe * p;
-                            // MassMatrix<true>: w_i w_j det J (source/MassMatrix.cpp:6-28)
-                            mrow[l] = Real(1) / (W * (Xxi * Yeta - Yxi * Xeta));
-                            // du(i, j) += sum_l D(l, i) F(l, j)  (div_2d_c, source/Div.cpp:131-179)
-#pragma unroll
-                            for (int i = 0; i < N; ++i)
-                            {
-                                const Real d = Tab<Real>::D(N, l + N * i);
-                                ap[i] += d * Fp;
-                                au[i] += d * Fu;
-                                av[i] += d * Fv;
-                            }
-                        }
-                    }
-                    else
-                    {
-#pragma unroll
-                        for (int l = 0; l < N; ++l)
-                        {
-                            const Real xl = Tab<Real>::x(N, l);
-                            const Real Xeta = Real(0.25) * ((Real(1) - xl) * ex0 + (Real(1) + xl) * ex1);
-                            const Real Yeta = Real(0.25) * ((Real(1) - xl) * ey0 + (Real(1) + xl) * ey1);
-                            mrow[l] = Real(1) / (Tab<Real>::w(N, l) * wj * (Xxi * Yeta - Yxi * Xeta));
-                        }
-                    }
-                    // face nodes of the row: (0, j) on side 3, (n-1, j) on side 1, face-node index j
-                    ws_face<N, Real, 3>(codes, flags, c01, c23, c45, c67, wj, ln, row, halo_e, ap[0], au[0], av[0]);
-                    ws_face<N, Real, 1>(codes, flags, c01, c23, c45, c67, wj, ln, row + 3 * (N - 1), halo_e,
-                                        ap[N - 1], au[N - 1], av[N - 1]);
-                    Real *rx = Rx + (el_l * NN + N * ln) * 3;
-#pragma unroll
-                    for (int i = 0; i < N; ++i)
-                    {
-                        rx[3 * i] = ap[i];
-                        rx[3 * i + 1] = au[i];
-                        rx[3 * i + 2] = av[i];
-                    }
-                }
-                __syncwarp();
-                if (act)
-                {
-                    // ---- column pass: column i = ln.  G = W (-y_xi u + x_xi v, -y_xi p, x_xi p);
-                    // along a column x_eta, y_eta are constant and x_xi, y_xi vary with eta.
+                    // ---- column pass: column i = ln.  Contravariant eta-fluxes of the wave system
+                    // (source/Div.cpp:5-53): G = W (-y_xi u + x_xi v, -y_xi p, x_xi p); along a
+                    // column x_eta, y_eta are constant and x_xi, y_xi vary linearly with eta.
                     const int i = ln;
                     const Real wi = wm;
                     const Real dx0 = Real(c23.x - c01.x), dx1 = Real(c45.x - c67.x);
@@ -433,7 +370,7 @@ namespace wdg
                             const Real p = nd[0], u = nd[1], v = nd[2];
                             const Real WYx = W * Yxi, WXx = W * Xxi;
                             const Real Gp = -WYx * u + WXx * v, Gu = -WYx * p, Gv = WXx * p;
-                            // du(i, j) += sum_l D(l, j) G(i, l)
+                            // du(i, j) += sum_l D(l, j) G(i, l)  (div_2d_c, source/Div.cpp:131-179)
 #pragma unroll
                             for (int j = 0; j < N; ++j)
                             {
@@ -448,18 +385,75 @@ namespace wdg
                     ws_face<N, Real, 0>(codes, flags, c01, c23, c45, c67, wi, i, ue + 3 * i, halo_e, sp[0], su[0], sv[0]);
                     ws_face<N, Real, 2>(codes, flags, c01, c23, c45, c67, wi, i, ue + 3 * (i + N * (N - 1)), halo_e,
                                         sp[N - 1], su[N - 1], sv[N - 1]);
-
-                    // ---- epilogue per node of the column: + row-pass sums, forcing, M^{-1}, RK
-                    // update in place (wavedg/ode.hpp:66-93)
-                    const Real *rx = Rx + el_l * NN * 3;
-                    const Real *mi = Mi + el_l * NN;
-                    Real *de = dus + le * ND;
 #pragma unroll
                     for (int j = 0; j < N; ++j)
                     {
-                        const int node = i + N * j;
-                        Real r0 = sp[j] + rx[3 * node], r1 = su[j] + rx[3 * node + 1], r2 = sv[j] + rx[3 * node + 2];
-                        const size_t g = (size_t)(el0 + le) * ND + 3 * node;
+                        Real *o = rc + 3 * (i + N * j);
+                        o[0] = sp[j];
+                        o[1] = su[j];
+                        o[2] = sv[j];
+                    }
+                }
+                __syncwarp();
+                if (act)
+                {
+                    // ---- row pass: row j = ln.  F = W (y_eta u - x_eta v, y_eta p, -x_eta p); along a
+                    // row x_xi, y_xi are constant and x_eta, y_eta vary linearly with xi.
+                    const int j = ln;
+                    const Real eta = xm, wj = wm;
+                    const Real Xxi = Real(0.25) * ((Real(1) - eta) * Real(c23.x - c01.x) + (Real(1) + eta) * Real(c45.x - c67.x));
+                    const Real Yxi = Real(0.25) * ((Real(1) - eta) * Real(c23.y - c01.y) + (Real(1) + eta) * Real(c45.y - c67.y));
+                    const Real ex0 = Real(c67.x - c01.x), ex1 = Real(c45.x - c23.x);
+                    const Real ey0 = Real(c67.y - c01.y), ey1 = Real(c45.y - c23.y);
+                    Real *row = ue + 3 * N * j;
+                    Real q0[N], q1[N], q2[N], mv[N];
+                    Real ap[N], au[N], av[N];
+#pragma unroll
+                    for (int l = 0; l < N; ++l)
+                    {
+                        q0[l] = row[3 * l];
+                        q1[l] = row[3 * l + 1];
+                        q2[l] = row[3 * l + 2];
+                        ap[l] = au[l] = av[l] = 0;
+                    }
+#pragma unroll
+                    for (int l = 0; l < N; ++l)
+                    {
+                        const Real xl = Tab<Real>::x(N, l);
+                        const Real Xeta = Real(0.25) * ((Real(1) - xl) * ex0 + (Real(1) + xl) * ex1);
+                        const Real Yeta = Real(0.25) * ((Real(1) - xl) * ey0 + (Real(1) + xl) * ey1);
+                        const Real W = Tab<Real>::w(N, l) * wj;
+                        // MassMatrix<true>: w_i w_j det J (source/MassMatrix.cpp:6-28)
+                        mv[l] = Real(1) / (W * (Xxi * Yeta - Yxi * Xeta));
+                        if (flags & F_VOL)
+                        {
+                            const Real WYe = W * Yeta, WXe = W * Xeta;
+                            const Real Fp = WYe * q1[l] - WXe * q2[l], Fu = WYe * q0[l], Fv = -WXe * q0[l];
+                            // du(i, j) += sum_l D(l, i) F(l, j)
+#pragma unroll
+                            for (int i = 0; i < N; ++i)
+                            {
+                                const Real d = Tab<Real>::D(N, l + N * i);
+                                ap[i] += d * Fp;
+                                au[i] += d * Fu;
+                                av[i] += d * Fv;
+                            }
+                        }
+                    }
+                    // face nodes of the row: (0, j) on side 3, (n-1, j) on side 1, face-node index j
+                    ws_face<N, Real, 3>(codes, flags, c01, c23, c45, c67, wj, j, row, halo_e, ap[0], au[0], av[0]);
+                    ws_face<N, Real, 1>(codes, flags, c01, c23, c45, c67, wj, j, row + 3 * (N - 1), halo_e,
+                                        ap[N - 1], au[N - 1], av[N - 1]);
+
+                    // ---- epilogue per node of the row: + column-pass sums, forcing, M^{-1}, RK
+                    // update in place (wavedg/ode.hpp:66-93); the row is this lane's alone
+                    Real *drow = dus + le * ND + 3 * N * j;
+#pragma unroll
+                    for (int i = 0; i < N; ++i)
+                    {
+                        const Real *cr = rc + 3 * (i + N * j);
+                        Real r0 = ap[i] + cr[0], r1 = au[i] + cr[1], r2 = av[i] + cr[2];
+                        const size_t g = (size_t)(el0 + le) * ND + 3 * (i + N * j);
                         if (EXTRA && (flags & F_FORCE))
                         {
                             r0 += a.fscale * a.F[g];
@@ -468,23 +462,21 @@ namespace wdg
                         }
                         if (flags & F_MINV)
                         {
-                            const Real mv = mi[node];
-                            r0 *= mv;
-                            r1 *= mv;
-                            r2 *= mv;
+                            r0 *= mv[i];
+                            r1 *= mv[i];
+                            r2 *= mv[i];
                         }
-                        Real *un = ue + 3 * node;
-                        Real *dn = de + 3 * node;
+                        Real *dn = drow + 3 * i;
                         const Real d0 = has_du ? a.rk_a * dn[0] + a.dt * r0 : a.dt * r0;
                         const Real d1 = has_du ? a.rk_a * dn[1] + a.dt * r1 : a.dt * r1;
                         const Real d2 = has_du ? a.rk_a * dn[2] + a.dt * r2 : a.dt * r2;
-                        const Real u0 = un[0] + a.rk_b * d0, u1 = un[1] + a.rk_b * d1, u2 = un[2] + a.rk_b * d2;
+                        const Real u0 = q0[i] + a.rk_b * d0, u1 = q1[i] + a.rk_b * d1, u2 = q2[i] + a.rk_b * d2;
                         dn[0] = d0;
                         dn[1] = d1;
                         dn[2] = d2;
-                        un[0] = u0;
-                        un[1] = u1;
-                        un[2] = u2;
+                        row[3 * i] = u0;
+                        row[3 * i + 1] = u1;
+                        row[3 * i + 2] = u2;
                         if (EXTRA && (flags & F_FILTER))
                         {
                             a.acc[g] += a.acc_c * (double)u0;
