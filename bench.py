@@ -47,7 +47,8 @@ def parse():
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-extras", action="store_true", help="skip the FP32 companion measurement")
+    ap.add_argument("--no-extras", action="store_true", help="skip the FP32 and WaveHoltz companion measurements")
+    ap.add_argument("--no-waveholtz", action="store_true", help="skip the WaveHoltz solve measurement")
     ap.add_argument("--tile", type=int, default=0, help="elements per block (0: autotune)")
     ap.add_argument("--stages", type=int, default=0, help="pipeline depth with --tile (0: default)")
     ap.add_argument("--kernel", choices=["auto", "warp", "tiled", "ws"], default="auto",
@@ -229,17 +230,22 @@ def run_ours(args, rank, world, local_rank):
     e2e_ms = float(e2e_t.item())
     e2e_value = world * ndof * 5 * e2e_steps / (e2e_ms / 1e3)
 
-    # roofline of the stage kernel: algorithmic bytes per step / device time per step
+    # roofline of the stage kernel (the only kernel in the timed region, 5 launches per step):
+    # average algorithmic bytes per launch / average launch time, both from the timed steps
     peak, peak_kind = peak_hbm()
     bytes_step = algorithmic_bytes_per_step(ndof, nel, real)
-    achieved = bytes_step / (ms_step / 1e3) / 1e9
+    bytes_launch = bytes_step / 5
+    launch_s = ms_step / 5 / 1e3
+    achieved = bytes_launch / launch_s / 1e9
     traffic = None
     prof = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
-    if os.path.exists(prof):
+    if os.path.exists(prof) and args.n == 512 and args.P == 4:
         try:
-            traffic = json.load(open(prof)).get(f"{args.precision}_bytes_per_step_512")
+            traffic = json.load(open(prof)).get(f"{args.precision}_bytes_per_launch_512")
         except Exception:
             traffic = None
+    kernel_name = {"ws": "ws_stage_kernel", "tiled": "stage_kernel", "warp": "warp_stage_kernel"}.get(
+        sys_.launch_config()["kernel"], "stage_kernel")
 
     extra = {"energy_final": energy, "t_final": t_end, "dt": dt, "launch": sys_.launch_config(), "peak_kind": peak_kind}
     if not args.no_extras and args.precision == "fp64":
@@ -250,6 +256,9 @@ def run_ours(args, rank, world, local_rank):
                          "hbm_gbs": b32 / (ms32 / args.steps / 1e3) / 1e9,
                          "frac": b32 / (ms32 / args.steps / 1e3) / 1e9 / peak}
         del s32
+
+    if not args.no_extras and not args.no_waveholtz and args.precision == "fp64":
+        extra["waveholtz_c3"] = waveholtz_c3(local_rank)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -270,7 +279,8 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "inputs larger than L2 (three 157 MB state buffers rotate)",
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "stage_kernel", "bytes_per_step": bytes_step},
+                     "traffic": traffic, "kernel": kernel_name, "bytes_per_launch": bytes_launch,
+                     "launch_us": launch_s * 1e6, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": ndof * 8, "d2h_bytes_per_step": ndof * 8,
                 "steps": e2e_steps, "api": "wdg_rk4_steps(host pinned u, nsteps=1)"},
         "gpu_launches": 5 * args.steps,
@@ -279,6 +289,44 @@ def run_ours(args, rank, world, local_rank):
         "extra": extra,
     }
     print(json.dumps(out), flush=True)
+
+
+def waveholtz_c3(device: int, seed: int = 3) -> dict:
+    """One WaveHoltz Helmholtz solve on 128 x 128 uniform quads of [-1, 1]^2, P = 4, outflow
+    boundary, omega = 20, f = omega^2 exp(-|x - x0|^2 / (2 0.05^2)) with x0 seeded in
+    [-0.5, 0.5]^2, from a zero guess to 1e-6 relative residual: FP64 stepping, then FP32 stepping
+    with the FP64 filter / residual.  Wall time of the solve call (host-synchronous: it reads the
+    residual back every iteration), GPU synchronised on both sides."""
+    import torch
+
+    import wavedg_b200 as W
+
+    x0 = np.random.default_rng(seed).uniform(-0.5, 0.5, size=2)
+    omega = 20.0
+    mesh = W.Mesh2D.uniform_rect(128, -1.0, 1.0, 128, -1.0, 1.0)
+    basis = W.QuadratureRule.quadrature_rule(5, W.QuadratureRule.GaussLobatto)
+    bc = np.zeros(mesh.n_edges(1), dtype=np.int32)
+    out, sols = {}, {}
+    for prec in ("fp64", "fp32"):
+        sys_ = W.WaveSystem(mesh, basis, bc, precision=prec, device=device)
+        wh = W.WaveHoltz(omega, mesh, basis, bc, True, precision=prec, system=sys_)
+        F = torch.zeros(sys_.ndof, dtype=torch.float64, device="cuda")
+        sys_.load_gaussians([x0], [0.05], [omega ** 2], 1.0, 0, False, out=F)
+        Wd = torch.zeros_like(F)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, it, res = wh.solve(F, 1e-6, 1000, W=Wd)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        sols[prec] = Wd
+        out[prec] = {"iterations": it, "residual": res, "seconds": el, "solves_per_s": 1.0 / el,
+                     "steps_per_period": wh.nt, "dt": wh.dt,
+                     "dof_stage_per_s": sys_.ndof * 5 * wh.nt * (it + 1) / el}
+    d = (sols["fp32"] - sols["fp64"]).norm().item() / sols["fp64"].norm().item()
+    out["fp32"]["rel_diff_vs_fp64_gpu"] = d
+    out["workload"] = "waveholtz_128x128_P4_omega20_outflow_tol1e-6"
+    out["x0"] = [float(x0[0]), float(x0[1])]
+    return out
 
 
 # ----------------------------------------------------------- CPU side
