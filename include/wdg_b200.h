@@ -201,6 +201,33 @@ int wdg_waveholtz_postprocess(wdg_waveholtz *wh, double *H, const double *w);
 int wdg_waveholtz_solve(wdg_waveholtz *wh, const double *F, double tol, int maxit, double *W, int *iters,
                         double *residual);
 
+/* ------------------------------------------------------ batched WaveHoltz */
+/* Up to 64 independent WaveHoltz solves, each on its own discretisation (mesh, degree) with
+ * its own omega, advanced together: one persistent kernel launch per RK stage over a work
+ * list of (solve, chunk of elements), blocks of steps replayed as a CUDA graph.  Per solve,
+ * T, dt and nt follow WaveHoltz::WaveHoltz (source/WaveHoltz.cpp:24-29), and the iteration is
+ * the fixed-point loop of examples/waveholtz2d.cpp:165-185 with its residual
+ * ||W - W_prev|| / ||pi0|| (each iteration runs one forced period from W, which equals
+ * S W + pi0).  All discretisations must share device and precision (WDG_FP32 steps in FP32
+ * with the filter, iterate and residual in FP64); a discretisation may appear once per batch
+ * and must not be stepped elsewhere while the batch solves. */
+typedef struct wdg_whbatch wdg_whbatch;
+int wdg_whbatch_create(int n_solves, wdg_wave *const *waves, const double *omegas, wdg_whbatch **out);
+void wdg_whbatch_destroy(wdg_whbatch *batch);
+int wdg_whbatch_params(const wdg_whbatch *batch, int solve, double *T, double *dt, int *nt);
+/* chunk = rounds x (4 warps x floor(32 / n) elements) per solve; ring = chunk slots (2..6) */
+int wdg_whbatch_set_launch(wdg_whbatch *batch, int rounds, int ring);
+int wdg_whbatch_get_launch(const wdg_whbatch *batch, int *rounds, int *ring, int *grid);
+/* times `steps` batch steps of every launch shape that fits and keeps the fastest */
+int wdg_whbatch_autotune(wdg_whbatch *batch, int steps, float *best_ms_per_step);
+/* F[s], W[s]: FP64 arrays (host or device) of solve s.  warm (nullable): warm[s] != 0 starts
+ * solve s from W[s] (one extra period from zero then gives |pi0|), else from zero.  A solve
+ * stops at residual < tol (status 0), after maxit iterations (1), or when stall_limit > 0
+ * updates in a row bring no new smallest residual (2: the stepping precision's floor).
+ * W[s] receives the last iterate; iters, residuals, status (nullable) get one entry per solve. */
+int wdg_whbatch_solve(wdg_whbatch *batch, const double *const *F, double tol, int maxit, int stall_limit,
+                      double *const *W, const int *warm, int *iters, double *residuals, int *status);
+
 #ifdef __cplusplus
 }
 #endif

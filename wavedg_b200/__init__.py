@@ -19,6 +19,7 @@ from .dg import (  # noqa: F401
     WaveBC,
     WaveEquation,
     WaveHoltz,
+    WaveHoltzBatch,
     WaveSystem,
     error,
     make_face_prolongator,
@@ -27,6 +28,6 @@ from .dg import (  # noqa: F401
 
 __all__ = [
     "Discretisation", "Div", "EdgeFlux", "FaceProlongator", "FaceType", "LinearFunctional2D", "MassMatrix",
-    "Mesh2D", "Operator", "QuadratureRule", "RungeKutta4", "WaveBC", "WaveEquation", "WaveHoltz", "WaveSystem",
+    "Mesh2D", "Operator", "QuadratureRule", "RungeKutta4", "WaveBC", "WaveEquation", "WaveHoltz", "WaveHoltzBatch", "WaveSystem",
     "WdgError", "WDG_FP32", "WDG_FP64", "error", "lib", "make_face_prolongator", "norm",
 ]

@@ -95,6 +95,13 @@ SIGNATURES = {
     "wdg_waveholtz_S": ([_v, _v], _i),
     "wdg_waveholtz_postprocess": ([_v, _v, _v], _i),
     "wdg_waveholtz_solve": ([_v, _v, _d, _i, _v, _ip, _dp], _i),
+    "wdg_whbatch_create": ([_i, _v, _v, _vp], _i),
+    "wdg_whbatch_destroy": ([_v], None),
+    "wdg_whbatch_params": ([_v, _i, _dp, _dp, _ip], _i),
+    "wdg_whbatch_set_launch": ([_v, _i, _i], _i),
+    "wdg_whbatch_get_launch": ([_v, _ip, _ip, _ip], _i),
+    "wdg_whbatch_autotune": ([_v, _i, C.POINTER(C.c_float)], _i),
+    "wdg_whbatch_solve": ([_v, _v, _d, _i, _i, _v, _v, _v, _v, _v], _i),
 }
 
 _lib = None

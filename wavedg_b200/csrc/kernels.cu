@@ -1003,10 +1003,19 @@ namespace wdg
 } // namespace wdg
 
 #include "stage_ws.cuh"
+#include "stage_ws_batch.cuh"
 
 namespace wdg
 {
     int ws_chunk_unit(int n) { return kWsConsumers * ws_epw(n); }
+    int ws_slot_bytes(int n, bool fp32, int chunk)
+    {
+        return fp32 ? ws_slot<float>(n, chunk).bytes : ws_slot<double>(n, chunk).bytes;
+    }
+    int ws_warp_scratch_bytes(int n, bool fp32)
+    {
+        return fp32 ? ws_layout<float>(n, 0, 0).warp_scratch : ws_layout<double>(n, 0, 0).warp_scratch;
+    }
     size_t ws_smem_bytes(int n, bool fp32, int chunk, int ring)
     {
         return fp32 ? (size_t)ws_layout<float>(n, chunk, ring).total : (size_t)ws_layout<double>(n, chunk, ring).total;

@@ -76,6 +76,61 @@ namespace wdg
     constexpr int kWsDefaultRing = 2;
     int ws_default_chunk(int n, bool fp32);   // most rounds (<= 4) whose default ring fits 3 CTAs per SM
 
+    // warp-specialised stage kernels: one producer warp + kWsConsumers consumer warps per CTA
+    constexpr int kWsConsumers = 4;
+    int ws_slot_bytes(int n, bool fp32, int chunk); // one ring slot of an n, chunk-element chunk
+    int ws_warp_scratch_bytes(int n, bool fp32);    // one consumer warp's scratch
+
+    // ---- batched WaveHoltz (kernels in stage_ws_batch.cuh, C-ABI in whbatch.cu)
+    constexpr int kMaxBatch = 64;
+
+    template <typename Real>
+    struct WhbSolve
+    {
+        Real *buf[3]; // rotation buffers: [0] the state between steps, [1], [2]
+        Real *du;
+        const Real *F;
+        double *acc, *W, *part;
+        const double *corners;
+        const int4 *fbase;
+        const uint32_t *fcode;
+        int nel, n, chunk, item0; // item0: the solve's first work item
+        int nt;
+        double dt, omega, c0;
+    };
+
+    struct WhbState
+    {
+        int k;      // step within the current period
+        int phase;  // 0: the pi0 period of a warm start, 1: fixed-point periods
+        int active; // 0 once converged, out of iterations or stalled
+        int iter;   // fixed-point updates done
+        int stall;  // consecutive updates without a new smallest residual
+        int zero_start, nt, nparts;
+        int maxit, stall_limit, status, pad; // status: 0 converged, 1 iteration limit, 2 stalled, -1 running
+        double pi0sq, residual, best, tol;
+        double *part;
+    };
+
+    template <typename Real>
+    struct WhbArgs
+    {
+        int nsolves, nitems, stage, ring;
+        int slot_bytes, warp_scratch;
+        WhbState *state;
+        unsigned *err;
+        WhbSolve<Real> s[kMaxBatch];
+    };
+
+    extern const double rk4a[5], rk4b[5], rk4c[5];
+    int upload_rk4_tables(int device); // once per device
+    int whb_smem_bytes(int slot_bytes, int warp_scratch, int ring, bool fp32);
+    template <typename Real>
+    cudaError_t launch_whb_stage(const WhbArgs<Real> &a, int grid, size_t smem, cudaStream_t s);
+    template <typename Real>
+    cudaError_t whb_occupancy(size_t smem, int *grid);
+    cudaError_t launch_whb_step_end(WhbState *state, int nsolves, cudaStream_t s);
+
     // fused stage: RK = true for the time-stepping epilogue
     template <typename Real>
     cudaError_t launch_stage(int n, bool rk, const StageArgs<Real> &a, int grid_limit, cudaStream_t s);

@@ -45,7 +45,6 @@ namespace wdg
         static constexpr int NN = N * N, ND = 3 * NN, NF = 4 * N;
         static constexpr int EW = 32 / N; // elements per warp-round, one lane per line
     };
-    constexpr int kWsConsumers = 4;
     constexpr int kWsThreads = 32 * (kWsConsumers + 1);
 
     int ws_epw(int n) { return 32 / n; }
@@ -56,25 +55,10 @@ namespace wdg
     //   scratch = per warp, per element of a round: column-pass sums [n^2][3]
     struct WsLayout
     {
-        int ub, hb, cb, kb, slot, tab, slots, scratch, warp_scratch, total;
+        int slot, tab, slots, scratch, warp_scratch, total;
     };
     template <typename Real>
-    __host__ __device__ inline WsLayout ws_layout(int n, int chunk, int stages)
-    {
-        WsLayout L;
-        const int nn = n * n, ew = 32 / n;
-        L.ub = chunk * 3 * nn * (int)sizeof(Real);
-        L.hb = 2 * L.ub;                                   // halo
-        L.cb = L.hb + chunk * 12 * n * (int)sizeof(Real);  // corners
-        L.kb = L.cb + chunk * 64;                          // side codes
-        L.slot = L.kb + chunk * 4;
-        L.tab = 128;
-        L.slots = (L.tab + 2 * n * (int)sizeof(Real) + 127) & ~127;
-        L.scratch = L.slots + stages * L.slot;
-        L.warp_scratch = ((ew * 3 * nn * (int)sizeof(Real)) + 15) & ~15;
-        L.total = L.scratch + kWsConsumers * L.warp_scratch;
-        return L;
-    }
+    __host__ __device__ inline WsLayout ws_layout(int n, int chunk, int stages);
 
     __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
     {
@@ -126,212 +110,196 @@ namespace wdg
         r2 = r[2];
     }
 
-    template <int N, typename Real, bool EXTRA>
-    __global__ void __launch_bounds__(kWsThreads, 2) ws_stage_kernel(const StageArgs<Real> a)
+
+    // One chunk of one RK stage as both roles see it (the single-solve kernel fills it from
+    // its launch arguments, the batched kernel from its solve table).
+    template <typename Real>
+    struct WsChunk
+    {
+        const Real *u;  // state in (the stage's input array; neighbour traces come from it)
+        Real *out;      // u' (never aliases u)
+        Real *du;       // RK register, read (stages > 0) and written in place
+        const Real *F;  // forcing (F_FORCE)
+        double *acc;    // FP64 filter accumulator (F_FILTER)
+        const double *corners;
+        const int4 *fbase;
+        const uint32_t *fcode;
+        unsigned *err;
+        int nel, el0, ne, chunk, flags;
+        Real rk_a, rk_b, dt, fscale;
+        double acc_c;
+        // batched WaveHoltz, last stage of a period: 1 = fixed-point update W <- filter,
+        // 2 = end of the separate pi0 period (only its norm is kept); 0 = neither
+        int pend;
+        double *W;    // FP64 iterate
+        double c0;    // 0.5 dt K(0): the filter's first term at a period start
+        double *part; // this chunk's partial sums: per consumer warp (sum (W' - W)^2, sum W'^2)
+    };
+
+    // slot offsets (bytes) of an n, chunk-C slot:
+    //   u (C, 3 n^2) | du (C, 3 n^2) | halo (C, 4 n, 3) | corners (C, 8 doubles) | fcode (C, u32)
+    struct WsSlot
+    {
+        int ub, hb, cb, kb, bytes;
+    };
+    template <typename Real>
+    __host__ __device__ inline WsSlot ws_slot(int n, int chunk)
+    {
+        WsSlot o;
+        o.ub = chunk * 3 * n * n * (int)sizeof(Real);
+        o.hb = 2 * o.ub;
+        o.cb = o.hb + chunk * 12 * n * (int)sizeof(Real);
+        o.kb = o.cb + chunk * 64;
+        o.bytes = o.kb + chunk * 4;
+        return o;
+    }
+
+    // ---------------------------------------------------------------- producer: load one chunk
+    // u, du, corners and side codes by cp.async.bulk on `full` (plain copies for a ragged
+    // chunk), then the neighbour traces of every interior face node by cp.async, one lane
+    // per (element, side); the table reads of a batch go out together, so a chunk costs one
+    // L2 round trip per batch rather than one per face node.
+    template <int N, typename Real>
+    __device__ __forceinline__ void ws_load(const WsChunk<Real> &c, unsigned char *base, uint64_t *full, int lane)
+    {
+        constexpr int ND = 3 * N * N, NF = 4 * N;
+        const WsSlot o = ws_slot<Real>(N, c.chunk);
+        const bool has_du = (c.flags & F_READ_DU) != 0;
+        const int el0 = c.el0, ne = c.ne, C = c.chunk;
+        if (ne == C)
+        {
+            if (lane == 0)
+            {
+                mbar_expect_tx(full, (uint32_t)(o.ub * (has_du ? 2 : 1) + C * 68));
+                bulk_g2s(base, c.u + (size_t)el0 * ND, (uint32_t)o.ub, full);
+                if (has_du)
+                    bulk_g2s(base + o.ub, c.du + (size_t)el0 * ND, (uint32_t)o.ub, full);
+                bulk_g2s(base + o.cb, c.corners + 8 * (size_t)el0, (uint32_t)(64 * C), full);
+                bulk_g2s(base + o.kb, c.fcode + el0, (uint32_t)(4 * C), full);
+            }
+        }
+        else
+        {
+            Real *us = reinterpret_cast<Real *>(base), *dus = us + C * ND;
+            for (int i = lane; i < ne * ND; i += 32)
+            {
+                us[i] = c.u[(size_t)el0 * ND + i];
+                if (has_du)
+                    dus[i] = c.du[(size_t)el0 * ND + i];
+            }
+            double *cw = reinterpret_cast<double *>(base + o.cb);
+            for (int i = lane; i < ne * 8; i += 32)
+                cw[i] = c.corners[8 * (size_t)el0 + i];
+            uint32_t *kw = reinterpret_cast<uint32_t *>(base + o.kb);
+            for (int i = lane; i < ne; i += 32)
+                kw[i] = c.fcode[el0 + i];
+            __threadfence_block();
+            __syncwarp();
+            if (lane == 0)
+                mbar_arrive(full);
+        }
+        if (c.flags & F_INT)
+        {
+            Real *halo = reinterpret_cast<Real *>(base + o.hb);
+            const int limit = c.nel * ND;
+            constexpr int B = 4; // (element, side) pairs per lane per batch
+            for (int p0 = 0; p0 < ne * 4; p0 += 32 * B)
+            {
+                uint32_t code[B];
+                int off[B];
+#pragma unroll
+                for (int b = 0; b < B; ++b)
+                {
+                    const int pr = p0 + 32 * b + lane, le = pr >> 2, s = pr & 3;
+                    code[b] = 0x80u;
+                    off[b] = -1;
+                    if (pr < ne * 4)
+                    {
+                        code[b] = (__ldg(c.fcode + el0 + le) >> (8 * s)) & 0xffu;
+                        off[b] = __ldg(reinterpret_cast<const int *>(c.fbase + el0 + le) + s);
+                    }
+                }
+#pragma unroll
+                for (int b = 0; b < B; ++b)
+                {
+                    const int pr = p0 + 32 * b + lane, le = pr >> 2, s = pr & 3;
+                    if (code[b] & 0x80u)
+                        continue; // boundary side (or past the chunk): no neighbour
+                    const int stride = partner_stride<N>(code[b]);
+                    if (off[b] < 0 || off[b] + (N - 1) * stride < 0 || off[b] + 3 > limit ||
+                        off[b] + (N - 1) * stride + 3 > limit)
+                    {
+                        atomicOr(c.err, 2u);
+                        continue;
+                    }
+                    Real *dst = halo + 3 * (le * NF + s * N);
+#pragma unroll
+                    for (int k = 0; k < N; ++k)
+                    {
+                        const Real *src = c.u + off[b] + k * stride;
+                        cp_async<sizeof(Real)>(dst + 3 * k, src);
+                        cp_async<sizeof(Real)>(dst + 3 * k + 1, src + 1);
+                        cp_async<sizeof(Real)>(dst + 3 * k + 2, src + 2);
+                    }
+                }
+            }
+        }
+        cp_async_mbar_arrive(full);
+    }
+
+    // ---------------------------------------------------------------- producer: store one chunk
+    template <int N, typename Real>
+    __device__ __forceinline__ void ws_store(const WsChunk<Real> &c, const unsigned char *base, int lane)
+    {
+        constexpr int ND = 3 * N * N;
+        const WsSlot o = ws_slot<Real>(N, c.chunk);
+        const int el0 = c.el0, ne = c.ne;
+        if (ne == c.chunk)
+        {
+            if (lane == 0)
+            {
+                bulk_s2g(c.out + (size_t)el0 * ND, base, (uint32_t)o.ub);
+                bulk_s2g(c.du + (size_t)el0 * ND, base + o.ub, (uint32_t)o.ub);
+                bulk_commit();
+            }
+        }
+        else
+        {
+            const Real *us = reinterpret_cast<const Real *>(base), *dus = us + c.chunk * ND;
+            for (int i = lane; i < ne * ND; i += 32)
+            {
+                c.out[(size_t)el0 * ND + i] = us[i];
+                c.du[(size_t)el0 * ND + i] = dus[i];
+            }
+        }
+    }
+
+    // ---------------------------------------------------------------- consumer: one chunk
+    // Warp `cw` takes rounds of EW whole elements; Rc is its scratch for the column sums.
+    template <int N, typename Real, bool EXTRA, bool BATCH>
+    __device__ __forceinline__ void ws_consume(const WsChunk<Real> &c, unsigned char *base, Real *Rc,
+                                               const Real *xtab, const Real *wtab, int cw, int lane)
     {
         using Sh = WsShape<N>;
         constexpr int NN = Sh::NN, ND = Sh::ND, NF = Sh::NF, EW = Sh::EW;
-        const int C = a.chunk, S = a.ring, G = gridDim.x;
-        const int flags = a.flags;
+        const WsSlot o = ws_slot<Real>(N, c.chunk);
+        const int flags = c.flags;
         const bool has_du = (flags & F_READ_DU) != 0;
-        const int nchunks = (a.nel + C - 1) / C;
-        const WsLayout L = ws_layout<Real>(N, C, S);
-
-        extern __shared__ __align__(128) unsigned char smem[];
-        uint64_t *full = reinterpret_cast<uint64_t *>(smem);
-        uint64_t *done = full + S;
-        Real *xt = reinterpret_cast<Real *>(smem + L.tab); // GLL nodes, then weights
-        Real *wt = xt + N;
-        unsigned char *slots = smem + L.slots;
-
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        if (threadIdx.x == 0)
-        {
-            for (int q = 0; q < S; ++q)
-            {
-                mbar_init(&full[q], 1 + 32); // the bulk-copy arrive + one cp.async arrive per producer lane
-                mbar_init(&done[q], kWsConsumers);
-            }
-            fence_mbar_init();
-        }
-        for (int q = threadIdx.x; q < 2 * N; q += blockDim.x)
-            xt[q] = (q < N) ? Tab<Real>::x(N, q) : Tab<Real>::w(N, q - N);
-        __syncthreads();
-
-        // this CTA's chunks: k_m = blockIdx.x + m G
-        const int M = ((int)blockIdx.x < nchunks) ? (nchunks - 1 - (int)blockIdx.x) / G + 1 : 0;
-        auto chunk_el0 = [&](int m) { return ((int)blockIdx.x + m * G) * C; };
-
-        if (warp == kWsConsumers)
-        {
-            // ------------------------------------------------------------ producer
-            auto load = [&](int m)
-            {
-                const int el0 = chunk_el0(m), ne = min(C, a.nel - el0), q = m % S;
-                unsigned char *base = slots + q * L.slot;
-                if (ne == C)
-                {
-                    if (lane == 0)
-                    {
-                        mbar_expect_tx(&full[q], (uint32_t)(L.ub * (has_du ? 2 : 1) + C * 68));
-                        bulk_g2s(base, a.u + (size_t)el0 * ND, (uint32_t)L.ub, &full[q]);
-                        if (has_du)
-                            bulk_g2s(base + L.ub, a.du + (size_t)el0 * ND, (uint32_t)L.ub, &full[q]);
-                        bulk_g2s(base + L.cb, a.corners + 8 * (size_t)el0, (uint32_t)(64 * C), &full[q]);
-                        bulk_g2s(base + L.kb, a.fcode + el0, (uint32_t)(4 * C), &full[q]);
-                    }
-                }
-                else
-                {
-                    // ragged last chunk: plain copies by the warp, then an ordinary arrive
-                    Real *us = reinterpret_cast<Real *>(base), *dus = us + C * ND;
-                    for (int i = lane; i < ne * ND; i += 32)
-                    {
-                        us[i] = a.u[(size_t)el0 * ND + i];
-                        if (has_du)
-                            dus[i] = a.du[(size_t)el0 * ND + i];
-                    }
-                    double *cw = reinterpret_cast<double *>(base + L.cb);
-                    for (int i = lane; i < ne * 8; i += 32)
-                        cw[i] = a.corners[8 * (size_t)el0 + i];
-                    uint32_t *kw = reinterpret_cast<uint32_t *>(base + L.kb);
-                    for (int i = lane; i < ne; i += 32)
-                        kw[i] = a.fcode[el0 + i];
-                    __threadfence_block();
-                    __syncwarp();
-                    if (lane == 0)
-                        mbar_arrive(&full[q]);
-                }
-                // neighbour traces of every interior face node of the chunk: one lane per
-                // (element, side); the table reads of a batch go out together, so a chunk
-                // costs one L2 round trip per batch rather than one per face node
-                if (flags & F_INT)
-                {
-                    Real *halo = reinterpret_cast<Real *>(base + L.hb);
-                    const int limit = a.nel * ND;
-                    constexpr int B = 4; // (element, side) pairs per lane per batch
-                    for (int p0 = 0; p0 < ne * 4; p0 += 32 * B)
-                    {
-                        uint32_t code[B];
-                        int off[B];
-#pragma unroll
-                        for (int b = 0; b < B; ++b)
-                        {
-                            const int pr = p0 + 32 * b + lane, le = pr >> 2, s = pr & 3;
-                            code[b] = 0x80u;
-                            off[b] = -1;
-                            if (pr < ne * 4)
-                            {
-                                code[b] = (__ldg(a.fcode + el0 + le) >> (8 * s)) & 0xffu;
-                                off[b] = __ldg(reinterpret_cast<const int *>(a.fbase + el0 + le) + s);
-                            }
-                        }
-#pragma unroll
-                        for (int b = 0; b < B; ++b)
-                        {
-                            const int pr = p0 + 32 * b + lane, le = pr >> 2, s = pr & 3;
-                            if (code[b] & 0x80u)
-                                continue; // boundary side (or past the chunk): no neighbour
-                            const int stride = partner_stride<N>(code[b]);
-                            if (off[b] < 0 || off[b] + (N - 1) * stride < 0 || off[b] + 3 > limit ||
-                                off[b] + (N - 1) * stride + 3 > limit)
-                            {
-                                atomicOr(a.err, 2u);
-                                continue;
-                            }
-                            Real *dst = halo + 3 * (le * NF + s * N);
-#pragma unroll
-                            for (int k = 0; k < N; ++k)
-                            {
-                                const Real *src = a.u + off[b] + k * stride;
-                                cp_async<sizeof(Real)>(dst + 3 * k, src);
-                                cp_async<sizeof(Real)>(dst + 3 * k + 1, src + 1);
-                                cp_async<sizeof(Real)>(dst + 3 * k + 2, src + 2);
-                            }
-                        }
-                    }
-                }
-                cp_async_mbar_arrive(&full[q]);
-            };
-            for (int m = 0; m < min(S, M); ++m)
-                load(m);
-            int m = 0;
-            for (; m < M; ++m)
-            {
-                const int q = m % S, el0 = chunk_el0(m), ne = min(C, a.nel - el0);
-                // a warp-uniform verdict, so no lane leaves while others go on
-                if (!__all_sync(0xffffffffu, mbar_wait(&done[q], (m / S) & 1)))
-                    break;
-                unsigned char *base = slots + q * L.slot;
-                if (ne == C)
-                {
-                    if (lane == 0)
-                    {
-                        bulk_s2g(a.out + (size_t)el0 * ND, base, (uint32_t)L.ub);
-                        bulk_s2g(a.du + (size_t)el0 * ND, base + L.ub, (uint32_t)L.ub);
-                        bulk_commit();
-                    }
-                }
-                else
-                {
-                    const Real *us = reinterpret_cast<const Real *>(base), *dus = us + C * ND;
-                    for (int i = lane; i < ne * ND; i += 32)
-                    {
-                        a.out[(size_t)el0 * ND + i] = us[i];
-                        a.du[(size_t)el0 * ND + i] = dus[i];
-                    }
-                }
-                if (m + S < M)
-                {
-                    if (lane == 0)
-                        bulk_wait_read(); // the store above has read the slot
-                    __syncwarp();
-                    load(m + S);
-                }
-            }
-            if (m < M)
-            {
-                // a consumer gave up: record it, let the loads already issued land, leave
-                if (lane == 0)
-                {
-                    atomicOr(a.err, 1u);
-                    for (int r = m; r < min(m + S, M); ++r)
-                        mbar_wait(&full[r % S], (r / S) & 1);
-                }
-            }
-            if (lane == 0)
-                bulk_wait_all();
-            return;
-        }
-
-        // ---------------------------------------------------------------- consumers
-        const int cw = warp;
-        const int R = C / (kWsConsumers * EW); // warp-rounds per chunk
-        Real *Rc = reinterpret_cast<Real *>(smem + L.scratch + cw * L.warp_scratch); // [EW][NN][3] column-pass sums
+        const int R = c.chunk / (kWsConsumers * EW); // warp-rounds per chunk
         const int el_l = lane / N, ln = lane - el_l * N; // element of the round, grid line
         const bool lane_on = lane < EW * N;
-        const Real xm = lane_on ? xt[ln] : Real(0), wm = lane_on ? wt[ln] : Real(0);
+        const Real xm = lane_on ? xtab[ln] : Real(0), wm = lane_on ? wtab[ln] : Real(0);
+        Real *us = reinterpret_cast<Real *>(base);
+        Real *dus = us + c.chunk * ND;
+        const Real *halo = reinterpret_cast<const Real *>(base + o.hb);
+        const double *cs = reinterpret_cast<const double *>(base + o.cb);
+        const uint32_t *fks = reinterpret_cast<const uint32_t *>(base + o.kb);
+        double dsum = 0.0, nsum = 0.0;
 
-        for (int m = 0; m < M; ++m)
+        for (int r = 0; r < R; ++r)
         {
-            const int q = m % S, el0 = chunk_el0(m), ne = min(C, a.nel - el0);
-            if (!__all_sync(0xffffffffu, mbar_wait(&full[q], (m / S) & 1)))
-            {
-                if (lane == 0)
-                    atomicOr(a.err, 1u);
-                break;
-            }
-            unsigned char *base = slots + q * L.slot;
-            Real *us = reinterpret_cast<Real *>(base);
-            Real *dus = us + C * ND;
-            const Real *halo = reinterpret_cast<const Real *>(base + L.hb);
-            const double *cs = reinterpret_cast<const double *>(base + L.cb);
-            const uint32_t *fks = reinterpret_cast<const uint32_t *>(base + L.kb);
-
-            for (int r = 0; r < R; ++r)
-            {
                 const int le = (cw * R + r) * EW + el_l; // chunk-local element of this lane
-                const bool act = lane_on && le < ne;
+                const bool act = lane_on && le < c.ne;
                 double2 c01, c23, c45, c67;
                 uint32_t codes = 0;
                 const Real *halo_e = halo + le * NF * 3;
@@ -453,12 +421,12 @@ namespace wdg
                     {
                         const Real *cr = rc + 3 * (i + N * j);
                         Real r0 = ap[i] + cr[0], r1 = au[i] + cr[1], r2 = av[i] + cr[2];
-                        const size_t g = (size_t)(el0 + le) * ND + 3 * (i + N * j);
+                        const size_t g = (size_t)(c.el0 + le) * ND + 3 * (i + N * j);
                         if (EXTRA && (flags & F_FORCE))
                         {
-                            r0 += a.fscale * a.F[g];
-                            r1 += a.fscale * a.F[g + 1];
-                            r2 += a.fscale * a.F[g + 2];
+                            r0 += c.fscale * c.F[g];
+                            r1 += c.fscale * c.F[g + 1];
+                            r2 += c.fscale * c.F[g + 2];
                         }
                         if (flags & F_MINV)
                         {
@@ -467,26 +435,187 @@ namespace wdg
                             r2 *= mv[i];
                         }
                         Real *dn = drow + 3 * i;
-                        const Real d0 = has_du ? a.rk_a * dn[0] + a.dt * r0 : a.dt * r0;
-                        const Real d1 = has_du ? a.rk_a * dn[1] + a.dt * r1 : a.dt * r1;
-                        const Real d2 = has_du ? a.rk_a * dn[2] + a.dt * r2 : a.dt * r2;
-                        const Real u0 = q0[i] + a.rk_b * d0, u1 = q1[i] + a.rk_b * d1, u2 = q2[i] + a.rk_b * d2;
+                        const Real d0 = has_du ? c.rk_a * dn[0] + c.dt * r0 : c.dt * r0;
+                        const Real d1 = has_du ? c.rk_a * dn[1] + c.dt * r1 : c.dt * r1;
+                        const Real d2 = has_du ? c.rk_a * dn[2] + c.dt * r2 : c.dt * r2;
+                        Real uo[3] = {q0[i] + c.rk_b * d0, q1[i] + c.rk_b * d1, q2[i] + c.rk_b * d2};
                         dn[0] = d0;
                         dn[1] = d1;
                         dn[2] = d2;
-                        row[3 * i] = u0;
-                        row[3 * i + 1] = u1;
-                        row[3 * i + 2] = u2;
-                        if (EXTRA && (flags & F_FILTER))
+                        if (BATCH && c.pend)
                         {
-                            a.acc[g] += a.acc_c * (double)u0;
-                            a.acc[g + 1] += a.acc_c * (double)u1;
-                            a.acc[g + 2] += a.acc_c * (double)u2;
+                            // last step of a period: the filter's last term completes the period's
+                            // result; the state and the filter restart from the new iterate
+#pragma unroll
+                            for (int f = 0; f < 3; ++f)
+                            {
+                                const double fin = c.acc[g + f] + c.acc_c * (double)uo[f];
+                                nsum += fin * fin;
+                                double w0;
+                                if (c.pend == 1)
+                                {
+                                    const double dw = fin - c.W[g + f];
+                                    dsum += dw * dw;
+                                    c.W[g + f] = fin;
+                                    w0 = fin;
+                                }
+                                else
+                                    w0 = c.W[g + f];
+                                c.acc[g + f] = c.c0 * w0;
+                                uo[f] = (Real)w0;
+                            }
                         }
+                        else if (EXTRA && (flags & F_FILTER))
+                        {
+                            c.acc[g] += c.acc_c * (double)uo[0];
+                            c.acc[g + 1] += c.acc_c * (double)uo[1];
+                            c.acc[g + 2] += c.acc_c * (double)uo[2];
+                        }
+                        row[3 * i] = uo[0];
+                        row[3 * i + 1] = uo[1];
+                        row[3 * i + 2] = uo[2];
                     }
                 }
                 __syncwarp(); // the scratch is reused by the next round
+        }
+        if (BATCH && c.pend)
+        {
+#pragma unroll
+            for (int sh = 16; sh > 0; sh >>= 1)
+            {
+                dsum += __shfl_xor_sync(0xffffffffu, dsum, sh);
+                nsum += __shfl_xor_sync(0xffffffffu, nsum, sh);
             }
+            if (lane == 0)
+            {
+                c.part[2 * cw] = dsum;
+                c.part[2 * cw + 1] = nsum;
+            }
+        }
+    }
+
+    template <typename Real>
+    __host__ __device__ inline WsLayout ws_layout(int n, int chunk, int stages)
+    {
+        WsLayout L;
+        const int nn = n * n, ew = 32 / n;
+        L.slot = ws_slot<Real>(n, chunk).bytes;
+        L.tab = 128;
+        L.slots = (L.tab + 2 * n * (int)sizeof(Real) + 127) & ~127;
+        L.scratch = L.slots + stages * L.slot;
+        L.warp_scratch = ((ew * 3 * nn * (int)sizeof(Real)) + 15) & ~15;
+        L.total = L.scratch + kWsConsumers * L.warp_scratch;
+        return L;
+    }
+
+    template <int N, typename Real, bool EXTRA>
+    __global__ void __launch_bounds__(kWsThreads, 2) ws_stage_kernel(const StageArgs<Real> a)
+    {
+        const int C = a.chunk, S = a.ring, G = gridDim.x;
+        const int nchunks = (a.nel + C - 1) / C;
+        const WsLayout L = ws_layout<Real>(N, C, S);
+
+        extern __shared__ __align__(128) unsigned char smem[];
+        uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+        uint64_t *done = full + S;
+        Real *xt = reinterpret_cast<Real *>(smem + L.tab); // GLL nodes, then weights
+        Real *wt = xt + N;
+        unsigned char *slots = smem + L.slots;
+
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (threadIdx.x == 0)
+        {
+            for (int q = 0; q < S; ++q)
+            {
+                mbar_init(&full[q], 1 + 32); // the bulk-copy arrive + one cp.async arrive per producer lane
+                mbar_init(&done[q], kWsConsumers);
+            }
+            fence_mbar_init();
+        }
+        for (int q = threadIdx.x; q < 2 * N; q += blockDim.x)
+            xt[q] = (q < N) ? Tab<Real>::x(N, q) : Tab<Real>::w(N, q - N);
+        __syncthreads();
+
+        // this CTA's chunks: k_m = blockIdx.x + m G
+        const int M = ((int)blockIdx.x < nchunks) ? (nchunks - 1 - (int)blockIdx.x) / G + 1 : 0;
+        WsChunk<Real> c{};
+        c.u = a.u;
+        c.out = a.out;
+        c.du = a.du;
+        c.F = a.F;
+        c.acc = a.acc;
+        c.corners = a.corners;
+        c.fbase = a.fbase;
+        c.fcode = a.fcode;
+        c.err = a.err;
+        c.nel = a.nel;
+        c.chunk = C;
+        c.flags = a.flags;
+        c.rk_a = a.rk_a;
+        c.rk_b = a.rk_b;
+        c.dt = a.dt;
+        c.fscale = a.fscale;
+        c.acc_c = a.acc_c;
+        auto at = [&](int m)
+        {
+            c.el0 = ((int)blockIdx.x + m * G) * C;
+            c.ne = min(C, a.nel - c.el0);
+        };
+
+        if (warp == kWsConsumers)
+        {
+            // ------------------------------------------------------------ producer
+            for (int m = 0; m < min(S, M); ++m)
+            {
+                at(m);
+                ws_load<N, Real>(c, slots + (m % S) * L.slot, &full[m % S], lane);
+            }
+            int m = 0;
+            for (; m < M; ++m)
+            {
+                const int q = m % S;
+                // a warp-uniform verdict, so no lane leaves while others go on
+                if (!__all_sync(0xffffffffu, mbar_wait(&done[q], (m / S) & 1)))
+                    break;
+                at(m);
+                ws_store<N, Real>(c, slots + q * L.slot, lane);
+                if (m + S < M)
+                {
+                    if (lane == 0)
+                        bulk_wait_read(); // the store above has read the slot
+                    __syncwarp();
+                    at(m + S);
+                    ws_load<N, Real>(c, slots + q * L.slot, &full[q], lane);
+                }
+            }
+            if (m < M)
+            {
+                // a consumer gave up: record it, let the loads already issued land, leave
+                if (lane == 0)
+                {
+                    atomicOr(a.err, 1u);
+                    for (int r = m; r < min(m + S, M); ++r)
+                        mbar_wait(&full[r % S], (r / S) & 1);
+                }
+            }
+            if (lane == 0)
+                bulk_wait_all();
+            return;
+        }
+
+        // ---------------------------------------------------------------- consumers
+        Real *Rc = reinterpret_cast<Real *>(smem + L.scratch + warp * L.warp_scratch); // [EW][NN][3] column sums
+        for (int m = 0; m < M; ++m)
+        {
+            const int q = m % S;
+            if (!__all_sync(0xffffffffu, mbar_wait(&full[q], (m / S) & 1)))
+            {
+                if (lane == 0)
+                    atomicOr(a.err, 1u);
+                break;
+            }
+            at(m);
+            ws_consume<N, Real, EXTRA, false>(c, slots + q * L.slot, Rc, xt, wt, warp, lane);
             // results are in the slot: hand them to the async proxy, then release the slot
             fence_async_smem();
             __syncwarp();

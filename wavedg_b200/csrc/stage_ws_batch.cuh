@@ -1,0 +1,349 @@
+// Batched WaveHoltz: one persistent launch per RK stage over a work list of
+// (solve, chunk) items of up to kMaxBatch independent solves (included by kernels.cu).
+//
+// Every solve has its own mesh, degree, frequency, period length nt and state; the
+// work list holds its chunks back to back (items item0 .. item0 + nchunks - 1).  A CTA
+// walks items blockIdx.x, blockIdx.x + G, ... skipping solves that have finished, and
+// runs the same producer / consumer pair as the single-solve kernel on each item, with
+// the degree dispatched per item (warp-uniform).  Per-solve stage scalars come from the
+// solve's own step counter k:  forcing scale -sin(omega (k + c_s) dt) / omega, filter
+// weight dt K((k + 1) dt) (halved on the last step of a period).
+//
+// Each iteration is one forced period from the current iterate W (by linearity of the
+// scheme this equals S W + pi0 of the reference's loop): the state starts at W, the
+// filter at 0.5 dt K(0) W.  On the last stage of a period the consumer epilogue
+// finishes the filter, writes W' and restarts state and filter from it, and leaves
+// per-chunk partial sums of (W' - W)^2 and W'^2; whb_step_end_kernel reduces them in a
+// fixed order and updates the solve's residual and status.  A warm-started solve first
+// runs one forced period from zero only to obtain |pi0|, the residual's scale.
+namespace wdg
+{
+    __constant__ double c_rk4a[5], c_rk4b[5], c_rk4c[5];
+
+    // node/weight tables of every degree in shared memory: degree n at offset sum_{m<n} 2m
+    constexpr int kWhbTab = 88; // sum_{n=2}^{9} 2 n
+
+    __host__ __device__ inline int whb_slots_offset(int real_size)
+    {
+        return (128 + kWhbTab * real_size + 3 * kMaxBatch * 4 + 127) & ~127;
+    }
+
+    // degree-dispatched calls; n is warp-uniform (one item at a time per warp)
+#define WDG_WHB_DISPATCH(n, CALL)                                                              \
+    switch (n)                                                                                 \
+    {                                                                                          \
+    case 2: { constexpr int NV = 2; CALL; } break;                                             \
+    case 3: { constexpr int NV = 3; CALL; } break;                                             \
+    case 4: { constexpr int NV = 4; CALL; } break;                                             \
+    case 5: { constexpr int NV = 5; CALL; } break;                                             \
+    case 6: { constexpr int NV = 6; CALL; } break;                                             \
+    case 7: { constexpr int NV = 7; CALL; } break;                                             \
+    case 8: { constexpr int NV = 8; CALL; } break;                                             \
+    default: { constexpr int NV = 9; CALL; } break;                                            \
+    }
+
+    template <typename Real>
+    __global__ void __launch_bounds__(kWsThreads, 2) whb_stage_kernel(const __grid_constant__ WhbArgs<Real> a)
+    {
+        const int S = a.ring, G = gridDim.x, st = a.stage;
+        extern __shared__ __align__(128) unsigned char smem[];
+        uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+        uint64_t *done = full + S;
+        Real *tab = reinterpret_cast<Real *>(smem + 128);
+        int *act = reinterpret_cast<int *>(smem + 128 + kWhbTab * sizeof(Real)); // per solve: k, phase, active
+        unsigned char *slots = smem + whb_slots_offset((int)sizeof(Real));
+        unsigned char *scratch = slots + S * a.slot_bytes;
+
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (threadIdx.x == 0)
+        {
+            for (int q = 0; q < S; ++q)
+            {
+                mbar_init(&full[q], 1 + 32); // the bulk-copy arrive + one cp.async arrive per producer lane
+                mbar_init(&done[q], kWsConsumers);
+            }
+            fence_mbar_init();
+        }
+        for (int q = threadIdx.x; q < kWhbTab; q += blockDim.x)
+        {
+            int n = 2, off = 0;
+            while (q >= off + 2 * n)
+            {
+                off += 2 * n;
+                ++n;
+            }
+            const int r = q - off;
+            tab[q] = (r < n) ? Tab<Real>::x(n, r) : Tab<Real>::w(n, r - n);
+        }
+        for (int q = threadIdx.x; q < a.nsolves; q += blockDim.x)
+        {
+            act[3 * q] = a.state[q].k;
+            act[3 * q + 1] = a.state[q].phase;
+            act[3 * q + 2] = a.state[q].active;
+        }
+        __syncthreads();
+
+        // item -> solve: the solves' items are contiguous and ascending
+        auto solve_of = [&](int item)
+        {
+            int lo = 0, hi = a.nsolves - 1;
+            while (lo < hi)
+            {
+                const int mid = (lo + hi + 1) >> 1;
+                if (a.s[mid].item0 <= item)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            return lo;
+        };
+        // the next item of this CTA at or after k whose solve is still running; producer and
+        // consumers walk the same sequence, so their ring positions agree
+        auto advance = [&](int k)
+        {
+            while (k < a.nitems && !act[3 * solve_of(k) + 2])
+                k += G;
+            return k;
+        };
+        WsChunk<Real> c{};
+        int cur_n = 2;
+        auto build = [&](int item)
+        {
+            const int si = solve_of(item);
+            const WhbSolve<Real> &P = a.s[si];
+            const int ci = item - P.item0;
+            const int k = act[3 * si], phase = act[3 * si + 1];
+            // the RK4 buffer rotation A -> B -> C -> B -> C -> A
+            const int src = (st == 0) ? 0 : (st % 2 == 1) ? 1 : 2;
+            const int dst = (st == 4) ? 0 : (st % 2 == 0) ? 1 : 2;
+            cur_n = P.n;
+            c.u = P.buf[src];
+            c.out = P.buf[dst];
+            c.du = P.du;
+            c.F = P.F;
+            c.acc = P.acc;
+            c.corners = P.corners;
+            c.fbase = P.fbase;
+            c.fcode = P.fcode;
+            c.err = a.err;
+            c.nel = P.nel;
+            c.chunk = P.chunk;
+            c.el0 = ci * P.chunk;
+            c.ne = min(P.chunk, P.nel - c.el0);
+            c.flags = F_ALL | F_FORCE | (st > 0 ? F_READ_DU : 0) | (st == 4 ? F_FILTER : 0);
+            c.rk_a = (Real)c_rk4a[st];
+            c.rk_b = (Real)c_rk4b[st];
+            c.dt = (Real)P.dt;
+            // forcing F s(t), s(t) = -sin(omega t) / omega at the stage time (WaveHoltz.cpp:57-68)
+            const double ts = (k + c_rk4c[st]) * P.dt;
+            c.fscale = (Real)(-sin(P.omega * ts) / P.omega);
+            // filter weight of the step's end: dt K(t), halved on the period's last step
+            const bool last = (k + 1 == P.nt);
+            const double t1 = (k + 1) * P.dt;
+            c.acc_c = (st == 4) ? (last ? 0.5 : 1.0) * P.dt * (P.omega / M_PI * (cos(P.omega * t1) - 0.25)) : 0.0;
+            c.pend = (st == 4 && last) ? (phase == 0 ? 2 : 1) : 0;
+            c.W = P.W;
+            c.c0 = P.c0;
+            c.part = P.part + (size_t)ci * kWsConsumers * 2;
+        };
+
+        if (warp == kWsConsumers)
+        {
+            // ------------------------------------------------------------ producer
+            int kl = advance((int)blockIdx.x), nl = 0; // next item to load, loads issued
+            for (; nl < S && kl < a.nitems; ++nl)
+            {
+                build(kl);
+                WDG_WHB_DISPATCH(cur_n, (ws_load<NV, Real>(c, slots + (nl % S) * a.slot_bytes, &full[nl % S], lane)));
+                kl = advance(kl + G);
+            }
+            int ks = advance((int)blockIdx.x), m = 0; // next item to store, stores done
+            bool ok = true;
+            for (; ks < a.nitems; ++m)
+            {
+                const int q = m % S;
+                if (!__all_sync(0xffffffffu, mbar_wait(&done[q], (m / S) & 1)))
+                {
+                    ok = false;
+                    break;
+                }
+                build(ks);
+                WDG_WHB_DISPATCH(cur_n, (ws_store<NV, Real>(c, slots + q * a.slot_bytes, lane)));
+                ks = advance(ks + G);
+                if (kl < a.nitems)
+                {
+                    if (lane == 0)
+                        bulk_wait_read(); // the store above has read the slot
+                    __syncwarp();
+                    build(kl);
+                    WDG_WHB_DISPATCH(cur_n, (ws_load<NV, Real>(c, slots + q * a.slot_bytes, &full[q], lane)));
+                    kl = advance(kl + G);
+                    ++nl;
+                }
+            }
+            if (!ok && lane == 0)
+            {
+                // a consumer gave up: record it, let the loads already issued land, leave
+                atomicOr(a.err, 1u);
+                for (int r = m; r < nl; ++r)
+                    mbar_wait(&full[r % S], (r / S) & 1);
+            }
+            if (lane == 0)
+                bulk_wait_all();
+            return;
+        }
+
+        // ---------------------------------------------------------------- consumers
+        Real *Rc = reinterpret_cast<Real *>(scratch + warp * a.warp_scratch);
+        int kc = advance((int)blockIdx.x);
+        for (int m = 0; kc < a.nitems; ++m)
+        {
+            const int q = m % S;
+            if (!__all_sync(0xffffffffu, mbar_wait(&full[q], (m / S) & 1)))
+            {
+                if (lane == 0)
+                    atomicOr(a.err, 1u);
+                break;
+            }
+            build(kc);
+            int toff = 0;
+            for (int n = 2; n < cur_n; ++n)
+                toff += 2 * n;
+            WDG_WHB_DISPATCH(cur_n, (ws_consume<NV, Real, true, true>(c, slots + q * a.slot_bytes, Rc, tab + toff,
+                                                                      tab + toff + NV, warp, lane)));
+            // results are in the slot: hand them to the async proxy, then release the slot
+            fence_async_smem();
+            __syncwarp();
+            if (lane == 0)
+                mbar_arrive(&done[q]);
+            kc = advance(kc + G);
+        }
+    }
+#undef WDG_WHB_DISPATCH
+
+    // After the fifth stage of every step: advance each running solve's step counter; at the
+    // end of a period reduce its partial sums in a fixed order and update residual and status
+    // (examples/waveholtz2d.cpp:165-185: ||W - W_prev|| / ||pi0|| against tol, maxit).
+    __global__ void whb_step_end_kernel(WhbState *state, int nsolves)
+    {
+        const int s = blockIdx.x;
+        if (s >= nsolves)
+            return;
+        WhbState &P = state[s];
+        if (!P.active)
+            return;
+        const int k = P.k + 1;
+        if (k < P.nt)
+        {
+            __syncthreads();
+            if (threadIdx.x == 0)
+                P.k = k;
+            return;
+        }
+        __shared__ double sd[256], sn[256];
+        double d = 0.0, nrm = 0.0;
+        for (int i = threadIdx.x; i < P.nparts; i += blockDim.x)
+        {
+            d += P.part[2 * i];
+            nrm += P.part[2 * i + 1];
+        }
+        sd[threadIdx.x] = d;
+        sn[threadIdx.x] = nrm;
+        __syncthreads();
+        for (int h = blockDim.x / 2; h > 0; h >>= 1)
+        {
+            if ((int)threadIdx.x < h)
+            {
+                sd[threadIdx.x] += sd[threadIdx.x + h];
+                sn[threadIdx.x] += sn[threadIdx.x + h];
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x != 0)
+            return;
+        P.k = 0;
+        if (P.phase == 0)
+        {
+            P.pi0sq = sn[0];
+            P.phase = 1;
+            return;
+        }
+        if (P.iter == 0 && P.zero_start)
+            P.pi0sq = sn[0]; // the first period from zero is pi0 itself
+        const double scale = P.pi0sq > 0.0 ? sqrt(P.pi0sq) : 1.0;
+        P.residual = sqrt(sd[0]) / scale;
+        P.iter += 1;
+        if (P.residual < P.best)
+        {
+            P.best = P.residual;
+            P.stall = 0;
+        }
+        else
+            P.stall += 1;
+        if (P.residual < P.tol)
+        {
+            P.active = 0;
+            P.status = 0;
+        }
+        else if (P.iter >= P.maxit)
+        {
+            P.active = 0;
+            P.status = 1;
+        }
+        else if (P.stall_limit > 0 && P.stall >= P.stall_limit)
+        {
+            P.active = 0;
+            P.status = 2;
+        }
+    }
+
+    int whb_smem_bytes(int slot_bytes, int warp_scratch, int ring, bool fp32)
+    {
+        return whb_slots_offset(fp32 ? 4 : 8) + ring * slot_bytes + kWsConsumers * warp_scratch;
+    }
+
+    template <typename Real>
+    cudaError_t whb_occupancy(size_t smem, int *grid)
+    {
+        int dev = 0, per_sm = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaError_t e = cudaFuncSetAttribute(whb_stage_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             227 * 1024);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, whb_stage_kernel<Real>, kWsThreads, smem);
+        if (e == cudaSuccess)
+            e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        *grid = std::max(1, per_sm) * sms;
+        return e;
+    }
+    template <typename Real>
+    cudaError_t launch_whb_stage(const WhbArgs<Real> &a, int grid, size_t smem, cudaStream_t s)
+    {
+        whb_stage_kernel<Real><<<grid, kWsThreads, smem, s>>>(a);
+        return cudaGetLastError();
+    }
+    cudaError_t launch_whb_step_end(WhbState *state, int nsolves, cudaStream_t s)
+    {
+        whb_step_end_kernel<<<nsolves, 256, 0, s>>>(state, nsolves);
+        return cudaGetLastError();
+    }
+    int upload_rk4_tables(int device)
+    {
+        static std::mutex mu;
+        static uint64_t done = 0;
+        std::lock_guard<std::mutex> lock(mu);
+        if (device < 0 || device >= 64)
+            return fail(WDG_ERR_ARG, "device ordinal out of range");
+        if (done & (1ull << device))
+            return WDG_OK;
+        WDG_CUDA(cudaMemcpyToSymbol(c_rk4a, rk4a, sizeof(double) * 5));
+        WDG_CUDA(cudaMemcpyToSymbol(c_rk4b, rk4b, sizeof(double) * 5));
+        WDG_CUDA(cudaMemcpyToSymbol(c_rk4c, rk4c, sizeof(double) * 5));
+        done |= (1ull << device);
+        return WDG_OK;
+    }
+    template cudaError_t launch_whb_stage<double>(const WhbArgs<double> &, int, size_t, cudaStream_t);
+    template cudaError_t launch_whb_stage<float>(const WhbArgs<float> &, int, size_t, cudaStream_t);
+    template cudaError_t whb_occupancy<double>(size_t, int *);
+    template cudaError_t whb_occupancy<float>(size_t, int *);
+} // namespace wdg

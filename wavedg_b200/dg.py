@@ -560,6 +560,77 @@ class WaveHoltz:
         return W, it.value, res.value
 
 
+class WaveHoltzBatch:
+    """Many independent WaveHoltz solves advanced together (wdg_whbatch_*): each solve has its
+    own WaveSystem (mesh, degree; all of one precision and device) and its own omega.  One
+    persistent kernel launch per RK stage covers every running solve."""
+
+    STATUS = {0: "converged", 1: "iteration limit", 2: "stalled", -1: "running"}
+
+    def __init__(self, systems, omegas):
+        self.systems = list(systems)
+        n = len(self.systems)
+        om = np.ascontiguousarray(np.broadcast_to(np.asarray(omegas, dtype=np.float64), (n,)))
+        hs = (C.c_void_p * n)(*[s._h for s in self.systems])
+        h = C.c_void_p()
+        check(lib().wdg_whbatch_create(n, hs, C.c_void_p(om.ctypes.data), C.byref(h)), "WaveHoltzBatch")
+        self._h = h
+        self.omegas = om
+        self.n = n
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().wdg_whbatch_destroy(h)
+            self._h = None
+
+    def params(self, solve: int):
+        T, dt, nt = C.c_double(), C.c_double(), C.c_int()
+        check(lib().wdg_whbatch_params(self._h, int(solve), C.byref(T), C.byref(dt), C.byref(nt)))
+        return T.value, dt.value, nt.value
+
+    def set_launch(self, rounds: int, ring: int) -> None:
+        check(lib().wdg_whbatch_set_launch(self._h, int(rounds), int(ring)), "WaveHoltzBatch.set_launch")
+
+    def launch_config(self) -> dict:
+        r, g, grid = C.c_int(), C.c_int(), C.c_int()
+        check(lib().wdg_whbatch_get_launch(self._h, C.byref(r), C.byref(g), C.byref(grid)))
+        return {"rounds": r.value, "ring": g.value, "grid": grid.value}
+
+    def autotune(self, steps: int = 64) -> float:
+        ms = C.c_float()
+        check(lib().wdg_whbatch_autotune(self._h, int(steps), C.byref(ms)), "WaveHoltzBatch.autotune")
+        return ms.value
+
+    def solve(self, F, tol: float = 1e-6, maxit: int = 1000, W=None, warm=None, stall_limit: int = 0):
+        """Solve every problem.  F, W: one float64 array per solve (numpy or CUDA tensors);
+        W (optional) holds initial guesses where warm[s] is true and receives the iterates.
+        Returns (W, iters, residuals, status)."""
+        n = self.n
+        if len(F) != n:
+            raise ValueError("one forcing per solve")
+        if W is None:
+            W = [np.zeros(s.ndof) for s in self.systems]
+        keep = []
+        fp, wp = (C.c_void_p * n)(), (C.c_void_p * n)()
+        for s in range(n):
+            pf, kf = _ptr(F[s], name="F")
+            pw, kw = _ptr(W[s], True, "W")
+            keep += [kf, kw]
+            fp[s], wp[s] = pf, pw
+        wm = None
+        if warm is not None:
+            wm = np.ascontiguousarray(np.broadcast_to(np.asarray(warm, dtype=np.int32), (n,)))
+        it = np.zeros(n, dtype=np.int32)
+        res = np.zeros(n)
+        stt = np.zeros(n, dtype=np.int32)
+        check(lib().wdg_whbatch_solve(self._h, fp, float(tol), int(maxit), int(stall_limit), wp,
+                                      None if wm is None else C.c_void_p(wm.ctypes.data),
+                                      C.c_void_p(it.ctypes.data), C.c_void_p(res.ctypes.data),
+                                      C.c_void_p(stt.ctypes.data)), "WaveHoltzBatch.solve")
+        return W, it, res, stt
+
+
 def norm(x, system: Discretisation) -> float:
     return system.norm(x)
 
