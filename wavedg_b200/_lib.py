@@ -102,6 +102,21 @@ SIGNATURES = {
     "wdg_whbatch_get_launch": ([_v, _ip, _ip, _ip], _i),
     "wdg_whbatch_autotune": ([_v, _i, C.POINTER(C.c_float)], _i),
     "wdg_whbatch_solve": ([_v, _v, _d, _i, _i, _v, _v, _v, _v, _v], _i),
+    # learned warm start (include/wdg_fno.h)
+    "wdg_fno_gemm": ([_v, _v, _v, _i, _i, _i, _ll, _ll, _ll, _ll, _ll, _ll, _i, _i, _i, C.c_float, C.c_float, _i,
+                      _v], _i),
+    "wdg_fno_dft_y": ([_v, _v, _v, _v, _v, _i, _i, _i, _i, _i, C.c_float, _v], _i),
+    "wdg_fno_mix": ([_v, _v, _v, _i, _i, _i, _i, _v], _i),
+    "wdg_fno_mix_bwd": ([_v, _v, _v, _v, _v, _i, _i, _i, _i, _i, _v], _i),
+    "wdg_fno_bias_act": ([_v, _v, _v, _v, _i, _i, _ll, _i, _v], _i),
+    "wdg_fno_act_bwd": ([_v, _v, _v, _v, _ll, _i, _v], _i),
+    "wdg_fno_bias_grad": ([_v, _v, _i, _i, _ll, _i, _v], _i),
+    "wdg_fno_to_bf16": ([_v, _v, _ll, _v], _i),
+    "wdg_fno_mse": ([_v, _v, _v, _v, _ll, C.c_float, _v], _i),
+    "wdg_fno_adam": ([_v, _v, _v, _v, _ll, C.c_float, C.c_float, C.c_float, C.c_float, _i, C.c_float, _v], _i),
+    "wdg_fno_inputs": ([_v, _i, _d, _d, _d, _d, _v], _i),
+    "wdg_fno_nodes_to_grid": ([_v, _v, _i, _i, _v, _v, _i, C.c_float, _v], _i),
+    "wdg_fno_grid_to_nodes": ([_v, _v, _i, _i, _v, _i, _d, _v], _i),
 }
 
 _lib = None
