@@ -260,6 +260,7 @@ def run_ours(args, rank, world, local_rank):
 
     if not args.no_extras and not args.no_waveholtz and args.precision == "fp64":
         extra["waveholtz_c3"] = waveholtz_c3(local_rank)
+        extra["waveholtz_batched"] = waveholtz_batched(local_rank)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -295,9 +296,12 @@ def run_ours(args, rank, world, local_rank):
 def waveholtz_c3(device: int, seed: int = 3) -> dict:
     """One WaveHoltz Helmholtz solve on 128 x 128 uniform quads of [-1, 1]^2, P = 4, outflow
     boundary, omega = 20, f = omega^2 exp(-|x - x0|^2 / (2 0.05^2)) with x0 seeded in
-    [-0.5, 0.5]^2, from a zero guess to 1e-6 relative residual: FP64 stepping, then FP32 stepping
-    with the FP64 filter / residual.  Wall time of the solve call (host-synchronous: it reads the
-    residual back every iteration), GPU synchronised on both sides."""
+    [-0.5, 0.5]^2, from a zero guess to 1e-6 relative residual.
+      fp64        FP64 stepping throughout (the plain method);
+      fp32_fp64   FP32 stepping (FP64 filter / residual) to 3e-6, where FP32 rounding starts to
+                  floor the residual, then FP64 iterations from that iterate to 1e-6 -- the
+                  plain iteration decides convergence.
+    Wall time of the solve calls (host-synchronous: they read the residual every iteration)."""
     import torch
 
     import wavedg_b200 as W
@@ -307,27 +311,102 @@ def waveholtz_c3(device: int, seed: int = 3) -> dict:
     mesh = W.Mesh2D.uniform_rect(128, -1.0, 1.0, 128, -1.0, 1.0)
     basis = W.QuadratureRule.quadrature_rule(5, W.QuadratureRule.GaussLobatto)
     bc = np.zeros(mesh.n_edges(1), dtype=np.int32)
-    out, sols = {}, {}
-    for prec in ("fp64", "fp32"):
-        sys_ = W.WaveSystem(mesh, basis, bc, precision=prec, device=device)
-        wh = W.WaveHoltz(omega, mesh, basis, bc, True, precision=prec, system=sys_)
-        F = torch.zeros(sys_.ndof, dtype=torch.float64, device="cuda")
-        sys_.load_gaussians([x0], [0.05], [omega ** 2], 1.0, 0, False, out=F)
-        Wd = torch.zeros_like(F)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        _, it, res = wh.solve(F, 1e-6, 1000, W=Wd)
-        torch.cuda.synchronize()
-        el = time.perf_counter() - t0
-        sols[prec] = Wd
-        out[prec] = {"iterations": it, "residual": res, "seconds": el, "solves_per_s": 1.0 / el,
-                     "steps_per_period": wh.nt, "dt": wh.dt,
-                     "dof_stage_per_s": sys_.ndof * 5 * wh.nt * (it + 1) / el}
-    d = (sols["fp32"] - sols["fp64"]).norm().item() / sols["fp64"].norm().item()
-    out["fp32"]["rel_diff_vs_fp64_gpu"] = d
+    s64 = W.WaveSystem(mesh, basis, bc, precision="fp64", device=device)
+    s32 = W.WaveSystem(mesh, basis, bc, precision="fp32", device=device)
+    wh64 = W.WaveHoltz(omega, mesh, basis, bc, True, system=s64)
+    wh32 = W.WaveHoltz(omega, mesh, basis, bc, True, precision="fp32", system=s32)
+    F = torch.zeros(s64.ndof, dtype=torch.float64, device="cuda")
+    s64.load_gaussians([x0], [0.05], [omega ** 2], 1.0, 0, False, out=F)
+    out = {}
+    W64 = torch.zeros_like(F)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _, it, res = wh64.solve(F, 1e-6, 1000, W=W64)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    out["fp64"] = {"iterations": it, "residual": res, "seconds": el, "solves_per_s": 1.0 / el,
+                   "steps_per_period": wh64.nt, "dt": wh64.dt,
+                   "dof_stage_per_s": s64.ndof * 5 * wh64.nt * (it + 1) / el}
+    Wm = torch.zeros_like(F)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _, it32, res32 = wh32.solve(F, 3e-6, 1000, W=Wm)
+    _, it64, res64 = wh64.solve(F, 1e-6, 1000, W=Wm)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    out["fp32_fp64"] = {"fp32_iterations": it32, "fp32_residual": res32, "fp64_iterations": it64,
+                        "residual": res64, "seconds": el, "solves_per_s": 1.0 / el,
+                        "rel_diff_vs_fp64": (Wm - W64).norm().item() / W64.norm().item()}
     out["workload"] = "waveholtz_128x128_P4_omega20_outflow_tol1e-6"
     out["x0"] = [float(x0[0]), float(x0[1])]
     return out
+
+
+def waveholtz_batched(device: int, count: int = 16, seed: int = 4) -> dict:
+    """Batched WaveHoltz on a draw from the batched-solve distribution at a quarter of its mesh
+    sizes (n in {16, 24, 32, 48, 64} elements per side instead of {64, ..., 256}): omega uniform in
+    [10, 40], P in {3, 4, 6}, 1-4 Gaussian sources (sigma 0.05, centres in [-0.8, 0.8]^2, N(0, 1)
+    amplitudes), outflow, tolerance 1e-6.  The same problems solved (a) one at a time with plain
+    FP64 WaveHoltz and (b) as one batch: FP32 stepping with FP64 filter / residual until the
+    FP32 floor (3e-6 or a 3-iteration stall), then an FP64 batch from those iterates to 1e-6."""
+    import torch
+
+    import wavedg_b200 as W
+
+    rng = np.random.default_rng(seed)
+    probs = []
+    for _ in range(count):
+        n = int(rng.choice([16, 24, 32, 48, 64]))
+        P = int(rng.choice([3, 4, 6]))
+        om = float(rng.uniform(10.0, 40.0))
+        k = int(rng.integers(1, 5))
+        probs.append((n, P, om, rng.uniform(-0.8, 0.8, size=(k, 2)), rng.standard_normal(k)))
+    s64, s32, Fs, whs = [], [], [], []
+    for (n, P, om, cs, amps) in probs:
+        mesh = W.Mesh2D.uniform_rect(n, -1.0, 1.0, n, -1.0, 1.0)
+        basis = W.QuadratureRule.quadrature_rule(P + 1, W.QuadratureRule.GaussLobatto)
+        bc = np.zeros(mesh.n_edges(1), dtype=np.int32)
+        a = W.WaveSystem(mesh, basis, bc, precision="fp64", device=device)
+        s64.append(a)
+        s32.append(W.WaveSystem(mesh, basis, bc, precision="fp32", device=device))
+        F = torch.zeros(a.ndof, dtype=torch.float64, device="cuda")
+        a.load_gaussians(cs, [0.05] * len(amps), amps * om ** 2, 1.0, 0, False, out=F)
+        Fs.append(F)
+        whs.append(W.WaveHoltz(om, mesh, basis, bc, True, system=a))
+    oms = [p[2] for p in probs]
+    ndof = sum(a.ndof for a in s64)
+    # (a) plain FP64, one solve at a time
+    Wp, itp = [], []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for F, wh in zip(Fs, whs):
+        Wx = torch.zeros_like(F)
+        _, it, _ = wh.solve(F, 1e-6, 2000, W=Wx)
+        Wp.append(Wx)
+        itp.append(it)
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    # (b) batched FP32 then FP64 finish
+    b32 = W.WaveHoltzBatch(s32, oms)
+    b64 = W.WaveHoltzBatch(s64, oms)
+    b32.autotune(64)
+    Wb = [torch.zeros_like(F) for F in Fs]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _, it32, _, _ = b32.solve(Fs, 3e-6, 2000, W=Wb, stall_limit=3)
+    _, it64, r64, st = b64.solve(Fs, 1e-6, 2000, W=Wb, warm=[1] * count)
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    err = max((Wb[i] - Wp[i]).norm().item() / Wp[i].norm().item() for i in range(count))
+    return {"workload": f"waveholtz_batch_{count}_solves_n16-64_P3-6_omega10-40_tol1e-6",
+            "solves": count, "total_dof": ndof,
+            "plain_fp64": {"seconds": t_plain, "solves_per_s": count / t_plain, "iterations_mean": float(np.mean(itp))},
+            "batched_fp32_fp64": {"seconds": t_batch, "solves_per_s": count / t_batch,
+                                  "fp32_iterations_mean": float(np.mean(it32)),
+                                  "fp64_iterations_mean": float(np.mean(it64)),
+                                  "all_converged": bool((st == 0).all() and (r64 < 1e-6).all()),
+                                  "max_rel_diff_vs_plain": err, "launch": b32.launch_config()},
+            "speedup": t_plain / t_batch}
 
 
 # ----------------------------------------------------------- CPU side

@@ -203,8 +203,9 @@ int wdg_waveholtz_solve(wdg_waveholtz *wh, const double *F, double tol, int maxi
 
 /* ------------------------------------------------------ batched WaveHoltz */
 /* Up to 64 independent WaveHoltz solves, each on its own discretisation (mesh, degree) with
- * its own omega, advanced together: one persistent kernel launch per RK stage over a work
- * list of (solve, chunk of elements), blocks of steps replayed as a CUDA graph.  Per solve,
+ * its own omega, advanced together: per RK stage one persistent kernel launch per degree
+ * over a work list of (solve, chunk of elements), the degrees' launches concurrent, blocks
+ * of steps replayed as a CUDA graph.  Per solve,
  * T, dt and nt follow WaveHoltz::WaveHoltz (source/WaveHoltz.cpp:24-29), and the iteration is
  * the fixed-point loop of examples/waveholtz2d.cpp:165-185 with its residual
  * ||W - W_prev|| / ||pi0|| (each iteration runs one forced period from W, which equals
@@ -224,7 +225,9 @@ int wdg_whbatch_autotune(wdg_whbatch *batch, int steps, float *best_ms_per_step)
  * solve s from W[s] (one extra period from zero then gives |pi0|), else from zero.  A solve
  * stops at residual < tol (status 0), after maxit iterations (1), or when stall_limit > 0
  * updates in a row bring no new smallest residual (2: the stepping precision's floor).
- * W[s] receives the last iterate; iters, residuals, status (nullable) get one entry per solve. */
+ * W[s] receives the last iterate; iters, residuals, status (nullable) get one entry per solve.
+ * Runs after the work already queued on the solves' streams (device inputs written there are
+ * complete before they are read) and returns when the results are written. */
 int wdg_whbatch_solve(wdg_whbatch *batch, const double *const *F, double tol, int maxit, int stall_limit,
                       double *const *W, const int *warm, int *iters, double *residuals, int *status);
 

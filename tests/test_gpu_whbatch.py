@@ -103,6 +103,32 @@ def test_warm_start_and_early_exit(gpu_lib):
         assert rel(Ws[s], W0[s]) < 1e-6
 
 
+def test_device_inputs_written_just_before_the_solve(gpu_lib):
+    """Warm starts and forcing written on the caller's stream right before solve() are read
+    only once complete (the batch orders its own stream after the solves' streams)."""
+    import torch
+
+    W, probs, systems, Fs = _batch_problems()
+    b = W.WaveHoltzBatch(systems, [p[3] for p in probs])
+    ref, its0, _, _ = b.solve(Fs, 1e-8, 400)
+    ref = [x.copy() for x in ref]
+    for _ in range(2):
+        Fd, W0 = [], []
+        for s in range(3):
+            # a long chain of queued work (exact: powers of two) ending in the inputs' values
+            f = torch.from_numpy(Fs[s]).cuda()
+            w = torch.from_numpy(ref[s]).cuda()
+            for _ in range(200):
+                f.mul_(2.0).mul_(0.5)
+                w.mul_(2.0).mul_(0.5)
+            Fd.append(f)
+            W0.append(w)
+        Ws, its, res, st = b.solve(Fd, 1e-8, 400, W=W0, warm=[1, 1, 1])
+        assert (st == 0).all() and (its <= 2).all(), its
+        for s in range(3):
+            assert rel(Ws[s].cpu().numpy(), ref[s]) < 1e-7
+
+
 def test_fp32_batch_and_fp64_finish(gpu_lib):
     """FP32 stepping stops on the stall rule or at tol; an FP64 batch warm-started from its
     iterates then meets the FP64 tolerance (the plain iteration is the judge)."""

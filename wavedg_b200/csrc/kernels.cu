@@ -1008,9 +1008,10 @@ namespace wdg
 namespace wdg
 {
     int ws_chunk_unit(int n) { return kWsConsumers * ws_epw(n); }
-    int ws_slot_bytes(int n, bool fp32, int chunk)
+    int ws_slot_bytes(int n, bool fp32, int chunk, bool extra)
     {
-        return fp32 ? ws_slot<float>(n, chunk).bytes : ws_slot<double>(n, chunk).bytes;
+        return fp32 ? ws_slot<float>(n, chunk, WsStage<float, true>::value && extra).bytes
+                    : ws_slot<double>(n, chunk, WsStage<double, true>::value && extra).bytes;
     }
     int ws_warp_scratch_bytes(int n, bool fp32)
     {
@@ -1092,7 +1093,7 @@ namespace wdg
     {
 #define WDG_CASE(NV)                                                                       \
     case NV:                                                                               \
-        if (a.family == 2 && rk && a.use_tma && a.tma_out)                                 \
+        if (a.family == 2 && rk && a.use_tma && a.tma_out && ws_fits<NV, Real>(a))         \
             return launch_ws_n<NV, Real>(a, grid_limit, s);                                \
         if (a.family == 0)                                                                 \
             return rk ? launch_warp_n<NV, Real, true>(a, s) : launch_warp_n<NV, Real, false>(a, s); \

@@ -78,7 +78,8 @@ namespace wdg
 
     // warp-specialised stage kernels: one producer warp + kWsConsumers consumer warps per CTA
     constexpr int kWsConsumers = 4;
-    int ws_slot_bytes(int n, bool fp32, int chunk); // one ring slot of an n, chunk-element chunk
+    // one ring slot of an n, chunk-element chunk (extra: of a launch with forcing and filter)
+    int ws_slot_bytes(int n, bool fp32, int chunk, bool extra = false);
     int ws_warp_scratch_bytes(int n, bool fp32);    // one consumer warp's scratch
 
     // ---- batched WaveHoltz (kernels in stage_ws_batch.cuh, C-ABI in whbatch.cu)
@@ -112,10 +113,11 @@ namespace wdg
         double *part;
     };
 
+    // one launch covers the solves [s_lo, s_hi) (all of one degree) and their items [it_lo, it_hi)
     template <typename Real>
     struct WhbArgs
     {
-        int nsolves, nitems, stage, ring;
+        int nsolves, s_lo, s_hi, it_lo, it_hi, stage, ring;
         int slot_bytes, warp_scratch;
         WhbState *state;
         unsigned *err;
@@ -124,11 +126,11 @@ namespace wdg
 
     extern const double rk4a[5], rk4b[5], rk4c[5];
     int upload_rk4_tables(int device); // once per device
-    int whb_smem_bytes(int slot_bytes, int warp_scratch, int ring, bool fp32);
+    int whb_smem_bytes(int n, int slot_bytes, int warp_scratch, int ring, bool fp32);
     template <typename Real>
-    cudaError_t launch_whb_stage(const WhbArgs<Real> &a, int grid, size_t smem, cudaStream_t s);
+    cudaError_t launch_whb_stage(const WhbArgs<Real> &a, int n, int grid, size_t smem, cudaStream_t s);
     template <typename Real>
-    cudaError_t whb_occupancy(size_t smem, int *grid);
+    cudaError_t whb_occupancy(int n, size_t smem, int *grid);
     cudaError_t launch_whb_step_end(WhbState *state, int nsolves, cudaStream_t s);
 
     // fused stage: RK = true for the time-stepping epilogue

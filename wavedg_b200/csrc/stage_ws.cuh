@@ -58,7 +58,7 @@ namespace wdg
         int slot, tab, slots, scratch, warp_scratch, total;
     };
     template <typename Real>
-    __host__ __device__ inline WsLayout ws_layout(int n, int chunk, int stages);
+    __host__ __device__ inline WsLayout ws_layout(int n, int chunk, int stages, bool staged = false);
 
     __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
     {
@@ -138,19 +138,29 @@ namespace wdg
 
     // slot offsets (bytes) of an n, chunk-C slot:
     //   u (C, 3 n^2) | du (C, 3 n^2) | halo (C, 4 n, 3) | corners (C, 8 doubles) | fcode (C, u32)
+    //   [ | F (C, 3 n^2) | filter (C, 3 n^2, FP64) ]   staged: FP32 launches with forcing / filter
+    // Staging F and the filter through the slot keeps their latency off the consumers; FP64
+    // launches read them directly, since the larger slot would cost a CTA per SM.
     struct WsSlot
     {
-        int ub, hb, cb, kb, bytes;
+        int ub, hb, cb, kb, fb, ab, bytes;
+    };
+    template <typename Real, bool EXTRA>
+    struct WsStage
+    {
+        static constexpr bool value = EXTRA && sizeof(Real) == 4;
     };
     template <typename Real>
-    __host__ __device__ inline WsSlot ws_slot(int n, int chunk)
+    __host__ __device__ inline WsSlot ws_slot(int n, int chunk, bool staged = false)
     {
         WsSlot o;
         o.ub = chunk * 3 * n * n * (int)sizeof(Real);
         o.hb = 2 * o.ub;
         o.cb = o.hb + chunk * 12 * n * (int)sizeof(Real);
         o.kb = o.cb + chunk * 64;
-        o.bytes = o.kb + chunk * 4;
+        o.fb = o.kb + chunk * 4;
+        o.ab = o.fb + (staged ? o.ub : 0);
+        o.bytes = o.ab + (staged ? chunk * 3 * n * n * 8 : 0);
         return o;
     }
 
@@ -159,23 +169,30 @@ namespace wdg
     // chunk), then the neighbour traces of every interior face node by cp.async, one lane
     // per (element, side); the table reads of a batch go out together, so a chunk costs one
     // L2 round trip per batch rather than one per face node.
-    template <int N, typename Real>
+    template <int N, typename Real, bool EXTRA = false>
     __device__ __forceinline__ void ws_load(const WsChunk<Real> &c, unsigned char *base, uint64_t *full, int lane)
     {
         constexpr int ND = 3 * N * N, NF = 4 * N;
-        const WsSlot o = ws_slot<Real>(N, c.chunk);
+        constexpr bool STG = WsStage<Real, EXTRA>::value;
+        const WsSlot o = ws_slot<Real>(N, c.chunk, STG);
         const bool has_du = (c.flags & F_READ_DU) != 0;
+        const bool sF = STG && (c.flags & F_FORCE), sA = STG && (c.flags & F_FILTER);
         const int el0 = c.el0, ne = c.ne, C = c.chunk;
         if (ne == C)
         {
             if (lane == 0)
             {
-                mbar_expect_tx(full, (uint32_t)(o.ub * (has_du ? 2 : 1) + C * 68));
+                mbar_expect_tx(full, (uint32_t)(o.ub * ((has_du ? 2 : 1) + (sF ? 1 : 0)) + C * 68 +
+                                                 (sA ? C * ND * 8 : 0)));
                 bulk_g2s(base, c.u + (size_t)el0 * ND, (uint32_t)o.ub, full);
                 if (has_du)
                     bulk_g2s(base + o.ub, c.du + (size_t)el0 * ND, (uint32_t)o.ub, full);
                 bulk_g2s(base + o.cb, c.corners + 8 * (size_t)el0, (uint32_t)(64 * C), full);
                 bulk_g2s(base + o.kb, c.fcode + el0, (uint32_t)(4 * C), full);
+                if (sF)
+                    bulk_g2s(base + o.fb, c.F + (size_t)el0 * ND, (uint32_t)o.ub, full);
+                if (sA)
+                    bulk_g2s(base + o.ab, c.acc + (size_t)el0 * ND, (uint32_t)(C * ND * 8), full);
             }
         }
         else
@@ -186,6 +203,10 @@ namespace wdg
                 us[i] = c.u[(size_t)el0 * ND + i];
                 if (has_du)
                     dus[i] = c.du[(size_t)el0 * ND + i];
+                if (sF)
+                    reinterpret_cast<Real *>(base + o.fb)[i] = c.F[(size_t)el0 * ND + i];
+                if (sA)
+                    reinterpret_cast<double *>(base + o.ab)[i] = c.acc[(size_t)el0 * ND + i];
             }
             double *cw = reinterpret_cast<double *>(base + o.cb);
             for (int i = lane; i < ne * 8; i += 32)
@@ -248,11 +269,13 @@ namespace wdg
     }
 
     // ---------------------------------------------------------------- producer: store one chunk
-    template <int N, typename Real>
+    template <int N, typename Real, bool EXTRA = false>
     __device__ __forceinline__ void ws_store(const WsChunk<Real> &c, const unsigned char *base, int lane)
     {
         constexpr int ND = 3 * N * N;
-        const WsSlot o = ws_slot<Real>(N, c.chunk);
+        constexpr bool STG = WsStage<Real, EXTRA>::value;
+        const WsSlot o = ws_slot<Real>(N, c.chunk, STG);
+        const bool sA = STG && (c.flags & F_FILTER);
         const int el0 = c.el0, ne = c.ne;
         if (ne == c.chunk)
         {
@@ -260,16 +283,21 @@ namespace wdg
             {
                 bulk_s2g(c.out + (size_t)el0 * ND, base, (uint32_t)o.ub);
                 bulk_s2g(c.du + (size_t)el0 * ND, base + o.ub, (uint32_t)o.ub);
+                if (sA)
+                    bulk_s2g(c.acc + (size_t)el0 * ND, base + o.ab, (uint32_t)(c.chunk * ND * 8));
                 bulk_commit();
             }
         }
         else
         {
             const Real *us = reinterpret_cast<const Real *>(base), *dus = us + c.chunk * ND;
+            const double *as = reinterpret_cast<const double *>(base + o.ab);
             for (int i = lane; i < ne * ND; i += 32)
             {
                 c.out[(size_t)el0 * ND + i] = us[i];
                 c.du[(size_t)el0 * ND + i] = dus[i];
+                if (sA)
+                    c.acc[(size_t)el0 * ND + i] = as[i];
             }
         }
     }
@@ -282,8 +310,12 @@ namespace wdg
     {
         using Sh = WsShape<N>;
         constexpr int NN = Sh::NN, ND = Sh::ND, NF = Sh::NF, EW = Sh::EW;
-        const WsSlot o = ws_slot<Real>(N, c.chunk);
+        constexpr bool STG = WsStage<Real, EXTRA>::value;
+        const WsSlot o = ws_slot<Real>(N, c.chunk, STG);
         const int flags = c.flags;
+        // forcing and filter: staged in the slot (chunk-local index) or read in place
+        const Real *Fx = STG ? reinterpret_cast<const Real *>(base + o.fb) - (size_t)c.el0 * ND : c.F;
+        double *Ax = STG ? reinterpret_cast<double *>(base + o.ab) - (size_t)c.el0 * ND : c.acc;
         const bool has_du = (flags & F_READ_DU) != 0;
         const int R = c.chunk / (kWsConsumers * EW); // warp-rounds per chunk
         const int el_l = lane / N, ln = lane - el_l * N; // element of the round, grid line
@@ -424,9 +456,9 @@ namespace wdg
                         const size_t g = (size_t)(c.el0 + le) * ND + 3 * (i + N * j);
                         if (EXTRA && (flags & F_FORCE))
                         {
-                            r0 += c.fscale * c.F[g];
-                            r1 += c.fscale * c.F[g + 1];
-                            r2 += c.fscale * c.F[g + 2];
+                            r0 += c.fscale * Fx[g];
+                            r1 += c.fscale * Fx[g + 1];
+                            r2 += c.fscale * Fx[g + 2];
                         }
                         if (flags & F_MINV)
                         {
@@ -449,7 +481,7 @@ namespace wdg
 #pragma unroll
                             for (int f = 0; f < 3; ++f)
                             {
-                                const double fin = c.acc[g + f] + c.acc_c * (double)uo[f];
+                                const double fin = Ax[g + f] + c.acc_c * (double)uo[f];
                                 nsum += fin * fin;
                                 double w0;
                                 if (c.pend == 1)
@@ -461,15 +493,15 @@ namespace wdg
                                 }
                                 else
                                     w0 = c.W[g + f];
-                                c.acc[g + f] = c.c0 * w0;
+                                Ax[g + f] = c.c0 * w0;
                                 uo[f] = (Real)w0;
                             }
                         }
                         else if (EXTRA && (flags & F_FILTER))
                         {
-                            c.acc[g] += c.acc_c * (double)uo[0];
-                            c.acc[g + 1] += c.acc_c * (double)uo[1];
-                            c.acc[g + 2] += c.acc_c * (double)uo[2];
+                            Ax[g] += c.acc_c * (double)uo[0];
+                            Ax[g + 1] += c.acc_c * (double)uo[1];
+                            Ax[g + 2] += c.acc_c * (double)uo[2];
                         }
                         row[3 * i] = uo[0];
                         row[3 * i + 1] = uo[1];
@@ -495,11 +527,11 @@ namespace wdg
     }
 
     template <typename Real>
-    __host__ __device__ inline WsLayout ws_layout(int n, int chunk, int stages)
+    __host__ __device__ inline WsLayout ws_layout(int n, int chunk, int stages, bool staged)
     {
         WsLayout L;
         const int nn = n * n, ew = 32 / n;
-        L.slot = ws_slot<Real>(n, chunk).bytes;
+        L.slot = ws_slot<Real>(n, chunk, staged).bytes;
         L.tab = 128;
         L.slots = (L.tab + 2 * n * (int)sizeof(Real) + 127) & ~127;
         L.scratch = L.slots + stages * L.slot;
@@ -513,7 +545,7 @@ namespace wdg
     {
         const int C = a.chunk, S = a.ring, G = gridDim.x;
         const int nchunks = (a.nel + C - 1) / C;
-        const WsLayout L = ws_layout<Real>(N, C, S);
+        const WsLayout L = ws_layout<Real>(N, C, S, WsStage<Real, EXTRA>::value);
 
         extern __shared__ __align__(128) unsigned char smem[];
         uint64_t *full = reinterpret_cast<uint64_t *>(smem);
@@ -568,7 +600,7 @@ namespace wdg
             for (int m = 0; m < min(S, M); ++m)
             {
                 at(m);
-                ws_load<N, Real>(c, slots + (m % S) * L.slot, &full[m % S], lane);
+                ws_load<N, Real, EXTRA>(c, slots + (m % S) * L.slot, &full[m % S], lane);
             }
             int m = 0;
             for (; m < M; ++m)
@@ -578,14 +610,14 @@ namespace wdg
                 if (!__all_sync(0xffffffffu, mbar_wait(&done[q], (m / S) & 1)))
                     break;
                 at(m);
-                ws_store<N, Real>(c, slots + q * L.slot, lane);
+                ws_store<N, Real, EXTRA>(c, slots + q * L.slot, lane);
                 if (m + S < M)
                 {
                     if (lane == 0)
                         bulk_wait_read(); // the store above has read the slot
                     __syncwarp();
                     at(m + S);
-                    ws_load<N, Real>(c, slots + q * L.slot, &full[q], lane);
+                    ws_load<N, Real, EXTRA>(c, slots + q * L.slot, &full[q], lane);
                 }
             }
             if (m < M)
@@ -624,12 +656,23 @@ namespace wdg
         }
     }
 
+    // whether a launch's shared memory (the forcing / filter staging included) fits a CTA
+    template <int N, typename Real>
+    static bool ws_fits(const StageArgs<Real> &a)
+    {
+        const bool extra = (a.flags & (F_FORCE | F_FILTER)) != 0;
+        const size_t smem = (size_t)ws_layout<Real>(N, a.chunk, a.ring, extra && WsStage<Real, true>::value).total;
+        return smem <= 227 * 1024;
+    }
+
     template <int N, typename Real>
     static cudaError_t launch_ws_n(const StageArgs<Real> &a, int grid_limit, cudaStream_t s)
     {
         const bool extra = (a.flags & (F_FORCE | F_FILTER)) != 0;
         auto kern = extra ? ws_stage_kernel<N, Real, true> : ws_stage_kernel<N, Real, false>;
-        const size_t smem = (size_t)ws_layout<Real>(N, a.chunk, a.ring).total;
+        const size_t smem = (size_t)(extra ? ws_layout<Real>(N, a.chunk, a.ring, WsStage<Real, true>::value).total
+                                           : ws_layout<Real>(N, a.chunk, a.ring).total);
+
         int dev = 0;
         cudaGetDevice(&dev);
         static bool attr_set[2][64] = {};

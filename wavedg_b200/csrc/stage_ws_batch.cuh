@@ -1,13 +1,13 @@
-// Batched WaveHoltz: one persistent launch per RK stage over a work list of
-// (solve, chunk) items of up to kMaxBatch independent solves (included by kernels.cu).
+// Batched WaveHoltz: per RK stage, one persistent launch per polynomial degree over a work
+// list of (solve, chunk) items of the batch's solves of that degree (included by kernels.cu).
 //
-// Every solve has its own mesh, degree, frequency, period length nt and state; the
-// work list holds its chunks back to back (items item0 .. item0 + nchunks - 1).  A CTA
-// walks items blockIdx.x, blockIdx.x + G, ... skipping solves that have finished, and
-// runs the same producer / consumer pair as the single-solve kernel on each item, with
-// the degree dispatched per item (warp-uniform).  Per-solve stage scalars come from the
-// solve's own step counter k:  forcing scale -sin(omega (k + c_s) dt) / omega, filter
-// weight dt K((k + 1) dt) (halved on the last step of a period).
+// Every solve has its own mesh, frequency, period length nt and state; a launch covers the
+// solves [s_lo, s_hi) of one degree, whose chunks are listed back to back (items
+// it_lo .. it_hi).  A CTA walks items it_lo + blockIdx.x, + G, ... skipping solves that have
+// finished, and runs the same producer / consumer pair as the single-solve kernel on each
+// item.  Per-solve stage scalars come from the solve's own step counter k:  forcing scale
+// -sin(omega (k + c_s) dt) / omega, filter weight dt K((k + 1) dt) (halved on the last step
+// of a period).
 //
 // Each iteration is one forced period from the current iterate W (by linearity of the
 // scheme this equals S W + pi0 of the reference's loop): the state starts at W, the
@@ -20,38 +20,24 @@ namespace wdg
 {
     __constant__ double c_rk4a[5], c_rk4b[5], c_rk4c[5];
 
-    // node/weight tables of every degree in shared memory: degree n at offset sum_{m<n} 2m
-    constexpr int kWhbTab = 88; // sum_{n=2}^{9} 2 n
-
-    __host__ __device__ inline int whb_slots_offset(int real_size)
+    // shared memory: [2 S mbarriers | pad 128][x (n), w (n)][per solve: k, phase, active]
+    //                [pad 128][S slots][consumer scratch]
+    __host__ __device__ inline int whb_slots_offset(int n, int real_size)
     {
-        return (128 + kWhbTab * real_size + 3 * kMaxBatch * 4 + 127) & ~127;
+        return (128 + 2 * n * real_size + 3 * kMaxBatch * 4 + 127) & ~127;
     }
 
-    // degree-dispatched calls; n is warp-uniform (one item at a time per warp)
-#define WDG_WHB_DISPATCH(n, CALL)                                                              \
-    switch (n)                                                                                 \
-    {                                                                                          \
-    case 2: { constexpr int NV = 2; CALL; } break;                                             \
-    case 3: { constexpr int NV = 3; CALL; } break;                                             \
-    case 4: { constexpr int NV = 4; CALL; } break;                                             \
-    case 5: { constexpr int NV = 5; CALL; } break;                                             \
-    case 6: { constexpr int NV = 6; CALL; } break;                                             \
-    case 7: { constexpr int NV = 7; CALL; } break;                                             \
-    case 8: { constexpr int NV = 8; CALL; } break;                                             \
-    default: { constexpr int NV = 9; CALL; } break;                                            \
-    }
-
-    template <typename Real>
+    template <int N, typename Real>
     __global__ void __launch_bounds__(kWsThreads, 2) whb_stage_kernel(const __grid_constant__ WhbArgs<Real> a)
     {
         const int S = a.ring, G = gridDim.x, st = a.stage;
         extern __shared__ __align__(128) unsigned char smem[];
         uint64_t *full = reinterpret_cast<uint64_t *>(smem);
         uint64_t *done = full + S;
-        Real *tab = reinterpret_cast<Real *>(smem + 128);
-        int *act = reinterpret_cast<int *>(smem + 128 + kWhbTab * sizeof(Real)); // per solve: k, phase, active
-        unsigned char *slots = smem + whb_slots_offset((int)sizeof(Real));
+        Real *xt = reinterpret_cast<Real *>(smem + 128); // GLL nodes, then weights
+        Real *wt = xt + N;
+        int *act = reinterpret_cast<int *>(smem + 128 + 2 * N * sizeof(Real)); // per solve: k, phase, active
+        unsigned char *slots = smem + whb_slots_offset(N, (int)sizeof(Real));
         unsigned char *scratch = slots + S * a.slot_bytes;
 
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -64,18 +50,9 @@ namespace wdg
             }
             fence_mbar_init();
         }
-        for (int q = threadIdx.x; q < kWhbTab; q += blockDim.x)
-        {
-            int n = 2, off = 0;
-            while (q >= off + 2 * n)
-            {
-                off += 2 * n;
-                ++n;
-            }
-            const int r = q - off;
-            tab[q] = (r < n) ? Tab<Real>::x(n, r) : Tab<Real>::w(n, r - n);
-        }
-        for (int q = threadIdx.x; q < a.nsolves; q += blockDim.x)
+        for (int q = threadIdx.x; q < 2 * N; q += blockDim.x)
+            xt[q] = (q < N) ? Tab<Real>::x(N, q) : Tab<Real>::w(N, q - N);
+        for (int q = a.s_lo + (int)threadIdx.x; q < a.s_hi; q += blockDim.x)
         {
             act[3 * q] = a.state[q].k;
             act[3 * q + 1] = a.state[q].phase;
@@ -83,10 +60,10 @@ namespace wdg
         }
         __syncthreads();
 
-        // item -> solve: the solves' items are contiguous and ascending
+        // item -> solve: the launch's solves' items are contiguous and ascending
         auto solve_of = [&](int item)
         {
-            int lo = 0, hi = a.nsolves - 1;
+            int lo = a.s_lo, hi = a.s_hi - 1;
             while (lo < hi)
             {
                 const int mid = (lo + hi + 1) >> 1;
@@ -101,12 +78,11 @@ namespace wdg
         // consumers walk the same sequence, so their ring positions agree
         auto advance = [&](int k)
         {
-            while (k < a.nitems && !act[3 * solve_of(k) + 2])
+            while (k < a.it_hi && !act[3 * solve_of(k) + 2])
                 k += G;
             return k;
         };
         WsChunk<Real> c{};
-        int cur_n = 2;
         auto build = [&](int item)
         {
             const int si = solve_of(item);
@@ -116,7 +92,6 @@ namespace wdg
             // the RK4 buffer rotation A -> B -> C -> B -> C -> A
             const int src = (st == 0) ? 0 : (st % 2 == 1) ? 1 : 2;
             const int dst = (st == 4) ? 0 : (st % 2 == 0) ? 1 : 2;
-            cur_n = P.n;
             c.u = P.buf[src];
             c.out = P.buf[dst];
             c.du = P.du;
@@ -147,19 +122,20 @@ namespace wdg
             c.part = P.part + (size_t)ci * kWsConsumers * 2;
         };
 
+        const int first = a.it_lo + (int)blockIdx.x;
         if (warp == kWsConsumers)
         {
             // ------------------------------------------------------------ producer
-            int kl = advance((int)blockIdx.x), nl = 0; // next item to load, loads issued
-            for (; nl < S && kl < a.nitems; ++nl)
+            int kl = advance(first), nl = 0; // next item to load, loads issued
+            for (; nl < S && kl < a.it_hi; ++nl)
             {
                 build(kl);
-                WDG_WHB_DISPATCH(cur_n, (ws_load<NV, Real>(c, slots + (nl % S) * a.slot_bytes, &full[nl % S], lane)));
+                ws_load<N, Real, true>(c, slots + (nl % S) * a.slot_bytes, &full[nl % S], lane);
                 kl = advance(kl + G);
             }
-            int ks = advance((int)blockIdx.x), m = 0; // next item to store, stores done
+            int ks = advance(first), m = 0; // next item to store, stores done
             bool ok = true;
-            for (; ks < a.nitems; ++m)
+            for (; ks < a.it_hi; ++m)
             {
                 const int q = m % S;
                 if (!__all_sync(0xffffffffu, mbar_wait(&done[q], (m / S) & 1)))
@@ -168,15 +144,15 @@ namespace wdg
                     break;
                 }
                 build(ks);
-                WDG_WHB_DISPATCH(cur_n, (ws_store<NV, Real>(c, slots + q * a.slot_bytes, lane)));
+                ws_store<N, Real, true>(c, slots + q * a.slot_bytes, lane);
                 ks = advance(ks + G);
-                if (kl < a.nitems)
+                if (kl < a.it_hi)
                 {
                     if (lane == 0)
                         bulk_wait_read(); // the store above has read the slot
                     __syncwarp();
                     build(kl);
-                    WDG_WHB_DISPATCH(cur_n, (ws_load<NV, Real>(c, slots + q * a.slot_bytes, &full[q], lane)));
+                    ws_load<N, Real, true>(c, slots + q * a.slot_bytes, &full[q], lane);
                     kl = advance(kl + G);
                     ++nl;
                 }
@@ -195,8 +171,8 @@ namespace wdg
 
         // ---------------------------------------------------------------- consumers
         Real *Rc = reinterpret_cast<Real *>(scratch + warp * a.warp_scratch);
-        int kc = advance((int)blockIdx.x);
-        for (int m = 0; kc < a.nitems; ++m)
+        int kc = advance(first);
+        for (int m = 0; kc < a.it_hi; ++m)
         {
             const int q = m % S;
             if (!__all_sync(0xffffffffu, mbar_wait(&full[q], (m / S) & 1)))
@@ -206,11 +182,7 @@ namespace wdg
                 break;
             }
             build(kc);
-            int toff = 0;
-            for (int n = 2; n < cur_n; ++n)
-                toff += 2 * n;
-            WDG_WHB_DISPATCH(cur_n, (ws_consume<NV, Real, true, true>(c, slots + q * a.slot_bytes, Rc, tab + toff,
-                                                                      tab + toff + NV, warp, lane)));
+            ws_consume<N, Real, true, true>(c, slots + q * a.slot_bytes, Rc, xt, wt, warp, lane);
             // results are in the slot: hand them to the async proxy, then release the slot
             fence_async_smem();
             __syncwarp();
@@ -219,7 +191,6 @@ namespace wdg
             kc = advance(kc + G);
         }
     }
-#undef WDG_WHB_DISPATCH
 
     // After the fifth stage of every step: advance each running solve's step counter; at the
     // end of a period reduce its partial sums in a fixed order and update residual and status
@@ -297,31 +268,55 @@ namespace wdg
         }
     }
 
-    int whb_smem_bytes(int slot_bytes, int warp_scratch, int ring, bool fp32)
+    int whb_smem_bytes(int n, int slot_bytes, int warp_scratch, int ring, bool fp32)
     {
-        return whb_slots_offset(fp32 ? 4 : 8) + ring * slot_bytes + kWsConsumers * warp_scratch;
+        return whb_slots_offset(n, fp32 ? 4 : 8) + ring * slot_bytes + kWsConsumers * warp_scratch;
     }
 
+#define WDG_WHB_CASES(X) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9)
     template <typename Real>
-    cudaError_t whb_occupancy(size_t smem, int *grid)
+    cudaError_t whb_occupancy(int n, size_t smem, int *grid)
     {
         int dev = 0, per_sm = 0, sms = 0;
         cudaGetDevice(&dev);
-        cudaError_t e = cudaFuncSetAttribute(whb_stage_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             227 * 1024);
-        if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, whb_stage_kernel<Real>, kWsThreads, smem);
+        cudaError_t e = cudaErrorInvalidValue;
+        switch (n)
+        {
+#define WDG_X(NV)                                                                                           \
+    case NV:                                                                                                \
+        e = cudaFuncSetAttribute(whb_stage_kernel<NV, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
+                                 227 * 1024);                                                               \
+        if (e == cudaSuccess)                                                                               \
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, whb_stage_kernel<NV, Real>,          \
+                                                              kWsThreads, smem);                            \
+        break;
+            WDG_WHB_CASES(WDG_X)
+#undef WDG_X
+        default:
+            break;
+        }
         if (e == cudaSuccess)
             e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         *grid = std::max(1, per_sm) * sms;
         return e;
     }
     template <typename Real>
-    cudaError_t launch_whb_stage(const WhbArgs<Real> &a, int grid, size_t smem, cudaStream_t s)
+    cudaError_t launch_whb_stage(const WhbArgs<Real> &a, int n, int grid, size_t smem, cudaStream_t s)
     {
-        whb_stage_kernel<Real><<<grid, kWsThreads, smem, s>>>(a);
+        switch (n)
+        {
+#define WDG_X(NV)                                                  \
+    case NV:                                                       \
+        whb_stage_kernel<NV, Real><<<grid, kWsThreads, smem, s>>>(a); \
+        break;
+            WDG_WHB_CASES(WDG_X)
+#undef WDG_X
+        default:
+            return cudaErrorInvalidValue;
+        }
         return cudaGetLastError();
     }
+#undef WDG_WHB_CASES
     cudaError_t launch_whb_step_end(WhbState *state, int nsolves, cudaStream_t s)
     {
         whb_step_end_kernel<<<nsolves, 256, 0, s>>>(state, nsolves);
@@ -342,8 +337,8 @@ namespace wdg
         done |= (1ull << device);
         return WDG_OK;
     }
-    template cudaError_t launch_whb_stage<double>(const WhbArgs<double> &, int, size_t, cudaStream_t);
-    template cudaError_t launch_whb_stage<float>(const WhbArgs<float> &, int, size_t, cudaStream_t);
-    template cudaError_t whb_occupancy<double>(size_t, int *);
-    template cudaError_t whb_occupancy<float>(size_t, int *);
+    template cudaError_t launch_whb_stage<double>(const WhbArgs<double> &, int, int, size_t, cudaStream_t);
+    template cudaError_t launch_whb_stage<float>(const WhbArgs<float> &, int, int, size_t, cudaStream_t);
+    template cudaError_t whb_occupancy<double>(int, size_t, int *);
+    template cudaError_t whb_occupancy<float>(int, size_t, int *);
 } // namespace wdg

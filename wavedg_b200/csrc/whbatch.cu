@@ -1,6 +1,7 @@
 // C-ABI: batched WaveHoltz -- many independent Helmholtz solves (each its own mesh,
-// degree, frequency and forcing) advanced together by one persistent launch per RK
-// stage over a work list of (solve, chunk) items.  Blocks of steps are captured once
+// degree, frequency and forcing) advanced together: per RK stage one persistent launch
+// per polynomial degree over a work list of (solve, chunk) items, the degrees' launches
+// running concurrently on forked streams.  Blocks of steps are captured once
 // into a CUDA graph on a private stream and replayed until every solve has finished;
 // each solve's step counter, period ends, residual and status live on the device
 // (WhbState), so a replay needs no host decision.  Iteration and residual follow the
@@ -15,16 +16,28 @@
 
 using namespace wdg;
 
+// the solves of one degree: one launch per RK stage
+struct WhbGroup
+{
+    int n = 0, s_lo = 0, s_hi = 0, it_lo = 0, it_hi = 0;
+    int slot_bytes = 0, warp_scratch = 0, grid = 0;
+    size_t smem = 0;
+    cudaStream_t st = nullptr; // forked stream of the captured graph (groups run concurrently)
+    cudaEvent_t done = nullptr;
+};
+
 struct wdg_whbatch
 {
     int device = 0, precision = WDG_FP64, n = 0;
+    // solves are held sorted by degree; perm[i] is the caller's index of internal solve i
+    std::vector<int> perm;
+    std::vector<WhbGroup> groups;
+    cudaEvent_t fork = nullptr;
     std::vector<wdg_wave *> w;
     std::vector<double> omega, T, dt, c0;
     std::vector<int> nt, nchunks, item0, chunk;
     std::vector<size_t> part_cap;
-    int nitems = 0, rounds = 1, ring = 2, grid = 0;
-    size_t smem = 0;
-    int slot_bytes = 0, warp_scratch = 0;
+    int nitems = 0, rounds = 1, ring = 2;
     cudaStream_t cs = nullptr;
     std::vector<double *> d_W, d_acc, d_part;
     std::vector<void *> d_F;
@@ -55,25 +68,33 @@ namespace
         }
     };
 
-    // launch shape: chunk = rounds x unit(n) per solve; slot and scratch sized for the largest
+    // launch shape: chunk = rounds x unit(n) per solve; one launch per degree group
     int shape(wdg_whbatch *b, int rounds, int ring)
     {
         const bool fp32 = b->precision == WDG_FP32;
-        int slot = 0, scr = 0, items = 0;
         std::vector<int> chunk(b->n), nch(b->n), it0(b->n);
+        int items = 0;
         for (int s = 0; s < b->n; ++s)
         {
-            const int nn = b->w[s]->n;
-            chunk[s] = rounds * ws_chunk_unit(nn);
-            slot = std::max(slot, ws_slot_bytes(nn, fp32, chunk[s]));
-            scr = std::max(scr, ws_warp_scratch_bytes(nn, fp32));
+            chunk[s] = rounds * ws_chunk_unit(b->w[s]->n);
             nch[s] = (b->w[s]->nel + chunk[s] - 1) / chunk[s];
             it0[s] = items;
             items += nch[s];
         }
-        const size_t smem = (size_t)whb_smem_bytes(slot, scr, ring, fp32);
-        if (smem > 227 * 1024)
-            return fail(WDG_ERR_ARG, "batched WaveHoltz: chunk x ring too large for shared memory");
+        std::vector<WhbGroup> gs = b->groups;
+        for (WhbGroup &g : gs)
+        {
+            g.slot_bytes = ws_slot_bytes(g.n, fp32, rounds * ws_chunk_unit(g.n), true);
+            g.warp_scratch = ws_warp_scratch_bytes(g.n, fp32);
+            g.smem = (size_t)whb_smem_bytes(g.n, g.slot_bytes, g.warp_scratch, ring, fp32);
+            if (g.smem > 227 * 1024)
+                return fail(WDG_ERR_ARG, "batched WaveHoltz: chunk x ring too large for shared memory");
+            g.it_lo = it0[g.s_lo];
+            g.it_hi = it0[g.s_hi - 1] + nch[g.s_hi - 1];
+            int grid = 0;
+            WDG_CUDA(fp32 ? whb_occupancy<float>(g.n, g.smem, &grid) : whb_occupancy<double>(g.n, g.smem, &grid));
+            g.grid = std::max(1, std::min(grid, g.it_hi - g.it_lo));
+        }
         // partial sums: nchunks x consumer warps x 2 per solve, grown as needed
         for (int s = 0; s < b->n; ++s)
         {
@@ -88,16 +109,11 @@ namespace
                 b->part_cap[s] = need;
             }
         }
-        int grid = 0;
-        WDG_CUDA(fp32 ? whb_occupancy<float>(smem, &grid) : whb_occupancy<double>(smem, &grid));
+        b->groups = gs;
         b->chunk = chunk;
         b->nchunks = nch;
         b->item0 = it0;
         b->nitems = items;
-        b->slot_bytes = slot;
-        b->warp_scratch = scr;
-        b->smem = smem;
-        b->grid = std::min(grid, std::max(1, items));
         b->rounds = rounds;
         b->ring = ring;
         if (b->graph)
@@ -109,15 +125,18 @@ namespace
     }
 
     template <typename Real>
-    WhbArgs<Real> make_args(const wdg_whbatch *b, int stage)
+    WhbArgs<Real> make_args(const wdg_whbatch *b, const WhbGroup &g, int stage)
     {
         WhbArgs<Real> a{};
         a.nsolves = b->n;
-        a.nitems = b->nitems;
+        a.s_lo = g.s_lo;
+        a.s_hi = g.s_hi;
+        a.it_lo = g.it_lo;
+        a.it_hi = g.it_hi;
         a.stage = stage;
         a.ring = b->ring;
-        a.slot_bytes = b->slot_bytes;
-        a.warp_scratch = b->warp_scratch;
+        a.slot_bytes = g.slot_bytes;
+        a.warp_scratch = g.warp_scratch;
         a.state = b->d_state;
         a.err = b->w[0]->d_err;
         for (int s = 0; s < b->n; ++s)
@@ -146,39 +165,54 @@ namespace
         return a;
     }
 
-    // kGraphSteps steps (5 stage launches + the step-end update each) as one graph
+    template <typename Real>
+    cudaError_t launch_group(const wdg_whbatch *b, const WhbGroup &g, int stage, cudaStream_t st)
+    {
+        const WhbArgs<Real> a = make_args<Real>(b, g, stage);
+        return launch_whb_stage<Real>(a, g.n, g.grid, g.smem, st);
+    }
+
+    // kGraphSteps steps (per stage one launch per degree group, the groups on forked streams,
+    // then the step-end update) as one graph
     int record(wdg_whbatch *b)
     {
         const bool fp32 = b->precision == WDG_FP32;
-        std::vector<WhbArgs<double>> a64(fp32 ? 0 : 5);
-        std::vector<WhbArgs<float>> a32(fp32 ? 5 : 0);
-        for (int st = 0; st < 5; ++st)
-        {
-            if (fp32)
-                a32[st] = make_args<float>(b, st);
-            else
-                a64[st] = make_args<double>(b, st);
-        }
+        const bool fork = b->groups.size() > 1;
         WDG_CUDA(cudaStreamBeginCapture(b->cs, cudaStreamCaptureModeThreadLocal));
         cudaError_t e = cudaSuccess;
         for (int k = 0; k < kGraphSteps && e == cudaSuccess; ++k)
         {
-            for (int st = 0; st < 5 && e == cudaSuccess; ++st)
-                e = fp32 ? launch_whb_stage<float>(a32[st], b->grid, b->smem, b->cs)
-                         : launch_whb_stage<double>(a64[st], b->grid, b->smem, b->cs);
+            for (int stg = 0; stg < 5 && e == cudaSuccess; ++stg)
+            {
+                if (fork)
+                    e = cudaEventRecord(b->fork, b->cs);
+                for (const WhbGroup &g : b->groups)
+                {
+                    cudaStream_t st = fork ? g.st : b->cs;
+                    if (e == cudaSuccess && fork)
+                        e = cudaStreamWaitEvent(st, b->fork, 0);
+                    if (e == cudaSuccess)
+                        e = fp32 ? launch_group<float>(b, g, stg, st) : launch_group<double>(b, g, stg, st);
+                    if (e == cudaSuccess && fork)
+                        e = cudaEventRecord(g.done, st);
+                }
+                for (const WhbGroup &g : b->groups)
+                    if (e == cudaSuccess && fork)
+                        e = cudaStreamWaitEvent(b->cs, g.done, 0);
+            }
             if (e == cudaSuccess)
                 e = launch_whb_step_end(b->d_state, b->n, b->cs);
         }
-        cudaGraph_t g = nullptr;
-        const cudaError_t e2 = cudaStreamEndCapture(b->cs, &g);
+        cudaGraph_t gph = nullptr;
+        const cudaError_t e2 = cudaStreamEndCapture(b->cs, &gph);
         if (e != cudaSuccess || e2 != cudaSuccess)
         {
-            if (g)
-                cudaGraphDestroy(g);
+            if (gph)
+                cudaGraphDestroy(gph);
             return cuda_fail(e != cudaSuccess ? e : e2, "batched WaveHoltz: graph capture");
         }
-        e = cudaGraphInstantiate(&b->graph, g, 0);
-        cudaGraphDestroy(g);
+        e = cudaGraphInstantiate(&b->graph, gph, 0);
+        cudaGraphDestroy(gph);
         if (e != cudaSuccess)
             return cuda_fail(e, "cudaGraphInstantiate");
         b->graph_steps = kGraphSteps;
@@ -191,6 +225,22 @@ namespace
         wdg_wave *w = b->w[s];
         WDG_CUDA(cudaMemsetAsync(w->d_state[0], 0, w->real_size() * (size_t)w->ndof, b->cs));
         WDG_CUDA(cudaMemsetAsync(b->d_acc[s], 0, sizeof(double) * (size_t)w->ndof, b->cs));
+        return WDG_OK;
+    }
+
+    // order the private stream after every solve handle's stream, so inputs the caller wrote
+    // there (forcing, warm starts) are complete before the batch reads them
+    int after_callers(wdg_whbatch *b)
+    {
+        std::vector<cudaStream_t> seen;
+        for (const wdg_wave *w : b->w)
+        {
+            if (std::find(seen.begin(), seen.end(), w->stream) != seen.end())
+                continue;
+            seen.push_back(w->stream);
+            WDG_CUDA(cudaEventRecord(b->fork, w->stream));
+            WDG_CUDA(cudaStreamWaitEvent(b->cs, b->fork, 0));
+        }
         return WDG_OK;
     }
 
@@ -242,13 +292,31 @@ extern "C"
         b->d_part.assign(n_solves, nullptr);
         b->part_cap.assign(n_solves, 0);
         b->d_F.assign(n_solves, nullptr);
+        // internal order: sorted by degree (stable), one group of solves per degree
+        b->perm.resize(n_solves);
+        for (int s = 0; s < n_solves; ++s)
+            b->perm[s] = s;
+        std::stable_sort(b->perm.begin(), b->perm.end(), [&](int x, int y) { return waves[x]->n < waves[y]->n; });
+        for (int s = 0; s < n_solves; ++s)
+        {
+            const int nn = waves[b->perm[s]]->n;
+            if (b->groups.empty() || b->groups.back().n != nn)
+            {
+                WhbGroup gr;
+                gr.n = nn;
+                gr.s_lo = s;
+                b->groups.push_back(gr);
+            }
+            b->groups.back().s_hi = s + 1;
+        }
         for (int s = 0; s < n_solves && st == WDG_OK; ++s)
         {
-            wdg_wave *w = waves[s];
+            const int u = b->perm[s];
+            wdg_wave *w = waves[u];
             b->w.push_back(w);
-            b->omega.push_back(omegas[s]);
+            b->omega.push_back(omegas[u]);
             // WaveHoltz::WaveHoltz (source/WaveHoltz.cpp:24-29)
-            const double T = 2.0 * M_PI / omegas[s];
+            const double T = 2.0 * M_PI / omegas[u];
             const double p = w->n;
             double dt = 0.5 * w->min_h / (p * p);
             const int nt = (int)std::ceil(T / dt);
@@ -256,7 +324,7 @@ extern "C"
             b->T.push_back(T);
             b->dt.push_back(dt);
             b->nt.push_back(nt);
-            b->c0.push_back(0.5 * dt * K(omegas[s], 0.0));
+            b->c0.push_back(0.5 * dt * K(omegas[u], 0.0));
             st = ensure_states(w);
             const size_t nd = (size_t)w->ndof;
             cudaError_t e = cudaSuccess;
@@ -272,6 +340,15 @@ extern "C"
         cudaError_t e = cudaSuccess;
         if (st == WDG_OK)
             e = cudaStreamCreateWithFlags(&b->cs, cudaStreamNonBlocking);
+        if (st == WDG_OK && e == cudaSuccess)
+            e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+        for (WhbGroup &gr : b->groups)
+        {
+            if (st == WDG_OK && e == cudaSuccess)
+                e = cudaStreamCreateWithFlags(&gr.st, cudaStreamNonBlocking);
+            if (st == WDG_OK && e == cudaSuccess)
+                e = cudaEventCreateWithFlags(&gr.done, cudaEventDisableTiming);
+        }
         if (st == WDG_OK && e == cudaSuccess)
             e = cudaMalloc(&b->d_state, sizeof(WhbState) * n_solves);
         if (st == WDG_OK && e == cudaSuccess)
@@ -315,6 +392,15 @@ extern "C"
             cudaFree(b->d_state);
         if (b->h_state)
             cudaFreeHost(b->h_state);
+        for (WhbGroup &gr : b->groups)
+        {
+            if (gr.done)
+                cudaEventDestroy(gr.done);
+            if (gr.st)
+                cudaStreamDestroy(gr.st);
+        }
+        if (b->fork)
+            cudaEventDestroy(b->fork);
         if (b->cs)
             cudaStreamDestroy(b->cs);
         delete b;
@@ -324,9 +410,10 @@ extern "C"
     {
         if (!b || solve < 0 || solve >= b->n)
             return fail(WDG_ERR_ARG, "wdg_whbatch_params: bad arguments");
-        if (T) *T = b->T[solve];
-        if (dt) *dt = b->dt[solve];
-        if (nt) *nt = b->nt[solve];
+        const int i = (int)(std::find(b->perm.begin(), b->perm.end(), solve) - b->perm.begin());
+        if (T) *T = b->T[i];
+        if (dt) *dt = b->dt[i];
+        if (nt) *nt = b->nt[i];
         return WDG_OK;
     }
 
@@ -344,7 +431,12 @@ extern "C"
             return fail(WDG_ERR_ARG, "null batch");
         if (rounds) *rounds = b->rounds;
         if (ring) *ring = b->ring;
-        if (grid) *grid = b->grid;
+        if (grid)
+        {
+            *grid = 0;
+            for (const WhbGroup &gr : b->groups)
+                *grid += gr.grid;
+        }
         return WDG_OK;
     }
 
@@ -357,12 +449,14 @@ extern "C"
             if (!F[s] || !W[s])
                 return fail(WDG_ERR_ARG, "wdg_whbatch_solve: every solve needs F and W");
         Dev g(b->device);
+        WDG_TRY(after_callers(b));
         for (int s = 0; s < b->n; ++s)
         {
             wdg_wave *w = b->w[s];
             const size_t nd = (size_t)w->ndof;
             // forcing in the stepping precision (d_W serves as the FP64 staging buffer)
-            WDG_CUDA(cudaMemcpyAsync(b->d_W[s], F[s], sizeof(double) * nd, cudaMemcpyDefault, b->cs));
+            const int u = b->perm[s]; // the caller's index of internal solve s
+            WDG_CUDA(cudaMemcpyAsync(b->d_W[s], F[u], sizeof(double) * nd, cudaMemcpyDefault, b->cs));
             if (b->precision == WDG_FP32)
                 WDG_CUDA(launch_convert<double, float>(b->d_W[s], static_cast<float *>(b->d_F[s]), (long long)nd,
                                                        b->cs));
@@ -370,9 +464,9 @@ extern "C"
                 WDG_CUDA(cudaMemcpyAsync(b->d_F[s], b->d_W[s], sizeof(double) * nd, cudaMemcpyDeviceToDevice, b->cs));
             // zero start: fixed-point periods from W = 0 (the first yields pi0); warm start:
             // a pi0 period from zero first (its norm scales the residual), then from W
-            const bool ws = warm && warm[s];
+            const bool ws = warm && warm[u];
             if (ws)
-                WDG_CUDA(cudaMemcpyAsync(b->d_W[s], W[s], sizeof(double) * nd, cudaMemcpyDefault, b->cs));
+                WDG_CUDA(cudaMemcpyAsync(b->d_W[s], W[u], sizeof(double) * nd, cudaMemcpyDefault, b->cs));
             else
                 WDG_CUDA(cudaMemsetAsync(b->d_W[s], 0, sizeof(double) * nd, b->cs));
             WDG_TRY(zero_period(b, s));
@@ -401,13 +495,14 @@ extern "C"
         }
         for (int s = 0; s < b->n; ++s)
         {
-            WDG_CUDA(cudaMemcpyAsync(W[s], b->d_W[s], sizeof(double) * b->w[s]->ndof, cudaMemcpyDefault, b->cs));
+            const int u = b->perm[s];
+            WDG_CUDA(cudaMemcpyAsync(W[u], b->d_W[s], sizeof(double) * b->w[s]->ndof, cudaMemcpyDefault, b->cs));
             if (iters)
-                iters[s] = b->h_state[s].iter;
+                iters[u] = b->h_state[s].iter;
             if (residuals)
-                residuals[s] = b->h_state[s].residual;
+                residuals[u] = b->h_state[s].residual;
             if (status)
-                status[s] = b->h_state[s].status;
+                status[u] = b->h_state[s].status;
         }
         WDG_CUDA(cudaStreamSynchronize(b->cs));
         if (running)
