@@ -20,11 +20,11 @@ namespace wdg
 {
     __constant__ double c_rk4a[5], c_rk4b[5], c_rk4c[5];
 
-    // shared memory: [2 S mbarriers | pad 128][x (n), w (n)][per solve: k, phase, active]
-    //                [pad 128][S slots][consumer scratch]
+    // shared memory: [2 S mbarriers | pad 128][per solve: forcing scale, filter weight (FP64)]
+    //                [x (n), w (n)][per solve: k, phase, active][pad 128][S slots][consumer scratch]
     __host__ __device__ inline int whb_slots_offset(int n, int real_size)
     {
-        return (128 + 2 * n * real_size + 3 * kMaxBatch * 4 + 127) & ~127;
+        return (128 + 16 * kMaxBatch + 2 * n * real_size + 3 * kMaxBatch * 4 + 127) & ~127;
     }
 
     template <int N, typename Real>
@@ -34,9 +34,10 @@ namespace wdg
         extern __shared__ __align__(128) unsigned char smem[];
         uint64_t *full = reinterpret_cast<uint64_t *>(smem);
         uint64_t *done = full + S;
-        Real *xt = reinterpret_cast<Real *>(smem + 128); // GLL nodes, then weights
+        double *sc = reinterpret_cast<double *>(smem + 128);                // per solve: fscale, acc_c
+        Real *xt = reinterpret_cast<Real *>(smem + 128 + 16 * kMaxBatch); // GLL nodes, then weights
         Real *wt = xt + N;
-        int *act = reinterpret_cast<int *>(smem + 128 + 2 * N * sizeof(Real)); // per solve: k, phase, active
+        int *act = reinterpret_cast<int *>(smem + 128 + 16 * kMaxBatch + 2 * N * sizeof(Real)); // k, phase, active
         unsigned char *slots = smem + whb_slots_offset(N, (int)sizeof(Real));
         unsigned char *scratch = slots + S * a.slot_bytes;
 
@@ -54,9 +55,20 @@ namespace wdg
             xt[q] = (q < N) ? Tab<Real>::x(N, q) : Tab<Real>::w(N, q - N);
         for (int q = a.s_lo + (int)threadIdx.x; q < a.s_hi; q += blockDim.x)
         {
-            act[3 * q] = a.state[q].k;
+            const int k = a.state[q].k;
+            act[3 * q] = k;
             act[3 * q + 1] = a.state[q].phase;
             act[3 * q + 2] = a.state[q].active;
+            // the solve's stage scalars, once per CTA rather than once per item:
+            // forcing F s(t), s(t) = -sin(omega t) / omega at the stage time (WaveHoltz.cpp:57-68);
+            // filter weight of the step's end dt K(t), halved on the period's last step
+            const WhbSolve<Real> &P = a.s[q];
+            const double ts = (k + c_rk4c[st]) * P.dt;
+            sc[2 * q] = -sin(P.omega * ts) / P.omega;
+            const double t1 = (k + 1) * P.dt;
+            sc[2 * q + 1] = (st == 4) ? ((k + 1 == P.nt) ? 0.5 : 1.0) * P.dt *
+                                            (P.omega / M_PI * (cos(P.omega * t1) - 0.25))
+                                      : 0.0;
         }
         __syncthreads();
 
@@ -109,14 +121,9 @@ namespace wdg
             c.rk_a = (Real)c_rk4a[st];
             c.rk_b = (Real)c_rk4b[st];
             c.dt = (Real)P.dt;
-            // forcing F s(t), s(t) = -sin(omega t) / omega at the stage time (WaveHoltz.cpp:57-68)
-            const double ts = (k + c_rk4c[st]) * P.dt;
-            c.fscale = (Real)(-sin(P.omega * ts) / P.omega);
-            // filter weight of the step's end: dt K(t), halved on the period's last step
-            const bool last = (k + 1 == P.nt);
-            const double t1 = (k + 1) * P.dt;
-            c.acc_c = (st == 4) ? (last ? 0.5 : 1.0) * P.dt * (P.omega / M_PI * (cos(P.omega * t1) - 0.25)) : 0.0;
-            c.pend = (st == 4 && last) ? (phase == 0 ? 2 : 1) : 0;
+            c.fscale = (Real)sc[2 * si];
+            c.acc_c = sc[2 * si + 1];
+            c.pend = (st == 4 && k + 1 == P.nt) ? (phase == 0 ? 2 : 1) : 0;
             c.W = P.W;
             c.c0 = P.c0;
             c.part = P.part + (size_t)ci * kWsConsumers * 2;
