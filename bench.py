@@ -394,7 +394,7 @@ def waveholtz_batched(device: int, count: int = 16, seed: int = 4) -> dict:
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     _, it32, _, _ = b32.solve(Fs, 3e-6, 2000, W=Wb, stall_limit=3)
-    _, it64, r64, st = b64.solve(Fs, 1e-6, 2000, W=Wb, warm=[1] * count)
+    _, it64, r64, st = b64.solve(Fs, 1e-6, 2000, W=Wb, warm=[1] * count, pi0_norm=b32.pi0_norm)
     torch.cuda.synchronize()
     t_batch = time.perf_counter() - t0
     err = max((Wb[i] - Wp[i]).norm().item() / Wp[i].norm().item() for i in range(count))

@@ -218,18 +218,23 @@ void wdg_whbatch_destroy(wdg_whbatch *batch);
 int wdg_whbatch_params(const wdg_whbatch *batch, int solve, double *T, double *dt, int *nt);
 /* chunk = rounds x (4 warps x floor(32 / n) elements) per solve; ring = chunk slots (2..6) */
 int wdg_whbatch_set_launch(wdg_whbatch *batch, int rounds, int ring);
+/* grid: CTAs of one launch of an RK stage without the filter, summed over the degree groups */
 int wdg_whbatch_get_launch(const wdg_whbatch *batch, int *rounds, int *ring, int *grid);
 /* times `steps` batch steps of every launch shape that fits and keeps the fastest */
 int wdg_whbatch_autotune(wdg_whbatch *batch, int steps, float *best_ms_per_step);
 /* F[s], W[s]: FP64 arrays (host or device) of solve s.  warm (nullable): warm[s] != 0 starts
- * solve s from W[s] (one extra period from zero then gives |pi0|), else from zero.  A solve
- * stops at residual < tol (status 0), after maxit iterations (1), or when stall_limit > 0
- * updates in a row bring no new smallest residual (2: the stepping precision's floor).
+ * solve s from W[s] (one extra period from zero then gives |pi0|), else from zero.
+ * pi0_norm (nullable, in/out): a warm-started solve with pi0_norm[s] > 0 takes that value as
+ * |pi0| and skips the extra period (e.g. the norm an FP32 batch of the same problems measured);
+ * on return pi0_norm[s] holds the |pi0| that scaled solve s's residual.  A solve stops at
+ * residual < tol (status 0), after maxit iterations (1), or when stall_limit > 0 updates in a
+ * row bring no new smallest residual (2: the stepping precision's floor).
  * W[s] receives the last iterate; iters, residuals, status (nullable) get one entry per solve.
  * Runs after the work already queued on the solves' streams (device inputs written there are
  * complete before they are read) and returns when the results are written. */
 int wdg_whbatch_solve(wdg_whbatch *batch, const double *const *F, double tol, int maxit, int stall_limit,
-                      double *const *W, const int *warm, int *iters, double *residuals, int *status);
+                      double *const *W, const int *warm, double *pi0_norm, int *iters, double *residuals,
+                      int *status);
 
 #ifdef __cplusplus
 }

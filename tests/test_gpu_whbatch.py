@@ -103,6 +103,26 @@ def test_warm_start_and_early_exit(gpu_lib):
         assert rel(Ws[s], W0[s]) < 1e-6
 
 
+def test_known_pi0_skips_the_extra_period(gpu_lib):
+    """A warm start given |pi0| starts from W at once and follows the same iterates as one
+    that measures |pi0| first; the norms reported match the zero start's first period."""
+    W, probs, systems, Fs = _batch_problems()
+    b = W.WaveHoltzBatch(systems, [p[3] for p in probs])
+    W0, _, _, _ = b.solve(Fs, 1e-8, 400)
+    p0 = b.pi0_norm.copy()
+    assert (p0 > 0).all()
+    rng = np.random.default_rng(2)
+    guess = [x + 1e-4 * np.linalg.norm(x) / np.sqrt(x.size) * rng.standard_normal(x.size) for x in W0]
+    Wa, ita, ra, sa = b.solve(Fs, 1e-8, 400, W=[x.copy() for x in guess], warm=[1, 1, 1])
+    assert np.array_equal(b.pi0_norm, p0)
+    Wb, itb, rb, sb = b.solve(Fs, 1e-8, 400, W=[x.copy() for x in guess], warm=[1, 1, 1], pi0_norm=p0)
+    assert np.array_equal(b.pi0_norm, p0)
+    assert (sa == 0).all() and (sb == 0).all() and (ita == itb).all()
+    for s in range(3):
+        assert rel(Wb[s], Wa[s]) < 1e-13
+        assert abs(rb[s] - ra[s]) <= 1e-12 * ra[s]
+
+
 def test_device_inputs_written_just_before_the_solve(gpu_lib):
     """Warm starts and forcing written on the caller's stream right before solve() are read
     only once complete (the batch orders its own stream after the solves' streams)."""
@@ -139,8 +159,14 @@ def test_fp32_batch_and_fp64_finish(gpu_lib):
     print("FP32 batch: iterations", it32.tolist(), "residuals", res32.tolist(), "status", st32.tolist())
     _, _, systems64, _ = _batch_problems("fp64")
     b64 = W.WaveHoltzBatch(systems64, [p[3] for p in probs])
+    p32 = b32.pi0_norm.copy()
     Wf, itf, resf, stf = b64.solve(Fs, 1e-6, 300, W=[x.copy() for x in W32], warm=[1, 1, 1])
     assert (stf == 0).all() and (resf < 1e-6).all()
+    p64 = b64.pi0_norm.copy()
+    # the FP32 batch's |pi0| serves the FP64 finish in place of its own pi0 period
+    assert np.allclose(p32, p64, rtol=1e-5, atol=0)
+    Wk, itk, resk, stk = b64.solve(Fs, 1e-6, 300, W=[x.copy() for x in W32], warm=[1, 1, 1], pi0_norm=p32)
+    assert (stk == 0).all() and (resk < 1e-6).all() and (np.abs(itk - itf) <= 1).all()
     Wd, itd, _, _ = b64.solve(Fs, 1e-6, 300)
     for s in range(3):
         err32 = rel(W32[s], Wd[s])

@@ -101,7 +101,7 @@ SIGNATURES = {
     "wdg_whbatch_set_launch": ([_v, _i, _i], _i),
     "wdg_whbatch_get_launch": ([_v, _ip, _ip, _ip], _i),
     "wdg_whbatch_autotune": ([_v, _i, C.POINTER(C.c_float)], _i),
-    "wdg_whbatch_solve": ([_v, _v, _d, _i, _i, _v, _v, _v, _v, _v], _i),
+    "wdg_whbatch_solve": ([_v, _v, _d, _i, _i, _v, _v, _v, _v, _v, _v], _i),
     # learned warm start (include/wdg_fno.h)
     "wdg_fno_gemm": ([_v, _v, _v, _i, _i, _i, _ll, _ll, _ll, _ll, _ll, _ll, _i, _i, _i, C.c_float, C.c_float, _i,
                       _v], _i),

@@ -1008,10 +1008,11 @@ namespace wdg
 namespace wdg
 {
     int ws_chunk_unit(int n) { return kWsConsumers * ws_epw(n); }
-    int ws_slot_bytes(int n, bool fp32, int chunk, bool extra)
+    int ws_slot_bytes(int n, bool fp32, int chunk, bool extra, bool filter)
     {
-        return fp32 ? ws_slot<float>(n, chunk, WsStage<float, true>::value && extra).bytes
-                    : ws_slot<double>(n, chunk, WsStage<double, true>::value && extra).bytes;
+        const bool staged = extra && (fp32 ? WsStage<float, true>::value : WsStage<double, true>::value);
+        const WsSlot o = fp32 ? ws_slot<float>(n, chunk, staged) : ws_slot<double>(n, chunk, staged);
+        return (staged && !filter) ? o.ab : o.bytes;
     }
     int ws_warp_scratch_bytes(int n, bool fp32)
     {

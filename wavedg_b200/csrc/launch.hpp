@@ -78,8 +78,10 @@ namespace wdg
 
     // warp-specialised stage kernels: one producer warp + kWsConsumers consumer warps per CTA
     constexpr int kWsConsumers = 4;
-    // one ring slot of an n, chunk-element chunk (extra: of a launch with forcing and filter)
-    int ws_slot_bytes(int n, bool fp32, int chunk, bool extra = false);
+    // one ring slot of an n, chunk-element chunk (extra: of a launch with forcing and filter;
+    // filter false: a staged launch that does not touch the filter, whose slot stops before
+    // the filter accumulator's region, the slot's last)
+    int ws_slot_bytes(int n, bool fp32, int chunk, bool extra = false, bool filter = true);
     int ws_warp_scratch_bytes(int n, bool fp32);    // one consumer warp's scratch
 
     // ---- batched WaveHoltz (kernels in stage_ws_batch.cuh, C-ABI in whbatch.cu)

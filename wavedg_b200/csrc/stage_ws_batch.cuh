@@ -27,8 +27,13 @@ namespace wdg
         return (128 + 16 * kMaxBatch + 2 * n * real_size + 3 * kMaxBatch * 4 + 127) & ~127;
     }
 
+    // CTAs per SM the registers are budgeted for: FP32 stages of degree <= 4 fit three
+    // (at most 65536 / (3 x 160) registers a thread, no spills); the rest keep two
     template <int N, typename Real>
-    __global__ void __launch_bounds__(kWsThreads, 2) whb_stage_kernel(const __grid_constant__ WhbArgs<Real> a)
+    constexpr int whb_min_blocks() { return (sizeof(Real) == 4 && N <= 5) ? 3 : 2; }
+
+    template <int N, typename Real>
+    __global__ void __launch_bounds__(kWsThreads, whb_min_blocks<N, Real>()) whb_stage_kernel(const __grid_constant__ WhbArgs<Real> a)
     {
         const int S = a.ring, G = gridDim.x, st = a.stage;
         extern __shared__ __align__(128) unsigned char smem[];

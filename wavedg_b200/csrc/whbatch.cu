@@ -16,12 +16,15 @@
 
 using namespace wdg;
 
-// the solves of one degree: one launch per RK stage
+// the solves of one degree: one launch per RK stage.  The filter stage (the fifth) stages the
+// FP64 filter accumulator through its slots as well; the other four stop their slots before
+// it, so FP32 launches of those stages fit more CTAs per SM (`_nf`: no filter)
 struct WhbGroup
 {
     int n = 0, s_lo = 0, s_hi = 0, it_lo = 0, it_hi = 0;
     int slot_bytes = 0, warp_scratch = 0, grid = 0;
-    size_t smem = 0;
+    int slot_nf = 0, grid_nf = 0;
+    size_t smem = 0, smem_nf = 0;
     cudaStream_t st = nullptr; // forked stream of the captured graph (groups run concurrently)
     cudaEvent_t done = nullptr;
 };
@@ -84,16 +87,22 @@ namespace
         std::vector<WhbGroup> gs = b->groups;
         for (WhbGroup &g : gs)
         {
-            g.slot_bytes = ws_slot_bytes(g.n, fp32, rounds * ws_chunk_unit(g.n), true);
+            const int ch = rounds * ws_chunk_unit(g.n);
+            g.slot_bytes = ws_slot_bytes(g.n, fp32, ch, true, true);
+            g.slot_nf = ws_slot_bytes(g.n, fp32, ch, true, false);
             g.warp_scratch = ws_warp_scratch_bytes(g.n, fp32);
             g.smem = (size_t)whb_smem_bytes(g.n, g.slot_bytes, g.warp_scratch, ring, fp32);
+            g.smem_nf = (size_t)whb_smem_bytes(g.n, g.slot_nf, g.warp_scratch, ring, fp32);
             if (g.smem > 227 * 1024)
                 return fail(WDG_ERR_ARG, "batched WaveHoltz: chunk x ring too large for shared memory");
             g.it_lo = it0[g.s_lo];
             g.it_hi = it0[g.s_hi - 1] + nch[g.s_hi - 1];
-            int grid = 0;
+            int grid = 0, grid_nf = 0;
             WDG_CUDA(fp32 ? whb_occupancy<float>(g.n, g.smem, &grid) : whb_occupancy<double>(g.n, g.smem, &grid));
+            WDG_CUDA(fp32 ? whb_occupancy<float>(g.n, g.smem_nf, &grid_nf)
+                          : whb_occupancy<double>(g.n, g.smem_nf, &grid_nf));
             g.grid = std::max(1, std::min(grid, g.it_hi - g.it_lo));
+            g.grid_nf = std::max(1, std::min(grid_nf, g.it_hi - g.it_lo));
         }
         // partial sums: nchunks x consumer warps x 2 per solve, grown as needed
         for (int s = 0; s < b->n; ++s)
@@ -135,7 +144,7 @@ namespace
         a.it_hi = g.it_hi;
         a.stage = stage;
         a.ring = b->ring;
-        a.slot_bytes = g.slot_bytes;
+        a.slot_bytes = stage == 4 ? g.slot_bytes : g.slot_nf;
         a.warp_scratch = g.warp_scratch;
         a.state = b->d_state;
         a.err = b->w[0]->d_err;
@@ -169,7 +178,8 @@ namespace
     cudaError_t launch_group(const wdg_whbatch *b, const WhbGroup &g, int stage, cudaStream_t st)
     {
         const WhbArgs<Real> a = make_args<Real>(b, g, stage);
-        return launch_whb_stage<Real>(a, g.n, g.grid, g.smem, st);
+        return stage == 4 ? launch_whb_stage<Real>(a, g.n, g.grid, g.smem, st)
+                          : launch_whb_stage<Real>(a, g.n, g.grid_nf, g.smem_nf, st);
     }
 
     // kGraphSteps steps (per stage one launch per degree group, the groups on forked streams,
@@ -244,11 +254,14 @@ namespace
         return WDG_OK;
     }
 
-    WhbState fresh_state(const wdg_whbatch *b, int s, bool warm, double tol, int maxit, int stall_limit)
+    // known_pi0sq > 0 (warm starts only): |pi0|^2 given, so the solve skips its pi0 period
+    WhbState fresh_state(const wdg_whbatch *b, int s, bool warm, double tol, int maxit, int stall_limit,
+                         double known_pi0sq = 0.0)
     {
         WhbState S{};
         S.k = 0;
-        S.phase = warm ? 0 : 1;
+        S.phase = (warm && !(known_pi0sq > 0.0)) ? 0 : 1;
+        S.pi0sq = warm ? known_pi0sq : 0.0;
         S.active = 1;
         S.zero_start = warm ? 0 : 1;
         S.nt = b->nt[s];
@@ -435,13 +448,14 @@ extern "C"
         {
             *grid = 0;
             for (const WhbGroup &gr : b->groups)
-                *grid += gr.grid;
+                *grid += gr.grid_nf;
         }
         return WDG_OK;
     }
 
     int wdg_whbatch_solve(wdg_whbatch *b, const double *const *F, double tol, int maxit, int stall_limit,
-                          double *const *W, const int *warm, int *iters, double *residuals, int *status)
+                          double *const *W, const int *warm, double *pi0_norm, int *iters, double *residuals,
+                          int *status)
     {
         if (!b || !F || !W || maxit < 1 || stall_limit < 0 || !(tol > 0.0))
             return fail(WDG_ERR_ARG, "wdg_whbatch_solve: bad arguments");
@@ -463,14 +477,26 @@ extern "C"
             else
                 WDG_CUDA(cudaMemcpyAsync(b->d_F[s], b->d_W[s], sizeof(double) * nd, cudaMemcpyDeviceToDevice, b->cs));
             // zero start: fixed-point periods from W = 0 (the first yields pi0); warm start:
-            // a pi0 period from zero first (its norm scales the residual), then from W
+            // a pi0 period from zero first (its norm scales the residual), then from W --
+            // or, with |pi0| given, straight from W (state W, filter 0.5 dt K(0) W)
             const bool ws = warm && warm[u];
+            const double known = (ws && pi0_norm && pi0_norm[u] > 0.0) ? pi0_norm[u] * pi0_norm[u] : 0.0;
             if (ws)
                 WDG_CUDA(cudaMemcpyAsync(b->d_W[s], W[u], sizeof(double) * nd, cudaMemcpyDefault, b->cs));
             else
                 WDG_CUDA(cudaMemsetAsync(b->d_W[s], 0, sizeof(double) * nd, b->cs));
-            WDG_TRY(zero_period(b, s));
-            b->h_state[s] = fresh_state(b, s, ws, tol, maxit, stall_limit);
+            if (known > 0.0)
+            {
+                if (b->precision == WDG_FP32)
+                    WDG_CUDA(launch_scale_into<float>(b->d_W[s], static_cast<float *>(w->d_state[0]), b->d_acc[s],
+                                                      b->c0[s], (long long)nd, b->cs));
+                else
+                    WDG_CUDA(launch_scale_into<double>(b->d_W[s], static_cast<double *>(w->d_state[0]),
+                                                       b->d_acc[s], b->c0[s], (long long)nd, b->cs));
+            }
+            else
+                WDG_TRY(zero_period(b, s));
+            b->h_state[s] = fresh_state(b, s, ws, tol, maxit, stall_limit, known);
         }
         WDG_CUDA(cudaMemcpyAsync(b->d_state, b->h_state, sizeof(WhbState) * b->n, cudaMemcpyHostToDevice, b->cs));
         if (!b->graph)
@@ -503,6 +529,8 @@ extern "C"
                 residuals[u] = b->h_state[s].residual;
             if (status)
                 status[u] = b->h_state[s].status;
+            if (pi0_norm)
+                pi0_norm[u] = std::sqrt(std::max(0.0, b->h_state[s].pi0sq));
         }
         WDG_CUDA(cudaStreamSynchronize(b->cs));
         if (running)

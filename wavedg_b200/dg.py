@@ -577,6 +577,7 @@ class WaveHoltzBatch:
         self._h = h
         self.omegas = om
         self.n = n
+        self.pi0_norm = None  # |pi0| per solve, after a solve
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -602,10 +603,13 @@ class WaveHoltzBatch:
         check(lib().wdg_whbatch_autotune(self._h, int(steps), C.byref(ms)), "WaveHoltzBatch.autotune")
         return ms.value
 
-    def solve(self, F, tol: float = 1e-6, maxit: int = 1000, W=None, warm=None, stall_limit: int = 0):
+    def solve(self, F, tol: float = 1e-6, maxit: int = 1000, W=None, warm=None, stall_limit: int = 0,
+              pi0_norm=None):
         """Solve every problem.  F, W: one float64 array per solve (numpy or CUDA tensors);
         W (optional) holds initial guesses where warm[s] is true and receives the iterates.
-        Returns (W, iters, residuals, status)."""
+        pi0_norm (optional): per solve a known |pi0| (> 0) that lets a warm-started solve skip
+        the period that measures it.  After the call `self.pi0_norm` holds the |pi0| each solve
+        used.  Returns (W, iters, residuals, status)."""
         n = self.n
         if len(F) != n:
             raise ValueError("one forcing per solve")
@@ -624,10 +628,13 @@ class WaveHoltzBatch:
         it = np.zeros(n, dtype=np.int32)
         res = np.zeros(n)
         stt = np.zeros(n, dtype=np.int32)
+        p0 = np.zeros(n) if pi0_norm is None else np.array(np.broadcast_to(np.asarray(pi0_norm, dtype=np.float64), (n,)))
         check(lib().wdg_whbatch_solve(self._h, fp, float(tol), int(maxit), int(stall_limit), wp,
                                       None if wm is None else C.c_void_p(wm.ctypes.data),
+                                      C.c_void_p(p0.ctypes.data),
                                       C.c_void_p(it.ctypes.data), C.c_void_p(res.ctypes.data),
                                       C.c_void_p(stt.ctypes.data)), "WaveHoltzBatch.solve")
+        self.pi0_norm = p0
         return W, it, res, stt
 
 

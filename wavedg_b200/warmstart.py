@@ -8,7 +8,8 @@ Pipeline (all on one GPU, all through this library's kernels):
             training tolerance, resampled from the DG nodes to the FNO grid (exact element
             polynomials), scaled to unit RMS;
   train     the FNO (fno.FNO, BF16 operands, FP32 accumulation, hand-written backward),
-            Adam with a cosine learning-rate schedule, MSE on the grid;
+            Adam with a cosine learning-rate schedule, MSE on the grid, each sample moved by a
+            random symmetry of the square (eight pairs per solve);
   evaluate  fresh seeded problems solved three ways, each to the same FP64 residual 1e-6:
             plain FP64 WaveHoltz one solve at a time (the baseline), batched FP32 +
             FP64 finish from zero, and the same from the network's prediction.  The plain
@@ -30,6 +31,53 @@ OMEGA, SIGMA, NE, NCOLLOC = 20.0, 0.05, 128, 5
 
 def centers(count: int, seed: int) -> np.ndarray:
     return np.random.default_rng(seed).uniform(-0.5, 0.5, size=(count, 2))
+
+
+# The family is invariant under the eight symmetries of the square (uniform mesh of [-1, 1]^2,
+# the same boundary code on every wall, source centres drawn from a symmetric box): the
+# solution for the source at R c is (p, v)(x) -> (p(R^T x), R v(R^T x)).  Symmetry k applies,
+# in this order, x -> -x (bit 0), y -> -y (bit 1), x <-> y (bit 2).  The discrete operator
+# shares them, so one solve gives eight training pairs.
+def sym_centers(cs, k: int) -> np.ndarray:
+    c = np.array(cs, dtype=np.float64).reshape(-1, 2)
+    if k & 1:
+        c[:, 0] = -c[:, 0]
+    if k & 2:
+        c[:, 1] = -c[:, 1]
+    if k & 4:
+        c = c[:, ::-1].copy()
+    return c
+
+
+def sym_grid(g, k: int):
+    """Symmetry k of grid fields g[..., d, iy, ix] (d: p, v_x, v_y; torch tensor)."""
+    import torch
+
+    if k & 1:
+        g = torch.flip(g, dims=(-1,))
+        g = torch.stack((g[..., 0, :, :], -g[..., 1, :, :], g[..., 2, :, :]), dim=-3)
+    if k & 2:
+        g = torch.flip(g, dims=(-2,))
+        g = torch.stack((g[..., 0, :, :], g[..., 1, :, :], -g[..., 2, :, :]), dim=-3)
+    if k & 4:
+        g = g.transpose(-1, -2)
+        g = torch.stack((g[..., 0, :, :], g[..., 2, :, :], g[..., 1, :, :]), dim=-3)
+    return g.contiguous()
+
+
+def sym_nodes(u, ne: int, n: int, k: int) -> np.ndarray:
+    """Symmetry k of a DG state of the uniform ne x ne mesh (element ex + ne ey, node a + n b,
+    fields p, v_x, v_y interleaved per node; numpy)."""
+    q = np.asarray(u).reshape(ne, ne, n, n, 3).copy()  # [ey, ex, b, a, d]
+    if k & 1:
+        q = q[:, ::-1, :, ::-1, :].copy()
+        q[..., 1] *= -1
+    if k & 2:
+        q = q[::-1, :, ::-1, :, :].copy()
+        q[..., 2] *= -1
+    if k & 4:
+        q = q.transpose(1, 0, 3, 2, 4)[..., [0, 2, 1]].copy()
+    return q.reshape(-1)
 
 
 class Family:
@@ -72,7 +120,8 @@ class Family:
         W, it32, r32, s32 = self.b32.solve(F, max(tol, tol32), maxit, W=W, warm=warm, stall_limit=3)
         if not fp64_finish:
             return W, it32, np.zeros_like(it32), r32, s32
-        W, it64, r64, s64 = self.b64.solve(F, tol, maxit, W=W, warm=[1] * n)
+        # the FP32 batch measured |pi0| (FP64 sums): the FP64 finish starts from W at once
+        W, it64, r64, s64 = self.b64.solve(F, tol, maxit, W=W, warm=[1] * n, pi0_norm=self.b32.pi0_norm)
         return W, it32, it64, r64, s64
 
 
@@ -98,7 +147,10 @@ def make_dataset(fam: Family, count: int, seed: int, tol: float, G: int, log=pri
     return cs, grids
 
 
-def train(net, cs, grids, epochs: int, batch: int = 4, lr: float = 2e-3, seed: int = 0, log=print):
+def train(net, cs, grids, epochs: int, batch: int = 4, lr: float = 2e-3, seed: int = 0, symmetries: bool = True,
+          log=print):
+    """Adam with a cosine schedule on the MSE; with `symmetries`, every sample of a batch is
+    moved by a random one of the square's eight symmetries (source and solution alike)."""
     from .fno import inputs
 
     t = net.torch
@@ -112,8 +164,13 @@ def train(net, cs, grids, epochs: int, batch: int = 4, lr: float = 2e-3, seed: i
         tot = 0.0
         for b0 in range(0, n, batch):
             idx = order[b0:b0 + batch]
-            inp = inputs(net.G, cs[idx], SIGMA, 1.0)
-            tgt = grids[t.from_numpy(idx).to("cuda")].contiguous()
+            if symmetries:
+                ks = rng.integers(0, 8, size=len(idx))
+                inp = inputs(net.G, np.concatenate([sym_centers(cs[i], int(q)) for i, q in zip(idx, ks)]), SIGMA, 1.0)
+                tgt = t.stack([sym_grid(grids[int(i)], int(q)) for i, q in zip(idx, ks)]).contiguous()
+            else:
+                inp = inputs(net.G, cs[idx], SIGMA, 1.0)
+                tgt = grids[t.from_numpy(idx).to("cuda")].contiguous()
             y = net.forward(inp, keep=True)
             sse, dy = net.mse(y, tgt)
             net.backward(dy)
@@ -207,6 +264,7 @@ def main(argv=None):
     ap.add_argument("--weights", default=None, help="load (if present) / save the network here")
     ap.add_argument("--json", default=None)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-symmetries", action="store_true", help="train without the square's symmetries")
     a = ap.parse_args(argv)
     import os
 
@@ -227,8 +285,9 @@ def main(argv=None):
         scale = math.sqrt(grids.square().mean().item())
         grids /= scale
         gen = time.perf_counter() - t0
-        hist, ttrain = train(net, cs, grids, a.epochs, seed=a.seed)
-        out["data"] = {"solutions": a.train, "tol": a.train_tol, "seconds": gen}
+        hist, ttrain = train(net, cs, grids, a.epochs, seed=a.seed, symmetries=not a.no_symmetries)
+        out["data"] = {"solutions": a.train, "tol": a.train_tol, "seconds": gen,
+                       "symmetries": 1 if a.no_symmetries else 8}
         out["training"] = {"epochs": a.epochs, "seconds": ttrain, "rel_rms_error": hist}
         del grids
         if a.weights:
