@@ -132,7 +132,7 @@ namespace wdg
     template <typename Real>
     cudaError_t launch_whb_stage(const WhbArgs<Real> &a, int n, int grid, size_t smem, cudaStream_t s);
     template <typename Real>
-    cudaError_t whb_occupancy(int n, size_t smem, int *grid);
+    cudaError_t whb_occupancy(int n, bool last, size_t smem, int *grid); // last: the fifth stage's kernel
     cudaError_t launch_whb_step_end(WhbState *state, int nsolves, cudaStream_t s);
 
     // fused stage: RK = true for the time-stepping epilogue

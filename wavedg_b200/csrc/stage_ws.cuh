@@ -87,11 +87,26 @@ namespace wdg
         // side SIDE runs from corner p0 to p1: 0: 0->1, 1: 1->2, 2: 3->2, 3: 0->3
         const double2 a0 = (SIDE == 0 || SIDE == 3) ? c01 : (SIDE == 1) ? c23 : c67;
         const double2 a1 = (SIDE == 0) ? c23 : (SIDE == 3) ? c67 : c45;
-        const double dx = a1.x - a0.x, dy = a1.y - a0.y;
-        const double s2 = dx * dx + dy * dy, rs = rsqrt(s2);
-        const double sgn = (SIDE >= 2) ? -1.0 : 1.0;
-        const Real nx = (Real)(sgn * dy * rs), ny = (Real)(-sgn * dx * rs);
-        const Real h = wk * (Real)(0.25 * s2 * rs);
+        Real nx, ny, h;
+        if constexpr (sizeof(Real) == 4)
+        {
+            // FP32 stepping: the side's length and normal in FP32 from FP64 corner differences
+            const float dx = (float)(a1.x - a0.x), dy = (float)(a1.y - a0.y);
+            const float s2 = dx * dx + dy * dy, rs = rsqrtf(s2);
+            const float sgn = (SIDE >= 2) ? -1.f : 1.f;
+            nx = sgn * dy * rs;
+            ny = -sgn * dx * rs;
+            h = wk * (0.25f * s2 * rs);
+        }
+        else
+        {
+            const double dx = a1.x - a0.x, dy = a1.y - a0.y;
+            const double s2 = dx * dx + dy * dy, rs = rsqrt(s2);
+            const double sgn = (SIDE >= 2) ? -1.0 : 1.0;
+            nx = (Real)(sgn * dy * rs);
+            ny = (Real)(-sgn * dx * rs);
+            h = wk * (Real)(0.25 * s2 * rs);
+        }
         const Real q[3] = {own[0], own[1], own[2]};
         Real x[3];
         if (bnd)
@@ -424,7 +439,10 @@ namespace wdg
                         const Real Yeta = Real(0.25) * ((Real(1) - xl) * ey0 + (Real(1) + xl) * ey1);
                         const Real W = Tab<Real>::w(N, l) * wj;
                         // MassMatrix<true>: w_i w_j det J (source/MassMatrix.cpp:6-28)
-                        mv[l] = Real(1) / (W * (Xxi * Yeta - Yxi * Xeta));
+                        if constexpr (sizeof(Real) == 4)
+                            mv[l] = __frcp_rn(W * (Xxi * Yeta - Yxi * Xeta));
+                        else
+                            mv[l] = Real(1) / (W * (Xxi * Yeta - Yxi * Xeta));
                         if (flags & F_VOL)
                         {
                             const Real WYe = W * Yeta, WXe = W * Xeta;

@@ -21,10 +21,11 @@ namespace wdg
     __constant__ double c_rk4a[5], c_rk4b[5], c_rk4c[5];
 
     // shared memory: [2 S mbarriers | pad 128][per solve: forcing scale, filter weight (FP64)]
-    //                [x (n), w (n)][per solve: k, phase, active][pad 128][S slots][consumer scratch]
+    //                [x (n), w (n)][per solve: k, phase, active][first item per solve, + end]
+    //                [pad 128][S slots][consumer scratch]
     __host__ __device__ inline int whb_slots_offset(int n, int real_size)
     {
-        return (128 + 16 * kMaxBatch + 2 * n * real_size + 3 * kMaxBatch * 4 + 127) & ~127;
+        return (128 + 16 * kMaxBatch + 2 * n * real_size + 3 * kMaxBatch * 4 + 4 * (kMaxBatch + 1) + 127) & ~127;
     }
 
     // CTAs per SM the registers are budgeted for: FP32 stages of degree <= 4 fit three
@@ -32,7 +33,8 @@ namespace wdg
     template <int N, typename Real>
     constexpr int whb_min_blocks() { return (sizeof(Real) == 4 && N <= 5) ? 3 : 2; }
 
-    template <int N, typename Real>
+    // LAST: the fifth RK stage (filter, period ends); the other four compile without that code
+    template <int N, typename Real, bool LAST>
     __global__ void __launch_bounds__(kWsThreads, whb_min_blocks<N, Real>()) whb_stage_kernel(const __grid_constant__ WhbArgs<Real> a)
     {
         const int S = a.ring, G = gridDim.x, st = a.stage;
@@ -43,6 +45,7 @@ namespace wdg
         Real *xt = reinterpret_cast<Real *>(smem + 128 + 16 * kMaxBatch); // GLL nodes, then weights
         Real *wt = xt + N;
         int *act = reinterpret_cast<int *>(smem + 128 + 16 * kMaxBatch + 2 * N * sizeof(Real)); // k, phase, active
+        int *it0 = act + 3 * kMaxBatch; // first item of each solve; it0[s_hi] = it_hi
         unsigned char *slots = smem + whb_slots_offset(N, (int)sizeof(Real));
         unsigned char *scratch = slots + S * a.slot_bytes;
 
@@ -71,24 +74,31 @@ namespace wdg
             const double ts = (k + c_rk4c[st]) * P.dt;
             sc[2 * q] = -sin(P.omega * ts) / P.omega;
             const double t1 = (k + 1) * P.dt;
-            sc[2 * q + 1] = (st == 4) ? ((k + 1 == P.nt) ? 0.5 : 1.0) * P.dt *
-                                            (P.omega / M_PI * (cos(P.omega * t1) - 0.25))
-                                      : 0.0;
+            sc[2 * q + 1] = LAST ? ((k + 1 == P.nt) ? 0.5 : 1.0) * P.dt * (P.omega / M_PI * (cos(P.omega * t1) - 0.25))
+                                 : 0.0;
+            it0[q] = P.item0;
         }
+        if (threadIdx.x == 0)
+            it0[a.s_hi] = a.it_hi;
         __syncthreads();
 
-        // item -> solve: the launch's solves' items are contiguous and ascending
+        // item -> solve: the launch's solves' items are contiguous and ascending.  A thread's
+        // successive items mostly fall in the solve of its previous one: try that first.
+        int hint = a.s_lo;
         auto solve_of = [&](int item)
         {
+            if (item >= it0[hint] && item < it0[hint + 1])
+                return hint;
             int lo = a.s_lo, hi = a.s_hi - 1;
             while (lo < hi)
             {
                 const int mid = (lo + hi + 1) >> 1;
-                if (a.s[mid].item0 <= item)
+                if (it0[mid] <= item)
                     lo = mid;
                 else
                     hi = mid - 1;
             }
+            hint = lo;
             return lo;
         };
         // the next item of this CTA at or after k whose solve is still running; producer and
@@ -104,11 +114,11 @@ namespace wdg
         {
             const int si = solve_of(item);
             const WhbSolve<Real> &P = a.s[si];
-            const int ci = item - P.item0;
+            const int ci = item - it0[si];
             const int k = act[3 * si], phase = act[3 * si + 1];
             // the RK4 buffer rotation A -> B -> C -> B -> C -> A
             const int src = (st == 0) ? 0 : (st % 2 == 1) ? 1 : 2;
-            const int dst = (st == 4) ? 0 : (st % 2 == 0) ? 1 : 2;
+            const int dst = LAST ? 0 : (st % 2 == 0) ? 1 : 2;
             c.u = P.buf[src];
             c.out = P.buf[dst];
             c.du = P.du;
@@ -122,13 +132,13 @@ namespace wdg
             c.chunk = P.chunk;
             c.el0 = ci * P.chunk;
             c.ne = min(P.chunk, P.nel - c.el0);
-            c.flags = F_ALL | F_FORCE | (st > 0 ? F_READ_DU : 0) | (st == 4 ? F_FILTER : 0);
+            c.flags = F_ALL | F_FORCE | (st > 0 ? F_READ_DU : 0) | (LAST ? F_FILTER : 0);
             c.rk_a = (Real)c_rk4a[st];
             c.rk_b = (Real)c_rk4b[st];
             c.dt = (Real)P.dt;
             c.fscale = (Real)sc[2 * si];
             c.acc_c = sc[2 * si + 1];
-            c.pend = (st == 4 && k + 1 == P.nt) ? (phase == 0 ? 2 : 1) : 0;
+            c.pend = (LAST && k + 1 == P.nt) ? (phase == 0 ? 2 : 1) : 0;
             c.W = P.W;
             c.c0 = P.c0;
             c.part = P.part + (size_t)ci * kWsConsumers * 2;
@@ -194,7 +204,7 @@ namespace wdg
                 break;
             }
             build(kc);
-            ws_consume<N, Real, true, true>(c, slots + q * a.slot_bytes, Rc, xt, wt, warp, lane);
+            ws_consume<N, Real, true, LAST>(c, slots + q * a.slot_bytes, Rc, xt, wt, warp, lane);
             // results are in the slot: hand them to the async proxy, then release the slot
             fence_async_smem();
             __syncwarp();
@@ -286,8 +296,16 @@ namespace wdg
     }
 
 #define WDG_WHB_CASES(X) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9)
+    template <typename K>
+    cudaError_t whb_occupancy_of(K kern, size_t smem, int *per_sm)
+    {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kern, kWsThreads, smem);
+        return e;
+    }
     template <typename Real>
-    cudaError_t whb_occupancy(int n, size_t smem, int *grid)
+    cudaError_t whb_occupancy(int n, bool last, size_t smem, int *grid)
     {
         int dev = 0, per_sm = 0, sms = 0;
         cudaGetDevice(&dev);
@@ -296,11 +314,10 @@ namespace wdg
         {
 #define WDG_X(NV)                                                                                           \
     case NV:                                                                                                \
-        e = cudaFuncSetAttribute(whb_stage_kernel<NV, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
-                                 227 * 1024);                                                               \
-        if (e == cudaSuccess)                                                                               \
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, whb_stage_kernel<NV, Real>,          \
-                                                              kWsThreads, smem);                            \
+        if (last)                                                                                           \
+            e = whb_occupancy_of(whb_stage_kernel<NV, Real, true>, smem, &per_sm);                          \
+        else                                                                                                \
+            e = whb_occupancy_of(whb_stage_kernel<NV, Real, false>, smem, &per_sm);                         \
         break;
             WDG_WHB_CASES(WDG_X)
 #undef WDG_X
@@ -315,11 +332,15 @@ namespace wdg
     template <typename Real>
     cudaError_t launch_whb_stage(const WhbArgs<Real> &a, int n, int grid, size_t smem, cudaStream_t s)
     {
+        const bool last = a.stage == 4;
         switch (n)
         {
-#define WDG_X(NV)                                                  \
-    case NV:                                                       \
-        whb_stage_kernel<NV, Real><<<grid, kWsThreads, smem, s>>>(a); \
+#define WDG_X(NV)                                                                \
+    case NV:                                                                     \
+        if (last)                                                                \
+            whb_stage_kernel<NV, Real, true><<<grid, kWsThreads, smem, s>>>(a);  \
+        else                                                                     \
+            whb_stage_kernel<NV, Real, false><<<grid, kWsThreads, smem, s>>>(a); \
         break;
             WDG_WHB_CASES(WDG_X)
 #undef WDG_X
@@ -351,6 +372,6 @@ namespace wdg
     }
     template cudaError_t launch_whb_stage<double>(const WhbArgs<double> &, int, int, size_t, cudaStream_t);
     template cudaError_t launch_whb_stage<float>(const WhbArgs<float> &, int, int, size_t, cudaStream_t);
-    template cudaError_t whb_occupancy<double>(int, size_t, int *);
-    template cudaError_t whb_occupancy<float>(int, size_t, int *);
+    template cudaError_t whb_occupancy<double>(int, bool, size_t, int *);
+    template cudaError_t whb_occupancy<float>(int, bool, size_t, int *);
 } // namespace wdg

@@ -98,9 +98,10 @@ namespace
             g.it_lo = it0[g.s_lo];
             g.it_hi = it0[g.s_hi - 1] + nch[g.s_hi - 1];
             int grid = 0, grid_nf = 0;
-            WDG_CUDA(fp32 ? whb_occupancy<float>(g.n, g.smem, &grid) : whb_occupancy<double>(g.n, g.smem, &grid));
-            WDG_CUDA(fp32 ? whb_occupancy<float>(g.n, g.smem_nf, &grid_nf)
-                          : whb_occupancy<double>(g.n, g.smem_nf, &grid_nf));
+            WDG_CUDA(fp32 ? whb_occupancy<float>(g.n, true, g.smem, &grid)
+                          : whb_occupancy<double>(g.n, true, g.smem, &grid));
+            WDG_CUDA(fp32 ? whb_occupancy<float>(g.n, false, g.smem_nf, &grid_nf)
+                          : whb_occupancy<double>(g.n, false, g.smem_nf, &grid_nf));
             g.grid = std::max(1, std::min(grid, g.it_hi - g.it_lo));
             g.grid_nf = std::max(1, std::min(grid_nf, g.it_hi - g.it_lo));
         }

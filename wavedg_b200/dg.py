@@ -30,6 +30,15 @@ from . import _lib
 from ._lib import WDG_FP32, WDG_FP64, WdgError, check, lib
 
 
+
+def _destroy(name: str, h) -> None:
+    """Release a handle from a finaliser.  At interpreter exit the loader's module state may
+    already be torn down; the process is ending and its device memory goes with it."""
+    try:
+        getattr(lib(), name)(h)
+    except Exception:
+        pass
+
 class FaceType:
     INTERIOR = 0
     BOUNDARY = 1
@@ -124,7 +133,7 @@ class Mesh2D:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            lib().wdg_mesh_destroy(h)
+            _destroy("wdg_mesh_destroy", h)
             self._h = None
 
     @staticmethod
@@ -209,7 +218,7 @@ class Discretisation:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            lib().wdg_wave_destroy(h)
+            _destroy("wdg_wave_destroy", h)
             self._h = None
 
     def set_stream(self, stream) -> None:
@@ -527,7 +536,7 @@ class WaveHoltz:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            lib().wdg_waveholtz_destroy(h)
+            _destroy("wdg_waveholtz_destroy", h)
             self._h = None
 
     def K(self, t: float) -> float:
@@ -582,7 +591,7 @@ class WaveHoltzBatch:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            lib().wdg_whbatch_destroy(h)
+            _destroy("wdg_whbatch_destroy", h)
             self._h = None
 
     def params(self, solve: int):

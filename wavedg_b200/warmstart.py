@@ -81,21 +81,22 @@ def sym_nodes(u, ne: int, n: int, k: int) -> np.ndarray:
 
 
 class Family:
-    """`nb` discretisations of the family's mesh per precision, batched."""
+    """`nb` discretisations of the family's mesh per precision, batched (ne x ne elements,
+    frequency omega; the defaults are the family above)."""
 
-    def __init__(self, nb: int = 64, device: int = 0):
+    def __init__(self, nb: int = 64, device: int = 0, ne: int = NE, omega: float = OMEGA):
         import torch
 
         from . import dg
 
-        self.torch, self.nb, self.device = torch, nb, device
-        self.mesh = dg.Mesh2D.uniform_rect(NE, -1.0, 1.0, NE, -1.0, 1.0)
+        self.torch, self.nb, self.device, self.ne, self.omega = torch, nb, device, ne, omega
+        self.mesh = dg.Mesh2D.uniform_rect(ne, -1.0, 1.0, ne, -1.0, 1.0)
         self.basis = dg.QuadratureRule.quadrature_rule(NCOLLOC, dg.QuadratureRule.GaussLobatto)
         self.bc = np.zeros(self.mesh.n_edges(1), dtype=np.int32)
         self.sys32 = [dg.WaveSystem(self.mesh, self.basis, self.bc, "fp32", device) for _ in range(nb)]
         self.sys64 = [dg.WaveSystem(self.mesh, self.basis, self.bc, "fp64", device) for _ in range(nb)]
-        self.b32 = dg.WaveHoltzBatch(self.sys32, [OMEGA] * nb)
-        self.b64 = dg.WaveHoltzBatch(self.sys64, [OMEGA] * nb)
+        self.b32 = dg.WaveHoltzBatch(self.sys32, [omega] * nb)
+        self.b64 = dg.WaveHoltzBatch(self.sys64, [omega] * nb)
         self.ndof = self.sys64[0].ndof
 
     def forcing(self, cs):
@@ -103,7 +104,7 @@ class Family:
         out = []
         for i, (cx, cy) in enumerate(cs):
             F = t.zeros(self.ndof, dtype=t.float64, device="cuda")
-            self.sys64[i % self.nb].load_gaussians([[cx, cy]], [SIGMA], [OMEGA ** 2], 1.0, 0, False, out=F)
+            self.sys64[i % self.nb].load_gaussians([[cx, cy]], [SIGMA], [self.omega ** 2], 1.0, 0, False, out=F)
             out.append(F)
         return out
 
@@ -125,12 +126,13 @@ class Family:
         return W, it32, it64, r64, s64
 
 
-def make_dataset(fam: Family, count: int, seed: int, tol: float, G: int, log=print):
-    """Solutions of `count` seeded problems on the G x G grid, plus their centres."""
+def make_dataset(fam: Family, count: int, seed: int, tol: float, G: int, net=None, scale: float = 1.0, log=print):
+    """Solutions of `count` seeded problems on the G x G grid, plus their centres.  With a
+    network, each solve starts from its prediction (fewer iterations to the same tolerance)."""
     from .fno import NodalGrid
 
     t = fam.torch
-    rs = NodalGrid(NE, NCOLLOC, G)
+    rs = NodalGrid(fam.ne, NCOLLOC, G)
     cs = centers(count, seed)
     grids = t.empty((count, 3, G, G), dtype=t.float32, device="cuda")
     for b0 in range(0, count, fam.nb):
@@ -138,7 +140,8 @@ def make_dataset(fam: Family, count: int, seed: int, tol: float, G: int, log=pri
         pad = fam.nb - len(blk)
         blk_full = np.concatenate([blk, blk[:pad]]) if pad else blk
         t0 = time.perf_counter()
-        W, it32, _, res, st = fam.solve(fam.forcing(blk_full), tol, fp64_finish=False)
+        W0 = predict(net, fam, blk_full, scale) if net is not None else None
+        W, it32, _, res, st = fam.solve(fam.forcing(blk_full), tol, W0=W0, fp64_finish=False)
         t.cuda.synchronize()
         log(f"  data {b0 + len(blk)}/{count}: FP32 iterations {int(it32.min())}-{int(it32.max())}, "
             f"{time.perf_counter() - t0:.1f} s")
@@ -184,19 +187,22 @@ def train(net, cs, grids, epochs: int, batch: int = 4, lr: float = 2e-3, seed: i
     return hist, time.perf_counter() - t0
 
 
-def predict(net, fam: Family, cs, scale: float):
-    """Warm starts at the DG nodes of the family's mesh for the problems centred at cs."""
+def predict(net, fam: Family, cs, scale: float, batch: int = 8):
+    """Warm starts at the DG nodes of the family's mesh for the problems centred at cs
+    (forward passes of `batch` problems at a time)."""
     from .fno import NodalGrid, inputs
 
-    rs = NodalGrid(NE, NCOLLOC, net.G)
+    rs = NodalGrid(fam.ne, NCOLLOC, net.G)
+    cs = np.asarray(cs, dtype=np.float64).reshape(-1, 2)
     out = []
-    for c in cs:
-        y = net.forward(inputs(net.G, np.asarray([c]), SIGMA, 1.0))
-        out.append(rs.to_nodes(y[0], scale))
+    for b0 in range(0, len(cs), batch):
+        y = net.forward(inputs(net.G, cs[b0:b0 + batch], SIGMA, 1.0))
+        out += [rs.to_nodes(y[i], scale) for i in range(y.shape[0])]
     return out
 
 
-def evaluate(net, fam: Family, count: int, seed: int, scale: float, n_plain: int = 4, log=print) -> dict:
+def evaluate(net, fam: Family, count: int, seed: int, scale: float, n_plain: int = 4, arms=("cold", "warm"),
+             log=print) -> dict:
     """Fresh problems to FP64 residual 1e-6: plain single FP64 solves (a sample of n_plain),
     batched cold, batched warm."""
     from . import dg
@@ -205,7 +211,7 @@ def evaluate(net, fam: Family, count: int, seed: int, scale: float, n_plain: int
     cs = centers(count, seed)
     res = {"problems": count, "tol": 1e-6}
     # plain FP64 WaveHoltz, one solve at a time (the reference's algorithm on the GPU)
-    wh = dg.WaveHoltz(OMEGA, fam.mesh, fam.basis, fam.bc, True)
+    wh = dg.WaveHoltz(fam.omega, fam.mesh, fam.basis, fam.bc, True)
     Fp = fam.forcing(cs[:n_plain])
     t.cuda.synchronize()
     t0 = time.perf_counter()
@@ -220,7 +226,7 @@ def evaluate(net, fam: Family, count: int, seed: int, scale: float, n_plain: int
     res["plain_fp64"] = {"solves": n_plain, "seconds": tp, "solves_per_s": n_plain / tp,
                          "iterations_mean": float(np.mean(plain_it))}
     log(f"  plain FP64: {n_plain} solves in {tp:.1f} s, iterations {plain_it}")
-    for arm in ("cold", "warm"):
+    for arm in arms:
         secs, it32s, it64s, errs = 0.0, [], [], []
         for b0 in range(0, count, fam.nb):
             blk = cs[b0:b0 + fam.nb]
@@ -247,9 +253,46 @@ def evaluate(net, fam: Family, count: int, seed: int, scale: float, n_plain: int
         log(f"  batched {arm}: {done} solves in {secs:.1f} s, FP32 iterations {np.mean(it32s):.1f}, "
             f"FP64 finish {np.mean(it64s):.1f}")
     base = res["plain_fp64"]["solves_per_s"]
-    res["speedup_batched_cold_vs_plain"] = res["batched_cold"]["solves_per_s"] / base
-    res["speedup_batched_warm_vs_plain"] = res["batched_warm"]["solves_per_s"] / base
+    for arm in arms:
+        res[f"speedup_batched_{arm}_vs_plain"] = res[f"batched_{arm}"]["solves_per_s"] / base
     return res
+
+
+def time_batch(nb: int, periods: int = 3, precisions=("fp32", "fp64"), autotune: bool = True, log=print) -> dict:
+    """Wall time of whole forced periods of an nb-solve batch of the family (fresh seeded
+    sources), per precision: seconds per period, per solve-period, and DOF-stage updates/s."""
+    import torch
+
+    from . import dg
+
+    mesh = dg.Mesh2D.uniform_rect(NE, -1.0, 1.0, NE, -1.0, 1.0)
+    basis = dg.QuadratureRule.quadrature_rule(NCOLLOC, dg.QuadratureRule.GaussLobatto)
+    bc = np.zeros(mesh.n_edges(1), dtype=np.int32)
+    out = {}
+    for prec in precisions:
+        ss = [dg.WaveSystem(mesh, basis, bc, prec) for _ in range(nb)]
+        b = dg.WaveHoltzBatch(ss, [OMEGA] * nb)
+        F = []
+        for i, c in enumerate(centers(nb, 9)):
+            f = torch.zeros(ss[0].ndof, dtype=torch.float64, device="cuda")
+            ss[i].load_gaussians([c], [SIGMA], [OMEGA ** 2], 1.0, 0, False, out=f)
+            F.append(f)
+        ms = b.autotune(64) if autotune else None
+        W = [torch.zeros_like(f) for f in F]
+        b.solve(F, 1e-30, 1, W=W)  # warm-up: one period (graph capture included)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b.solve(F, 1e-30, periods, W=W)
+        torch.cuda.synchronize()
+        per = (time.perf_counter() - t0) / periods
+        _, _, nt = b.params(0)
+        rec = {"solves": nb, "launch": b.launch_config(), "autotune_ms_per_step": ms, "seconds_per_period": per,
+               "ms_per_solve_period": per / nb * 1e3, "dof_stage_per_s": nb * ss[0].ndof * 5 * nt / per}
+        log(f"  {prec}: {nb} solves, {rec['launch']}, {per:.3f} s per period = {rec['ms_per_solve_period']:.1f} ms "
+            f"per solve-period, {rec['dof_stage_per_s']:.3e} DOF-stage/s")
+        out[prec] = rec
+        del b, ss
+    return out
 
 
 def main(argv=None):
@@ -265,8 +308,24 @@ def main(argv=None):
     ap.add_argument("--json", default=None)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-symmetries", action="store_true", help="train without the square's symmetries")
+    ap.add_argument("--finetune", action="store_true",
+                    help="load --weights, train further on fresh solutions (warm-started by the network), save")
+    ap.add_argument("--data-seed", type=int, default=None, help="seed of the training sources (default 1000 + seed)")
+    ap.add_argument("--lr", type=float, default=2e-3, help="peak learning rate")
+    ap.add_argument("--save", default=None, help="save the trained network here (default: --weights)")
+    ap.add_argument("--arms", default="cold,warm", help="batched arms evaluated (cold, warm)")
+    ap.add_argument("--time-batch", type=int, default=0, help="only time whole periods of a batch of this many solves")
+    ap.add_argument("--periods", type=int, default=3, help="--time-batch: periods timed")
+    ap.add_argument("--precision", choices=["fp32", "fp64", "both"], default="both", help="--time-batch precision")
+    ap.add_argument("--no-autotune", action="store_true", help="--time-batch: default launch shape")
     a = ap.parse_args(argv)
     import os
+
+    if a.time_batch:
+        prec = ("fp32", "fp64") if a.precision == "both" else (a.precision,)
+        out = time_batch(a.time_batch, a.periods, prec, not a.no_autotune)
+        print(json.dumps(out), flush=True)
+        return
 
     from .fno import FNO
 
@@ -274,27 +333,34 @@ def main(argv=None):
     net = FNO(grid=a.grid, width=32, modes=16, layers=4, hidden=64, seed=a.seed)
     out = {"family": "waveholtz_128x128_P4_omega20_outflow", "grid": a.grid,
            "fno": {"layers": 4, "width": 32, "modes": 16, "hidden": 64}}
-    if a.weights and os.path.exists(a.weights):
+    loaded = bool(a.weights and os.path.exists(a.weights))
+    if loaded:
         sd = dict(np.load(a.weights))
         scale = float(sd.pop("__scale__"))
         net.load_state_dict(sd)
         out["trained"] = "loaded"
-    else:
+    if not loaded or a.finetune:
         t0 = time.perf_counter()
-        cs, grids = make_dataset(fam, a.train, 1000 + a.seed, a.train_tol, a.grid)
-        scale = math.sqrt(grids.square().mean().item())
+        dseed = 1000 + a.seed if a.data_seed is None else a.data_seed
+        cs, grids = make_dataset(fam, a.train, dseed, a.train_tol, a.grid, net if loaded else None,
+                                 scale if loaded else 1.0)
+        if not loaded:
+            scale = math.sqrt(grids.square().mean().item())
         grids /= scale
         gen = time.perf_counter() - t0
-        hist, ttrain = train(net, cs, grids, a.epochs, seed=a.seed, symmetries=not a.no_symmetries)
-        out["data"] = {"solutions": a.train, "tol": a.train_tol, "seconds": gen,
-                       "symmetries": 1 if a.no_symmetries else 8}
-        out["training"] = {"epochs": a.epochs, "seconds": ttrain, "rel_rms_error": hist}
+        hist, ttrain = train(net, cs, grids, a.epochs, lr=a.lr, seed=a.seed, symmetries=not a.no_symmetries)
+        out["data"] = {"solutions": a.train, "seed": dseed, "tol": a.train_tol, "seconds": gen,
+                       "symmetries": 1 if a.no_symmetries else 8, "warm_started": loaded}
+        out["training"] = {"epochs": a.epochs, "lr": a.lr, "seconds": ttrain, "rel_rms_error": hist,
+                           "finetune": loaded}
         del grids
-        if a.weights:
+        dst = a.save or a.weights
+        if dst:
             sd = net.state_dict()
             sd["__scale__"] = np.array(scale)
-            np.savez(a.weights, **sd)
-    out["eval"] = evaluate(net, fam, a.eval, 5000 + a.seed, scale, a.plain)
+            np.savez(dst, **sd)
+    if a.eval:
+        out["eval"] = evaluate(net, fam, a.eval, 5000 + a.seed, scale, a.plain, arms=tuple(a.arms.split(",")))
     print(json.dumps(out), flush=True)
     if a.json:
         with open(a.json, "w") as f:
