@@ -70,6 +70,10 @@ int wdg_supported_degrees(int *n_colloc, int cap);
 int wdg_mesh_from_vertices(int n_vert, const double *xy, int n_elem, const int *quads, wdg_mesh **out);
 /* dg::Mesh2D::uniform_rect (source/Mesh2D.cpp:130-163) */
 int wdg_mesh_uniform_rect(int nx, double ax, double bx, int ny, double ay, double by, wdg_mesh **out);
+/* dg::Mesh2D::from_file (source/Mesh2D.cpp:94-128): dir/info.txt "n_points n_elements",
+ * dir/coordinates.txt one "x y" per point, dir/elements.txt four 0-based point indices per
+ * element; then as wdg_mesh_from_vertices.  Missing or short files are errors. */
+int wdg_mesh_from_file(const char *dir, wdg_mesh **out);
 /* Adopt the tables of an existing dg::Mesh2D (what a C++ drop-in reads through the reference's
  * public API): corners (2, 4, n_elem) = QuadElement::corner(c) (wavedg/Element.hpp:123-126);
  * per edge (el0, s0, el1, s1, delta) = Edge::{elements, sides, delta} (wavedg/Edge.hpp:37-49),
@@ -82,6 +86,12 @@ int wdg_mesh_n_edges(const wdg_mesh *mesh, int face_type);               /* Mesh
 int wdg_mesh_edges(const wdg_mesh *mesh, int face_type, int *out);        /* (el0, s0, el1, s1, delta) rows */
 int wdg_mesh_min_h(const wdg_mesh *mesh, double *h);                      /* Mesh2D::min_h (source/Mesh2D.cpp:751-767) */
 int wdg_mesh_boundary_midpoints(const wdg_mesh *mesh, double *xy);         /* edge_metrics(1-pt rule, BOUNDARY).physical_coordinates() */
+
+/* ------------------------------------------------------------------ snapshots */
+/* dg::to_file (examples/examples.hpp:14-19): n doubles as raw native-order bytes; u on the
+ * host or on the GPU.  wdg_read_raw reads such a file back (its size must be 8 n bytes). */
+int wdg_write_raw(const char *fname, long long n, const double *u);
+int wdg_read_raw(const char *fname, long long n, double *u);
 
 /* QuadratureRule::gauss_lobatto (source/QuadratureRule.cpp:32-97) and
  * lagrange_basis_deriv at the nodes (source/lagrange_interpolation.cpp:33-50):

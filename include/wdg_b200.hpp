@@ -208,6 +208,60 @@ namespace b200
         WaveSystem sys_;
         std::shared_ptr<wdg_waveholtz> h_;
     };
+
+    // Many independent WaveHoltz solves advanced together (wdg_whbatch_*; no reference
+    // counterpart: the reference runs one WaveHoltz object at a time).  The systems must share
+    // one precision and device and outlive the batch.
+    class WaveHoltzBatch
+    {
+    public:
+        struct Result
+        {
+            std::vector<int> iterations, status; // status 0 converged, 1 maxit, 2 stalled
+            std::vector<double> residual, pi0_norm;
+        };
+        WaveHoltzBatch(const std::vector<const WaveSystem *> &systems, const std::vector<double> &omegas)
+            : n_((int)systems.size())
+        {
+            if (omegas.size() != systems.size())
+                throw std::runtime_error("wdg_b200: one frequency per solve");
+            std::vector<wdg_wave *> w;
+            for (const WaveSystem *s : systems)
+                w.push_back(s->get());
+            wdg_whbatch *h = nullptr;
+            check(wdg_whbatch_create(n_, w.data(), omegas.data(), &h));
+            h_.reset(h, wdg_whbatch_destroy);
+        }
+        float autotune(int steps = 64) const
+        {
+            float ms = 0.f;
+            check(wdg_whbatch_autotune(h_.get(), steps, &ms));
+            return ms;
+        }
+        // F[s], W[s]: FP64 arrays of solve s (host or device); W receives the iterates.
+        // warm (optional): per solve, start from W[s]; pi0_norm (optional): known |pi0| per solve
+        Result solve(const std::vector<const double *> &F, const std::vector<double *> &W, double tol, int maxit,
+                     int stall_limit = 0, const std::vector<int> &warm = {},
+                     const std::vector<double> &pi0_norm = {}) const
+        {
+            if ((int)F.size() != n_ || (int)W.size() != n_ || (!warm.empty() && (int)warm.size() != n_) ||
+                (!pi0_norm.empty() && (int)pi0_norm.size() != n_))
+                throw std::runtime_error("wdg_b200: one forcing, iterate (and flag) per solve");
+            Result r;
+            r.iterations.assign(n_, 0);
+            r.status.assign(n_, -1);
+            r.residual.assign(n_, 0.0);
+            r.pi0_norm = pi0_norm.empty() ? std::vector<double>(n_, 0.0) : pi0_norm;
+            check(wdg_whbatch_solve(h_.get(), F.data(), tol, maxit, stall_limit, W.data(),
+                                    warm.empty() ? nullptr : warm.data(), r.pi0_norm.data(), r.iterations.data(),
+                                    r.residual.data(), r.status.data()));
+            return r;
+        }
+
+    private:
+        int n_;
+        std::shared_ptr<wdg_whbatch> h_;
+    };
 } // namespace b200
 } // namespace dg
 

@@ -31,6 +31,7 @@ _v, _i, _d = C.c_void_p, C.c_int, C.c_double
 
 _SIGS = {
     "mesh_create": ([_i, _dp, _i, _ip], _v),
+    "mesh_from_file": ([C.c_char_p], _v),
     "mesh_destroy": ([_v], None),
     "mesh_n_elem": ([_v], _i),
     "mesh_n_edges": ([_v, _i], _i),
@@ -98,6 +99,58 @@ def lib(kind: str = "oracle"):
     return ns
 
 
+_REF_READER = r"""
+import ctypes as C, struct, sys
+L = C.CDLL(sys.argv[1])
+L.ref_mesh_from_file.restype = C.c_void_p
+L.ref_mesh_from_file.argtypes = [C.c_char_p]
+L.ref_mesh_min_h.restype = C.c_double
+for f in ("ref_mesh_n_elem", "ref_mesh_n_edges", "ref_mesh_min_h", "ref_mesh_edges", "ref_mesh_boundary_midpoints",
+          "ref_mesh_destroy"):
+    getattr(L, f).argtypes = None
+h = L.ref_mesh_from_file(sys.argv[2].encode())
+with open(sys.argv[3], "wb") as out:
+    if not h:
+        out.write(struct.pack("<i", -1))
+        sys.exit(0)
+    h = C.c_void_p(h)
+    ne, ni, nb = L.ref_mesh_n_elem(h), L.ref_mesh_n_edges(h, 0), L.ref_mesh_n_edges(h, 1)
+    ei, eb, mp = (C.c_int * (5 * ni))(), (C.c_int * (5 * nb))(), (C.c_double * (2 * nb))()
+    L.ref_mesh_edges(h, 0, ei)
+    L.ref_mesh_edges(h, 1, eb)
+    L.ref_mesh_boundary_midpoints(h, mp)
+    out.write(struct.pack("<iiid", ne, ni, nb, L.ref_mesh_min_h(h)))
+    out.write(bytes(ei) + bytes(eb) + bytes(mp))
+"""
+
+
+def reference_mesh_from_file(directory):
+    """The reference's own Mesh2D::from_file (source/Mesh2D.cpp:94-128) through the compiled
+    reference, in a child process: its reader uses iostreams and the library carries its own
+    C++ runtime, which must not meet another one in the same process.  Returns the mesh tables
+    {n_elem, edges_interior, edges_boundary, min_h, midpoints}, or None on a reader error."""
+    import sys
+    import tempfile
+
+    path = LIBS["reference"][0]
+    with tempfile.TemporaryDirectory() as td:
+        f = os.path.join(td, "tables.bin")
+        subprocess.run([sys.executable, "-c", _REF_READER, path, str(directory), f], check=True, timeout=120)
+        raw = open(f, "rb").read()
+    ne = int(np.frombuffer(raw[:4], dtype="<i4")[0])
+    if ne < 0:
+        return None
+    ni, nb = (int(x) for x in np.frombuffer(raw[4:12], dtype="<i4"))
+    mh = float(np.frombuffer(raw[12:20], dtype="<f8")[0])
+    o = 20
+    ei = np.frombuffer(raw[o:o + 20 * ni], dtype=np.int32).reshape(ni, 5)
+    o += 20 * ni
+    eb = np.frombuffer(raw[o:o + 20 * nb], dtype=np.int32).reshape(nb, 5)
+    o += 20 * nb
+    mp = np.frombuffer(raw[o:o + 16 * nb], dtype=np.float64).reshape(nb, 2)
+    return {"n_elem": ne, "edges_interior": ei, "edges_boundary": eb, "min_h": mh, "midpoints": mp}
+
+
 def _f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
 
@@ -110,6 +163,15 @@ class Mesh:
         self.verts = _f64(verts).reshape(-1, 2)
         self.quads = np.ascontiguousarray(quads, dtype=np.int32).reshape(-1, 4)
         self.h = self.L.mesh_create(len(self.verts), self.verts.ravel(), len(self.quads), self.quads.ravel())
+
+    @classmethod
+    def from_file(cls, directory, kind="oracle"):
+        """Mesh2D::from_file on the CPU checker; None if the checker reports an error."""
+        self = cls.__new__(cls)
+        self.L = lib(kind)
+        self.verts = self.quads = None
+        self.h = self.L.mesh_from_file(os.fsencode(directory))
+        return self if self.h else None
 
     def __del__(self):
         if getattr(self, "h", None):

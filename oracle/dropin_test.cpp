@@ -148,6 +148,20 @@ int main()
     gwh.postprocess(H2.data(), s1.data());
     report("WaveHoltz::postprocess", rel(H2, H1), 1e-12);
 
+    // the batched solver on the same two problems as two single solves (exact same periods)
+    {
+        b200::WaveSystem sa(small, basis, bc2.data()), sb(small, basis, bc2.data());
+        b200::WaveHoltz wa(2.0, small, basis, bc2.data(), true), wb(3.0, small, basis, bc2.data(), true);
+        std::vector<double> Wa(nd2, 0.0), Wb(nd2, 0.0), Ba(nd2, 0.0), Bb(nd2, 0.0), ra(1), rb(1);
+        const int ia = wa.solve(F.data(), 1e-8, 40, Wa.data(), ra.data());
+        const int ib = wb.solve(F.data(), 1e-8, 40, Wb.data(), rb.data());
+        b200::WaveHoltzBatch batch({&sa, &sb}, {2.0, 3.0});
+        const auto res = batch.solve({F.data(), F.data()}, {Ba.data(), Bb.data()}, 1e-8, 40);
+        report("WaveHoltzBatch vs WaveHoltz::solve, omega 2", rel(Ba, Wa), 1e-10);
+        report("WaveHoltzBatch vs WaveHoltz::solve, omega 3", rel(Bb, Wb), 1e-10);
+        report("WaveHoltzBatch iteration counts", std::abs(res.iterations[0] - ia) + std::abs(res.iterations[1] - ib), 0.5);
+    }
+
     std::printf("%s\n", failures ? "DROP-IN FAILED" : "drop-in ok");
     return failures ? 1 : 0;
 }

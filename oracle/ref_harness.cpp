@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <stdexcept>
 #include <vector>
 
 #include "wavedg.hpp"
@@ -285,6 +286,19 @@ extern "C"
     void *ref_mesh_create(int nv, const double *xy, int nel, const int *quads)
     {
         return new RefMesh(Mesh2D::from_vertices(nv, xy, nel, quads));
+    }
+    // Mesh2D::from_file (source/Mesh2D.cpp:94-128), the reference's own reader; nullptr when it
+    // reports an error
+    void *ref_mesh_from_file(const char *dir)
+    {
+        try
+        {
+            return new RefMesh(Mesh2D::from_file(dir));
+        }
+        catch (const std::exception &)
+        {
+            return nullptr;
+        }
     }
     void ref_mesh_destroy(void *m) { delete static_cast<RefMesh *>(m); }
     int ref_mesh_n_elem(void *m) { return static_cast<RefMesh *>(m)->mesh.n_elem(); }

@@ -21,7 +21,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
+#include <string>
 #include <unordered_map>
 #include <vector>
 
@@ -729,6 +731,29 @@ namespace
 extern "C"
 {
     void *orc_mesh_create(int nv, const double *xy, int nel, const int *quads) { return make_mesh(nv, xy, nel, quads); }
+    // Mesh2D::from_file (source/Mesh2D.cpp:94-128): info.txt "n_pts n_elem", coordinates.txt
+    // "x y" per point, elements.txt four point indices per element, then from_vertices;
+    // nullptr if a file is missing or short
+    void *orc_mesh_from_file(const char *dir)
+    {
+        // C stdio, not iostreams: this library may share a process with another C++ runtime
+        const std::string d(dir);
+        FILE *info = std::fopen((d + "/info.txt").c_str(), "r");
+        FILE *coo = std::fopen((d + "/coordinates.txt").c_str(), "r");
+        FILE *els = std::fopen((d + "/elements.txt").c_str(), "r");
+        int np = 0, ne = 0;
+        bool ok = info && coo && els && std::fscanf(info, "%d %d", &np, &ne) == 2 && np >= 1 && ne >= 1;
+        std::vector<double> xy(ok ? 2 * (size_t)np : 0);
+        std::vector<int> q(ok ? 4 * (size_t)ne : 0);
+        for (size_t i = 0; ok && i < xy.size(); ++i)
+            ok = std::fscanf(coo, "%lf", &xy[i]) == 1;
+        for (size_t i = 0; ok && i < q.size(); ++i)
+            ok = std::fscanf(els, "%d", &q[i]) == 1;
+        for (FILE *f : {info, coo, els})
+            if (f)
+                std::fclose(f);
+        return ok ? make_mesh(np, xy.data(), ne, q.data()) : nullptr;
+    }
     void orc_mesh_destroy(void *m) { delete static_cast<Mesh *>(m); }
     int orc_mesh_n_elem(void *m) { return static_cast<Mesh *>(m)->nel; }
     int orc_mesh_n_edges(void *m, int type)

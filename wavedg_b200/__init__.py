@@ -24,10 +24,12 @@ from .dg import (  # noqa: F401
     error,
     make_face_prolongator,
     norm,
+    read_file,
+    to_file,
 )
 
 __all__ = [
-    "Discretisation", "Div", "EdgeFlux", "FaceProlongator", "FaceType", "LinearFunctional2D", "MassMatrix",
+    "read_file", "to_file", "Discretisation", "Div", "EdgeFlux", "FaceProlongator", "FaceType", "LinearFunctional2D", "MassMatrix",
     "Mesh2D", "Operator", "QuadratureRule", "RungeKutta4", "WaveBC", "WaveEquation", "WaveHoltz", "WaveHoltzBatch", "WaveSystem",
     "WdgError", "WDG_FP32", "WDG_FP64", "error", "lib", "make_face_prolongator", "norm",
 ]

@@ -45,6 +45,9 @@ SIGNATURES = {
     "wdg_supported_degrees": ([_ip, _i], _i),
     "wdg_mesh_from_vertices": ([_i, _v, _i, _v, _vp], _i),
     "wdg_mesh_uniform_rect": ([_i, _d, _d, _i, _d, _d, _vp], _i),
+    "wdg_mesh_from_file": ([C.c_char_p, _vp], _i),
+    "wdg_write_raw": ([C.c_char_p, _ll, _v], _i),
+    "wdg_read_raw": ([C.c_char_p, _ll, _v], _i),
     "wdg_mesh_from_tables": ([_i, _v, _i, _v, _i, _v, _vp], _i),
     "wdg_mesh_destroy": ([_v], None),
     "wdg_mesh_n_elem": ([_v], _i),

@@ -4,6 +4,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <fstream>
+#include <string>
 #include <unordered_map>
 
 #include "common.hpp"
@@ -430,6 +432,95 @@ extern "C"
             const double x1 = c[2 * kSideTo[E.s0]], y1 = c[2 * kSideTo[E.s0] + 1];
             xy[2 * e] = x0 + (x1 - x0) * 0.5;
             xy[2 * e + 1] = y0 + (y1 - y0) * 0.5;
+        }
+        return WDG_OK;
+    }
+
+    // Mesh2D::from_file (source/Mesh2D.cpp:94-128): <dir>/info.txt holds "n_points n_elements",
+    // coordinates.txt one "x y" line per point, elements.txt four 0-based point indices per
+    // element; the mesh is then built as from_vertices does.  Unlike the reference, a short
+    // or unreadable file is an error rather than uninitialised data.
+    int wdg_mesh_from_file(const char *dir, wdg_mesh **out)
+    {
+        if (!dir || !out)
+            return fail(WDG_ERR_ARG, "wdg_mesh_from_file: bad arguments");
+        *out = nullptr;
+        const std::string d(dir);
+        std::ifstream info(d + "/info.txt");
+        if (!info)
+            return fail(WDG_ERR_ARG, "wdg_mesh_from_file: cannot open " + d + "/info.txt");
+        long long np = 0, ne = 0;
+        if (!(info >> np >> ne) || np < 3 || ne < 1 || np > (1ll << 30) || ne > (1ll << 29))
+            return fail(WDG_ERR_ARG, "wdg_mesh_from_file: " + d + "/info.txt must hold two positive counts");
+        std::ifstream coo(d + "/coordinates.txt");
+        if (!coo)
+            return fail(WDG_ERR_ARG, "wdg_mesh_from_file: cannot open " + d + "/coordinates.txt");
+        std::vector<double> xy(2 * (size_t)np);
+        for (long long i = 0; i < 2 * np; ++i)
+            if (!(coo >> xy[(size_t)i]))
+                return fail(WDG_ERR_ARG, "wdg_mesh_from_file: " + d + "/coordinates.txt has fewer than " +
+                                             std::to_string(np) + " points");
+        std::ifstream el(d + "/elements.txt");
+        if (!el)
+            return fail(WDG_ERR_ARG, "wdg_mesh_from_file: cannot open " + d + "/elements.txt");
+        std::vector<int> q(4 * (size_t)ne);
+        for (long long i = 0; i < 4 * ne; ++i)
+            if (!(el >> q[(size_t)i]))
+                return fail(WDG_ERR_ARG, "wdg_mesh_from_file: " + d + "/elements.txt has fewer than " +
+                                             std::to_string(ne) + " elements");
+        return wdg_mesh_from_vertices((int)np, xy.data(), (int)ne, q.data(), out);
+    }
+
+    // dg::to_file (examples/examples.hpp:14-19): n doubles, raw native byte order; u on the
+    // host or on a GPU
+    int wdg_write_raw(const char *fname, long long n, const double *u)
+    {
+        if (!fname || n < 0 || (n > 0 && !u))
+            return fail(WDG_ERR_ARG, "wdg_write_raw: bad arguments");
+        std::vector<double> host;
+        const double *src = u;
+        cudaPointerAttributes at{};
+        if (n > 0 && cudaPointerGetAttributes(&at, u) == cudaSuccess && at.type == cudaMemoryTypeDevice)
+        {
+            host.resize((size_t)n);
+            WDG_CUDA(cudaMemcpy(host.data(), u, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost));
+            src = host.data();
+        }
+        cudaGetLastError(); // a host pointer on a machine without a GPU leaves an error behind
+        std::ofstream f(fname, std::ios::out | std::ios::binary);
+        if (!f)
+            return fail(WDG_ERR_ARG, std::string("wdg_write_raw: cannot open ") + fname);
+        f.write(reinterpret_cast<const char *>(src), (std::streamsize)(sizeof(double) * (size_t)n));
+        if (!f)
+            return fail(WDG_ERR_ARG, std::string("wdg_write_raw: short write to ") + fname);
+        return WDG_OK;
+    }
+
+    // the inverse of wdg_write_raw: exactly n doubles (a file of another size is an error)
+    int wdg_read_raw(const char *fname, long long n, double *u)
+    {
+        if (!fname || n < 0 || (n > 0 && !u))
+            return fail(WDG_ERR_ARG, "wdg_read_raw: bad arguments");
+        std::ifstream f(fname, std::ios::in | std::ios::binary | std::ios::ate);
+        if (!f)
+            return fail(WDG_ERR_ARG, std::string("wdg_read_raw: cannot open ") + fname);
+        const long long bytes = (long long)f.tellg();
+        if (bytes != (long long)sizeof(double) * n)
+            return fail(WDG_ERR_ARG, std::string("wdg_read_raw: ") + fname + " holds " + std::to_string(bytes) +
+                                         " bytes, expected " + std::to_string(sizeof(double) * n));
+        f.seekg(0);
+        std::vector<double> host((size_t)n);
+        f.read(reinterpret_cast<char *>(host.data()), (std::streamsize)bytes);
+        if (!f)
+            return fail(WDG_ERR_ARG, std::string("wdg_read_raw: short read from ") + fname);
+        cudaPointerAttributes at{};
+        if (n > 0 && cudaPointerGetAttributes(&at, u) == cudaSuccess && at.type == cudaMemoryTypeDevice)
+            WDG_CUDA(cudaMemcpy(u, host.data(), (size_t)bytes, cudaMemcpyHostToDevice));
+        else
+        {
+            cudaGetLastError();
+            if (n > 0)
+                std::memcpy(u, host.data(), (size_t)bytes);
         }
         return WDG_OK;
     }

@@ -154,12 +154,21 @@ class Mesh2D:
 
     @staticmethod
     def from_file(directory: str) -> "Mesh2D":
-        """Mesh2D::from_file format: info.txt (n_pts n_elem), coordinates.txt, elements.txt."""
-        with open(os.path.join(directory, "info.txt")) as f:
-            n_pts, n_elem = (int(t) for t in f.read().split()[:2])
-        x = np.loadtxt(os.path.join(directory, "coordinates.txt"), dtype=np.float64).reshape(-1, 2)[:n_pts]
-        e = np.loadtxt(os.path.join(directory, "elements.txt"), dtype=np.int64).reshape(-1, 4)[:n_elem]
-        return Mesh2D.from_vertices(x, e.astype(np.int32))
+        """Mesh2D::from_file (wdg_mesh_from_file): directory/info.txt (n_pts n_elem),
+        coordinates.txt (x y per point), elements.txt (four 0-based point indices per element)."""
+        h = C.c_void_p()
+        check(lib().wdg_mesh_from_file(os.fsencode(directory), C.byref(h)), "Mesh2D.from_file")
+        return Mesh2D(h)
+
+    def to_file(self, directory: str) -> None:
+        """Write a mesh built from vertices in the from_file format (the inverse of from_file)."""
+        if self.verts is None:
+            raise WdgError(_lib.WDG_ERR_ARG, "Mesh2D.to_file: only meshes built from vertices keep their points")
+        os.makedirs(directory, exist_ok=True)
+        with open(os.path.join(directory, "info.txt"), "w") as f:
+            f.write(f"{len(self.verts)} {len(self.quads)}\n")
+        np.savetxt(os.path.join(directory, "coordinates.txt"), self.verts, fmt="%.18e")
+        np.savetxt(os.path.join(directory, "elements.txt"), self.quads, fmt="%d")
 
     @staticmethod
     def from_tables(corners, interior_edges, boundary_edges) -> "Mesh2D":
@@ -645,6 +654,19 @@ class WaveHoltzBatch:
                                       C.c_void_p(stt.ctypes.data)), "WaveHoltzBatch.solve")
         self.pi0_norm = p0
         return W, it, res, stt
+
+
+def to_file(fname: str, u) -> None:
+    """dg::to_file (examples/examples.hpp:14-19): a float64 array (numpy or CUDA tensor) as raw
+    native-order bytes."""
+    p, keep = _ptr(u, name="u")
+    check(lib().wdg_write_raw(os.fsencode(fname), _size(u), p), "to_file")
+
+
+def read_file(fname: str, out) -> None:
+    """Read a to_file snapshot into `out` (float64 numpy array or CUDA tensor of the right size)."""
+    p, keep = _ptr(out, True, "out")
+    check(lib().wdg_read_raw(os.fsencode(fname), _size(out), p), "read_file")
 
 
 def norm(x, system: Discretisation) -> float:
