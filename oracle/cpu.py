@@ -54,6 +54,16 @@ _SIGS = {
     "rhs": ([_v, _dp, _dp], None),
     "rhs_forced": ([_v, _dp, _dp, _dp, _d], None),
     "rk4": ([_v, _d, _i, C.POINTER(C.c_double), _dp], None),
+    "opq_create": ([_v, _i, _ip], _v),
+    "opq_destroy": ([_v], None),
+    "opq_div": ([_v, _dp, _dp], None),
+    "opq_flux": ([_v, _i, _dp, _dp], None),
+    "opq_wave_action": ([_v, _dp, _dp], None),
+    "opq_bc_action": ([_v, _dp, _dp], None),
+    "opq_mass_inv": ([_v, _i, _dp], None),
+    "opq_mass_action": ([_v, _i, _dp, _dp], None),
+    "opq_rhs": ([_v, _dp, _dp], None),
+    "opq_rk4": ([_v, _d, _i, C.POINTER(C.c_double), _dp], None),
     "load_gaussians": ([_v, _i, _dp, _dp, _dp, _dp, _d, _i, _i, _dp], None),
     "norm": ([_i, _dp], _d),
     "error": ([_i, _dp, _dp], _d),
@@ -317,3 +327,53 @@ class WaveHoltz:
         err = C.c_double()
         it = self.L.wh_solve(self.h, _f64(pi0), tol, maxit, W, C.byref(err))
         return W, it, err.value
+
+
+class OpQ:
+    """The same system with approx_quad = false (Div<false>, EdgeFlux<false>, MassMatrix<false>;
+    default quadrature rules) on the CPU checker."""
+
+    def __init__(self, mesh: Mesh, n: int, bc):
+        self.L, self.mesh, self.n = mesh.L, mesh, n
+        self.bc = np.ascontiguousarray(bc, dtype=np.int32)
+        assert len(self.bc) == mesh.n_edges(1)
+        self.h = self.L.opq_create(mesh.h, n, self.bc)
+        self.ndof = 3 * n * n * mesh.n_elem
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.opq_destroy(self.h)
+            self.h = None
+
+    def div(self, u, du):
+        self.L.opq_div(self.h, _f64(u), du)
+
+    def flux(self, kind, uf):
+        fb = np.zeros_like(uf)
+        self.L.opq_flux(self.h, kind, _f64(uf), fb)
+        return fb
+
+    def wave_action(self, u, du):
+        self.L.opq_wave_action(self.h, _f64(u), du)
+
+    def bc_action(self, u, du):
+        self.L.opq_bc_action(self.h, _f64(u), du)
+
+    def mass_inv(self, nv, x):
+        self.L.opq_mass_inv(self.h, nv, x)
+
+    def mass_action(self, nv, x):
+        y = np.zeros_like(x)
+        self.L.opq_mass_action(self.h, nv, _f64(x), y)
+        return y
+
+    def rhs(self, u):
+        du = np.zeros(self.ndof)
+        self.L.opq_rhs(self.h, _f64(u), du)
+        return du
+
+    def rk4(self, u, dt, nsteps, t=0.0):
+        u = _f64(u).copy()
+        tt = C.c_double(t)
+        self.L.opq_rk4(self.h, dt, nsteps, C.byref(tt), u)
+        return u, tt.value

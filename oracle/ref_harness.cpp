@@ -79,15 +79,17 @@ namespace
     {
         const int nB, n;
         std::unique_ptr<FaceProlongator> prol;
-        std::unique_ptr<EdgeFlux<true>> flx;
+        std::unique_ptr<Operator> flx; // EdgeFlux<true> or, exact quadrature, EdgeFlux<false>
         const double *normals;
         std::vector<int> bc;
         mutable FaceVector uB;
 
-        ComposedBC(const Mesh2D &mesh, const QuadratureRule *basis, const int *codes)
+        ComposedBC(const Mesh2D &mesh, const QuadratureRule *basis, const int *codes, bool approx = true)
             : nB(mesh.n_edges(FaceType::BOUNDARY)), n(basis->n),
               prol(make_face_prolongator(mesh, basis, FaceType::BOUNDARY)),
-              flx(new EdgeFlux<true>(3, mesh, FaceType::BOUNDARY, basis, kWaveA, true)),
+              flx(approx ? static_cast<Operator *>(new EdgeFlux<true>(3, mesh, FaceType::BOUNDARY, basis, kWaveA, true))
+                         : static_cast<Operator *>(new EdgeFlux<false>(3, mesh, FaceType::BOUNDARY, basis, kWaveA,
+                                                                      true, -1.0, -0.5, nullptr))),
               normals(mesh.edge_metrics(basis, FaceType::BOUNDARY).normals()),
               bc(codes, codes + mesh.n_edges(FaceType::BOUNDARY)),
               uB(3, mesh, FaceType::BOUNDARY, basis) {}
@@ -184,6 +186,43 @@ namespace
             if (F)
                 for (int i = 0; i < ndof; ++i)
                     du[i] += F[i] * s;
+            m.inv(3, du);
+        }
+    };
+
+    // The same system with approx_quad = false: WaveEquation(mesh, basis, false)
+    // (source/WaveEquation.cpp:5-30: Div<false>, EdgeFlux<false> with the default rules),
+    // the composed boundary operator over EdgeFlux<false> (WaveBC with approx_quad = false,
+    // :70-105) and MassMatrix<false> (source/MassMatrix.cpp:84-230).
+    struct RefOpQ
+    {
+        const Mesh2D &mesh;
+        const QuadratureRule *basis;
+        const int n, nel, ndof;
+        WaveEquation a;
+        ComposedBC bc;
+        MassMatrix<false> m;
+        Div<false> div;
+        EdgeFlux<false> flxI, flxB;
+
+        RefOpQ(const Mesh2D &mesh_, int n_colloc, const int *bc_)
+            : mesh(mesh_), basis(QuadratureRule::quadrature_rule(n_colloc, QuadratureRule::GaussLobatto)),
+              n(n_colloc), nel(mesh_.n_elem()), ndof(3 * n_colloc * n_colloc * mesh_.n_elem()),
+              a(mesh_, basis, false),
+              bc(mesh_, basis, bc_, false),
+              m(mesh_, basis),
+              div(3, mesh_, basis, kWaveA, true, nullptr),
+              flxI(3, mesh_, FaceType::INTERIOR, basis, kWaveA, true, -1.0, -0.5, nullptr),
+              flxB(3, mesh_, FaceType::BOUNDARY, basis, kWaveA, true, -1.0, -0.5, nullptr)
+        {
+        }
+
+        void rhs(const double *u, double *du) const
+        {
+            for (int i = 0; i < ndof; ++i)
+                du[i] = 0.0;
+            a.action(u, du);
+            bc.action(u, du);
             m.inv(3, du);
         }
     };
@@ -396,6 +435,35 @@ extern "C"
         ode::RungeKutta4 rk(op->ndof);
         auto f = [op](double *dudt, const double, const double *v)
         { op->rhs(v, dudt, nullptr, 0.0); };
+        for (int s = 0; s < nsteps; ++s)
+            rk.step(dt, f, *t, u);
+    }
+
+    // ---- exact quadrature (approx_quad = false) ----
+    void *ref_opq_create(void *m, int n_colloc, const int *bc)
+    {
+        return new RefOpQ(static_cast<RefMesh *>(m)->mesh, n_colloc, bc);
+    }
+    void ref_opq_destroy(void *o) { delete static_cast<RefOpQ *>(o); }
+    void ref_opq_div(void *o, const double *u, double *du) { static_cast<RefOpQ *>(o)->div.action(u, du); }
+    void ref_opq_flux(void *o, int type, const double *uf, double *fb)
+    {
+        RefOpQ *op = static_cast<RefOpQ *>(o);
+        (type == 0 ? op->flxI : op->flxB).action(uf, fb);
+    }
+    void ref_opq_wave_action(void *o, const double *u, double *du) { static_cast<RefOpQ *>(o)->a.action(u, du); }
+    void ref_opq_bc_action(void *o, const double *u, double *du) { static_cast<RefOpQ *>(o)->bc.action(u, du); }
+    void ref_opq_mass_inv(void *o, int n_var, double *x) { static_cast<RefOpQ *>(o)->m.inv(n_var, x); }
+    void ref_opq_mass_action(void *o, int n_var, const double *x, double *y)
+    {
+        static_cast<RefOpQ *>(o)->m.action(n_var, x, y);
+    }
+    void ref_opq_rhs(void *o, const double *u, double *du) { static_cast<RefOpQ *>(o)->rhs(u, du); }
+    void ref_opq_rk4(void *o, double dt, int nsteps, double *t, double *u)
+    {
+        RefOpQ *op = static_cast<RefOpQ *>(o);
+        ode::RungeKutta4 rk(op->ndof);
+        auto f = [op](double *dudt, const double, const double *v) { op->rhs(v, dudt); };
         for (int s = 0; s < nsteps; ++s)
             rk.step(dt, f, *t, u);
     }

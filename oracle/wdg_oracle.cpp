@@ -640,6 +640,327 @@ namespace
         t += dt;
     }
 
+    // D(i, j) = phi_j'(xq_i) at points off (or on) the nodes: lagrange_basis_deriv with the
+    // two branches of lagrange_derivative (lagrange_interpolation.cpp:33-50, 96-139)
+    void deriv_at(int n, const double *x, int nq, const double *xq, double *D)
+    {
+        double lw[16], B[16 * 16];
+        bary(x, n, lw);
+        interp_matrix(n, x, nq, xq, B);
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < nq; ++i)
+            {
+                const double x0 = xq[i], p = B[i + nq * j];
+                int at = -1;
+                for (int k = 0; k < n; ++k)
+                    if (x0 == x[k] || std::abs(x0 - x[k]) <= 2.220446049250313e-16)
+                        at = k;
+                double A = 0.0, Bs = 0.0;
+                if (at >= 0)
+                {
+                    Bs = -lw[at];
+                    for (int k = 0; k < n; ++k)
+                        if (k != at)
+                            A += lw[k] * (p - (k == j ? 1.0 : 0.0)) / (x0 - x[k]);
+                }
+                else
+                    for (int k = 0; k < n; ++k)
+                    {
+                        const double t = lw[k] / (x0 - x[k]);
+                        A += t * (p - (k == j ? 1.0 : 0.0)) / (x0 - x[k]);
+                        Bs += t;
+                    }
+                D[i + nq * j] = A / Bs;
+            }
+    }
+
+    // The wave system with approx_quad = false (exact quadrature): Div<false>
+    // (source/Div.cpp:312-361 with op_2d_cc, and div_2d_q :469-588), EdgeFlux<false>
+    // (source/EdgeFlux.cpp:496-535, flux_action_2d_q :548-622), MassMatrix<false>
+    // (source/MassMatrix.cpp:84-230 with chol / solve_chol / mult_chol, linalg.cpp:5-100).
+    // Default rules (Gauss-Legendre): Div p = 1 + ((n-2) + (n-1) + 1) / 2 points,
+    // EdgeFlux and MassMatrix p = 1 + (2 (n-1) + 2) / 2.  Prolongation and exterior states
+    // are the Lobatto ones of Op.
+    struct OpQ
+    {
+        const Op base;
+        const Mesh &m;
+        int n, nel, ndof, nqd, nqf, nqm;
+        vec xd, wd, Pd, Dd; // Div rule and P(i, k) = phi_k(xq_i), D(i, k) = phi_k'(xq_i)
+        vec xf, wf, Pf;     // face rule
+        vec L;              // Cholesky factors of the element mass matrices (c2d, c2d, nel)
+
+        OpQ(const Mesh &m_, int n_, const int *codes)
+            : base(m_, n_, codes), m(m_), n(n_), nel(m_.nel), ndof(3 * n_ * n_ * m_.nel)
+        {
+            nqd = 1 + ((n - 2) + (n - 1) + 1) / 2;
+            nqf = 1 + (2 * (n - 1) + 2) / 2;
+            nqm = nqf;
+            xd.resize(nqd);
+            wd.resize(nqd);
+            gl(nqd, xd.data(), wd.data());
+            Pd.resize(nqd * n);
+            Dd.resize(nqd * n);
+            interp_matrix(n, base.x.data(), nqd, xd.data(), Pd.data());
+            deriv_at(n, base.x.data(), nqd, xd.data(), Dd.data());
+            xf.resize(nqf);
+            wf.resize(nqf);
+            gl(nqf, xf.data(), wf.data());
+            Pf.resize(nqf * n);
+            interp_matrix(n, base.x.data(), nqf, xf.data(), Pf.data());
+            // element mass matrices on the nqm x nqm rule, lower triangle, then chol
+            vec xm(nqm), wm(nqm), Bm(nqm * n);
+            gl(nqm, xm.data(), wm.data());
+            interp_matrix(n, base.x.data(), nqm, xm.data(), Bm.data());
+            const int c = n * n, q2 = nqm * nqm;
+            L.assign((size_t)c * c * nel, 0.0);
+            vec detJ(q2);
+            for (int el = 0; el < nel; ++el)
+            {
+                const double *cr = &m.corners[8 * (size_t)el];
+                for (int p = 0; p < q2; ++p)
+                {
+                    double J[4];
+                    jacobian(cr, xm[p % nqm], xm[p / nqm], J);
+                    detJ[p] = J[0] * J[3] - J[2] * J[1];
+                }
+                double *M = &L[(size_t)c * c * el];
+                for (int j = 0; j < c; ++j)
+                    for (int i = j; i < c; ++i)
+                    {
+                        double mij = 0.0;
+                        for (int p = 0; p < q2; ++p)
+                        {
+                            const double bi = Bm[p % nqm + nqm * (i % n)] * Bm[p / nqm + nqm * (i / n)];
+                            const double bj = Bm[p % nqm + nqm * (j % n)] * Bm[p / nqm + nqm * (j / n)];
+                            mij += bi * bj * detJ[p] * wm[p % nqm] * wm[p / nqm];
+                        }
+                        M[i + c * j] = mij;
+                    }
+                for (int k = 0; k < c; ++k)
+                {
+                    for (int j = k + 1; j < c; ++j)
+                    {
+                        const double sc = M[j + c * k] / M[k + c * k];
+                        for (int i = j; i < c; ++i)
+                            M[i + c * j] -= sc * M[i + c * k];
+                    }
+                    const double sc = 1.0 / std::sqrt(M[k + c * k]);
+                    for (int i = k; i < c; ++i)
+                        M[i + c * k] *= sc;
+                }
+            }
+        }
+
+        // div_2d_q: u -> quadrature points, contravariant fluxes, (F, grad v) back; accumulates
+        void div(const double *u, double *du) const
+        {
+            const int q = nqd;
+            vec Pu((size_t)n * 3 * q), Uq((size_t)3 * q * q), Fq((size_t)2 * 3 * q * q), Df((size_t)q * 3 * n),
+                Pg((size_t)q * 3 * n);
+            for (int el = 0; el < nel; ++el)
+            {
+                const double *ue = u + (size_t)3 * n * n * el;
+                const double *cr = &m.corners[8 * (size_t)el];
+                for (int i = 0; i < q; ++i)
+                    for (int l = 0; l < n; ++l)
+                        for (int d = 0; d < 3; ++d)
+                        {
+                            double s = 0.0;
+                            for (int k = 0; k < n; ++k)
+                                s += Pd[i + q * k] * ue[d + 3 * (k + n * l)];
+                            Pu[l + n * (d + 3 * i)] = s;
+                        }
+                for (int j = 0; j < q; ++j)
+                    for (int i = 0; i < q; ++i)
+                        for (int d = 0; d < 3; ++d)
+                        {
+                            double s = 0.0;
+                            for (int l = 0; l < n; ++l)
+                                s += Pd[j + q * l] * Pu[l + n * (d + 3 * i)];
+                            Uq[d + 3 * (i + q * j)] = s;
+                        }
+                for (int j = 0; j < q; ++j)
+                    for (int i = 0; i < q; ++i)
+                    {
+                        double J[4];
+                        jacobian(cr, xd[i], xd[j], J);
+                        const double W = wd[i] * wd[j];
+                        const double Xxi = J[0] * W, Yxi = J[1] * W, Xeta = J[2] * W, Yeta = J[3] * W;
+                        const double *U = &Uq[3 * (i + q * j)];
+                        double *F = &Fq[2 * 3 * (i + q * j)];
+                        // wave system: a(0,1,0) = a(1,0,0) = a(0,2,1) = a(2,0,1) = 1
+                        F[0] = Yeta * U[1] - Xeta * U[2];
+                        F[1] = -Yxi * U[1] + Xxi * U[2];
+                        F[2] = Yeta * U[0];
+                        F[3] = -Yxi * U[0];
+                        F[4] = -Xeta * U[0];
+                        F[5] = Xxi * U[0];
+                    }
+                for (int j = 0; j < q; ++j)
+                    for (int k = 0; k < n; ++k)
+                        for (int d = 0; d < 3; ++d)
+                        {
+                            double df = 0.0, pg = 0.0;
+                            for (int i = 0; i < q; ++i)
+                            {
+                                df += Dd[i + q * k] * Fq[2 * d + 6 * (i + q * j)];
+                                pg += Pd[i + q * k] * Fq[2 * d + 1 + 6 * (i + q * j)];
+                            }
+                            Df[j + q * (d + 3 * k)] = df;
+                            Pg[j + q * (d + 3 * k)] = pg;
+                        }
+                double *de = du + (size_t)3 * n * n * el;
+                for (int l = 0; l < n; ++l)
+                    for (int k = 0; k < n; ++k)
+                        for (int d = 0; d < 3; ++d)
+                        {
+                            double s = 0.0;
+                            for (int j = 0; j < q; ++j)
+                                s += Pd[j + q * l] * Df[j + q * (d + 3 * k)] + Dd[j + q * l] * Pg[j + q * (d + 3 * k)];
+                            de[d + 3 * (k + n * l)] += s;
+                        }
+            }
+        }
+
+        // flux_action_2d_q: traces -> face points, upwind flux (w_q |E|/2 Fs), back; side 1 = -side 0
+        void flux(bool interior, const double *ub, double *fb) const
+        {
+            const int q = nqf;
+            const std::vector<int> &list = interior ? m.interior : m.boundary;
+            const int N = (int)list.size();
+            static const double a[] = {0, 1, 0, 1, 0, 0, 0, 0, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0};
+            vec uf((size_t)q * 3);
+            for (int e = 0; e < N; ++e)
+            {
+                const Edge &E = m.edges[list[e]];
+                double nA[9], R[9], ev[3], Fs[2][9];
+                for (int d = 0; d < 9; ++d)
+                    nA[d] = E.n[0] * a[d] + E.n[1] * a[d + 9];
+                sym_eig3(nA, R, ev);
+                for (int s = 0; s < 2; ++s)
+                {
+                    const double sgn = (s == 0) ? 1.0 : -1.0;
+                    for (int i = 0; i < 3; ++i)
+                        for (int j = 0; j < 3; ++j)
+                        {
+                            double acc = 0.0;
+                            for (int k = 0; k < 3; ++k)
+                                acc += R[i + 3 * k] * (0.5 * -1.0 * ev[k] + sgn * -0.5 * std::abs(ev[k])) * R[j + 3 * k];
+                            Fs[s][i + 3 * j] = acc;
+                        }
+                }
+                std::fill(uf.begin(), uf.end(), 0.0);
+                for (int s = 0; s < 2; ++s)
+                    for (int i = 0; i < q; ++i)
+                    {
+                        double Uq[3];
+                        for (int d = 0; d < 3; ++d)
+                        {
+                            double v = 0.0;
+                            for (int j = 0; j < n; ++j)
+                                v += ub[j + n * (d + 3 * (s + 2 * (size_t)e))] * Pf[i + q * j];
+                            Uq[d] = v;
+                        }
+                        const double w = wf[i] * E.meas;
+                        for (int d = 0; d < 3; ++d)
+                        {
+                            double f = 0.0;
+                            for (int c = 0; c < 3; ++c)
+                                f += (w * Fs[s][c + 3 * d]) * Uq[c];
+                            uf[i + q * d] += f;
+                        }
+                    }
+                for (int d = 0; d < 3; ++d)
+                    for (int i = 0; i < n; ++i)
+                    {
+                        double f = 0.0;
+                        for (int j = 0; j < q; ++j)
+                            f += uf[j + q * d] * Pf[j + q * i];
+                        fb[i + n * (d + 3 * (0 + 2 * (size_t)e))] = f;
+                        fb[i + n * (d + 3 * (1 + 2 * (size_t)e))] = -f;
+                    }
+            }
+        }
+
+        void wave_action(const double *u, double *du) const
+        {
+            div(u, du);
+            vec uf((size_t)n * 3 * 2 * m.interior.size());
+            base.prolong(true, u, uf.data());
+            flux(true, uf.data(), uf.data());
+            base.prolong_t(true, uf.data(), du);
+        }
+        void bc_action(const double *u, double *du) const
+        {
+            vec uB((size_t)n * 3 * 2 * m.boundary.size());
+            base.prolong(false, u, uB.data());
+            base.apply_bc(uB.data());
+            flux(false, uB.data(), uB.data());
+            base.prolong_t(false, uB.data(), du);
+        }
+        // solve_chol: L \ x, then L^T \ x, nv right-hand sides interleaved per node
+        void mass_inv(int nv, double *x) const
+        {
+            const int c = n * n;
+            for (int el = 0; el < nel; ++el)
+            {
+                const double *M = &L[(size_t)c * c * el];
+                double *X = x + (size_t)nv * c * el;
+                for (int j = 0; j < c; ++j)
+                {
+                    for (int d = 0; d < nv; ++d)
+                        X[d + nv * j] /= M[j + c * j];
+                    for (int i = j + 1; i < c; ++i)
+                        for (int d = 0; d < nv; ++d)
+                            X[d + nv * i] -= M[i + c * j] * X[d + nv * j];
+                }
+                for (int j = c - 1; j >= 0; --j)
+                {
+                    for (int d = 0; d < nv; ++d)
+                        X[d + nv * j] /= M[j + c * j];
+                    for (int i = 0; i < j; ++i)
+                        for (int d = 0; d < nv; ++d)
+                            X[d + nv * i] -= M[j + c * i] * X[d + nv * j];
+                }
+            }
+        }
+        // mult_chol: y = L (L^T x)
+        void mass_action(int nv, const double *x, double *y) const
+        {
+            const int c = n * n;
+            std::copy(x, x + (size_t)nv * c * nel, y);
+            for (int el = 0; el < nel; ++el)
+            {
+                const double *M = &L[(size_t)c * c * el];
+                double *Y = y + (size_t)nv * c * el;
+                for (int i = 0; i < c; ++i)
+                    for (int d = 0; d < nv; ++d)
+                    {
+                        double t = 0.0;
+                        for (int j = i; j < c; ++j)
+                            t += M[j + c * i] * Y[d + nv * j];
+                        Y[d + nv * i] = t;
+                    }
+                for (int i = c - 1; i >= 0; --i)
+                    for (int d = 0; d < nv; ++d)
+                    {
+                        double t = 0.0;
+                        for (int j = 0; j <= i; ++j)
+                            t += M[i + c * j] * Y[d + nv * j];
+                        Y[d + nv * i] = t;
+                    }
+            }
+        }
+        void rhs(const double *u, double *du) const
+        {
+            std::fill(du, du + ndof, 0.0);
+            wave_action(u, du);
+            bc_action(u, du);
+            mass_inv(3, du);
+        }
+    };
+
     double min_h(const Mesh &m)
     {
         double h = INFINITY;
@@ -882,6 +1203,23 @@ extern "C"
     double orc_norm(int nd, const double *x) { return norm2(nd, x); }
     double orc_error(int nd, const double *x, const double *y) { return err2(nd, x, y); }
 
+    void *orc_opq_create(void *m, int n, const int *bc) { return new OpQ(*static_cast<Mesh *>(m), n, bc); }
+    void orc_opq_destroy(void *o) { delete static_cast<OpQ *>(o); }
+    void orc_opq_div(void *o, const double *u, double *du) { static_cast<OpQ *>(o)->div(u, du); }
+    void orc_opq_flux(void *o, int type, const double *uf, double *fb) { static_cast<OpQ *>(o)->flux(type == 0, uf, fb); }
+    void orc_opq_wave_action(void *o, const double *u, double *du) { static_cast<OpQ *>(o)->wave_action(u, du); }
+    void orc_opq_bc_action(void *o, const double *u, double *du) { static_cast<OpQ *>(o)->bc_action(u, du); }
+    void orc_opq_mass_inv(void *o, int nv, double *x) { static_cast<OpQ *>(o)->mass_inv(nv, x); }
+    void orc_opq_mass_action(void *o, int nv, const double *x, double *y) { static_cast<OpQ *>(o)->mass_action(nv, x, y); }
+    void orc_opq_rhs(void *o, const double *u, double *du) { static_cast<OpQ *>(o)->rhs(u, du); }
+    void orc_opq_rk4(void *o, double dt, int nsteps, double *t, double *u)
+    {
+        OpQ *op = static_cast<OpQ *>(o);
+        vec p(op->ndof), du(op->ndof);
+        auto f = [op](double *dudt, double, const double *v) { op->rhs(v, dudt); };
+        for (int s = 0; s < nsteps; ++s)
+            rk4_step(op->ndof, dt, f, *t, u, p, du);
+    }
     void *orc_wh_create(void *o, double omega) { return new WH(*static_cast<Op *>(o), omega); }
     void orc_wh_destroy(void *w) { delete static_cast<WH *>(w); }
     void orc_wh_params(void *w, double *T, double *dt, int *nt)

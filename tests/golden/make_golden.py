@@ -1,7 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the reference library.
 
     make -C oracle ref          # compiles the reference (needs its sources)
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [--exact-quadrature-only]
 
 Every output array is produced by the reference waveDG code compiled from its
 own sources (oracle/_ref/libwdgref.so, driven through oracle/ref_harness.cpp).
@@ -127,9 +127,44 @@ def waveholtz():
                         omega=2.0, F=F, pi0=p1, S_pi0=wh1.S(p1))
 
 
+def opq_fixture(name, v, q, m, n, seed):
+    """approx_quad = false: Div<false>, EdgeFlux<false> (interior and boundary), WaveEquation,
+    the composed boundary operator over EdgeFlux<false>, MassMatrix<false>, RHS, 5 RK4 steps."""
+    rng = np.random.default_rng(seed)
+    bc = rng.integers(0, 3, size=m.n_edges(1)).astype(np.int32)
+    op = cpu.OpQ(m, n, bc)
+    u = rng.standard_normal(op.ndof)
+    out = dict(verts=v, quads=q, n=n, bc=bc, u=u)
+    for nm in ("div", "wave_action", "bc_action"):
+        r = rng.standard_normal(op.ndof)
+        out[f"{nm}_in"] = r.copy()
+        getattr(op, nm)(u, r)
+        out[nm] = r
+    for k, tag in ((0, "interior"), (1, "boundary")):
+        uf = rng.standard_normal(n * 3 * 2 * m.n_edges(k))
+        out[f"flux_{tag}_in"] = uf
+        out[f"flux_{tag}"] = op.flux(k, uf)
+    x = u.copy()
+    op.mass_inv(3, x)
+    out["mass_inv"] = x
+    out["mass_action"] = op.mass_action(3, u)
+    out["rhs"] = op.rhs(u)
+    dt = 0.1 * m.min_h() / n ** 2
+    out["dt"] = dt
+    out["rk4_5"], _ = op.rk4(u, dt, 5)
+    np.savez_compressed(os.path.join(HERE, f"opq_{name}_n{n}.npz"), **out)
+
+
 def main():
     if not cpu.available("reference"):
         raise SystemExit("build the reference first: make -C oracle ref")
+    qcases = {"scrambled6": [3, 5], "lshape3": [4]}
+    if "--exact-quadrature-only" in sys.argv:
+        for seed, (name, v, q) in enumerate(meshes()):
+            for n in qcases.get(name, []):
+                opq_fixture(name, v, q, cpu.Mesh(v, q, KIND), n, 1000 + 100 * seed + n)
+        print("exact-quadrature fixtures written to", HERE)
+        return
     x = {}
     for n in range(2, 10):
         xs, ws, D = cpu.basis(n, KIND)
@@ -140,6 +175,8 @@ def main():
         m = mesh_fixture(name, v, q)
         for n in cases[name]:
             op_fixture(name, v, q, m, n, 100 * seed + n)
+        for n in qcases.get(name, []):
+            opq_fixture(name, v, q, m, n, 1000 + 100 * seed + n)
     config1()
     waveholtz()
     print("fixtures written to", HERE)

@@ -66,6 +66,29 @@ def test_operators(fname):
     assert rel(op.load_gaussians(cen, [0.3, 0.2], [1.0, -0.5], 2.0, 1, True), g["load_minv"]) < 1e-13
 
 
+@pytest.mark.parametrize("fname", golden_files("opq_"))
+def test_exact_quadrature_operators(fname):
+    """approx_quad = false: the oracle's Div<false>, EdgeFlux<false>, MassMatrix<false> and the
+    operators built from them against the reference's."""
+    g = golden(fname)
+    m = cpu.Mesh(g["verts"], g["quads"], "oracle")
+    op = cpu.OpQ(m, int(g["n"]), g["bc"])
+    u = g["u"]
+    for nm in ("div", "wave_action", "bc_action"):
+        r = g[f"{nm}_in"].copy()
+        getattr(op, nm)(u, r)
+        assert rel(r, g[nm]) < TOL, nm
+    for k, tag in ((0, "interior"), (1, "boundary")):
+        assert rel(op.flux(k, g[f"flux_{tag}_in"]), g[f"flux_{tag}"]) < TOL, tag
+    x = u.copy()
+    op.mass_inv(3, x)
+    assert rel(x, g["mass_inv"]) < TOL
+    assert rel(op.mass_action(3, u), g["mass_action"]) < TOL
+    assert rel(op.rhs(u), g["rhs"]) < TOL
+    un, _ = op.rk4(u, float(g["dt"]), 5)
+    assert rel(un, g["rk4_5"]) < TOL
+
+
 def test_config1_trajectory():
     g = golden("config1_32x32_P3.npz")
     m = cpu.Mesh(g["verts"], g["quads"], "oracle")
