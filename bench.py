@@ -261,6 +261,9 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_extras and not args.no_waveholtz and args.precision == "fp64":
         extra["waveholtz_c3"] = waveholtz_c3(local_rank)
         extra["waveholtz_batched"] = waveholtz_batched(local_rank)
+    if not args.no_extras and args.precision == "fp64":
+        extra["exact_quadrature"] = exact_quadrature(local_rank, cpu_leg=(rank == 0 and world == 1
+                                                                          and not args.no_cpu_baseline))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -416,6 +419,51 @@ def _ref_lib():
     if cpu.available("reference"):
         return "reference", cpu
     return "port", cpu
+
+
+def exact_quadrature(device: int, n_el: int = 128, P: int = 4, reps: int = 20, cpu_leg: bool = True) -> dict:
+    """The approx_quad = false operators (Div<false>, EdgeFlux<false>, MassMatrix<false>): time of
+    one RHS M^{-1}(A + B) u on the GPU (device arrays, CUDA events over `reps` calls) on a
+    perturbed n_el x n_el mesh, P = 4, outflow boundary; beside it the reference's own CPU
+    RHS on the same mesh (compiled from its sources, 1 thread), when present."""
+    import torch
+
+    import wavedg_b200 as W
+    from wavedg_b200 import meshgen as mg
+
+    v, q = mg.perturbed_rect(n_el, 0.2, seed=1)
+    mesh = W.Mesh2D.from_vertices(v, q)
+    bc = np.zeros(mesh.n_edges(1), dtype=np.int32)
+    d = W.ExactDiscretisation(mesh, P + 1, bc, device=device)
+    u = torch.from_numpy(np.random.default_rng(2).standard_normal(d.ndof)).cuda()
+    du = torch.empty_like(u)
+    for _ in range(3):
+        d.rhs(u, du)
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    s0.record()
+    for _ in range(reps):
+        d.rhs(u, du)
+    s1.record()
+    torch.cuda.synchronize()
+    ms = s0.elapsed_time(s1) / reps
+    c2 = (P + 1) ** 2
+    out = {"workload": f"rhs_exact_quadrature_{n_el}x{n_el}_P{P}_perturbed_outflow", "ndof": d.ndof,
+           "rules_div_face_mass": list(d.rules()), "ms_per_rhs": ms, "dof_per_s": d.ndof / (ms / 1e3),
+           # per element: state in/out (2 x 3 c2 doubles), M^{-1} factors (c2^2 doubles, read once per RHS)
+           "factor_bytes_per_rhs": 8 * c2 * c2 * mesh.n_elem()}
+    out["achieved_gbs"] = (8 * (6 * c2 + c2 * c2) * mesh.n_elem()) / (ms / 1e3) / 1e9
+    if cpu_leg:
+        kind, cpu = _ref_lib()
+        if kind == "reference":
+            m = cpu.Mesh(v, q, "reference")
+            op = cpu.OpQ(m, P + 1, bc)
+            uh = u.cpu().numpy()
+            t0 = time.perf_counter()
+            op.rhs(uh)
+            out["cpu_reference_ms_per_rhs"] = (time.perf_counter() - t0) * 1e3
+            out["cpu_reference"] = "the reference's WaveEquation / WaveBC / MassMatrix<false>, 1 thread, set-up excluded"
+    return out
 
 
 def cpu_baseline(v, q, bc, n, dt, u0, budget=30.0):

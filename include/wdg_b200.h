@@ -155,6 +155,30 @@ int wdg_rhs(wdg_wave *wave, const double *u, double *dudt, const double *F, doub
  * t advances by dt per step.  One fused kernel per RK stage. */
 int wdg_rk4_steps(wdg_wave *wave, double *u, double dt, double *t, int nsteps);
 
+/* ---- exact quadrature (approx_quad = false), FP64 ---- */
+/* WaveEquation(mesh, basis, false) (source/WaveEquation.cpp:5-30: Div<false>, EdgeFlux<false>),
+ * WaveBC(mesh, bc, basis, false) (:70-105) and MassMatrix<false>(mesh, basis)
+ * (source/MassMatrix.cpp:84-230), with the reference's default Gauss-Legendre rules for
+ * bilinear elements: Div 1 + ((n-2) + (n-1) + 1)/2 points per direction, EdgeFlux and
+ * MassMatrix 1 + (2(n-1) + 2)/2.  Arrays and semantics as the collocation entry points. */
+typedef struct wdg_waveq wdg_waveq;
+int wdg_waveq_create(const wdg_mesh *mesh, int n_colloc, const int *bc, int device, wdg_waveq **out);
+void wdg_waveq_destroy(wdg_waveq *wave);
+int wdg_waveq_rules(const wdg_waveq *wave, int *n_div, int *n_face, int *n_mass);
+/* the collocation handle it shares geometry, prolongation and staging with (owned by `wave`) */
+int wdg_waveq_wave(const wdg_waveq *wave, wdg_wave **collocation);
+int wdg_waveq_div_action(wdg_waveq *wave, const double *u, double *du);    /* Div<false>::action (Div.cpp:469-588, 658-673), du += */
+int wdg_waveq_wave_action(wdg_waveq *wave, const double *u, double *du);   /* WaveEquation::action, du += */
+int wdg_waveq_wavebc_action(wdg_waveq *wave, const double *u, double *du); /* WaveBC::action, du += */
+/* EdgeFlux<false>::action (EdgeFlux.cpp:548-640): fb side 0 <- flux, side 1 <- -flux; fb may equal ub */
+int wdg_waveq_edge_flux(wdg_waveq *wave, int face_type, const double *ub, double *fb);
+/* MassMatrix<false>::action (y = L L^T x) / ::inv (x <- L^-T L^-1 x) (MassMatrix.cpp:194-230) */
+int wdg_waveq_mass_action(wdg_waveq *wave, int n_var, const double *x, double *y);
+int wdg_waveq_mass_inv(wdg_waveq *wave, int n_var, double *x);
+/* dudt = M^{-1} (A u + B u + s F), F may be NULL; and nsteps of ode::RungeKutta4 on it */
+int wdg_waveq_rhs(wdg_waveq *wave, const double *u, double *dudt, const double *F, double s);
+int wdg_waveq_rk4_steps(wdg_waveq *wave, double *u, double dt, double *t, int nsteps);
+
 /* ---- resident state (stays on the GPU in the handle's precision) ---- */
 int wdg_state_upload(wdg_wave *wave, const double *u);
 int wdg_state_download(wdg_wave *wave, double *u);

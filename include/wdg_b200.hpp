@@ -105,8 +105,32 @@ namespace b200
     inline void require_approx(bool approx_quad)
     {
         if (!approx_quad)
-            throw std::runtime_error("wdg_b200: exact-quadrature operators are not built; use approx_quad = true");
+            throw std::runtime_error("wdg_b200: this class is built for approx_quad = true");
     }
+
+    // the same system with approx_quad = false: Div<false>, EdgeFlux<false>, MassMatrix<false>
+    // with the reference's default quadrature rules (FP64)
+    class ExactDiscretisation
+    {
+    public:
+        ExactDiscretisation(const dg::Mesh2D &mesh, const dg::QuadratureRule *basis, const int *bc,
+                            const dg::QuadratureRule *quad = nullptr, int device = -1)
+            : mesh_(mesh)
+        {
+            if (!basis || basis->type != dg::QuadratureRule::GaussLobatto)
+                throw std::runtime_error("wdg_b200: the GPU operators are built for Gauss-Lobatto bases");
+            if (quad)
+                throw std::runtime_error("wdg_b200: exact quadrature is built for the default rules (quad = nullptr)");
+            wdg_waveq *q = nullptr;
+            check(wdg_waveq_create(mesh_.get(), basis->n, bc, device, &q));
+            h_.reset(q, wdg_waveq_destroy);
+        }
+        wdg_waveq *get() const { return h_.get(); }
+
+    private:
+        Mesh mesh_;
+        std::shared_ptr<wdg_waveq> h_;
+    };
 
     // dg::WaveEquation (source/WaveEquation.cpp:5-68): du += Div(u) + P^T Flux(P u)
     class WaveEquation : public dg::Operator
@@ -114,12 +138,21 @@ namespace b200
     public:
         WaveEquation(const dg::Mesh2D &mesh, const dg::QuadratureRule *basis, bool approx_quad = false,
                      const dg::QuadratureRule *quad = nullptr)
-            : d_((require_approx(approx_quad), mesh), basis, nullptr) {}
-        void action(const double *u, double *du) const override { check(wdg_wave_action(d_.get(), u, du)); }
+        {
+            if (approx_quad)
+                d_ = std::make_shared<Discretisation>(mesh, basis, nullptr);
+            else
+                q_ = std::make_shared<ExactDiscretisation>(mesh, basis, nullptr, quad);
+        }
+        void action(const double *u, double *du) const override
+        {
+            check(d_ ? wdg_wave_action(d_->get(), u, du) : wdg_waveq_wave_action(q_->get(), u, du));
+        }
         void action(int, const double *u, double *du) const override { action(u, du); }
 
     private:
-        Discretisation d_;
+        std::shared_ptr<Discretisation> d_;
+        std::shared_ptr<ExactDiscretisation> q_;
     };
 
     // dg::WaveBC (source/WaveEquation.cpp:70-215); codes 0 absorbing, 1 reflecting, 2 Dirichlet p = 0
@@ -128,30 +161,50 @@ namespace b200
     public:
         WaveBC(const dg::Mesh2D &mesh, const int *bc, const dg::QuadratureRule *basis, bool approx_quad,
                const dg::QuadratureRule *quad = nullptr)
-            : d_((require_approx(approx_quad), mesh), basis, bc) {}
-        void action(const double *u, double *du) const override { check(wdg_wavebc_action(d_.get(), u, du)); }
+        {
+            if (approx_quad)
+                d_ = std::make_shared<Discretisation>(mesh, basis, bc);
+            else
+                q_ = std::make_shared<ExactDiscretisation>(mesh, basis, bc, quad);
+        }
+        void action(const double *u, double *du) const override
+        {
+            check(d_ ? wdg_wavebc_action(d_->get(), u, du) : wdg_waveq_wavebc_action(q_->get(), u, du));
+        }
         void action(int, const double *u, double *du) const override { action(u, du); }
 
     private:
-        Discretisation d_;
+        std::shared_ptr<Discretisation> d_;
+        std::shared_ptr<ExactDiscretisation> q_;
     };
 
-    // dg::MassMatrix<true> (source/MassMatrix.cpp:6-82)
+    // dg::MassMatrix<true> (source/MassMatrix.cpp:6-82) and, APPROX = false, MassMatrix<false>
+    // (block Cholesky of the exact element mass matrices, :84-230)
+    template <bool APPROX = true>
     class MassMatrix : public dg::InvertibleOperator
     {
     public:
         MassMatrix(const dg::Mesh2D &mesh, const dg::QuadratureRule *basis, const dg::QuadratureRule *quad = nullptr)
-            : d_(mesh, basis, nullptr) {}
+        {
+            if (APPROX)
+                d_ = std::make_shared<Discretisation>(mesh, basis, nullptr);
+            else
+                q_ = std::make_shared<ExactDiscretisation>(mesh, basis, nullptr, quad);
+        }
         void action(const double *x, double *y) const override { action(1, x, y); }
         void action(int n_var, const double *x, double *y) const override
         {
-            check(wdg_mass_action(d_.get(), n_var, x, y));
+            check(d_ ? wdg_mass_action(d_->get(), n_var, x, y) : wdg_waveq_mass_action(q_->get(), n_var, x, y));
         }
         void inv(double *x) const override { inv(1, x); }
-        void inv(int n_var, double *x) const override { check(wdg_mass_inv(d_.get(), n_var, x)); }
+        void inv(int n_var, double *x) const override
+        {
+            check(d_ ? wdg_mass_inv(d_->get(), n_var, x) : wdg_waveq_mass_inv(q_->get(), n_var, x));
+        }
 
     private:
-        Discretisation d_;
+        std::shared_ptr<Discretisation> d_;
+        std::shared_ptr<ExactDiscretisation> q_;
     };
 
     // The examples' time derivative M^{-1}(A + B) u as one fused operator, with the

@@ -148,6 +148,54 @@ int main()
     gwh.postprocess(H2.data(), s1.data());
     report("WaveHoltz::postprocess", rel(H2, H1), 1e-12);
 
+    // approx_quad = false: the reference's exact-quadrature operators against the drop-ins
+    {
+        WaveEquation aq(mesh, basis, false);
+        WaveBC bq(mesh, bc.data(), basis, false);
+        MassMatrix<false> mq(mesh, basis);
+        b200::WaveEquation gaq(mesh, basis, false);
+        b200::WaveBC gbq(mesh, bc.data(), basis, false);
+        b200::MassMatrix<false> gmq(mesh, basis);
+        std::vector<double> q1(ndof, 0.0), q2(ndof, 0.0);
+        aq.action(u.data(), q1.data());
+        gaq.action(u.data(), q2.data());
+        report("WaveEquation::action, approx_quad = false", rel(q2, q1), 1e-12);
+        bq.action(u.data(), q1.data());
+        gbq.action(u.data(), q2.data());
+        report("+ WaveBC::action, approx_quad = false", rel(q2, q1), 1e-12);
+        mq.inv(3, q1.data());
+        gmq.inv(3, q2.data());
+        report("MassMatrix<false>::inv", rel(q2, q1), 1e-12);
+        std::vector<double> y1(ndof), y2(ndof);
+        mq.action(3, u.data(), y1.data());
+        gmq.action(3, u.data(), y2.data());
+        report("MassMatrix<false>::action", rel(y2, y1), 1e-12);
+        auto fq_ref = [&](double *dudt, const double, const double *v)
+        {
+            for (int i = 0; i < ndof; ++i)
+                dudt[i] = 0.0;
+            aq.action(v, dudt);
+            bq.action(v, dudt);
+            mq.inv(3, dudt);
+        };
+        auto fq_gpu = [&](double *dudt, const double, const double *v)
+        {
+            for (int i = 0; i < ndof; ++i)
+                dudt[i] = 0.0;
+            gaq.action(v, dudt);
+            gbq.action(v, dudt);
+            gmq.inv(3, dudt);
+        };
+        std::vector<double> vr = u, vg = u;
+        double t1 = 0.0, t2 = 0.0;
+        for (int s = 0; s < 5; ++s)
+        {
+            rk.step(dt, fq_ref, t1, vr.data());
+            rk.step(dt, fq_gpu, t2, vg.data());
+        }
+        report("ode::RungeKutta4, exact quadrature, 5 steps", rel(vg, vr), 1e-11);
+    }
+
     // the batched solver on the same two problems as two single solves (exact same periods)
     {
         b200::WaveSystem sa(small, basis, bc2.data()), sb(small, basis, bc2.data());

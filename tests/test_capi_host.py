@@ -99,7 +99,9 @@ def test_errors_are_reported(L):
     assert L.wdg_mesh_uniform_rect(0, -1, 1, 4, -1, 1, C.byref(h)) == W._lib.WDG_ERR_ARG
     assert b"bad arguments" in L.wdg_last_error()
     with pytest.raises(W.WdgError):
-        W.WaveEquation(W.Mesh2D.uniform_rect(2, -1, 1, 2, -1, 1), W.QuadratureRule.quadrature_rule(4, 1), False)
+        # exact quadrature with a caller-chosen rule: only the reference's default rules are built
+        W.WaveEquation(W.Mesh2D.uniform_rect(2, -1, 1, 2, -1, 1), W.QuadratureRule.quadrature_rule(4, 1), False,
+                       quad=W.QuadratureRule.quadrature_rule(7, 0))
     with pytest.raises(W.WdgError):  # Gauss-Legendre bases are not the Lobatto path
         W.WaveEquation(W.Mesh2D.uniform_rect(2, -1, 1, 2, -1, 1), W.QuadratureRule.quadrature_rule(4, 0), True)
 

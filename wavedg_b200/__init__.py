@@ -7,6 +7,7 @@ from ._lib import WDG_FP32, WDG_FP64, WdgError, lib  # noqa: F401
 from .dg import (  # noqa: F401
     Discretisation,
     Div,
+    ExactDiscretisation,
     EdgeFlux,
     FaceProlongator,
     FaceType,
@@ -29,7 +30,7 @@ from .dg import (  # noqa: F401
 )
 
 __all__ = [
-    "read_file", "to_file", "Discretisation", "Div", "EdgeFlux", "FaceProlongator", "FaceType", "LinearFunctional2D", "MassMatrix",
+    "read_file", "to_file", "Discretisation", "Div", "ExactDiscretisation", "EdgeFlux", "FaceProlongator", "FaceType", "LinearFunctional2D", "MassMatrix",
     "Mesh2D", "Operator", "QuadratureRule", "RungeKutta4", "WaveBC", "WaveEquation", "WaveHoltz", "WaveHoltzBatch", "WaveSystem",
     "WdgError", "WDG_FP32", "WDG_FP64", "error", "lib", "make_face_prolongator", "norm",
 ]

@@ -46,6 +46,18 @@ SIGNATURES = {
     "wdg_mesh_from_vertices": ([_i, _v, _i, _v, _vp], _i),
     "wdg_mesh_uniform_rect": ([_i, _d, _d, _i, _d, _d, _vp], _i),
     "wdg_mesh_from_file": ([C.c_char_p, _vp], _i),
+    "wdg_waveq_create": ([_v, _i, _v, _i, _vp], _i),
+    "wdg_waveq_destroy": ([_v], None),
+    "wdg_waveq_rules": ([_v, _v, _v, _v], _i),
+    "wdg_waveq_wave": ([_v, _vp], _i),
+    "wdg_waveq_div_action": ([_v, _v, _v], _i),
+    "wdg_waveq_wave_action": ([_v, _v, _v], _i),
+    "wdg_waveq_wavebc_action": ([_v, _v, _v], _i),
+    "wdg_waveq_edge_flux": ([_v, _i, _v, _v], _i),
+    "wdg_waveq_mass_action": ([_v, _i, _v, _v], _i),
+    "wdg_waveq_mass_inv": ([_v, _i, _v], _i),
+    "wdg_waveq_rhs": ([_v, _v, _v, _v, _d], _i),
+    "wdg_waveq_rk4_steps": ([_v, _v, _d, _v, _i], _i),
     "wdg_write_raw": ([C.c_char_p, _ll, _v], _i),
     "wdg_read_raw": ([C.c_char_p, _ll, _v], _i),
     "wdg_mesh_from_tables": ([_i, _v, _i, _v, _i, _v, _vp], _i),

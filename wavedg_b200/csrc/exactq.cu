@@ -1,0 +1,702 @@
+// C-ABI: the wave system with exact quadrature (approx_quad = false).
+//
+//   WaveEquation(mesh, basis, false)  source/WaveEquation.cpp:5-30
+//     Div<false>       source/Div.cpp:312-361 (op_2d_cc), div_2d_q :469-588
+//     EdgeFlux<false>  source/EdgeFlux.cpp:496-535, flux_action_2d_q :548-622
+//   WaveBC(mesh, bc, basis, false)    source/WaveEquation.cpp:70-105, 190-215
+//   MassMatrix<false>(mesh, basis)    source/MassMatrix.cpp:84-230; chol, solve_chol,
+//                                     mult_chol in source/linalg.cpp:5-100
+//
+// Quadrature rules are the reference's defaults for bilinear elements (Gauss-Legendre):
+// Div 1 + ((n-2) + (n-1) + 1) / 2 points per direction, EdgeFlux and MassMatrix
+// 1 + (2 (n-1) + 2) / 2.  Face prolongation, the exterior states of the boundary codes and
+// the argument staging are the collocation handle's (an internal wdg_wave, FP64).
+//
+// FP64 only.  This is the accuracy path for callers that set approx_quad = false, not the
+// bandwidth-bound hot path: one CTA per element for the volume term, one thread per edge
+// for the face term, one thread per element for the block-Cholesky mass solves.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "wave_impl.hpp"
+
+using namespace wdg;
+
+struct wdg_waveq
+{
+    wdg_wave *w = nullptr;
+    int n = 0, nqd = 0, nqf = 0, nqm = 0;
+    double *d_xd = nullptr, *d_wd = nullptr, *d_Pd = nullptr, *d_Dd = nullptr; // Div rule, P(i,k), D(i,k)
+    double *d_wf = nullptr, *d_Pf = nullptr;                                   // face rule, P(i,k)
+    double *d_nI = nullptr, *d_nB = nullptr; // per edge (n_x, n_y, |E| / 2)
+    double *d_L = nullptr;                   // Cholesky factors (n^2, n^2, nel), column-major
+    double *d_uf = nullptr, *d_uB = nullptr; // face traces
+    double *d_rk = nullptr;                  // RK4: k and the stage derivative (2 ndof)
+};
+
+namespace
+{
+    constexpr int kMaxQ = 16;
+
+    int qdiv(int n) { return 1 + ((n - 2) + (n - 1) + 1) / 2; }
+    int qface(int n) { return 1 + (2 * (n - 1) + 2) / 2; }
+
+    // D(i, j) = phi_j'(xq_i) for the Lagrange basis on the nodes x, by the barycentric
+    // derivative formula: at a node the diagonal form, elsewhere the quotient form
+    // (lagrange_basis_deriv, source/lagrange_interpolation.cpp:33-50, 96-139)
+    void deriv_at(int n, const double *x, int nq, const double *xq, double *D)
+    {
+        std::vector<double> lw(n), B((size_t)nq * n);
+        for (int i = 0; i < n; ++i)
+        {
+            double p = 1.0;
+            for (int j = 0; j < n; ++j)
+                if (j != i)
+                    p *= x[i] - x[j];
+            lw[i] = 1.0 / p;
+        }
+        const auto mm = std::minmax_element(lw.begin(), lw.end());
+        const double diff = *mm.second - *mm.first;
+        for (double &v : lw)
+            v /= diff;
+        interp_matrix(n, x, nq, xq, B.data());
+        const double eps = 2.220446049250313e-16;
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < nq; ++i)
+            {
+                const double x0 = xq[i], p = B[i + (size_t)nq * j];
+                int at = -1;
+                for (int k = 0; k < n; ++k)
+                    if (x0 == x[k] || std::abs(x0 - x[k]) <= eps)
+                        at = k;
+                double A = 0.0, S = 0.0;
+                if (at >= 0)
+                {
+                    S = -lw[at];
+                    for (int k = 0; k < n; ++k)
+                        if (k != at)
+                            A += lw[k] * (p - (k == j ? 1.0 : 0.0)) / (x0 - x[k]);
+                }
+                else
+                    for (int k = 0; k < n; ++k)
+                    {
+                        const double t = lw[k] / (x0 - x[k]);
+                        A += t * (p - (k == j ? 1.0 : 0.0)) / (x0 - x[k]);
+                        S += t;
+                    }
+                D[i + (size_t)nq * j] = A / S;
+            }
+    }
+
+    // QuadElement::jacobian (source/Element.cpp:21-27): J = (x_xi, y_xi, x_eta, y_eta)
+    __host__ __device__ inline void jac(const double *c, double xi, double eta, double J[4])
+    {
+        J[0] = 0.25 * ((1.0 - eta) * (c[2] - c[0]) + (1.0 + eta) * (c[4] - c[6]));
+        J[1] = 0.25 * ((1.0 - eta) * (c[3] - c[1]) + (1.0 + eta) * (c[5] - c[7]));
+        J[2] = 0.25 * ((1.0 - xi) * (c[6] - c[0]) + (1.0 + xi) * (c[4] - c[2]));
+        J[3] = 0.25 * ((1.0 - xi) * (c[7] - c[1]) + (1.0 + xi) * (c[5] - c[3]));
+    }
+
+    // ---------------------------------------------------------------- Div<false>
+    // One CTA per element, shared memory per element: u, P u (one direction), U at the points,
+    // the two contravariant fluxes, and the two half-contracted sums.  Accumulates into du.
+    __global__ void qdiv_kernel(int n, int q, int nel, const double *__restrict__ corners,
+                                const double *__restrict__ xd, const double *__restrict__ wd,
+                                const double *__restrict__ Pd, const double *__restrict__ Dd,
+                                const double *__restrict__ u, double *du)
+    {
+        extern __shared__ double sm[];
+        const int nn = n * n, qq = q * q;
+        double *su = sm;                 // (3, n, n)
+        double *Pu = su + 3 * nn;        // (n, 3, q)
+        double *Uq = Pu + 3 * n * q;     // (3, q, q)
+        double *Fq = Uq + 3 * qq;        // (2, 3, q, q)
+        double *Df = Fq + 6 * qq;        // (q, 3, n)
+        double *Pg = Df + 3 * q * n;     // (q, 3, n)
+        const int t = threadIdx.x, T = blockDim.x;
+        for (int el = blockIdx.x; el < nel; el += gridDim.x)
+        {
+            const double *ue = u + (size_t)3 * nn * el;
+            for (int k = t; k < 3 * nn; k += T)
+                su[k] = ue[k];
+            __syncthreads();
+            // Pu(l, d, i) = sum_k P(i, k) u(d, k, l)
+            for (int o = t; o < 3 * n * q; o += T)
+            {
+                const int l = o % n, d = (o / n) % 3, i = o / (3 * n);
+                double s = 0.0;
+                for (int k = 0; k < n; ++k)
+                    s += Pd[i + q * k] * su[d + 3 * (k + n * l)];
+                Pu[o] = s;
+            }
+            __syncthreads();
+            // U(d, i, j) = sum_l P(j, l) Pu(l, d, i)
+            for (int o = t; o < 3 * qq; o += T)
+            {
+                const int d = o % 3, i = (o / 3) % q, j = o / (3 * q);
+                double s = 0.0;
+                for (int l = 0; l < n; ++l)
+                    s += Pd[j + q * l] * Pu[l + n * (d + 3 * i)];
+                Uq[o] = s;
+            }
+            __syncthreads();
+            // contravariant fluxes of the wave system at the points (op_2d_cc with the wave
+            // table: F = W (y_eta u - x_eta v, y_eta p, -x_eta p), G = W (-y_xi u + x_xi v, -y_xi p, x_xi p))
+            const double *ce = corners + 8 * (size_t)el;
+            for (int o = t; o < qq; o += T)
+            {
+                const int i = o % q, j = o / q;
+                double J[4];
+                jac(ce, xd[i], xd[j], J);
+                const double W = wd[i] * wd[j];
+                const double Xxi = J[0] * W, Yxi = J[1] * W, Xeta = J[2] * W, Yeta = J[3] * W;
+                const double *U = Uq + 3 * o;
+                double *F = Fq + 6 * o;
+                F[0] = Yeta * U[1] - Xeta * U[2];
+                F[1] = -Yxi * U[1] + Xxi * U[2];
+                F[2] = Yeta * U[0];
+                F[3] = -Yxi * U[0];
+                F[4] = -Xeta * U[0];
+                F[5] = Xxi * U[0];
+            }
+            __syncthreads();
+            // Df(j, d, k) = sum_i D(i, k) F(d, i, j);  Pg(j, d, k) = sum_i P(i, k) G(d, i, j)
+            for (int o = t; o < 3 * q * n; o += T)
+            {
+                const int j = o % q, d = (o / q) % 3, k = o / (3 * q);
+                double df = 0.0, pg = 0.0;
+                for (int i = 0; i < q; ++i)
+                {
+                    df += Dd[i + q * k] * Fq[2 * d + 6 * (i + q * j)];
+                    pg += Pd[i + q * k] * Fq[2 * d + 1 + 6 * (i + q * j)];
+                }
+                Df[o] = df;
+                Pg[o] = pg;
+            }
+            __syncthreads();
+            // du(d, k, l) += sum_j P(j, l) Df(j, d, k) + D(j, l) Pg(j, d, k)
+            double *de = du + (size_t)3 * nn * el;
+            for (int o = t; o < 3 * nn; o += T)
+            {
+                const int d = o % 3, k = (o / 3) % n, l = o / (3 * n);
+                double s = 0.0;
+                for (int j = 0; j < q; ++j)
+                    s += Pd[j + q * l] * Df[j + q * (d + 3 * k)] + Dd[j + q * l] * Pg[j + q * (d + 3 * k)];
+                de[o] += s;
+            }
+            __syncthreads();
+        }
+    }
+
+    // ---------------------------------------------------------------- EdgeFlux<false>
+    // One thread per edge: both sides' traces to the face points, upwind flux there (a = -1,
+    // b = -1/2 of the wave system, in closed form: side 0 contributes -1/2 v (v . U0),
+    // v = (1, n_x, n_y); side 1 +1/2 w (w . U1), w = (1, -n_x, -n_y)), weighted by
+    // w_q |E| / 2, then back to the nodes; side 1 gets the negative.  fb may equal ub.
+    __global__ void qflux_kernel(int n, int q, int ne, const double *__restrict__ nrm, const double *__restrict__ wf,
+                                 const double *__restrict__ Pf, const double *ub, double *fb)
+    {
+        const int e = blockIdx.x * blockDim.x + threadIdx.x;
+        if (e >= ne)
+            return;
+        const double nx = nrm[3 * e], ny = nrm[3 * e + 1], meas = nrm[3 * e + 2];
+        double uf[kMaxQ][3];
+        for (int i = 0; i < q; ++i)
+        {
+            double U0[3], U1[3];
+            for (int d = 0; d < 3; ++d)
+            {
+                double a = 0.0, b = 0.0;
+                for (int j = 0; j < n; ++j)
+                {
+                    a += ub[j + n * (d + 3 * (0 + 2 * (size_t)e))] * Pf[i + q * j];
+                    b += ub[j + n * (d + 3 * (1 + 2 * (size_t)e))] * Pf[i + q * j];
+                }
+                U0[d] = a;
+                U1[d] = b;
+            }
+            const double w = wf[i] * meas;
+            const double s0 = -0.5 * w * (U0[0] + nx * U0[1] + ny * U0[2]);
+            const double s1 = 0.5 * w * (U1[0] - nx * U1[1] - ny * U1[2]);
+            uf[i][0] = s0 + s1;
+            uf[i][1] = nx * (s0 - s1);
+            uf[i][2] = ny * (s0 - s1);
+        }
+        for (int d = 0; d < 3; ++d)
+            for (int i = 0; i < n; ++i)
+            {
+                double f = 0.0;
+                for (int j = 0; j < q; ++j)
+                    f += uf[j][d] * Pf[j + q * i];
+                fb[i + n * (d + 3 * (0 + 2 * (size_t)e))] = f;
+                fb[i + n * (d + 3 * (1 + 2 * (size_t)e))] = -f;
+            }
+    }
+
+    // ---------------------------------------------------------------- MassMatrix<false>
+    // One thread per element and right-hand side: L \ x then L^T \ x (inv), or L (L^T x)
+    // (action), x(d, node) interleaved as the state layout
+    __global__ void qmass_kernel(int c, int nel, int nv, const double *__restrict__ L, double *x, bool inverse)
+    {
+        const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+        if (id >= (long long)nel * nv)
+            return;
+        const int el = (int)(id / nv), d = (int)(id % nv);
+        const double *M = L + (size_t)c * c * el;
+        double *X = x + (size_t)nv * c * el + d;
+        if (inverse)
+        {
+            for (int j = 0; j < c; ++j)
+            {
+                const double xj = X[nv * j] / M[j + c * j];
+                X[nv * j] = xj;
+                for (int i = j + 1; i < c; ++i)
+                    X[nv * i] -= M[i + c * j] * xj;
+            }
+            for (int j = c - 1; j >= 0; --j)
+            {
+                const double xj = X[nv * j] / M[j + c * j];
+                X[nv * j] = xj;
+                for (int i = 0; i < j; ++i)
+                    X[nv * i] -= M[j + c * i] * xj;
+            }
+        }
+        else
+        {
+            for (int i = 0; i < c; ++i)
+            {
+                double t = 0.0;
+                for (int j = i; j < c; ++j)
+                    t += M[j + c * i] * X[nv * j];
+                X[nv * i] = t;
+            }
+            for (int i = c - 1; i >= 0; --i)
+            {
+                double t = 0.0;
+                for (int j = 0; j <= i; ++j)
+                    t += M[i + c * j] * X[nv * j];
+                X[nv * i] = t;
+            }
+        }
+    }
+
+    __global__ void axpy_kernel(double *y, const double *x, double a, long long n)
+    {
+        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+            y[i] += a * x[i];
+    }
+    // one low-storage RK4 stage update: k = a k + dt p; u += b k
+    __global__ void rk_stage_kernel(double *u, double *k, const double *p, double a, double b, double dt, bool first,
+                                    long long n)
+    {
+        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        {
+            const double ki = first ? dt * p[i] : a * k[i] + dt * p[i];
+            k[i] = ki;
+            u[i] += b * ki;
+        }
+    }
+
+    unsigned grid_for(long long n, int threads) { return (unsigned)std::min<long long>((n + threads - 1) / threads, 148LL * 32); }
+
+    template <typename T>
+    int dalloc(T **p, size_t count)
+    {
+        cudaError_t e = cudaMalloc((void **)p, sizeof(T) * std::max<size_t>(count, 1));
+        if (e != cudaSuccess)
+        {
+            *p = nullptr;
+            return cuda_fail(e, "cudaMalloc");
+        }
+        return WDG_OK;
+    }
+    template <typename T>
+    int put(T *d, const std::vector<T> &h)
+    {
+        if (!h.empty())
+            WDG_CUDA(cudaMemcpy(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+        return WDG_OK;
+    }
+
+    struct Dev
+    {
+        int prev = -1;
+        explicit Dev(int d)
+        {
+            cudaGetDevice(&prev);
+            if (prev != d)
+                cudaSetDevice(d);
+        }
+        ~Dev()
+        {
+            if (prev >= 0)
+                cudaSetDevice(prev);
+        }
+    };
+
+    size_t face_count(const wdg_waveq *h, int type)
+    {
+        return (size_t)h->n * 3 * 2 * (type == 0 ? h->w->nI : h->w->nB);
+    }
+
+    // ---------------------------------------------------------------- device-side operators
+    int div_dev(wdg_waveq *h, const double *u, double *du)
+    {
+        wdg_wave *w = h->w;
+        const int n = h->n, q = h->nqd;
+        const size_t smem = sizeof(double) * (3 * n * n + 3 * n * q + 3 * q * q + 6 * q * q + 6 * q * n);
+        qdiv_kernel<<<(unsigned)std::min(w->nel, 148 * 16), 64, smem, w->stream>>>(n, q, w->nel, w->d_corners, h->d_xd,
+                                                                                   h->d_wd, h->d_Pd, h->d_Dd, u, du);
+        WDG_CUDA(cudaGetLastError());
+        return WDG_OK;
+    }
+    int flux_dev(wdg_waveq *h, int type, const double *ub, double *fb)
+    {
+        wdg_wave *w = h->w;
+        const int ne = (type == 0) ? w->nI : w->nB;
+        if (ne == 0)
+            return WDG_OK;
+        qflux_kernel<<<(unsigned)((ne + 127) / 128), 128, 0, w->stream>>>(h->n, h->nqf, ne, type == 0 ? h->d_nI : h->d_nB,
+                                                                          h->d_wf, h->d_Pf, ub, fb);
+        WDG_CUDA(cudaGetLastError());
+        return WDG_OK;
+    }
+    int mass_dev(wdg_waveq *h, int nv, double *x, bool inverse)
+    {
+        wdg_wave *w = h->w;
+        const long long threads = (long long)w->nel * nv;
+        qmass_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, w->stream>>>(h->n * h->n, w->nel, nv, h->d_L, x, inverse);
+        WDG_CUDA(cudaGetLastError());
+        return WDG_OK;
+    }
+    // du += Div u + Prol_I^T Flux_I Prol_I u
+    int wave_dev(wdg_waveq *h, const double *u, double *du)
+    {
+        wdg_wave *w = h->w;
+        WDG_TRY(div_dev(h, u, du));
+        if (w->nI)
+        {
+            WDG_CUDA(launch_prolong(w->geo, 0, u, h->d_uf, w->stream));
+            WDG_TRY(flux_dev(h, 0, h->d_uf, h->d_uf));
+            WDG_CUDA(launch_prolong_t(w->geo, 0, h->d_uf, du, w->stream));
+        }
+        return WDG_OK;
+    }
+    // du += Prol_B^T Flux_B (exterior states) Prol_B u
+    int bc_dev(wdg_waveq *h, const double *u, double *du)
+    {
+        wdg_wave *w = h->w;
+        if (!w->nB)
+            return WDG_OK;
+        WDG_CUDA(launch_prolong(w->geo, 1, u, h->d_uB, w->stream));
+        WDG_CUDA(launch_apply_bc(w->geo, h->d_uB, w->stream));
+        WDG_TRY(flux_dev(h, 1, h->d_uB, h->d_uB));
+        WDG_CUDA(launch_prolong_t(w->geo, 1, h->d_uB, du, w->stream));
+        return WDG_OK;
+    }
+    // dudt = M^{-1} (A u + B u + s F)
+    int rhs_dev(wdg_waveq *h, const double *u, double *dudt, const double *F, double s)
+    {
+        wdg_wave *w = h->w;
+        WDG_CUDA(cudaMemsetAsync(dudt, 0, sizeof(double) * w->ndof, w->stream));
+        WDG_TRY(wave_dev(h, u, dudt));
+        WDG_TRY(bc_dev(h, u, dudt));
+        if (F)
+        {
+            axpy_kernel<<<grid_for(w->ndof, 256), 256, 0, w->stream>>>(dudt, F, s, w->ndof);
+            WDG_CUDA(cudaGetLastError());
+        }
+        return mass_dev(h, 3, dudt, true);
+    }
+
+    typedef int (*Unary)(wdg_waveq *, const double *, double *);
+    int accumulate_entry(wdg_waveq *h, const double *u, double *du, Unary f)
+    {
+        if (!h)
+            return fail(WDG_ERR_ARG, "null exact-quadrature discretisation");
+        if (u == du)
+            return fail(WDG_ERR_ARG, "input and output arrays must differ");
+        Dev g(h->w->device);
+        HostArg a[2];
+        WDG_TRY(bind_arg(h->w, 0, u, h->w->ndof, true, false, a[0]));
+        WDG_TRY(bind_arg(h->w, 1, du, h->w->ndof, true, true, a[1]));
+        WDG_TRY(f(h, a[0].dev, a[1].dev));
+        return finish_args(h->w, a, 2);
+    }
+} // namespace
+
+extern "C"
+{
+    int wdg_waveq_create(const wdg_mesh *mesh, int n_colloc, const int *bc, int device, wdg_waveq **out)
+    {
+        if (!mesh || !out)
+            return fail(WDG_ERR_ARG, "wdg_waveq_create: null argument");
+        *out = nullptr;
+        if (n_colloc < 2 || n_colloc > 9)
+            return fail(WDG_ERR_UNSUPPORTED, "wdg_waveq_create: n_colloc must be 2..9");
+        wdg_wave *w = nullptr;
+        WDG_TRY(wdg_wave_create(mesh, n_colloc, bc, WDG_FP64, device, &w));
+        wdg_waveq *h = new wdg_waveq;
+        h->w = w;
+        h->n = n_colloc;
+        h->nqd = qdiv(n_colloc);
+        h->nqf = qface(n_colloc);
+        h->nqm = qface(n_colloc);
+        Dev g(w->device);
+        const int n = n_colloc, c = n * n;
+        std::vector<double> x(n), wg(n);
+        gauss_lobatto(n, x.data(), wg.data());
+        // Div rule and its interpolation / derivative matrices
+        std::vector<double> xd(h->nqd), wd(h->nqd), Pd((size_t)h->nqd * n), Dd((size_t)h->nqd * n);
+        gauss_legendre(h->nqd, xd.data(), wd.data());
+        interp_matrix(n, x.data(), h->nqd, xd.data(), Pd.data());
+        deriv_at(n, x.data(), h->nqd, xd.data(), Dd.data());
+        // face rule
+        std::vector<double> xf(h->nqf), wf(h->nqf), Pf((size_t)h->nqf * n);
+        gauss_legendre(h->nqf, xf.data(), wf.data());
+        interp_matrix(n, x.data(), h->nqf, xf.data(), Pf.data());
+        // per edge: outward normal of elements[0] and |E| / 2 (StraightEdge, wavedg/Edge.hpp:107-122)
+        auto normals = [&](const std::vector<EdgeRec> &list)
+        {
+            std::vector<double> nr(3 * list.size());
+            for (size_t e = 0; e < list.size(); ++e)
+            {
+                const double *cr = &mesh->corners[8 * (size_t)list[e].el0];
+                const int s = list[e].s0;
+                const double dx = cr[2 * kSideTo[s]] - cr[2 * kSideFrom[s]];
+                const double dy = cr[2 * kSideTo[s] + 1] - cr[2 * kSideFrom[s] + 1];
+                const double len = std::sqrt(dx * dx + dy * dy), sgn = (s >= 2) ? -1.0 : 1.0;
+                nr[3 * e] = sgn * dy / len;
+                nr[3 * e + 1] = -sgn * dx / len;
+                nr[3 * e + 2] = 0.5 * len;
+            }
+            return nr;
+        };
+        const std::vector<double> nI = normals(mesh->interior), nB = normals(mesh->boundary);
+        // element mass matrices on the nqm x nqm rule (lower triangle), Cholesky in place
+        const int qm = h->nqm, q2 = qm * qm;
+        std::vector<double> xm(qm), wm(qm), Bm((size_t)qm * n), L((size_t)c * c * w->nel, 0.0), detJ(q2);
+        gauss_legendre(qm, xm.data(), wm.data());
+        interp_matrix(n, x.data(), qm, xm.data(), Bm.data());
+        int st = WDG_OK;
+        for (int el = 0; el < w->nel && st == WDG_OK; ++el)
+        {
+            const double *cr = &mesh->corners[8 * (size_t)el];
+            for (int p = 0; p < q2; ++p)
+            {
+                double J[4];
+                jac(cr, xm[p % qm], xm[p / qm], J);
+                detJ[p] = J[0] * J[3] - J[2] * J[1];
+            }
+            double *M = &L[(size_t)c * c * el];
+            for (int j = 0; j < c; ++j)
+                for (int i = j; i < c; ++i)
+                {
+                    double mij = 0.0;
+                    for (int p = 0; p < q2; ++p)
+                    {
+                        const double bi = Bm[p % qm + qm * (i % n)] * Bm[p / qm + qm * (i / n)];
+                        const double bj = Bm[p % qm + qm * (j % n)] * Bm[p / qm + qm * (j / n)];
+                        mij += bi * bj * detJ[p] * wm[p % qm] * wm[p / qm];
+                    }
+                    M[i + c * j] = mij;
+                }
+            for (int k = 0; k < c && st == WDG_OK; ++k)
+            {
+                for (int j = k + 1; j < c; ++j)
+                {
+                    const double sc = M[j + c * k] / M[k + c * k];
+                    for (int i = j; i < c; ++i)
+                        M[i + c * j] -= sc * M[i + c * k];
+                }
+                if (!(M[k + c * k] > 0.0))
+                    st = fail(WDG_ERR_ARG, "wdg_waveq_create: an element mass matrix is not positive definite");
+                else
+                {
+                    const double sc = 1.0 / std::sqrt(M[k + c * k]);
+                    for (int i = k; i < c; ++i)
+                        M[i + c * k] *= sc;
+                }
+            }
+        }
+        auto chk = [&](int r)
+        {
+            if (st == WDG_OK)
+                st = r;
+        };
+        chk(dalloc(&h->d_xd, xd.size()));
+        chk(dalloc(&h->d_wd, wd.size()));
+        chk(dalloc(&h->d_Pd, Pd.size()));
+        chk(dalloc(&h->d_Dd, Dd.size()));
+        chk(dalloc(&h->d_wf, wf.size()));
+        chk(dalloc(&h->d_Pf, Pf.size()));
+        chk(dalloc(&h->d_nI, nI.size()));
+        chk(dalloc(&h->d_nB, nB.size()));
+        chk(dalloc(&h->d_L, L.size()));
+        chk(dalloc(&h->d_uf, face_count(h, 0)));
+        chk(dalloc(&h->d_uB, face_count(h, 1)));
+        if (st == WDG_OK)
+        {
+            chk(put(h->d_xd, xd));
+            chk(put(h->d_wd, wd));
+            chk(put(h->d_Pd, Pd));
+            chk(put(h->d_Dd, Dd));
+            chk(put(h->d_wf, wf));
+            chk(put(h->d_Pf, Pf));
+            chk(put(h->d_nI, nI));
+            chk(put(h->d_nB, nB));
+            chk(put(h->d_L, L));
+        }
+        if (st == WDG_OK)
+        {
+            const int smax = (int)(sizeof(double) * (3 * c + 3 * n * h->nqd + 9 * h->nqd * h->nqd + 6 * h->nqd * n));
+            if (smax > 48 * 1024)
+            {
+                const cudaError_t e = cudaFuncSetAttribute(qdiv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smax);
+                if (e != cudaSuccess)
+                    st = cuda_fail(e, "wdg_waveq_create: shared memory attribute");
+            }
+        }
+        if (st != WDG_OK)
+        {
+            wdg_waveq_destroy(h);
+            return st;
+        }
+        *out = h;
+        return WDG_OK;
+    }
+
+    void wdg_waveq_destroy(wdg_waveq *h)
+    {
+        if (!h)
+            return;
+        {
+            Dev g(h->w ? h->w->device : 0);
+            for (double *p : {h->d_xd, h->d_wd, h->d_Pd, h->d_Dd, h->d_wf, h->d_Pf, h->d_nI, h->d_nB, h->d_L, h->d_uf,
+                              h->d_uB, h->d_rk})
+                if (p)
+                    cudaFree(p);
+        }
+        if (h->w)
+            wdg_wave_destroy(h->w);
+        delete h;
+    }
+
+    int wdg_waveq_rules(const wdg_waveq *h, int *n_div, int *n_face, int *n_mass)
+    {
+        if (!h)
+            return fail(WDG_ERR_ARG, "null exact-quadrature discretisation");
+        if (n_div)
+            *n_div = h->nqd;
+        if (n_face)
+            *n_face = h->nqf;
+        if (n_mass)
+            *n_mass = h->nqm;
+        return WDG_OK;
+    }
+
+    int wdg_waveq_wave(const wdg_waveq *h, wdg_wave **wave)
+    {
+        if (!h || !wave)
+            return fail(WDG_ERR_ARG, "wdg_waveq_wave: null argument");
+        *wave = h->w;
+        return WDG_OK;
+    }
+
+    int wdg_waveq_div_action(wdg_waveq *h, const double *u, double *du) { return accumulate_entry(h, u, du, div_dev); }
+    int wdg_waveq_wave_action(wdg_waveq *h, const double *u, double *du) { return accumulate_entry(h, u, du, wave_dev); }
+    int wdg_waveq_wavebc_action(wdg_waveq *h, const double *u, double *du) { return accumulate_entry(h, u, du, bc_dev); }
+
+    int wdg_waveq_edge_flux(wdg_waveq *h, int type, const double *ub, double *fb)
+    {
+        if (!h || (type != 0 && type != 1) || !ub || !fb)
+            return fail(WDG_ERR_ARG, "wdg_waveq_edge_flux: bad arguments");
+        Dev g(h->w->device);
+        const size_t cnt = face_count(h, type);
+        HostArg a[2];
+        if (ub == fb)
+        {
+            WDG_TRY(bind_arg(h->w, 0, ub, cnt, true, true, a[0]));
+            WDG_TRY(flux_dev(h, type, a[0].dev, a[0].dev));
+            return finish_args(h->w, a, 1);
+        }
+        WDG_TRY(bind_arg(h->w, 0, ub, cnt, true, false, a[0]));
+        WDG_TRY(bind_arg(h->w, 1, fb, cnt, false, true, a[1]));
+        WDG_TRY(flux_dev(h, type, a[0].dev, a[1].dev));
+        return finish_args(h->w, a, 2);
+    }
+
+    int wdg_waveq_mass_inv(wdg_waveq *h, int n_var, double *x)
+    {
+        if (!h || n_var < 1 || n_var > 16)
+            return fail(WDG_ERR_ARG, "wdg_waveq_mass_inv: bad arguments");
+        Dev g(h->w->device);
+        HostArg a;
+        WDG_TRY(bind_arg(h->w, 0, x, (size_t)n_var * h->n * h->n * h->w->nel, true, true, a));
+        WDG_TRY(mass_dev(h, n_var, a.dev, true));
+        return finish_args(h->w, &a, 1);
+    }
+
+    int wdg_waveq_mass_action(wdg_waveq *h, int n_var, const double *x, double *y)
+    {
+        if (!h || n_var < 1 || n_var > 16 || !x || !y)
+            return fail(WDG_ERR_ARG, "wdg_waveq_mass_action: bad arguments");
+        Dev g(h->w->device);
+        const size_t cnt = (size_t)n_var * h->n * h->n * h->w->nel;
+        HostArg a[2];
+        WDG_TRY(bind_arg(h->w, 0, x, cnt, true, false, a[0]));
+        WDG_TRY(bind_arg(h->w, 1, y, cnt, false, true, a[1]));
+        if (a[1].dev != a[0].dev)
+            WDG_CUDA(cudaMemcpyAsync(a[1].dev, a[0].dev, sizeof(double) * cnt, cudaMemcpyDeviceToDevice, h->w->stream));
+        WDG_TRY(mass_dev(h, n_var, a[1].dev, false));
+        return finish_args(h->w, a, 2);
+    }
+
+    int wdg_waveq_rhs(wdg_waveq *h, const double *u, double *dudt, const double *F, double s)
+    {
+        if (!h || !u || !dudt)
+            return fail(WDG_ERR_ARG, "wdg_waveq_rhs: bad arguments");
+        if (u == dudt)
+            return fail(WDG_ERR_ARG, "input and output arrays must differ");
+        Dev g(h->w->device);
+        HostArg a[3];
+        int na = 2;
+        WDG_TRY(bind_arg(h->w, 0, u, h->w->ndof, true, false, a[0]));
+        WDG_TRY(bind_arg(h->w, 1, dudt, h->w->ndof, false, true, a[1]));
+        if (F)
+        {
+            WDG_TRY(bind_arg(h->w, 2, F, h->w->ndof, true, false, a[2]));
+            na = 3;
+        }
+        WDG_TRY(rhs_dev(h, a[0].dev, a[1].dev, F ? a[2].dev : nullptr, s));
+        return finish_args(h->w, a, na);
+    }
+
+    int wdg_waveq_rk4_steps(wdg_waveq *h, double *u, double dt, double *t, int nsteps)
+    {
+        if (!h || !u || !t || nsteps < 0)
+            return fail(WDG_ERR_ARG, "wdg_waveq_rk4_steps: bad arguments");
+        Dev g(h->w->device);
+        wdg_wave *w = h->w;
+        if (!h->d_rk)
+            WDG_TRY(dalloc(&h->d_rk, 2 * (size_t)w->ndof));
+        double *k = h->d_rk, *p = h->d_rk + w->ndof;
+        HostArg a;
+        WDG_TRY(bind_arg(w, 0, u, w->ndof, true, true, a));
+        const unsigned gr = grid_for(w->ndof, 256);
+        for (int step = 0; step < nsteps; ++step)
+        {
+            for (int st = 0; st < 5; ++st)
+            {
+                WDG_TRY(rhs_dev(h, a.dev, p, nullptr, 0.0));
+                rk_stage_kernel<<<gr, 256, 0, w->stream>>>(a.dev, k, p, rk4a[st], rk4b[st], dt, st == 0, w->ndof);
+                WDG_CUDA(cudaGetLastError());
+            }
+            *t += dt; // ode::RungeKutta4::step advances t once per step
+        }
+        return finish_args(w, &a, 1);
+    }
+}

@@ -218,15 +218,7 @@ namespace
         }
     };
 
-    // An FP64 array argument: either the caller's device pointer or a staging
-    // buffer filled from (and, for outputs, copied back to) the host array.
-    struct Arg
-    {
-        const double *host_in = nullptr;
-        double *host_out = nullptr;
-        double *dev = nullptr;
-        size_t count = 0;
-    };
+    using Arg = wdg::HostArg;
 
     int bind(wdg_wave *w, int slot, const double *p, size_t count, bool read, bool write, Arg &a)
     {
@@ -357,6 +349,15 @@ namespace
         return WDG_OK;
     }
 } // namespace
+
+namespace wdg
+{
+    int bind_arg(wdg_wave *w, int slot, const double *p, size_t count, bool read, bool write, HostArg &a)
+    {
+        return bind(w, slot, p, count, read, write, a);
+    }
+    int finish_args(wdg_wave *w, HostArg *args, int nargs) { return finish(w, args, nargs); }
+} // namespace wdg
 
 extern "C"
 {

@@ -68,4 +68,18 @@ namespace wdg
     int rk4_run(wdg_wave *w, Real *A, double dt, double &t, int nsteps, const RKExtras &x);
 
     extern const double rk4a[5], rk4b[5], rk4c[5];
+
+    // An FP64 array argument of a C-ABI call: the caller's device pointer, or a staging buffer
+    // filled from (and, for outputs, copied back to) the caller's host array.
+    struct HostArg
+    {
+        const double *host_in = nullptr;
+        double *host_out = nullptr;
+        double *dev = nullptr;
+        size_t count = 0;
+    };
+    // slot: which of the handle's staging buffers a host array of at most ndof values uses
+    int bind_arg(wdg_wave *w, int slot, const double *p, size_t count, bool read, bool write, HostArg &a);
+    // copy host outputs back, release temporaries, wait when any argument was host memory
+    int finish_args(wdg_wave *w, HostArg *args, int nargs);
 } // namespace wdg

@@ -17,7 +17,8 @@ follow waveDG (arotem3/waveDG):
 Arrays are numpy float64 (host memory; results are back when the call
 returns) or CUDA float64 torch tensors (device memory; asynchronous on the
 handle's stream).  Errors raise WdgError, as the reference's wdg_error throws.
-Only the Gauss-Lobatto, approx_quad=True path is built for the GPU.
+Gauss-Lobatto bases.  approx_quad=True is the fused hot path; approx_quad=False (exact
+quadrature with the reference's default rules, FP64) goes through ExactDiscretisation.
 """
 from __future__ import annotations
 
@@ -360,9 +361,81 @@ class Discretisation:
 
 def _require_approx(approx_quad: bool) -> None:
     if not approx_quad:
-        raise WdgError(_lib.WDG_ERR_UNSUPPORTED,
-                       "exact-quadrature operators (Div<false>, EdgeFlux<false>, MassMatrix<false>) are not built; "
-                       "use approx_quad=True")
+        raise WdgError(_lib.WDG_ERR_UNSUPPORTED, "this operator is built for approx_quad=True only")
+
+
+class ExactDiscretisation:
+    """One wdg_waveq handle: the wave system with approx_quad = false (Div<false>,
+    EdgeFlux<false>, MassMatrix<false>; the reference's default Gauss-Legendre rules), FP64."""
+
+    def __init__(self, mesh: Mesh2D, n: int, bc=None, device: int = -1, quad=None):
+        if quad is not None:
+            raise WdgError(_lib.WDG_ERR_UNSUPPORTED, "exact quadrature is built for the default rules (quad=None)")
+        self.mesh, self.n = mesh, int(n)
+        codes = None
+        if bc is not None:
+            codes = np.ascontiguousarray(bc, dtype=np.int32)
+            if codes.size != mesh.n_edges(FaceType.BOUNDARY):
+                raise WdgError(_lib.WDG_ERR_ARG, "bc needs one code per boundary edge")
+        self._codes = codes
+        h = C.c_void_p()
+        check(lib().wdg_waveq_create(mesh._h, self.n, None if codes is None else C.c_void_p(codes.ctypes.data),
+                                     device, C.byref(h)), "wdg_waveq_create")
+        self._h = h
+        self.ndof = 3 * self.n * self.n * mesh.n_elem()
+        self.n_elem = mesh.n_elem()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _destroy("wdg_waveq_destroy", h)
+            self._h = None
+
+    def rules(self) -> tuple:
+        """(Div, EdgeFlux, MassMatrix) points per direction."""
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        check(lib().wdg_waveq_rules(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def _acc(self, fn, u, du, what):
+        pu, _ku = _ptr(u, name="u")
+        pd, _kd = _ptr(du, True, "du")
+        check(getattr(lib(), fn)(self._h, pu, pd), what)
+
+    def div_action(self, u, du) -> None:
+        self._acc("wdg_waveq_div_action", u, du, "Div<false>.action")
+
+    def wave_action(self, u, du) -> None:
+        self._acc("wdg_waveq_wave_action", u, du, "WaveEquation.action")
+
+    def wavebc_action(self, u, du) -> None:
+        self._acc("wdg_waveq_wavebc_action", u, du, "WaveBC.action")
+
+    def edge_flux(self, face_type: int, ub, fb) -> None:
+        pu, _ku = _ptr(ub, name="ub")
+        pf, _kf = _ptr(fb, True, "fb")
+        check(lib().wdg_waveq_edge_flux(self._h, int(face_type), pu, pf), "EdgeFlux<false>.action")
+
+    def mass_action(self, n_var: int, x, y) -> None:
+        px, _kx = _ptr(x, name="x")
+        py, _ky = _ptr(y, True, "y")
+        check(lib().wdg_waveq_mass_action(self._h, int(n_var), px, py), "MassMatrix<false>.action")
+
+    def mass_inv(self, n_var: int, x) -> None:
+        px, _kx = _ptr(x, True, "x")
+        check(lib().wdg_waveq_mass_inv(self._h, int(n_var), px), "MassMatrix<false>.inv")
+
+    def rhs(self, u, dudt, F=None, s: float = 0.0) -> None:
+        pu, _ku = _ptr(u, name="u")
+        pd, _kd = _ptr(dudt, True, "dudt")
+        pf, _kf = _ptr(F, name="F")
+        check(lib().wdg_waveq_rhs(self._h, pu, pd, pf, float(s)), "rhs")
+
+    def rk4_steps(self, u, dt: float, t: float, nsteps: int) -> float:
+        pu, _ku = _ptr(u, True, "u")
+        tt = C.c_double(t)
+        check(lib().wdg_waveq_rk4_steps(self._h, pu, float(dt), C.byref(tt), int(nsteps)), "rk4_steps")
+        return tt.value
 
 
 class Operator:
@@ -376,11 +449,18 @@ class WaveEquation(Operator):
     """du += Div(u) + P^T Flux(P u) over interior edges (source/WaveEquation.cpp:54-68)."""
 
     def __init__(self, mesh: Mesh2D, basis, approx_quad: bool = False, quad=None, precision="fp64"):
-        _require_approx(approx_quad)
-        self.disc = Discretisation(mesh, _gll_n(basis), None, precision)
+        self.exact = not approx_quad
+        if self.exact:
+            if precision != "fp64":
+                raise WdgError(_lib.WDG_ERR_UNSUPPORTED, "exact quadrature is built in FP64")
+            self.disc = ExactDiscretisation(mesh, _gll_n(basis), None, quad=quad)
+        else:
+            self.disc = Discretisation(mesh, _gll_n(basis), None, precision)
 
     def action(self, *args) -> None:
         u, du = args[-2], args[-1]  # action(u, du) or action(n_var, u, du); n_var is ignored
+        if self.exact:
+            return self.disc.wave_action(u, du)
         pu, _ku = _ptr(u, name="u")
         pd, _kd = _ptr(du, True, "du")
         check(lib().wdg_wave_action(self.disc._h, pu, pd), "WaveEquation.action")
@@ -390,11 +470,14 @@ class WaveBC(Operator):
     """du += boundary flux with exterior states from bc (source/WaveEquation.cpp:190-215)."""
 
     def __init__(self, mesh: Mesh2D, bc, basis, approx_quad: bool = False, quad=None):
-        _require_approx(approx_quad)
-        self.disc = Discretisation(mesh, _gll_n(basis), bc)
+        self.exact = not approx_quad
+        self.disc = (ExactDiscretisation(mesh, _gll_n(basis), bc, quad=quad) if self.exact
+                     else Discretisation(mesh, _gll_n(basis), bc))
 
     def action(self, *args) -> None:
         u, du = args[-2], args[-1]
+        if self.exact:
+            return self.disc.wavebc_action(u, du)
         pu, _ku = _ptr(u, name="u")
         pd, _kd = _ptr(du, True, "du")
         check(lib().wdg_wavebc_action(self.disc._h, pu, pd), "WaveBC.action")
@@ -402,18 +485,25 @@ class WaveBC(Operator):
     def apply_bc(self, uB) -> None:
         """apply_bc_2d on boundary traces (n, 3, 2, n_boundary): side 1 <- exterior state."""
         p, _k = _ptr(uB, True, "uB")
-        check(lib().wdg_apply_bc(self.disc._h, p), "apply_bc")
+        h = self.disc._h
+        if self.exact:
+            w = C.c_void_p()
+            check(lib().wdg_waveq_wave(h, C.byref(w)))
+            h = w
+        check(lib().wdg_apply_bc(h, p), "apply_bc")
 
 
 class Div(Operator):
     """Div<true> of the wave system: du += (F(u), grad phi) (source/Div.cpp:131-196)."""
 
     def __init__(self, mesh: Mesh2D, basis, approx_quad: bool = True):
-        _require_approx(approx_quad)
-        self.disc = Discretisation(mesh, _gll_n(basis))
+        self.exact = not approx_quad
+        self.disc = ExactDiscretisation(mesh, _gll_n(basis)) if self.exact else Discretisation(mesh, _gll_n(basis))
 
     def action(self, *args) -> None:
         u, du = args[-2], args[-1]
+        if self.exact:
+            return self.disc.div_action(u, du)
         pu, _ku = _ptr(u, name="u")
         pd, _kd = _ptr(du, True, "du")
         check(lib().wdg_div_action(self.disc._h, pu, pd), "Div.action")
@@ -453,32 +543,40 @@ class EdgeFlux(Operator):
     """EdgeFlux<true> of the wave system with the upwind defaults a = -1, b = -1/2."""
 
     def __init__(self, mesh: Mesh2D, face_type: int, basis, approx_quad: bool = True):
-        _require_approx(approx_quad)
-        self.disc = Discretisation(mesh, _gll_n(basis))
+        self.exact = not approx_quad
+        self.disc = ExactDiscretisation(mesh, _gll_n(basis)) if self.exact else Discretisation(mesh, _gll_n(basis))
         self.face_type = face_type
 
     def action(self, *args) -> None:
         ub, fb = args[-2], args[-1]
+        if self.exact:
+            return self.disc.edge_flux(self.face_type, ub, fb)
         pu, _ku = _ptr(ub, name="ub")
         pf, _kf = _ptr(fb, True, "fb")
         check(lib().wdg_edge_flux(self.disc._h, self.face_type, pu, pf), "EdgeFlux.action")
 
 
 class MassMatrix:
-    """MassMatrix<true>: diagonal w_i w_j detJ (source/MassMatrix.cpp:6-82)."""
+    """MassMatrix<true>: diagonal w_i w_j detJ (source/MassMatrix.cpp:6-82); with
+    approx_quad=False MassMatrix<false>: block Cholesky of the exact element mass matrices."""
 
     def __init__(self, mesh: Mesh2D, basis, quad=None, approx_quad: bool = True):
-        _require_approx(approx_quad)
-        self.disc = Discretisation(mesh, _gll_n(basis))
+        self.exact = not approx_quad
+        self.disc = (ExactDiscretisation(mesh, _gll_n(basis), quad=quad) if self.exact
+                     else Discretisation(mesh, _gll_n(basis)))
 
     def action(self, *args) -> None:
         n_var, x, y = (args if len(args) == 3 else (1, *args))
+        if self.exact:
+            return self.disc.mass_action(n_var, x, y)
         px, _kx = _ptr(x, name="x")
         py, _ky = _ptr(y, True, "y")
         check(lib().wdg_mass_action(self.disc._h, int(n_var), px, py), "MassMatrix.action")
 
     def inv(self, *args) -> None:
         n_var, x = (args if len(args) == 2 else (1, *args))
+        if self.exact:
+            return self.disc.mass_inv(n_var, x)
         px, _kx = _ptr(x, True, "x")
         check(lib().wdg_mass_inv(self.disc._h, int(n_var), px), "MassMatrix.inv")
 
