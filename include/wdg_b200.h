@@ -221,6 +221,10 @@ int wdg_error(wdg_wave *wave, const double *x, const double *y, double *result);
 /* dg::WaveHoltz(omega, mesh, basis, bc, approx_quad=true) (source/WaveHoltz.cpp:5-30) on a
  * discretisation: T = 2 pi / omega, dt = 0.5 min_h / n^2, nt = ceil(T / dt), dt = T / nt. */
 int wdg_waveholtz_create(wdg_wave *wave, double omega, wdg_waveholtz **out);
+/* WaveHoltz(omega, mesh, basis, bc, approx_quad = false): the same iteration over the exact-
+ * quadrature operators of `exact` (which must outlive the handle); every wdg_waveholtz_* call
+ * below works on it, FP64. */
+int wdg_waveholtz_create_exact(wdg_waveq *exact, double omega, wdg_waveholtz **out);
 void wdg_waveholtz_destroy(wdg_waveholtz *wh);
 int wdg_waveholtz_params(const wdg_waveholtz *wh, double *T, double *dt, int *nt);
 /* WaveHoltz::pi0 (source/WaveHoltz.cpp:55-89): w = Pi(0) for load vector F */

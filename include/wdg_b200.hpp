@@ -236,10 +236,21 @@ namespace b200
     public:
         WaveHoltz(double omega, const dg::Mesh2D &mesh, const dg::QuadratureRule *basis, const int *bc,
                   bool approx_quad = false, int precision = WDG_FP64)
-            : omega_(omega), sys_((require_approx(approx_quad), mesh), basis, bc, precision)
+            : omega_(omega)
         {
             wdg_waveholtz *h = nullptr;
-            check(wdg_waveholtz_create(sys_.get(), omega, &h));
+            if (approx_quad)
+            {
+                sys_ = std::make_shared<WaveSystem>(mesh, basis, bc, precision);
+                check(wdg_waveholtz_create(sys_->get(), omega, &h));
+            }
+            else
+            {
+                if (precision != WDG_FP64)
+                    throw std::runtime_error("wdg_b200: exact-quadrature WaveHoltz is FP64");
+                q_ = std::make_shared<ExactDiscretisation>(mesh, basis, bc);
+                check(wdg_waveholtz_create_exact(q_->get(), omega, &h));
+            }
             h_.reset(h, wdg_waveholtz_destroy);
         }
         double K(double t) const { return omega_ / M_PI * (std::cos(omega_ * t) - 0.25); }
@@ -258,8 +269,9 @@ namespace b200
 
     private:
         double omega_;
-        WaveSystem sys_;
-        std::shared_ptr<wdg_waveholtz> h_;
+        std::shared_ptr<WaveSystem> sys_;
+        std::shared_ptr<ExactDiscretisation> q_;
+        std::shared_ptr<wdg_waveholtz> h_; // released first (declared last)
     };
 
     // Many independent WaveHoltz solves advanced together (wdg_whbatch_*; no reference

@@ -68,6 +68,7 @@ _SIGS = {
     "norm": ([_i, _dp], _d),
     "error": ([_i, _dp, _dp], _d),
     "wh_create": ([_v, _d], _v),
+    "whq_create": ([_v, _d], _v),
     "wh_destroy": ([_v], None),
     "wh_params": ([_v, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int)], None),
     "wh_pi0": ([_v, _dp, _dp], None),
@@ -297,7 +298,7 @@ class Op:
 class WaveHoltz:
     def __init__(self, op: Op, omega: float):
         self.op, self.L = op, op.L
-        self.h = self.L.wh_create(op.h, omega)
+        self.h = (self.L.whq_create if isinstance(op, OpQ) else self.L.wh_create)(op.h, omega)
         T, dt, nt = C.c_double(), C.c_double(), C.c_int()
         self.L.wh_params(self.h, C.byref(T), C.byref(dt), C.byref(nt))
         self.T, self.dt, self.nt = T.value, dt.value, nt.value
@@ -344,6 +345,9 @@ class OpQ:
         if getattr(self, "h", None):
             self.L.opq_destroy(self.h)
             self.h = None
+
+    def zeros(self):
+        return np.zeros(self.ndof)
 
     def div(self, u, du):
         self.L.opq_div(self.h, _f64(u), du)

@@ -196,6 +196,20 @@ int main()
         report("ode::RungeKutta4, exact quadrature, 5 steps", rel(vg, vr), 1e-11);
     }
 
+    // WaveHoltz with approx_quad = false, reflecting walls: the reference's class against the drop-in
+    {
+        WaveHoltz whq(2.0, small, basis, bc2.data(), false);
+        b200::WaveHoltz gwhq(2.0, small, basis, bc2.data(), false);
+        std::vector<double> p1(nd2), p2(nd2);
+        whq.pi0(p1.data(), F.data());
+        gwhq.pi0(p2.data(), F.data());
+        report("WaveHoltz::pi0, approx_quad = false", rel(p2, p1), 1e-12);
+        std::vector<double> s1 = p1, s2 = p1;
+        whq.S(s1.data());
+        gwhq.S(s2.data());
+        report("WaveHoltz::S, approx_quad = false", rel(s2, s1), 1e-12);
+    }
+
     // the batched solver on the same two problems as two single solves (exact same periods)
     {
         b200::WaveSystem sa(small, basis, bc2.data()), sb(small, basis, bc2.data());

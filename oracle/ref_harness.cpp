@@ -122,6 +122,7 @@ namespace
 
     struct RefOp
     {
+        static constexpr bool approx = true;
         const Mesh2D &mesh;
         const QuadratureRule *basis;
         const int n, nel, ndof;
@@ -196,9 +197,12 @@ namespace
     // :70-105) and MassMatrix<false> (source/MassMatrix.cpp:84-230).
     struct RefOpQ
     {
+        static constexpr bool approx = false;
         const Mesh2D &mesh;
         const QuadratureRule *basis;
         const int n, nel, ndof;
+        std::vector<int> codes;
+        bool all_reflect = true;
         WaveEquation a;
         ComposedBC bc;
         MassMatrix<false> m;
@@ -208,6 +212,7 @@ namespace
         RefOpQ(const Mesh2D &mesh_, int n_colloc, const int *bc_)
             : mesh(mesh_), basis(QuadratureRule::quadrature_rule(n_colloc, QuadratureRule::GaussLobatto)),
               n(n_colloc), nel(mesh_.n_elem()), ndof(3 * n_colloc * n_colloc * mesh_.n_elem()),
+              codes(bc_, bc_ + mesh_.n_edges(FaceType::BOUNDARY)),
               a(mesh_, basis, false),
               bc(mesh_, basis, bc_, false),
               m(mesh_, basis),
@@ -215,14 +220,19 @@ namespace
               flxI(3, mesh_, FaceType::INTERIOR, basis, kWaveA, true, -1.0, -0.5, nullptr),
               flxB(3, mesh_, FaceType::BOUNDARY, basis, kWaveA, true, -1.0, -0.5, nullptr)
         {
+            for (int c : codes)
+                all_reflect = all_reflect && (c == 1);
         }
 
-        void rhs(const double *u, double *du) const
+        void rhs(const double *u, double *du, const double *F = nullptr, double s = 0.0) const
         {
             for (int i = 0; i < ndof; ++i)
                 du[i] = 0.0;
             a.action(u, du);
             bc.action(u, du);
+            if (F)
+                for (int i = 0; i < ndof; ++i)
+                    du[i] += F[i] * s;
             m.inv(3, du);
         }
     };
@@ -231,9 +241,10 @@ namespace
     // be used (the reference class hard-wires WaveBC).  Loop structure, time
     // accumulation and filter weights follow source/WaveHoltz.cpp:5-145; with
     // all-reflecting boundaries the reference class itself is used instead.
-    struct RefWH
+    template <class O>
+    struct RefWHT
     {
-        const RefOp &op;
+        const O &op;
         const double omega;
         double T, dt;
         int nt;
@@ -241,7 +252,7 @@ namespace
         ode::RungeKutta4 rk;
         mutable std::vector<double> p;
 
-        RefWH(const RefOp &op_, double omega_) : op(op_), omega(omega_), rk(op_.ndof), p(op_.ndof)
+        RefWHT(const O &op_, double omega_) : op(op_), omega(omega_), rk(op_.ndof), p(op_.ndof)
         {
             T = 2.0 * M_PI / omega;
             double h = op.mesh.min_h();
@@ -250,7 +261,7 @@ namespace
             nt = std::ceil(T / dt);
             dt = T / nt;
             if (op.all_reflect)
-                native.reset(new WaveHoltz(omega, op.mesh, op.basis, op.codes.data(), true));
+                native.reset(new WaveHoltz(omega, op.mesh, op.basis, op.codes.data(), O::approx));
         }
 
         double K(double t) const { return omega / M_PI * (std::cos(omega * t) - 0.25); }
@@ -318,6 +329,26 @@ namespace
             }
         }
     };
+    using RefWH = RefWHT<RefOp>;
+    using RefWHQ = RefWHT<RefOpQ>;
+} // namespace
+
+namespace
+{
+    // WaveHoltz handles are RefWH (collocation) or RefWHQ (exact quadrature); the first
+    // member records which
+    struct WHHandle
+    {
+        bool exact;
+        std::unique_ptr<RefWH> c;
+        std::unique_ptr<RefWHQ> q;
+    };
+    template <class F>
+    auto with_wh(void *w, F f)
+    {
+        WHHandle *h = static_cast<WHHandle *>(w);
+        return h->exact ? f(*h->q) : f(*h->c);
+    }
 } // namespace
 
 extern "C"
@@ -496,25 +527,31 @@ extern "C"
     double ref_norm(int n, const double *x) { return norm(n, x); }
     double ref_error(int n, const double *x, const double *y) { return error(n, x, y); }
 
-    void *ref_wh_create(void *o, double omega) { return new RefWH(*static_cast<RefOp *>(o), omega); }
-    void ref_wh_destroy(void *w) { delete static_cast<RefWH *>(w); }
+    void *ref_wh_create(void *o, double omega)
+    {
+        return new WHHandle{false, std::make_unique<RefWH>(*static_cast<RefOp *>(o), omega), nullptr};
+    }
+    void *ref_whq_create(void *o, double omega)
+    {
+        return new WHHandle{true, nullptr, std::make_unique<RefWHQ>(*static_cast<RefOpQ *>(o), omega)};
+    }
+    void ref_wh_destroy(void *w) { delete static_cast<WHHandle *>(w); }
     void ref_wh_params(void *w, double *T, double *dt, int *nt)
     {
-        RefWH *wh = static_cast<RefWH *>(w);
-        *T = wh->T;
-        *dt = wh->dt;
-        *nt = wh->nt;
+        with_wh(w, [&](auto &wh) { *T = wh.T; *dt = wh.dt; *nt = wh.nt; return 0; });
     }
-    int ref_wh_is_native(void *w) { return static_cast<RefWH *>(w)->native ? 1 : 0; }
-    void ref_wh_pi0(void *w, double *u, const double *F) { static_cast<RefWH *>(w)->pi0(u, F); }
-    void ref_wh_S(void *w, double *u) { static_cast<RefWH *>(w)->S(u); }
-    void ref_wh_postprocess(void *w, double *H, const double *U) { static_cast<RefWH *>(w)->postprocess(H, U); }
+    int ref_wh_is_native(void *w) { return with_wh(w, [](auto &wh) { return wh.native ? 1 : 0; }); }
+    void ref_wh_pi0(void *w, double *u, const double *F) { with_wh(w, [&](auto &wh) { wh.pi0(u, F); return 0; }); }
+    void ref_wh_S(void *w, double *u) { with_wh(w, [&](auto &wh) { wh.S(u); return 0; }); }
+    void ref_wh_postprocess(void *w, double *H, const double *U)
+    {
+        with_wh(w, [&](auto &wh) { wh.postprocess(H, U); return 0; });
+    }
 
     // the fixed-point loop of examples/waveholtz2d.cpp:165-185 from W (in/out)
     int ref_wh_solve(void *w, const double *pi0, double tol, int maxit, double *W, double *err_out)
     {
-        RefWH *wh = static_cast<RefWH *>(w);
-        const int ndof = wh->op.ndof;
+        const int ndof = with_wh(w, [](auto &wh) { return wh.op.ndof; });
         const double pz = norm(ndof, pi0);
         std::vector<double> prev(ndof);
         int it;
@@ -522,7 +559,7 @@ extern "C"
         for (it = 1; it <= maxit; ++it)
         {
             std::memcpy(prev.data(), W, sizeof(double) * ndof);
-            wh->S(W);
+            ref_wh_S(w, W);
             for (int i = 0; i < ndof; ++i)
                 W[i] += pi0[i];
             err = error(ndof, W, prev.data()) / pz;

@@ -952,11 +952,14 @@ namespace
                     }
             }
         }
-        void rhs(const double *u, double *du) const
+        void rhs(const double *u, double *du, const double *F = nullptr, double s = 0.0) const
         {
             std::fill(du, du + ndof, 0.0);
             wave_action(u, du);
             bc_action(u, du);
+            if (F)
+                for (int i = 0; i < ndof; ++i)
+                    du[i] += F[i] * s;
             mass_inv(3, du);
         }
     };
@@ -970,14 +973,25 @@ namespace
     }
 
     // WaveHoltz (source/WaveHoltz.cpp:5-145)
-    struct WH
+    // WaveHoltz over either operator set (collocation Op or exact-quadrature OpQ)
+    struct WHBase
     {
-        const Op &op;
-        double omega, T, dt;
-        int nt;
+        double omega = 0, T = 0, dt = 0;
+        int nt = 0, ndof = 0;
+        virtual ~WHBase() = default;
+        virtual void pi0(double *u, const double *F) const = 0;
+        virtual void S(double *u) const = 0;
+        virtual void postprocess(double *H, const double *U) const = 0;
+    };
+    template <class O>
+    struct WHT : WHBase
+    {
+        const O &op;
         mutable vec p, q, du;
-        WH(const Op &o, double om) : op(o), omega(om), p(o.ndof), q(o.ndof), du(o.ndof)
+        WHT(const O &o, double om) : op(o), p(o.ndof), q(o.ndof), du(o.ndof)
         {
+            omega = om;
+            ndof = o.ndof;
             T = 2.0 * M_PI / omega;
             const double h = min_h(o.m);
             const double pp = o.n;
@@ -986,7 +1000,7 @@ namespace
             dt = T / nt;
         }
         double K(double t) const { return omega / M_PI * (std::cos(omega * t) - 0.25); }
-        void pi0(double *u, const double *F) const
+        void pi0(double *u, const double *F) const override
         {
             auto f = [this, F](double *vt, double t, const double *v)
             { op.rhs(v, vt, F, -1.0 / omega * std::sin(omega * t)); };
@@ -1001,7 +1015,7 @@ namespace
                     u[i] += c * p[i];
             }
         }
-        void S(double *u) const
+        void S(double *u) const override
         {
             auto f = [this](double *vt, double, const double *v)
             { op.rhs(v, vt, nullptr, 0.0); };
@@ -1019,7 +1033,7 @@ namespace
                     u[i] += c * p[i];
             }
         }
-        void postprocess(double *H, const double *U) const
+        void postprocess(double *H, const double *U) const override
         {
             op.rhs(U, p.data(), nullptr, 0.0);
             for (int i = 0; i < op.ndof / 3; ++i)
@@ -1220,23 +1234,24 @@ extern "C"
         for (int s = 0; s < nsteps; ++s)
             rk4_step(op->ndof, dt, f, *t, u, p, du);
     }
-    void *orc_wh_create(void *o, double omega) { return new WH(*static_cast<Op *>(o), omega); }
-    void orc_wh_destroy(void *w) { delete static_cast<WH *>(w); }
+    void *orc_wh_create(void *o, double omega) { return static_cast<WHBase *>(new WHT<Op>(*static_cast<Op *>(o), omega)); }
+    void *orc_whq_create(void *o, double omega) { return static_cast<WHBase *>(new WHT<OpQ>(*static_cast<OpQ *>(o), omega)); }
+    void orc_wh_destroy(void *w) { delete static_cast<WHBase *>(w); }
     void orc_wh_params(void *w, double *T, double *dt, int *nt)
     {
-        WH *wh = static_cast<WH *>(w);
+        WHBase *wh = static_cast<WHBase *>(w);
         *T = wh->T;
         *dt = wh->dt;
         *nt = wh->nt;
     }
-    void orc_wh_pi0(void *w, double *u, const double *F) { static_cast<WH *>(w)->pi0(u, F); }
-    void orc_wh_S(void *w, double *u) { static_cast<WH *>(w)->S(u); }
-    void orc_wh_postprocess(void *w, double *H, const double *U) { static_cast<WH *>(w)->postprocess(H, U); }
+    void orc_wh_pi0(void *w, double *u, const double *F) { static_cast<WHBase *>(w)->pi0(u, F); }
+    void orc_wh_S(void *w, double *u) { static_cast<WHBase *>(w)->S(u); }
+    void orc_wh_postprocess(void *w, double *H, const double *U) { static_cast<WHBase *>(w)->postprocess(H, U); }
     // examples/waveholtz2d.cpp:165-185 from W (in/out)
     int orc_wh_solve(void *w, const double *pi0, double tol, int maxit, double *W, double *err_out)
     {
-        WH *wh = static_cast<WH *>(w);
-        const int nd = wh->op.ndof;
+        WHBase *wh = static_cast<WHBase *>(w);
+        const int nd = wh->ndof;
         const double pz = norm2(nd, pi0);
         vec prev(nd);
         int it;

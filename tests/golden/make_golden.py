@@ -127,6 +127,26 @@ def waveholtz():
                         omega=2.0, F=F, pi0=p1, S_pi0=wh1.S(p1))
 
 
+def waveholtz_exact():
+    """approx_quad = false WaveHoltz on the 5 x 5 perturbed mesh, P = 3, omega = 2: all-reflecting
+    walls through the reference's own WaveHoltz class (pi0, S); reflecting left/bottom and
+    absorbing elsewhere through the harness's restated loop over the exact operators (pi0, S,
+    a solve to 1e-6)."""
+    v, q = mg.perturbed_rect(5, 0.2, seed=21)
+    m = cpu.Mesh(v, q, KIND)
+    bc1 = np.ones(m.n_edges(1), dtype=np.int32)
+    F = cpu.Op(m, 4, bc1).load_gaussians([[0.1, 0.2]], [0.2], [1.0], 4.0, 0, False)
+    wh1 = cpu.WaveHoltz(cpu.OpQ(m, 4, bc1), 2.0)
+    p1 = wh1.pi0(F)
+    bc = mg.boundary_codes_by_wall(m.boundary_midpoints(), left=1, bottom=1, right=0, top=0)
+    wh = cpu.WaveHoltz(cpu.OpQ(m, 4, bc), 2.0)
+    p = wh.pi0(F)
+    W, it, err = wh.solve(p, 1e-6, 200)
+    np.savez_compressed(os.path.join(HERE, "waveholtz_exact_5x5_P3.npz"), verts=v, quads=q, n=4, omega=2.0, F=F,
+                        bc_reflect=bc1, pi0_reflect=p1, S_pi0_reflect=wh1.S(p1), bc=bc, T=wh.T, dt=wh.dt, nt=wh.nt,
+                        pi0=p, S_pi0=wh.S(p), W=W, iters=it, err=err)
+
+
 def opq_fixture(name, v, q, m, n, seed):
     """approx_quad = false: Div<false>, EdgeFlux<false> (interior and boundary), WaveEquation,
     the composed boundary operator over EdgeFlux<false>, MassMatrix<false>, RHS, 5 RK4 steps."""
@@ -163,6 +183,7 @@ def main():
         for seed, (name, v, q) in enumerate(meshes()):
             for n in qcases.get(name, []):
                 opq_fixture(name, v, q, cpu.Mesh(v, q, KIND), n, 1000 + 100 * seed + n)
+        waveholtz_exact()
         print("exact-quadrature fixtures written to", HERE)
         return
     x = {}
@@ -179,6 +200,7 @@ def main():
             opq_fixture(name, v, q, m, n, 1000 + 100 * seed + n)
     config1()
     waveholtz()
+    waveholtz_exact()
     print("fixtures written to", HERE)
 
 

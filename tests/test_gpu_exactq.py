@@ -92,3 +92,38 @@ def test_larger_mesh_against_oracle(gpu_lib):
         du = np.zeros_like(u)
         d.rhs(u, du)
         assert rel(du, op.rhs(u)) < TOL, n
+
+
+def test_waveholtz_exact_quadrature(gpu_lib):
+    """WaveHoltz(..., approx_quad=False): pi0 and S against the reference's own WaveHoltz class
+    (all-reflecting walls) and against the restated loop (mixed walls); the solve takes the
+    reference's iteration count; postprocess against the oracle."""
+    import wavedg_b200 as W
+    from oracle import cpu
+
+    g = golden("waveholtz_exact_5x5_P3.npz")
+    mesh = W.Mesh2D.from_vertices(g["verts"], g["quads"])
+    n, om = int(g["n"]), float(g["omega"])
+    basis = W.QuadratureRule.quadrature_rule(n, W.QuadratureRule.GaussLobatto)
+    wr = W.WaveHoltz(om, mesh, basis, g["bc_reflect"], False)
+    p = np.zeros_like(g["F"])
+    wr.pi0(p, g["F"])
+    assert rel(p, g["pi0_reflect"]) < 1e-12
+    s = g["pi0_reflect"].copy()
+    wr.S(s)
+    assert rel(s, g["S_pi0_reflect"]) < 1e-12
+    wh = W.WaveHoltz(om, mesh, basis, g["bc"], False)
+    assert (wh.T, wh.dt, wh.nt) == (g["T"], g["dt"], g["nt"])
+    p = np.zeros_like(g["F"])
+    wh.pi0(p, g["F"])
+    assert rel(p, g["pi0"]) < 1e-12
+    s = g["pi0"].copy()
+    wh.S(s)
+    assert rel(s, g["S_pi0"]) < 1e-12
+    Wx, it, res = wh.solve(g["F"], 1e-6, 200)
+    assert it == int(g["iters"])
+    assert rel(Wx, g["W"]) < 1e-10
+    H = np.zeros(2 * len(g["W"]) // 3)
+    wh.postprocess(H, g["W"])
+    ref = cpu.WaveHoltz(cpu.OpQ(cpu.Mesh(g["verts"], g["quads"], "oracle"), n, g["bc"]), om).postprocess(g["W"])
+    assert rel(H, ref) < TOL

@@ -127,6 +127,24 @@ def test_waveholtz_reflecting_uses_reference_class():
     assert rel(wh.S(g["pi0"]), g["S_pi0"]) < 1e-13
 
 
+def test_waveholtz_exact_quadrature():
+    """approx_quad = false: the reference's own WaveHoltz class (all-reflecting walls) and the
+    restated loop over the exact operators (mixed walls, solve to 1e-6)."""
+    g = golden("waveholtz_exact_5x5_P3.npz")
+    m = cpu.Mesh(g["verts"], g["quads"], "oracle")
+    n, om = int(g["n"]), float(g["omega"])
+    wh1 = cpu.WaveHoltz(cpu.OpQ(m, n, g["bc_reflect"]), om)
+    assert rel(wh1.pi0(g["F"]), g["pi0_reflect"]) < 1e-13
+    assert rel(wh1.S(g["pi0_reflect"]), g["S_pi0_reflect"]) < 1e-13
+    wh = cpu.WaveHoltz(cpu.OpQ(m, n, g["bc"]), om)
+    assert (wh.T, wh.dt, wh.nt) == (g["T"], g["dt"], g["nt"])
+    assert rel(wh.pi0(g["F"]), g["pi0"]) < 1e-13
+    assert rel(wh.S(g["pi0"]), g["S_pi0"]) < 1e-13
+    W, it, err = wh.solve(g["pi0"], 1e-6, 200)
+    assert it == g["iters"]
+    assert rel(W, g["W"]) < 1e-12
+
+
 def test_oracle_catches_planted_error():
     """A mistake planted in the oracle's inputs must show up as a parity failure."""
     g = golden("op_scrambled6_n5.npz")

@@ -14,7 +14,8 @@
 //
 // FP64 only.  This is the accuracy path for callers that set approx_quad = false, not the
 // bandwidth-bound hot path: one CTA per element for the volume term, one thread per edge
-// for the face term, one thread per element for the block-Cholesky mass solves.
+// for the face term, one warp per element for the mass matrix and its inverse (formed at
+// set-up from the block Cholesky factors, applied as dense products).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -32,7 +33,7 @@ struct wdg_waveq
     double *d_xd = nullptr, *d_wd = nullptr, *d_Pd = nullptr, *d_Dd = nullptr; // Div rule, P(i,k), D(i,k)
     double *d_wf = nullptr, *d_Pf = nullptr;                                   // face rule, P(i,k)
     double *d_nI = nullptr, *d_nB = nullptr; // per edge (n_x, n_y, |E| / 2)
-    double *d_L = nullptr;                   // Cholesky factors (n^2, n^2, nel), column-major
+    double *d_M = nullptr, *d_Minv = nullptr; // element mass matrices and their inverses (n^2, n^2, nel)
     double *d_uf = nullptr, *d_uB = nullptr; // face traces
     double *d_rk = nullptr;                  // RK4: k and the stage derivative (2 ndof)
 };
@@ -237,49 +238,32 @@ namespace
     }
 
     // ---------------------------------------------------------------- MassMatrix<false>
-    // One thread per element and right-hand side: L \ x then L^T \ x (inv), or L (L^T x)
-    // (action), x(d, node) interleaved as the state layout
-    __global__ void qmass_kernel(int c, int nel, int nv, const double *__restrict__ L, double *x, bool inverse)
+    // x <- A x per element for a dense n^2 x n^2 matrix A (the element mass matrix, or its
+    // inverse formed at set-up from the Cholesky factors), nv interleaved right-hand sides,
+    // in place: one warp per element, the element's x staged in shared memory; lanes take
+    // consecutive rows, so each column of A is read coalesced.
+    __global__ void qdense_kernel(int c, int nel, int nv, const double *__restrict__ A, double *x)
     {
-        const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-        if (id >= (long long)nel * nv)
-            return;
-        const int el = (int)(id / nv), d = (int)(id % nv);
-        const double *M = L + (size_t)c * c * el;
-        double *X = x + (size_t)nv * c * el + d;
-        if (inverse)
+        extern __shared__ double sx[];
+        const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+        double *xs = sx + (size_t)wib * nv * c;
+        const int m = nv * c;
+        for (int el = blockIdx.x * wpb + wib; el < nel; el += gridDim.x * wpb)
         {
-            for (int j = 0; j < c; ++j)
+            double *xe = x + (size_t)m * el;
+            const double *Ae = A + (size_t)c * c * el;
+            for (int o = lane; o < m; o += 32)
+                xs[o] = xe[o];
+            __syncwarp();
+            for (int o = lane; o < m; o += 32)
             {
-                const double xj = X[nv * j] / M[j + c * j];
-                X[nv * j] = xj;
-                for (int i = j + 1; i < c; ++i)
-                    X[nv * i] -= M[i + c * j] * xj;
+                const int i = o / nv, d = o - i * nv;
+                double y = 0.0;
+                for (int j = 0; j < c; ++j)
+                    y += Ae[i + (size_t)c * j] * xs[d + nv * j];
+                xe[o] = y;
             }
-            for (int j = c - 1; j >= 0; --j)
-            {
-                const double xj = X[nv * j] / M[j + c * j];
-                X[nv * j] = xj;
-                for (int i = 0; i < j; ++i)
-                    X[nv * i] -= M[j + c * i] * xj;
-            }
-        }
-        else
-        {
-            for (int i = 0; i < c; ++i)
-            {
-                double t = 0.0;
-                for (int j = i; j < c; ++j)
-                    t += M[j + c * i] * X[nv * j];
-                X[nv * i] = t;
-            }
-            for (int i = c - 1; i >= 0; --i)
-            {
-                double t = 0.0;
-                for (int j = 0; j <= i; ++j)
-                    t += M[i + c * j] * X[nv * j];
-                X[nv * i] = t;
-            }
+            __syncwarp();
         }
     }
 
@@ -367,8 +351,11 @@ namespace
     int mass_dev(wdg_waveq *h, int nv, double *x, bool inverse)
     {
         wdg_wave *w = h->w;
-        const long long threads = (long long)w->nel * nv;
-        qmass_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, w->stream>>>(h->n * h->n, w->nel, nv, h->d_L, x, inverse);
+        const int c = h->n * h->n;
+        const int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (48 * 1024) / (sizeof(double) * nv * c)));
+        const size_t smem = sizeof(double) * wpb * nv * c; // at most 48 KB (nv <= 16, c <= 81: 10.4 KB a warp)
+        qdense_kernel<<<(unsigned)std::min((w->nel + wpb - 1) / wpb, 148 * 32), 32 * wpb, smem, w->stream>>>(
+            c, w->nel, nv, inverse ? h->d_Minv : h->d_M, x);
         WDG_CUDA(cudaGetLastError());
         return WDG_OK;
     }
@@ -428,6 +415,49 @@ namespace
     }
 } // namespace
 
+namespace wdg
+{
+    // RK buffers and the resident state exist before a period is captured into a graph
+    int waveq_prepare(wdg_waveq *h)
+    {
+        Dev g(h->w->device);
+        WDG_TRY(ensure_states(h->w));
+        if (!h->d_rk)
+            WDG_TRY(dalloc(&h->d_rk, 2 * (size_t)h->w->ndof));
+        return WDG_OK;
+    }
+
+    // One WaveHoltz period on the exact-quadrature operators, the sequence rk4_run runs on the
+    // collocation kernels: nt RK4 steps of u' = M^{-1}(A u + B u + F s(t)), s(t) =
+    // -sin(omega t) / omega at the stage times (F may be NULL), then acc += c_filter[step] u
+    // after each step (source/WaveHoltz.cpp:55-121).  On the handle's current stream.
+    int waveq_period(wdg_waveq *h, double *u, double dt, int nt, const double *F, double omega, double *acc,
+                     const double *c_filter)
+    {
+        wdg_wave *w = h->w;
+        double *k = h->d_rk, *p = h->d_rk + w->ndof;
+        const unsigned gr = grid_for(w->ndof, 256);
+        double t = 0.0;
+        for (int step = 0; step < nt; ++step)
+        {
+            for (int st = 0; st < 5; ++st)
+            {
+                const double s = F ? -std::sin(omega * (t + rk4c[st] * dt)) / omega : 0.0;
+                WDG_TRY(rhs_dev(h, u, p, F, s));
+                rk_stage_kernel<<<gr, 256, 0, w->stream>>>(u, k, p, rk4a[st], rk4b[st], dt, st == 0, w->ndof);
+                WDG_CUDA(cudaGetLastError());
+            }
+            axpy_kernel<<<gr, 256, 0, w->stream>>>(acc, u, c_filter[step], w->ndof);
+            WDG_CUDA(cudaGetLastError());
+            t += dt;
+        }
+        return WDG_OK;
+    }
+
+    // P = M^{-1}(A + B) W on the exact operators (WaveHoltz::postprocess's RHS)
+    int waveq_rhs_device(wdg_waveq *h, const double *u, double *dudt) { return rhs_dev(h, u, dudt, nullptr, 0.0); }
+} // namespace wdg
+
 extern "C"
 {
     int wdg_waveq_create(const wdg_mesh *mesh, int n_colloc, const int *bc, int device, wdg_waveq **out)
@@ -478,7 +508,8 @@ extern "C"
         const std::vector<double> nI = normals(mesh->interior), nB = normals(mesh->boundary);
         // element mass matrices on the nqm x nqm rule (lower triangle), Cholesky in place
         const int qm = h->nqm, q2 = qm * qm;
-        std::vector<double> xm(qm), wm(qm), Bm((size_t)qm * n), L((size_t)c * c * w->nel, 0.0), detJ(q2);
+        std::vector<double> xm(qm), wm(qm), Bm((size_t)qm * n), L((size_t)c * c, 0.0), detJ(q2);
+        std::vector<double> Mf((size_t)c * c * w->nel), Mi((size_t)c * c * w->nel);
         gauss_legendre(qm, xm.data(), wm.data());
         interp_matrix(n, x.data(), qm, xm.data(), Bm.data());
         int st = WDG_OK;
@@ -491,7 +522,8 @@ extern "C"
                 jac(cr, xm[p % qm], xm[p / qm], J);
                 detJ[p] = J[0] * J[3] - J[2] * J[1];
             }
-            double *M = &L[(size_t)c * c * el];
+            double *M = L.data();
+            std::fill(L.begin(), L.end(), 0.0);
             for (int j = 0; j < c; ++j)
                 for (int i = j; i < c; ++i)
                 {
@@ -503,6 +535,8 @@ extern "C"
                         mij += bi * bj * detJ[p] * wm[p % qm] * wm[p / qm];
                     }
                     M[i + c * j] = mij;
+                    Mf[(size_t)c * c * el + i + c * j] = mij;
+                    Mf[(size_t)c * c * el + j + c * i] = mij;
                 }
             for (int k = 0; k < c && st == WDG_OK; ++k)
             {
@@ -521,6 +555,25 @@ extern "C"
                         M[i + c * k] *= sc;
                 }
             }
+            // M^{-1} column by column: solve_chol on the unit vectors (linalg.cpp:32-66)
+            for (int col = 0; col < c && st == WDG_OK; ++col)
+            {
+                double *X = &Mi[(size_t)c * c * el + (size_t)c * col];
+                for (int i = 0; i < c; ++i)
+                    X[i] = (i == col) ? 1.0 : 0.0;
+                for (int j = 0; j < c; ++j)
+                {
+                    X[j] /= M[j + c * j];
+                    for (int i = j + 1; i < c; ++i)
+                        X[i] -= M[i + c * j] * X[j];
+                }
+                for (int j = c - 1; j >= 0; --j)
+                {
+                    X[j] /= M[j + c * j];
+                    for (int i = 0; i < j; ++i)
+                        X[i] -= M[j + c * i] * X[j];
+                }
+            }
         }
         auto chk = [&](int r)
         {
@@ -535,7 +588,8 @@ extern "C"
         chk(dalloc(&h->d_Pf, Pf.size()));
         chk(dalloc(&h->d_nI, nI.size()));
         chk(dalloc(&h->d_nB, nB.size()));
-        chk(dalloc(&h->d_L, L.size()));
+        chk(dalloc(&h->d_M, Mf.size()));
+        chk(dalloc(&h->d_Minv, Mi.size()));
         chk(dalloc(&h->d_uf, face_count(h, 0)));
         chk(dalloc(&h->d_uB, face_count(h, 1)));
         if (st == WDG_OK)
@@ -548,7 +602,8 @@ extern "C"
             chk(put(h->d_Pf, Pf));
             chk(put(h->d_nI, nI));
             chk(put(h->d_nB, nB));
-            chk(put(h->d_L, L));
+            chk(put(h->d_M, Mf));
+            chk(put(h->d_Minv, Mi));
         }
         if (st == WDG_OK)
         {
@@ -575,7 +630,7 @@ extern "C"
             return;
         {
             Dev g(h->w ? h->w->device : 0);
-            for (double *p : {h->d_xd, h->d_wd, h->d_Pd, h->d_Dd, h->d_wf, h->d_Pf, h->d_nI, h->d_nB, h->d_L, h->d_uf,
+            for (double *p : {h->d_xd, h->d_wd, h->d_Pd, h->d_Dd, h->d_wf, h->d_Pf, h->d_nI, h->d_nB, h->d_M, h->d_Minv, h->d_uf,
                               h->d_uB, h->d_rk})
                 if (p)
                     cudaFree(p);

@@ -82,4 +82,10 @@ namespace wdg
     int bind_arg(wdg_wave *w, int slot, const double *p, size_t count, bool read, bool write, HostArg &a);
     // copy host outputs back, release temporaries, wait when any argument was host memory
     int finish_args(wdg_wave *w, HostArg *args, int nargs);
+
+    // exact-quadrature periods for WaveHoltz (exactq.cu)
+    int waveq_prepare(wdg_waveq *q);
+    int waveq_period(wdg_waveq *q, double *u, double dt, int nt, const double *F, double omega, double *acc,
+                     const double *c_filter);
+    int waveq_rhs_device(wdg_waveq *q, const double *u, double *dudt);
 } // namespace wdg

@@ -28,6 +28,7 @@ struct wdg_waveholtz
     void *d_F = nullptr; // forcing in the stepping precision
     cudaGraphExec_t g_S = nullptr, g_pi0 = nullptr;
     double pi0_norm = 0;
+    wdg_waveq *q = nullptr; // exact quadrature (approx_quad = false): periods on its operators
 };
 
 namespace
@@ -57,6 +58,10 @@ namespace
     int period(wdg_waveholtz *h, bool forced)
     {
         wdg_wave *w = h->w;
+        if (h->q)
+            return waveq_period(h->q, static_cast<double *>(w->d_state[0]), h->dt, h->nt,
+                                forced ? static_cast<const double *>(h->d_F) : nullptr, h->omega, h->d_acc,
+                                h->c_filter.data());
         RKExtras x;
         x.acc = h->d_acc;
         x.c_filter = h->c_filter.data();
@@ -208,6 +213,23 @@ extern "C"
         return WDG_OK;
     }
 
+    // WaveHoltz(omega, mesh, basis, bc, approx_quad = false): the same iteration on the exact-
+    // quadrature operators of q (which must outlive the handle)
+    int wdg_waveholtz_create_exact(wdg_waveq *q, double omega, wdg_waveholtz **out)
+    {
+        if (!q || !out)
+            return fail(WDG_ERR_ARG, "wdg_waveholtz_create_exact: null argument");
+        *out = nullptr;
+        wdg_wave *w = nullptr;
+        WDG_TRY(wdg_waveq_wave(q, &w));
+        WDG_TRY(waveq_prepare(q));
+        wdg_waveholtz *h = nullptr;
+        WDG_TRY(wdg_waveholtz_create(w, omega, &h));
+        h->q = q;
+        *out = h;
+        return WDG_OK;
+    }
+
     void wdg_waveholtz_destroy(wdg_waveholtz *h)
     {
         if (!h)
@@ -294,6 +316,8 @@ extern "C"
         {
             WDG_TRY(copy_in(h, h->d_W, W));
             // P = M^{-1}(A + B) W in FP64 (the postprocess is a single RHS)
+            if (h->q)
+                WDG_TRY(waveq_rhs_device(h->q, h->d_W, h->d_acc));
             StageArgs<double> a{};
             a.u = h->d_W;
             a.out = h->d_acc;
@@ -307,7 +331,8 @@ extern "C"
             a.flags = F_ALL;
             a.use_tma = 1;
             a.err = w->d_err;
-            WDG_CUDA(launch_stage<double>(w->n, false, a, 0, h->cs));
+            if (!h->q)
+                WDG_CUDA(launch_stage<double>(w->n, false, a, 0, h->cs));
             bool dev = false;
             WDG_TRY(is_device_ptr(w, H, dev));
             const long long npts = w->ndof / 3;

@@ -629,11 +629,17 @@ class WaveHoltz:
 
     def __init__(self, omega: float, mesh: Mesh2D, basis, bc, approx_quad: bool = False, precision="fp64",
                  device: int = -1, system: WaveSystem | None = None):
-        _require_approx(approx_quad)
         self.omega = float(omega)
-        self.system = system if system is not None else WaveSystem(mesh, basis, bc, precision, device)
         h = C.c_void_p()
-        check(lib().wdg_waveholtz_create(self.system._h, self.omega, C.byref(h)), "WaveHoltz")
+        if not approx_quad:
+            # exact quadrature (Div<false>, EdgeFlux<false>, MassMatrix<false>), FP64
+            if precision != "fp64" or system is not None:
+                raise WdgError(_lib.WDG_ERR_UNSUPPORTED, "exact-quadrature WaveHoltz is FP64 on its own operators")
+            self.system = ExactDiscretisation(mesh, _gll_n(basis), bc, device)
+            check(lib().wdg_waveholtz_create_exact(self.system._h, self.omega, C.byref(h)), "WaveHoltz")
+        else:
+            self.system = system if system is not None else WaveSystem(mesh, basis, bc, precision, device)
+            check(lib().wdg_waveholtz_create(self.system._h, self.omega, C.byref(h)), "WaveHoltz")
         self._h = h
         T, dt, nt = C.c_double(), C.c_double(), C.c_int()
         check(lib().wdg_waveholtz_params(h, C.byref(T), C.byref(dt), C.byref(nt)))
