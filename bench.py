@@ -258,12 +258,13 @@ def run_ours(args, rank, world, local_rank):
                          "frac": b32 / (ms32 / args.steps / 1e3) / 1e9 / peak}
         del s32
 
-    if not args.no_extras and not args.no_waveholtz and args.precision == "fp64":
+    # single-GPU companion measurements: skipped under torchrun so that a multi-GPU run holds
+    # its GPUs only for the replicated RK4 measurement
+    if not args.no_extras and not args.no_waveholtz and args.precision == "fp64" and world == 1:
         extra["waveholtz_c3"] = waveholtz_c3(local_rank)
         extra["waveholtz_batched"] = waveholtz_batched(local_rank)
-    if not args.no_extras and args.precision == "fp64":
-        extra["exact_quadrature"] = exact_quadrature(local_rank, cpu_leg=(rank == 0 and world == 1
-                                                                          and not args.no_cpu_baseline))
+    if not args.no_extras and args.precision == "fp64" and world == 1:
+        extra["exact_quadrature"] = exact_quadrature(local_rank, cpu_leg=not args.no_cpu_baseline)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
