@@ -15,7 +15,11 @@ Pipeline (all on one GPU, all through this library's kernels):
             FP64 finish from zero, and the same from the network's prediction.  The plain
             fixed-point iteration decides convergence in every arm.
 
-    python -m wavedg_b200.warmstart --train 256 --epochs 20 --eval 64 --weights W.npz --json out.json
+    python -m wavedg_b200.warmstart --train 256 --epochs 100 --eval 128 --weights A.npz
+    python -m wavedg_b200.warmstart --weights A.npz --finetune --data-seed 3000 --train 256 \
+        --epochs 150 --lr 1e-3 --save B.npz --eval 0
+    python -m wavedg_b200.warmstart --weights B.npz --eval 256 --plain 8 --json out.json
+    python -m wavedg_b200.warmstart --time-batch 64          # period timing of the batch alone
 """
 from __future__ import annotations
 
