@@ -155,6 +155,30 @@ int wdg_rhs(wdg_wave *wave, const double *u, double *dudt, const double *F, doub
  * t advances by dt per step.  One fused kernel per RK stage. */
 int wdg_rk4_steps(wdg_wave *wave, double *u, double dt, double *t, int nsteps);
 
+/* ---- domain decomposition (one rank's share of a mesh) ---- */
+/* The fused kernels' partner table of `mesh` (what Mesh2D::distribute and FaceVector need to
+ * know, source/Mesh2D.cpp:384-592): per element side the DOF offset of the neighbour node that
+ * faces face node 0 (fbase, 4 per element, -1 on the boundary) and per element four bytes
+ * (stride code in bits 0-1: +3, -3, +3n, -3n per face node; boundary code bits 3-4; boundary bit 7).
+ * Host only. */
+int wdg_mesh_partner_table(const wdg_mesh *mesh, int n_colloc, const int *bc, int *fbase, unsigned *fcode);
+/* A discretisation of the local elements of a decomposed mesh: `mesh` holds this rank's
+ * elements, so the sides it shares with other ranks are boundary sides of `mesh`; the n_halo
+ * sides (halo_elem[j], halo_side[j]) read their neighbour trace from halo slot j instead,
+ * n x 3 values (face-node order of this side) stored after the elements in every state
+ * buffer.  For RK stepping (wdg_rk4_stage) and the resident-state calls only. */
+int wdg_wave_create_halo(const wdg_mesh *mesh, int n_colloc, const int *bc, int precision, int device, int n_halo,
+                         const int *halo_elem, const int *halo_side, wdg_wave **out);
+int wdg_halo_info(const wdg_wave *wave, long long *elements_values, long long *halo_values);
+/* out[3 j + f] = state buffer `buffer` (0 resident, 1, 2 the RK rotation) at idx[j] + f, f < 3:
+ * the traces another rank's halo needs (idx, out: device arrays; the handle's precision) */
+int wdg_halo_gather(wdg_wave *wave, int buffer, const int *idx, int count, void *out);
+/* halo values [offset, offset + count) of state buffer `buffer` <- src (device or host) */
+int wdg_halo_put(wdg_wave *wave, int buffer, long long offset, const void *src, long long count);
+/* RK4 stage `stage` (0..4) of ode::RungeKutta4::step on the resident state: reads buffer
+ * 0, 1, 2, 1, 2 and writes 1, 2, 1, 2, 0; the stage's input halo must be filled first */
+int wdg_rk4_stage(wdg_wave *wave, int stage, double dt);
+
 /* ---- exact quadrature (approx_quad = false), FP64 ---- */
 /* WaveEquation(mesh, basis, false) (source/WaveEquation.cpp:5-30: Div<false>, EdgeFlux<false>),
  * WaveBC(mesh, bc, basis, false) (:70-105) and MassMatrix<false>(mesh, basis)

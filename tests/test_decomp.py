@@ -1,0 +1,158 @@
+"""Domain decomposition plans on the CPU: every halo slot receives exactly the neighbour trace
+the undivided mesh's kernels would read, for contiguous and scattered partitions, in one
+process and over two gloo ranks exchanging real messages."""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+
+@pytest.fixture(scope="module")
+def W():
+    from wavedg_b200 import build
+
+    build.build()
+    import wavedg_b200
+
+    return wavedg_b200
+
+
+def _mesh(W, nx=9, seed=3):
+    from wavedg_b200 import meshgen as mg
+
+    v, q = mg.perturbed_rect(nx, 0.2, seed=seed)
+    v, q = mg.scrambled(v, q, seed=seed + 1)
+    m = W.Mesh2D.from_vertices(v, q)
+    bc = np.random.default_rng(seed).integers(0, 3, size=m.n_edges(1)).astype(np.int32)
+    return m, bc
+
+
+def _check_halos(plans, U, fb, fc, n):
+    """Build each rank's halo from the other ranks' send lists and compare with the trace the
+    partner table of the undivided mesh points at."""
+    nd = 3 * n * n
+    stride = {0: 3, 1: -3, 2: 3 * n, 3: -3 * n}
+    for r, p in plans.items():
+        halo = np.zeros(3 * n * len(p.halo_elem))
+        for s, (first, cnt) in p.recv.items():
+            idx = plans[s].send[r]
+            local = U[plans[s].local].ravel()
+            vals = np.stack([local[idx + f] for f in range(3)], axis=1).ravel()
+            assert len(vals) == 3 * n * cnt
+            halo[3 * n * first: 3 * n * (first + cnt)] = vals
+        for j, (le, f) in enumerate(zip(p.halo_elem, p.halo_side)):
+            g = p.local[le]
+            code = (int(fc[g]) >> (8 * int(f))) & 3
+            for k in range(n):
+                off = fb[g, f] + k * stride[code]
+                np.testing.assert_array_equal(halo[3 * n * j + 3 * k: 3 * n * j + 3 * k + 3], U.ravel()[off: off + 3])
+        assert (p.local >= 0).all()
+    covered = np.sort(np.concatenate([p.local for p in plans.values()]))
+    np.testing.assert_array_equal(covered, np.arange(len(U)))
+
+
+@pytest.mark.parametrize("world,kind", [(2, "blocks"), (3, "blocks"), (4, "random")])
+def test_plans_deliver_the_partner_traces(W, world, kind):
+    from wavedg_b200 import decomp
+
+    m, bc = _mesh(W)
+    n = 4
+    nel = m.n_elem()
+    part = decomp.partition(nel, world) if kind == "blocks" else \
+        np.random.default_rng(7).integers(0, world, size=nel).astype(np.int32)
+    plans = {r: decomp.Plan(m, n, bc, part, r) for r in range(world)}
+    fb, fc = decomp.partner_table(m, n, bc)
+    U = np.random.default_rng(1).standard_normal((nel, 3 * n * n))
+    _check_halos(plans, U, fb, fc, n)
+    # every cut side is a halo slot on exactly one rank
+    assert sum(len(p.halo_elem) for p in plans.values()) == sum(len(v) for p in plans.values() for v in p.send.values()) // n
+
+
+def test_local_boundary_codes(W):
+    """Physical boundary sides keep their codes; cut sides become boundary sides of the local mesh."""
+    from wavedg_b200 import decomp
+
+    m, bc = _mesh(W)
+    part = decomp.partition(m.n_elem(), 3)
+    p = decomp.Plan(m, 3, bc, part, 1)
+    lm = W.Mesh2D.from_vertices(p.verts, p.quads)
+    codes = p.local_bc(lm)
+    e = lm.edges(1)
+    n_cut = len(p.halo_elem)
+    assert len(codes) == len(e)
+    phys = p._boundary[p.local[e[:, 0]], e[:, 1]]
+    assert (~phys).sum() == n_cut
+    # a halo side is a boundary side of the local mesh that is not a physical boundary side
+    cut_sides = {(int(a), int(b)) for a, b in zip(p.halo_elem, p.halo_side)}
+    assert cut_sides == {(int(a), int(b)) for (a, b), ph in zip(e[:, :2], phys) if not ph}
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _worker(rank, world, port, q):
+    import torch
+    import torch.distributed as dist
+
+    from wavedg_b200 import decomp
+
+    import wavedg_b200 as W
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        m, bc = _mesh(W)
+        n = 4
+        part = decomp.partition(m.n_elem(), world)
+        p = decomp.Plan(m, n, bc, part, rank)
+        U = np.random.default_rng(1).standard_normal((m.n_elem(), 3 * n * n))
+        local = torch.from_numpy(U[p.local].ravel().copy())
+        halo = torch.zeros(3 * n * len(p.halo_elem), dtype=torch.float64)
+        ops = []
+        for r in sorted(p.send):
+            idx = torch.from_numpy(p.send[r].astype(np.int64))
+            buf = torch.stack([local[idx + f] for f in range(3)], dim=1).reshape(-1).contiguous()
+            ops.append(dist.P2POp(dist.isend, buf, r))
+        recv = {s: torch.zeros(3 * n * cnt, dtype=torch.float64) for s, (_, cnt) in p.recv.items()}
+        for s in sorted(p.recv):
+            ops.append(dist.P2POp(dist.irecv, recv[s], s))
+        for req in dist.batch_isend_irecv(ops):
+            req.wait()
+        for s, (first, cnt) in p.recv.items():
+            halo[3 * n * first: 3 * n * (first + cnt)] = recv[s]
+        fb, fc = decomp.partner_table(m, n, bc)
+        stride = {0: 3, 1: -3, 2: 3 * n, 3: -3 * n}
+        bad = 0
+        for j, (le, f) in enumerate(zip(p.halo_elem, p.halo_side)):
+            g = p.local[le]
+            code = (int(fc[g]) >> (8 * int(f))) & 3
+            for k in range(n):
+                off = fb[g, f] + k * stride[code]
+                bad += int(not np.array_equal(halo[3 * n * j + 3 * k: 3 * n * j + 3 * k + 3].numpy(), U.ravel()[off: off + 3]))
+        q.put((rank, len(p.halo_elem), bad))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_exchange_halos(W):
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    res = [q.get(timeout=180) for _ in procs]
+    for pr in procs:
+        pr.join(timeout=60)
+        assert pr.exitcode == 0
+    for rank, nhalo, bad in res:
+        assert nhalo > 0 and bad == 0, (rank, nhalo, bad)

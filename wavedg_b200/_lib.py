@@ -59,6 +59,12 @@ SIGNATURES = {
     "wdg_waveq_rhs": ([_v, _v, _v, _v, _d], _i),
     "wdg_waveq_rk4_steps": ([_v, _v, _d, _v, _i], _i),
     "wdg_waveholtz_create_exact": ([_v, _d, _vp], _i),
+    "wdg_mesh_partner_table": ([_v, _i, _v, _v, _v], _i),
+    "wdg_wave_create_halo": ([_v, _i, _v, _i, _i, _i, _v, _v, _vp], _i),
+    "wdg_halo_info": ([_v, _v, _v], _i),
+    "wdg_halo_gather": ([_v, _i, _v, _i, _v], _i),
+    "wdg_halo_put": ([_v, _i, _ll, _v, _ll], _i),
+    "wdg_rk4_stage": ([_v, _i, _d], _i),
     "wdg_write_raw": ([C.c_char_p, _ll, _v], _i),
     "wdg_read_raw": ([C.c_char_p, _ll, _v], _i),
     "wdg_mesh_from_tables": ([_i, _v, _i, _v, _i, _v, _vp], _i),

@@ -422,7 +422,7 @@ namespace wdg
                 const int off = base + kk * stride;
                 if (off >= lo && off < hi)
                     continue; // read from the staged tile instead
-                if (off < 0 || off + 3 > a.nel * ND)
+                if (off < 0 || off + 3 > (a.nread > 0 ? a.nread : a.nel * ND))
                 {
                     atomicOr(a.err, 2u);
                     continue;
@@ -874,7 +874,7 @@ namespace wdg
                     continue;
                 const int off = ((f == 0) ? fb.x : (f == 1) ? fb.y : (f == 2) ? fb.z : fb.w) +
                                 fck[p][s] * partner_stride<N>(byte);
-                if (off < 0 || off + 3 > a.nel * 3 * NN)
+                if (off < 0 || off + 3 > (a.nread > 0 ? a.nread : a.nel * 3 * NN))
                 {
                     atomicOr(a.err, 2u);
                     fbyte[p][s] = 0x40u; // skip this face

@@ -47,6 +47,8 @@ namespace wdg
         Real rk_a, rk_b, dt, fscale;
         double acc_c;
         unsigned *err;        // device error word (bit 0: wait timeout, bit 1: bad neighbour index)
+        int nread;            // values of u neighbour traces may come from (0: nel * 3 n^2; a domain
+                              // of a decomposed mesh appends its halo traces after its elements)
     };
 
     struct Geometry

@@ -141,6 +141,7 @@ namespace wdg
         const uint32_t *fcode;
         unsigned *err;
         int nel, el0, ne, chunk, flags;
+        int nread; // readable values of u for neighbour traces (0: nel * 3 n^2)
         Real rk_a, rk_b, dt, fscale;
         double acc_c;
         // batched WaveHoltz, last stage of a period: 1 = fixed-point update W <- filter,
@@ -237,7 +238,7 @@ namespace wdg
         if (c.flags & F_INT)
         {
             Real *halo = reinterpret_cast<Real *>(base + o.hb);
-            const int limit = c.nel * ND;
+            const int limit = c.nread > 0 ? c.nread : c.nel * ND;
             constexpr int B = 4; // (element, side) pairs per lane per batch
             for (int p0 = 0; p0 < ne * 4; p0 += 32 * B)
             {
@@ -599,6 +600,7 @@ namespace wdg
         c.fcode = a.fcode;
         c.err = a.err;
         c.nel = a.nel;
+        c.nread = a.nread;
         c.chunk = C;
         c.flags = a.flags;
         c.rk_a = a.rk_a;

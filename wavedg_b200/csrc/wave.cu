@@ -64,7 +64,7 @@ namespace wdg
         for (int k = 0; k < 3; ++k)
             if (!w->d_state[k])
             {
-                cudaError_t e = cudaMalloc(&w->d_state[k], w->real_size() * (size_t)w->ndof + 64);
+                cudaError_t e = cudaMalloc(&w->d_state[k], w->real_size() * (size_t)(w->ndof + w->halo) + 64);
                 if (e != cudaSuccess)
                 {
                     w->d_state[k] = nullptr;
@@ -120,6 +120,7 @@ namespace wdg
         a.chunk = w->ws_chunk;
         a.ring = w->ws_ring;
         a.err = w->d_err;
+        a.nread = w->halo ? (int)(w->ndof + w->halo) : 0;
         return a;
     }
 
@@ -172,6 +173,33 @@ namespace wdg
     }
     template int rk4_run<double>(wdg_wave *, double *, double, double &, int, const RKExtras &);
     template int rk4_run<float>(wdg_wave *, float *, double, double &, int, const RKExtras &);
+
+    // stage st (0..4) of one RK4 step on the resident buffers, the rotation of rk4_run:
+    // reads A, B, C, B, C and writes B, C, B, C, A (A = the resident state)
+    template <typename Real>
+    int rk4_stage(wdg_wave *w, int st, double dt)
+    {
+        WDG_TRY(ensure_states(w));
+        Real *buf[3] = {static_cast<Real *>(w->d_state[0]), static_cast<Real *>(w->d_state[1]),
+                        static_cast<Real *>(w->d_state[2])};
+        static const int src_of[5] = {0, 1, 2, 1, 2}, dst_of[5] = {1, 2, 1, 2, 0};
+        StageArgs<Real> a = base_args<Real>(w);
+        a.du = static_cast<Real *>(w->d_du);
+        a.dt = (Real)dt;
+        a.u = buf[src_of[st]];
+        a.out = buf[dst_of[st]];
+        a.flags = F_ALL | (st > 0 ? F_READ_DU : 0);
+        a.rk_a = (Real)rk4a[st];
+        a.rk_b = (Real)rk4b[st];
+        a.use_tma = aligned16(a.u) ? 1 : 0;
+        a.tma_out = aligned16(a.out) ? 1 : 0;
+        cudaError_t e = launch_stage<Real>(w->n, true, a, w->max_ctas, w->stream);
+        if (e != cudaSuccess)
+            return cuda_fail(e, "stage kernel launch");
+        return WDG_OK;
+    }
+    template int rk4_stage<double>(wdg_wave *, int, double);
+    template int rk4_stage<float>(wdg_wave *, int, double);
 } // namespace wdg
 
 namespace

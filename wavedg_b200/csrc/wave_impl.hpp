@@ -16,6 +16,8 @@ struct wdg_wave
     int family = 0; // fused-kernel family: 0 warp-per-element, 1 tiled TMA pipeline, 2 warp-specialised
     int ws_chunk = 0, ws_ring = wdg::kWsDefaultRing; // family 2 launch shape
     long long ndof = 0;
+    long long halo = 0; // values of neighbour traces appended after the elements in each state
+                        // buffer (a domain of a decomposed mesh; 0 otherwise)
     int nI = 0, nB = 0;
     double min_h = 0.0;
 
@@ -66,6 +68,8 @@ namespace wdg
     };
     template <typename Real>
     int rk4_run(wdg_wave *w, Real *A, double dt, double &t, int nsteps, const RKExtras &x);
+    template <typename Real>
+    int rk4_stage(wdg_wave *w, int st, double dt);
 
     extern const double rk4a[5], rk4b[5], rk4c[5];
 

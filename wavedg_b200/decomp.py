@@ -1,0 +1,255 @@
+"""Domain decomposition of one mesh across ranks (one GPU per rank), RK4 stepping.
+
+The reference distributes a mesh with MPI (Mesh2D::distribute, source/Mesh2D.cpp:384-592)
+and exchanges the face traces of cut edges before each operator application
+(FaceVector::send_recv, source/FEMVector.cpp:153-216).  Here each rank holds a discretisation
+of its own elements (wdg_wave_create_halo) whose state buffers end in a halo: one n x 3 trace
+per cut side, in the face-node order of that side.  Before every RK stage the ranks exchange
+the traces of the stage's input buffer (gather on the sender, one message per neighbouring
+rank, write into the receiver's halo); then the stage runs as on an undivided mesh, and every
+element's arithmetic is the same as there.
+
+The plan is computed from the global mesh and the element -> rank map on every rank, without
+communication, and both sides of each exchange derive the same slot order from it: the
+receiver's cut sides sorted by (sending rank, local element, side).
+
+    part = decomp.partition(mesh.n_elem(), world)
+    dom = decomp.Domain(mesh, basis, bc, part, rank)
+    dom.upload(u_global)
+    dom.rk4_steps(dt, nsteps, decomp.dist_exchange(dom))      # torch.distributed, NCCL
+    dom.download(u_global)                                     # this rank's elements only
+
+On one GPU, several Domains of the same mesh can step together (`step_all`: device copies
+between them), which is how the tests check the decomposed result against
+the undivided one.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import WdgError, check, lib
+
+_STAGE_BUFFER = (0, 1, 2, 1, 2)  # the input buffer of RK stage st (rk4 rotation)
+
+
+def partition(n_elem: int, world: int) -> np.ndarray:
+    """Element -> rank: contiguous blocks of element ids, sizes within one of each other."""
+    if world < 1:
+        raise ValueError("world size must be positive")
+    return (np.arange(n_elem, dtype=np.int64) * world // max(n_elem, 1)).astype(np.int32)
+
+
+def partner_table(mesh, n: int, bc=None):
+    """(fbase (nel, 4), fcode (nel,)) of the fused kernels for `mesh` (wdg_mesh_partner_table)."""
+    nel = mesh.n_elem()
+    fb = np.zeros(4 * nel, dtype=np.int32)
+    fc = np.zeros(nel, dtype=np.uint32)
+    codes = None if bc is None else np.ascontiguousarray(bc, dtype=np.int32)
+    check(lib().wdg_mesh_partner_table(mesh._h, int(n), None if codes is None else C.c_void_p(codes.ctypes.data),
+                                       C.c_void_p(fb.ctypes.data), C.c_void_p(fc.ctypes.data)), "partner_table")
+    return fb.reshape(nel, 4), fc
+
+
+class Plan:
+    """This rank's share of a decomposed mesh and its exchange lists (pure host arithmetic)."""
+
+    def __init__(self, mesh, n: int, bc, part, rank: int):
+        part = np.asarray(part, dtype=np.int32)
+        nel = mesh.n_elem()
+        if part.shape != (nel,):
+            raise ValueError("one rank per element")
+        self.n, self.rank, self.world = int(n), int(rank), int(part.max()) + 1
+        nd = 3 * n * n
+        self.nd = nd
+        fb, fc = partner_table(mesh, n, bc)
+        side = np.arange(4)
+        byte = (fc[:, None] >> (8 * side[None, :]).astype(np.uint32)) & 0xFF
+        boundary = (byte & 0x80) != 0
+        nb = np.where(boundary, -1, fb // nd)
+        cut = ~boundary & (part[np.maximum(nb, 0)] != part[:, None])
+        stride = np.array([3, -3, 3 * n, -3 * n])[(byte & 3).astype(np.int64)]
+        self.local = np.nonzero(part == rank)[0].astype(np.int64)
+        g2l = np.full(nel, -1, dtype=np.int64)
+        for r in range(self.world):
+            ids = np.nonzero(part == r)[0]
+            g2l[ids] = np.arange(len(ids))
+        k = np.arange(n)
+
+        def slots(r):
+            """Rank r's cut sides in slot order: (src rank, global element, side), sorted."""
+            el, f = np.nonzero(cut & (part[:, None] == r))
+            src = part[nb[el, f]]
+            order = np.lexsort((f, el, src))
+            return el[order], f[order], src[order]
+
+        # receive side: this rank's halo slots, grouped by the sending rank
+        el, f, src = slots(rank)
+        self.halo_elem = g2l[el].astype(np.int32)
+        self.halo_side = f.astype(np.int32)
+        self.recv = {}  # src rank -> (first slot, slot count)
+        for s in np.unique(src):
+            idx = np.nonzero(src == s)[0]
+            self.recv[int(s)] = (int(idx[0]), len(idx))
+        # send side: for every rank whose halo holds traces of this rank's elements, the node
+        # offsets (this rank's numbering) in that rank's slot order
+        self.send = {}
+        for r in range(self.world):
+            if r == rank:
+                continue
+            el, f, src = slots(r)
+            m = src == rank
+            if not m.any():
+                continue
+            el, f = el[m], f[m]
+            off = fb[el, f][:, None] + k[None, :] * stride[el, f][:, None]  # global node offsets
+            nbe = off // nd
+            local_off = off - nbe * nd + g2l[nbe] * nd
+            self.send[r] = local_off.reshape(-1).astype(np.int32)
+        # the local mesh: this rank's elements (global vertex numbering), boundary codes of the
+        # physical boundary, 0 on cut sides (overridden by the halo)
+        self.quads = mesh.quads[self.local]
+        self.verts = mesh.verts
+        self._byte = byte
+        self._boundary = boundary
+
+    def local_bc(self, local_mesh):
+        """Boundary codes of the local mesh's boundary edges (in its edge order)."""
+        e = local_mesh.edges(1)
+        g = self.local[e[:, 0]]
+        s = e[:, 1]
+        phys = self._boundary[g, s]
+        return np.where(phys, (self._byte[g, s] >> 3) & 3, 0).astype(np.int32)
+
+
+class Domain:
+    """One rank's discretisation with its halo (wdg_wave_create_halo)."""
+
+    def __init__(self, mesh, basis, bc, part, rank: int, precision="fp64", device: int = -1):
+        import torch
+
+        from . import dg
+
+        if mesh.verts is None:
+            raise WdgError(-1, "decomposition needs a mesh built from vertices")
+        n = dg._gll_n(basis)
+        self.plan = Plan(mesh, n, bc, part, rank)
+        self.rank, self.n = rank, n
+        self.mesh = dg.Mesh2D.from_vertices(self.plan.verts, self.plan.quads)
+        codes = self.plan.local_bc(self.mesh)
+        self.precision = dg._precision(precision)
+        h = C.c_void_p()
+        p = self.plan
+        check(lib().wdg_wave_create_halo(self.mesh._h, n, C.c_void_p(codes.ctypes.data), self.precision, device,
+                                         len(p.halo_elem), C.c_void_p(p.halo_elem.ctypes.data),
+                                         C.c_void_p(p.halo_side.ctypes.data), C.byref(h)), "wdg_wave_create_halo")
+        self._h = h
+        nd, hv = C.c_longlong(), C.c_longlong()
+        check(lib().wdg_halo_info(h, C.byref(nd), C.byref(hv)))
+        self.ndof, self.halo = nd.value, hv.value
+        self.torch = torch
+        self.dtype = torch.float32 if precision == "fp32" else torch.float64
+        dev = torch.device("cuda", torch.cuda.current_device() if device < 0 else device)
+        self.device = dev
+        self._send_idx = {r: torch.from_numpy(v).to(dev) for r, v in p.send.items()}
+        self._send_buf = {r: torch.empty(3 * len(v), dtype=self.dtype, device=dev) for r, v in p.send.items()}
+        self._recv_buf = {s: torch.empty(3 * n * cnt, dtype=self.dtype, device=dev) for s, (_, cnt) in p.recv.items()}
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                lib().wdg_wave_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    # ------------------------------------------------------------- state
+    def upload(self, u_global) -> None:
+        """The local elements' values of a global state (float64 numpy array)."""
+        loc = np.ascontiguousarray(np.asarray(u_global, dtype=np.float64).reshape(-1, self.plan.nd)[self.plan.local])
+        check(lib().wdg_state_upload(self._h, C.c_void_p(loc.ctypes.data)), "Domain.upload")
+
+    def download(self, u_global) -> None:
+        """Write the local elements' values into a global state (float64 numpy array)."""
+        loc = np.zeros((len(self.plan.local), self.plan.nd))
+        check(lib().wdg_state_download(self._h, C.c_void_p(loc.ctypes.data)), "Domain.download")
+        u_global.reshape(-1, self.plan.nd)[self.plan.local] = loc
+
+    # ------------------------------------------------------------- exchange pieces
+    def gather(self, stage: int, dst: int):
+        """The traces rank `dst` needs from the input buffer of RK stage `stage` (device tensor)."""
+        idx, out = self._send_idx[dst], self._send_buf[dst]
+        check(lib().wdg_halo_gather(self._h, _STAGE_BUFFER[stage], C.c_void_p(idx.data_ptr()), int(idx.numel()),
+                                    C.c_void_p(out.data_ptr())), "halo gather")
+        return out
+
+    def put(self, stage: int, src: int, values) -> None:
+        """Traces received from rank `src` into the halo of stage `stage`'s input buffer."""
+        first, cnt = self.plan.recv[src]
+        check(lib().wdg_halo_put(self._h, _STAGE_BUFFER[stage], 3 * self.n * first, C.c_void_p(values.data_ptr()),
+                                 3 * self.n * cnt), "halo put")
+
+    def stage(self, stage: int, dt: float) -> None:
+        check(lib().wdg_rk4_stage(self._h, int(stage), float(dt)), "rk4 stage")
+
+    def sync(self) -> None:
+        check(lib().wdg_wave_sync(self._h))
+
+    def rk4_steps(self, dt: float, nsteps: int, exchange) -> None:
+        """nsteps of ode::RungeKutta4::step; exchange(stage) fills the stage's input halo."""
+        for _ in range(nsteps):
+            for st in range(5):
+                exchange(st)
+                self.stage(st, dt)
+
+
+def local_exchange(domains):
+    """Exchange among Domains of one process (one GPU): device copies, in stream order."""
+
+    def run(stage):
+        # gathers on each sender's stream, then (after they finish) the receivers' copies on
+        # theirs; the gather buffers are reused next stage, so every copy ends before returning
+        for d in domains:
+            for r in d.plan.send:
+                d.gather(stage, r)
+            d.sync()
+        for d in domains:
+            for r in d.plan.send:
+                domains[r].put(stage, d.rank, d._send_buf[r])
+        for d in domains:
+            d.sync()
+
+    return run
+
+
+def step_all(domains, dt: float, nsteps: int) -> None:
+    """RK4 steps of Domains sharing one process: per stage, exchange then every domain's stage."""
+    ex = local_exchange(domains)
+    for _ in range(nsteps):
+        for st in range(5):
+            ex(st)
+            for d in domains:
+                d.stage(st, dt)
+
+
+def dist_exchange(domain, group=None):
+    """Exchange over torch.distributed (NCCL between GPUs): one send and one receive per
+    neighbouring rank per stage, posted together."""
+    import torch.distributed as dist
+
+    def run(stage):
+        ops = []
+        for r in sorted(domain.plan.send):
+            ops.append(dist.P2POp(dist.isend, domain.gather(stage, r), r, group))
+        for s in sorted(domain.plan.recv):
+            ops.append(dist.P2POp(dist.irecv, domain._recv_buf[s], s, group))
+        domain.sync()
+        if ops:
+            for req in dist.batch_isend_irecv(ops):
+                req.wait()
+        for s in sorted(domain.plan.recv):
+            domain.put(stage, s, domain._recv_buf[s])
+
+    return run
