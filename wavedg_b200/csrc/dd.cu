@@ -20,13 +20,20 @@ using namespace wdg;
 
 namespace
 {
+    // out[3 j + f] = u[idx[j] + f]; an index outside the elements' values is skipped and
+    // recorded in the handle's error word (bit 1, as a bad neighbour index)
     template <typename Real>
     __global__ void halo_gather_kernel(const Real *__restrict__ u, const int *__restrict__ idx, int count,
-                                       Real *__restrict__ out)
+                                       long long limit, unsigned *err, Real *__restrict__ out)
     {
         for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x)
         {
             const int o = idx[j];
+            if (o < 0 || o + 3 > limit)
+            {
+                atomicOr(err, 2u);
+                continue;
+            }
             out[3 * j] = u[o];
             out[3 * j + 1] = u[o + 1];
             out[3 * j + 2] = u[o + 2];
@@ -131,10 +138,11 @@ extern "C"
         const unsigned grid = (unsigned)std::min(148 * 8, (count + 255) / 256);
         if (w->precision == WDG_FP32)
             halo_gather_kernel<float><<<grid, 256, 0, w->stream>>>(static_cast<const float *>(w->d_state[buffer]), idx,
-                                                                   count, static_cast<float *>(out));
+                                                                   count, w->ndof, w->d_err, static_cast<float *>(out));
         else
             halo_gather_kernel<double><<<grid, 256, 0, w->stream>>>(static_cast<const double *>(w->d_state[buffer]),
-                                                                    idx, count, static_cast<double *>(out));
+                                                                    idx, count, w->ndof, w->d_err,
+                                                                    static_cast<double *>(out));
         WDG_CUDA(cudaGetLastError());
         return WDG_OK;
     }
