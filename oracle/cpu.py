@@ -54,6 +54,12 @@ _SIGS = {
     "rhs": ([_v, _dp, _dp], None),
     "rhs_forced": ([_v, _dp, _dp, _dp, _d], None),
     "rk4": ([_v, _d, _i, C.POINTER(C.c_double), _dp], None),
+    "opa_create": ([_v, _i, _i, _dp], _v),
+    "opa_destroy": ([_v], None),
+    "opa_action": ([_v, _dp, _dp], None),
+    "opa_bc_action": ([_v, _dp, _dp], None),
+    "opa_rhs": ([_v, _dp, _dp], None),
+    "opa_rk4": ([_v, _d, _i, C.POINTER(C.c_double), _dp], None),
     "opq_create": ([_v, _i, _ip], _v),
     "opq_destroy": ([_v], None),
     "opq_div": ([_v, _dp, _dp], None),
@@ -380,4 +386,38 @@ class OpQ:
         u = _f64(u).copy()
         tt = C.c_double(t)
         self.L.opq_rk4(self.h, dt, nsteps, C.byref(tt), u)
+        return u, tt.value
+
+
+class OpA:
+    """Advection<true> + AdvectionHomogeneousBC<true> + MassMatrix<true> for n_var variables with
+    constant coefficients a (n_var, n_var, 2) on the CPU checker."""
+
+    def __init__(self, mesh: Mesh, n: int, nv: int, a):
+        self.L, self.mesh, self.n, self.nv = mesh.L, mesh, n, nv
+        self.a = _f64(a).reshape(-1)
+        assert self.a.size == 2 * nv * nv
+        self.h = self.L.opa_create(mesh.h, n, nv, self.a)
+        self.ndof = nv * n * n * mesh.n_elem
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.opa_destroy(self.h)
+            self.h = None
+
+    def action(self, u, du):
+        self.L.opa_action(self.h, _f64(u), du)
+
+    def bc_action(self, u, du):
+        self.L.opa_bc_action(self.h, _f64(u), du)
+
+    def rhs(self, u):
+        du = np.zeros(self.ndof)
+        self.L.opa_rhs(self.h, _f64(u), du)
+        return du
+
+    def rk4(self, u, dt, nsteps, t=0.0):
+        u = _f64(u).copy()
+        tt = C.c_double(t)
+        self.L.opa_rk4(self.h, dt, nsteps, C.byref(tt), u)
         return u, tt.value

@@ -237,6 +237,34 @@ namespace
         }
     };
 
+    // Advection<true> and AdvectionHomogeneousBC<true> (wavedg/Advection.hpp) with constant
+    // coefficients a (n_var, n_var, 2), and MassMatrix<true>
+    struct RefOpA
+    {
+        const Mesh2D &mesh;
+        const QuadratureRule *basis;
+        const int nv, ndof;
+        std::vector<double> a;
+        Advection<true> adv;
+        AdvectionHomogeneousBC<true> bc;
+        MassMatrix<true> m;
+
+        RefOpA(const Mesh2D &mesh_, int n_colloc, int nv_, const double *a_)
+            : mesh(mesh_), basis(QuadratureRule::quadrature_rule(n_colloc, QuadratureRule::GaussLobatto)), nv(nv_),
+              ndof(nv_ * n_colloc * n_colloc * mesh_.n_elem()), a(a_, a_ + 2 * nv_ * nv_),
+              adv(nv_, mesh_, basis, a.data(), true), bc(nv_, mesh_, basis, a.data(), true), m(mesh_, basis)
+        {
+        }
+        void rhs(const double *u, double *du) const
+        {
+            for (int i = 0; i < ndof; ++i)
+                du[i] = 0.0;
+            adv.action(u, du);
+            bc.action(u, du);
+            m.inv(nv, du);
+        }
+    };
+
     // WaveHoltz restated over RefOp so that the composed boundary operator can
     // be used (the reference class hard-wires WaveBC).  Loop structure, time
     // accumulation and filter weights follow source/WaveHoltz.cpp:5-145; with
@@ -466,6 +494,24 @@ extern "C"
         ode::RungeKutta4 rk(op->ndof);
         auto f = [op](double *dudt, const double, const double *v)
         { op->rhs(v, dudt, nullptr, 0.0); };
+        for (int s = 0; s < nsteps; ++s)
+            rk.step(dt, f, *t, u);
+    }
+
+    // ---- Advection<true> ----
+    void *ref_opa_create(void *m, int n_colloc, int nv, const double *a)
+    {
+        return new RefOpA(static_cast<RefMesh *>(m)->mesh, n_colloc, nv, a);
+    }
+    void ref_opa_destroy(void *o) { delete static_cast<RefOpA *>(o); }
+    void ref_opa_action(void *o, const double *u, double *du) { static_cast<RefOpA *>(o)->adv.action(u, du); }
+    void ref_opa_bc_action(void *o, const double *u, double *du) { static_cast<RefOpA *>(o)->bc.action(u, du); }
+    void ref_opa_rhs(void *o, const double *u, double *du) { static_cast<RefOpA *>(o)->rhs(u, du); }
+    void ref_opa_rk4(void *o, double dt, int nsteps, double *t, double *u)
+    {
+        RefOpA *op = static_cast<RefOpA *>(o);
+        ode::RungeKutta4 rk(op->ndof);
+        auto f = [op](double *dudt, const double, const double *v) { op->rhs(v, dudt); };
         for (int s = 0; s < nsteps; ++s)
             rk.step(dt, f, *t, u);
     }

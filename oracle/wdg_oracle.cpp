@@ -640,6 +640,206 @@ namespace
         t += dt;
     }
 
+    // cyclic Jacobi eigen-decomposition of a symmetric m x m matrix (column-major), m <= 8:
+    // A = R diag(e) R^T (the symmetric case of real_eig, eig.cpp:29-73)
+    void sym_eig(int m, const double *A_, double *R, double *e)
+    {
+        double A[64];
+        std::memcpy(A, A_, sizeof(double) * m * m);
+        for (int i = 0; i < m * m; ++i)
+            R[i] = (i % (m + 1) == 0) ? 1.0 : 0.0;
+        for (int sweep = 0; sweep < 100; ++sweep)
+        {
+            double off = 0.0;
+            for (int p = 0; p < m; ++p)
+                for (int q = p + 1; q < m; ++q)
+                    off += A[p + m * q] * A[p + m * q];
+            if (off < 1e-300)
+                break;
+            for (int p = 0; p < m; ++p)
+                for (int q = p + 1; q < m; ++q)
+                {
+                    const double apq = A[p + m * q];
+                    if (apq == 0.0)
+                        continue;
+                    const double theta = (A[q + m * q] - A[p + m * p]) / (2.0 * apq);
+                    const double t = (theta >= 0 ? 1.0 : -1.0) / (std::abs(theta) + std::sqrt(theta * theta + 1.0));
+                    const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+                    for (int k = 0; k < m; ++k)
+                    {
+                        const double akp = A[k + m * p], akq = A[k + m * q];
+                        A[k + m * p] = c * akp - sn * akq;
+                        A[k + m * q] = sn * akp + c * akq;
+                    }
+                    for (int k = 0; k < m; ++k)
+                    {
+                        const double apk = A[p + m * k], aqk = A[q + m * k];
+                        A[p + m * k] = c * apk - sn * aqk;
+                        A[q + m * k] = sn * apk + c * aqk;
+                    }
+                    for (int k = 0; k < m; ++k)
+                    {
+                        const double rkp = R[k + m * p], rkq = R[k + m * q];
+                        R[k + m * p] = c * rkp - sn * rkq;
+                        R[k + m * q] = sn * rkp + c * rkq;
+                    }
+                }
+        }
+        for (int i = 0; i < m; ++i)
+            e[i] = A[i + m * i];
+    }
+
+    // Advection<true> with constant coefficients (wavedg/Advection.hpp:17-142: Div<true> and
+    // EdgeFlux<true> with a = -1, b = -1/2 for any n_var) and AdvectionHomogeneousBC<true>
+    // (:144-273: u = 0 outside), for symmetric coefficient matrices A_0, A_1 (n_var x n_var,
+    // a(d, c, k) = a[d + nv (c + nv k)]); the Lobatto prolongation and mass of Op.
+    struct OpA
+    {
+        const Op base;
+        const Mesh &m;
+        int n, nv, nel, ndof;
+        vec a, FI, FB; // coefficients; flux tables (n, nv, nv, 2, edges), times w_i |E|/2
+
+        OpA(const Mesh &m_, int n_, int nv_, const double *a_)
+            : base(m_, n_, std::vector<int>(m_.boundary.size(), 0).data()), m(m_), n(n_), nv(nv_), nel(m_.nel),
+              ndof(nv_ * n_ * n_ * m_.nel), a(a_, a_ + 2 * nv_ * nv_)
+        {
+            flux_table(m.interior, FI);
+            flux_table(m.boundary, FB);
+        }
+
+        void flux_table(const std::vector<int> &list, vec &F) const
+        {
+            const int N = (int)list.size(), v2 = nv * nv;
+            F.resize((size_t)n * v2 * 2 * N);
+            for (int e = 0; e < N; ++e)
+            {
+                const Edge &E = m.edges[list[e]];
+                double nA[64], R[64], ev[8];
+                for (int d = 0; d < v2; ++d)
+                    nA[d] = E.n[0] * a[d] + E.n[1] * a[d + v2];
+                sym_eig(nv, nA, R, ev);
+                for (int s = 0; s < 2; ++s)
+                {
+                    const double sgn = (s == 0) ? 1.0 : -1.0;
+                    for (int c = 0; c < nv; ++c)
+                        for (int d = 0; d < nv; ++d)
+                        {
+                            double acc = 0.0;
+                            for (int k = 0; k < nv; ++k)
+                                acc += R[c + nv * k] * (-0.5 * ev[k] + sgn * -0.5 * std::abs(ev[k])) * R[d + nv * k];
+                            for (int i = 0; i < n; ++i)
+                                F[i + n * (c + nv * (d + nv * (s + 2 * (size_t)e)))] = base.w[i] * E.meas * acc;
+                        }
+                }
+            }
+        }
+        // div_2d_c with the op table of op_2d_cc (Div.cpp:5-53, 131-179): du += D^T F + D^T G
+        void div(const double *u, double *du) const
+        {
+            const int nn = n * n, v2 = nv * nv;
+            vec Fx((size_t)nv * nn), Gy((size_t)nv * nn);
+            for (int el = 0; el < nel; ++el)
+            {
+                const double *ue = u + (size_t)nv * nn * el;
+                for (int i = 0; i < nn; ++i)
+                {
+                    double J[4];
+                    jacobian(&m.corners[8 * (size_t)el], base.x[i % n], base.x[i / n], J);
+                    const double W = base.w[i / n] * base.w[i % n];
+                    const double Ye = J[3] * W, Xe = J[2] * W, Yx = J[1] * W, Xx = J[0] * W;
+                    for (int d = 0; d < nv; ++d)
+                    {
+                        double f = 0.0, g = 0.0;
+                        for (int c = 0; c < nv; ++c)
+                        {
+                            const double a0 = a[d + nv * c], a1 = a[d + nv * c + v2];
+                            f += (Ye * a0 - Xe * a1) * ue[c + nv * i];
+                            g += (-Yx * a0 + Xx * a1) * ue[c + nv * i];
+                        }
+                        Fx[d + nv * i] = f;
+                        Gy[d + nv * i] = g;
+                    }
+                }
+                for (int j = 0; j < n; ++j)
+                    for (int i = 0; i < n; ++i)
+                        for (int d = 0; d < nv; ++d)
+                        {
+                            double sum = 0.0;
+                            for (int l = 0; l < n; ++l)
+                                sum += base.D[l + n * i] * Fx[d + nv * (l + n * j)] + base.D[l + n * j] * Gy[d + nv * (i + n * l)];
+                            du[d + nv * (i + n * (j + (size_t)n * el))] += sum;
+                        }
+            }
+        }
+        void prolong(bool interior, const double *u, double *uf) const
+        {
+            const auto &v2e = interior ? base.v2eI : base.v2eB;
+            const int N = (int)(interior ? m.interior.size() : m.boundary.size());
+            std::fill(uf, uf + (size_t)n * nv * 2 * N, 0.0);
+            for (int e = 0; e < N; ++e)
+                for (int s = 0; s < (interior ? 2 : 1); ++s)
+                    for (int i = 0; i < n; ++i)
+                        for (int d = 0; d < nv; ++d)
+                            uf[i + n * (d + nv * (s + 2 * (size_t)e))] = u[d + nv * (size_t)v2e[i + n * (s + 2 * (size_t)e)]];
+        }
+        void prolong_t(bool interior, const double *uf, double *u) const
+        {
+            const auto &v2e = interior ? base.v2eI : base.v2eB;
+            const int N = (int)(interior ? m.interior.size() : m.boundary.size());
+            for (int e = 0; e < N; ++e)
+                for (int s = 0; s < (interior ? 2 : 1); ++s)
+                    for (int i = 0; i < n; ++i)
+                        for (int d = 0; d < nv; ++d)
+                            u[d + nv * (size_t)v2e[i + n * (s + 2 * (size_t)e)]] += uf[i + n * (d + nv * (s + 2 * (size_t)e))];
+        }
+        // flux_action_2d_c (EdgeFlux.cpp:289-325) for nv variables
+        void flux(bool interior, const double *ub, double *fb) const
+        {
+            const auto &F = interior ? FI : FB;
+            const int N = (int)(interior ? m.interior.size() : m.boundary.size());
+            vec uf((size_t)n * nv);
+            for (int e = 0; e < N; ++e)
+            {
+                std::fill(uf.begin(), uf.end(), 0.0);
+                for (int s = 0; s < 2; ++s)
+                    for (int d = 0; d < nv; ++d)
+                        for (int c = 0; c < nv; ++c)
+                            for (int i = 0; i < n; ++i)
+                                uf[i + n * d] += F[i + n * (c + nv * (d + nv * (s + 2 * (size_t)e)))] *
+                                                 ub[i + n * (c + nv * (s + 2 * (size_t)e))];
+                for (int d = 0; d < nv; ++d)
+                    for (int i = 0; i < n; ++i)
+                    {
+                        fb[i + n * (d + nv * (0 + 2 * (size_t)e))] = uf[i + n * d];
+                        fb[i + n * (d + nv * (1 + 2 * (size_t)e))] = -uf[i + n * d];
+                    }
+            }
+        }
+        void action(const double *u, double *du) const
+        {
+            div(u, du);
+            vec uf((size_t)n * nv * 2 * m.interior.size());
+            prolong(true, u, uf.data());
+            flux(true, uf.data(), uf.data());
+            prolong_t(true, uf.data(), du);
+        }
+        void bc_action(const double *u, double *du) const
+        {
+            vec uB((size_t)n * nv * 2 * m.boundary.size());
+            prolong(false, u, uB.data()); // side 1 stays 0: u = 0 outside
+            flux(false, uB.data(), uB.data());
+            prolong_t(false, uB.data(), du);
+        }
+        void rhs(const double *u, double *du) const
+        {
+            std::fill(du, du + ndof, 0.0);
+            action(u, du);
+            bc_action(u, du);
+            base.mass_inv(nv, du);
+        }
+    };
+
     // D(i, j) = phi_j'(xq_i) at points off (or on) the nodes: lagrange_basis_deriv with the
     // two branches of lagrange_derivative (lagrange_interpolation.cpp:33-50, 96-139)
     void deriv_at(int n, const double *x, int nq, const double *xq, double *D)
@@ -1217,6 +1417,19 @@ extern "C"
     double orc_norm(int nd, const double *x) { return norm2(nd, x); }
     double orc_error(int nd, const double *x, const double *y) { return err2(nd, x, y); }
 
+    void *orc_opa_create(void *m, int n, int nv, const double *a) { return new OpA(*static_cast<Mesh *>(m), n, nv, a); }
+    void orc_opa_destroy(void *o) { delete static_cast<OpA *>(o); }
+    void orc_opa_action(void *o, const double *u, double *du) { static_cast<OpA *>(o)->action(u, du); }
+    void orc_opa_bc_action(void *o, const double *u, double *du) { static_cast<OpA *>(o)->bc_action(u, du); }
+    void orc_opa_rhs(void *o, const double *u, double *du) { static_cast<OpA *>(o)->rhs(u, du); }
+    void orc_opa_rk4(void *o, double dt, int nsteps, double *t, double *u)
+    {
+        OpA *op = static_cast<OpA *>(o);
+        vec p(op->ndof), du(op->ndof);
+        auto f = [op](double *dudt, double, const double *v) { op->rhs(v, dudt); };
+        for (int s = 0; s < nsteps; ++s)
+            rk4_step(op->ndof, dt, f, *t, u, p, du);
+    }
     void *orc_opq_create(void *m, int n, const int *bc) { return new OpQ(*static_cast<Mesh *>(m), n, bc); }
     void orc_opq_destroy(void *o) { delete static_cast<OpQ *>(o); }
     void orc_opq_div(void *o, const double *u, double *du) { static_cast<OpQ *>(o)->div(u, du); }

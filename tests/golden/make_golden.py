@@ -1,7 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the reference library.
 
     make -C oracle ref          # compiles the reference (needs its sources)
-    python tests/golden/make_golden.py [--exact-quadrature-only]
+    python tests/golden/make_golden.py [--exact-quadrature-only | --advection-only]
 
 Every output array is produced by the reference waveDG code compiled from its
 own sources (oracle/_ref/libwdgref.so, driven through oracle/ref_harness.cpp).
@@ -147,6 +147,31 @@ def waveholtz_exact():
                         pi0=p, S_pi0=wh.S(p), W=W, iters=it, err=err)
 
 
+def advection_fixture(name, v, q, m, n, nv, seed):
+    """Advection<true> + AdvectionHomogeneousBC<true> with constant symmetric coefficients
+    (n_var = 1: a velocity; n_var > 1: random symmetric A_0, A_1), MassMatrix<true>, RHS, RK4."""
+    rng = np.random.default_rng(seed)
+    if nv == 1:
+        a = np.array([0.7, -0.4])
+    else:
+        A = rng.standard_normal((2, nv, nv))
+        A = A + A.transpose(0, 2, 1)
+        a = np.concatenate([A[0].reshape(-1, order="F"), A[1].reshape(-1, order="F")])  # a(d, c, k)
+    op = cpu.OpA(m, n, nv, a)
+    u = rng.standard_normal(op.ndof)
+    out = dict(verts=v, quads=q, n=n, nv=nv, a=a, u=u)
+    for nm in ("action", "bc_action"):
+        r = rng.standard_normal(op.ndof)
+        out[f"{nm}_in"] = r.copy()
+        getattr(op, nm)(u, r)
+        out[nm] = r
+    out["rhs"] = op.rhs(u)
+    dt = 0.1 * m.min_h() / n ** 2
+    out["dt"] = dt
+    out["rk4_5"], _ = op.rk4(u, dt, 5)
+    np.savez_compressed(os.path.join(HERE, f"adv_{name}_n{n}_v{nv}.npz"), **out)
+
+
 def opq_fixture(name, v, q, m, n, seed):
     """approx_quad = false: Div<false>, EdgeFlux<false> (interior and boundary), WaveEquation,
     the composed boundary operator over EdgeFlux<false>, MassMatrix<false>, RHS, 5 RK4 steps."""
@@ -179,6 +204,13 @@ def main():
     if not cpu.available("reference"):
         raise SystemExit("build the reference first: make -C oracle ref")
     qcases = {"scrambled6": [3, 5], "lshape3": [4]}
+    acases = {"scrambled6": [(5, 1), (4, 2)], "lshape3": [(3, 4)]}
+    if "--advection-only" in sys.argv:
+        for seed, (name, v, q) in enumerate(meshes()):
+            for n, nv in acases.get(name, []):
+                advection_fixture(name, v, q, cpu.Mesh(v, q, KIND), n, nv, 2000 + 100 * seed + 10 * n + nv)
+        print("advection fixtures written to", HERE)
+        return
     if "--exact-quadrature-only" in sys.argv:
         for seed, (name, v, q) in enumerate(meshes()):
             for n in qcases.get(name, []):
@@ -198,6 +230,8 @@ def main():
             op_fixture(name, v, q, m, n, 100 * seed + n)
         for n in qcases.get(name, []):
             opq_fixture(name, v, q, m, n, 1000 + 100 * seed + n)
+        for n, nv in acases.get(name, []):
+            advection_fixture(name, v, q, m, n, nv, 2000 + 100 * seed + 10 * n + nv)
     config1()
     waveholtz()
     waveholtz_exact()

@@ -89,6 +89,22 @@ def test_exact_quadrature_operators(fname):
     assert rel(un, g["rk4_5"]) < TOL
 
 
+@pytest.mark.parametrize("fname", golden_files("adv_"))
+def test_advection_operators(fname):
+    """Advection<true> and AdvectionHomogeneousBC<true> (constant coefficients, any n_var)."""
+    g = golden(fname)
+    m = cpu.Mesh(g["verts"], g["quads"], "oracle")
+    op = cpu.OpA(m, int(g["n"]), int(g["nv"]), g["a"])
+    u = g["u"]
+    for nm in ("action", "bc_action"):
+        r = g[f"{nm}_in"].copy()
+        getattr(op, nm)(u, r)
+        assert rel(r, g[nm]) < TOL, nm
+    assert rel(op.rhs(u), g["rhs"]) < TOL
+    un, _ = op.rk4(u, float(g["dt"]), 5)
+    assert rel(un, g["rk4_5"]) < TOL
+
+
 def test_config1_trajectory():
     g = golden("config1_32x32_P3.npz")
     m = cpu.Mesh(g["verts"], g["quads"], "oracle")
