@@ -265,6 +265,7 @@ def run_ours(args, rank, world, local_rank):
         extra["waveholtz_batched"] = waveholtz_batched(local_rank)
     if not args.no_extras and args.precision == "fp64" and world == 1:
         extra["exact_quadrature"] = exact_quadrature(local_rank, cpu_leg=not args.no_cpu_baseline)
+        extra["advection"] = advection(local_rank, cpu_leg=not args.no_cpu_baseline)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -464,6 +465,49 @@ def exact_quadrature(device: int, n_el: int = 128, P: int = 4, reps: int = 20, c
             op.rhs(uh)
             out["cpu_reference_ms_per_rhs"] = (time.perf_counter() - t0) * 1e3
             out["cpu_reference"] = "the reference's WaveEquation / WaveBC / MassMatrix<false>, 1 thread, set-up excluded"
+    return out
+
+
+def advection(device: int, n_el: int = 256, P: int = 4, nv: int = 2, reps: int = 20, cpu_leg: bool = True) -> dict:
+    """Linear advection with constant symmetric coefficients (Advection<true>,
+    AdvectionHomogeneousBC<true>, MassMatrix<true>), n_var = 2: time of one RHS on the GPU
+    (device arrays, CUDA events over `reps` calls) on a perturbed n_el x n_el mesh; beside it
+    the reference's own CPU RHS on the same mesh (1 thread), when present."""
+    import torch
+
+    import wavedg_b200 as W
+    from wavedg_b200 import meshgen as mg
+
+    v, q = mg.perturbed_rect(n_el, 0.2, seed=1)
+    mesh = W.Mesh2D.from_vertices(v, q)
+    basis = W.QuadratureRule.quadrature_rule(P + 1, W.QuadratureRule.GaussLobatto)
+    a = np.array([1.0, 0.5, 0.5, -0.3, 0.2, 0.0, 0.0, 0.8])  # symmetric A_0, A_1 (a(d, c, k))
+    s = W.AdvectionSystem(nv, mesh, basis, a, device=device)
+    u = torch.from_numpy(np.random.default_rng(2).standard_normal(s.ndof)).cuda()
+    du = torch.empty_like(u)
+    for _ in range(3):
+        s.rhs(u, du)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        s.rhs(u, du)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    out = {"workload": f"rhs_advection_nvar{nv}_{n_el}x{n_el}_P{P}_perturbed", "values": s.ndof,
+           "ms_per_rhs": ms, "values_per_s": s.ndof / (ms / 1e3),
+           # algorithmic bytes: u in, dudt out (the corners and edge tables are small)
+           "achieved_gbs": 16 * s.ndof / (ms / 1e3) / 1e9}
+    if cpu_leg:
+        kind, cpu = _ref_lib()
+        if kind == "reference":
+            op = cpu.OpA(cpu.Mesh(v, q, "reference"), P + 1, nv, a)
+            uh = u.cpu().numpy()
+            t0 = time.perf_counter()
+            op.rhs(uh)
+            out["cpu_reference_ms_per_rhs"] = (time.perf_counter() - t0) * 1e3
+            out["cpu_reference"] = "the reference's Advection / AdvectionHomogeneousBC / MassMatrix<true>, 1 thread"
     return out
 
 

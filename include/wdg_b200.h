@@ -155,6 +155,20 @@ int wdg_rhs(wdg_wave *wave, const double *u, double *dudt, const double *F, doub
  * t advances by dt per step.  One fused kernel per RK stage. */
 int wdg_rk4_steps(wdg_wave *wave, double *u, double dt, double *t, int nsteps);
 
+/* ---- linear advection, constant coefficients (the generic conservation-law path) ---- */
+/* Advection<true>(n_var, mesh, basis, a, true) (wavedg/Advection.hpp:17-142),
+ * AdvectionHomogeneousBC<true> (:144-273, u = 0 outside) and MassMatrix<true> for n_var <= 8
+ * variables; a = (A_0, A_1) with a(d, c, k) = a[d + n_var (c + n_var k)], both symmetric.
+ * Arrays u(d, i, j, el) with n_var fields; FP64. */
+typedef struct wdg_advect wdg_advect;
+int wdg_advect_create(const wdg_mesh *mesh, int n_colloc, int n_var, const double *a, int device, wdg_advect **out);
+void wdg_advect_destroy(wdg_advect *adv);
+int wdg_advect_action(wdg_advect *adv, const double *u, double *du);    /* Advection::action, du += */
+int wdg_advect_bc_action(wdg_advect *adv, const double *u, double *du); /* AdvectionHomogeneousBC::action, du += */
+/* dudt = M^{-1} (A u + B u) and nsteps of ode::RungeKutta4 on it */
+int wdg_advect_rhs(wdg_advect *adv, const double *u, double *dudt);
+int wdg_advect_rk4_steps(wdg_advect *adv, double *u, double dt, double *t, int nsteps);
+
 /* ---- domain decomposition (one rank's share of a mesh) ---- */
 /* The fused kernels' partner table of `mesh` (what Mesh2D::distribute and FaceVector need to
  * know, source/Mesh2D.cpp:384-592): per element side the DOF offset of the neighbour node that

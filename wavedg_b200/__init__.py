@@ -5,6 +5,9 @@ this package is its Python mirror of the reference's ``dg::`` classes.
 """
 from ._lib import WDG_FP32, WDG_FP64, WdgError, lib  # noqa: F401
 from .dg import (  # noqa: F401
+    Advection,
+    AdvectionHomogeneousBC,
+    AdvectionSystem,
     Discretisation,
     Div,
     ExactDiscretisation,
@@ -30,7 +33,7 @@ from .dg import (  # noqa: F401
 )
 
 __all__ = [
-    "read_file", "to_file", "Discretisation", "Div", "ExactDiscretisation", "EdgeFlux", "FaceProlongator", "FaceType", "LinearFunctional2D", "MassMatrix",
+    "Advection", "AdvectionHomogeneousBC", "AdvectionSystem", "read_file", "to_file", "Discretisation", "Div", "ExactDiscretisation", "EdgeFlux", "FaceProlongator", "FaceType", "LinearFunctional2D", "MassMatrix",
     "Mesh2D", "Operator", "QuadratureRule", "RungeKutta4", "WaveBC", "WaveEquation", "WaveHoltz", "WaveHoltzBatch", "WaveSystem",
     "WdgError", "WDG_FP32", "WDG_FP64", "error", "lib", "make_face_prolongator", "norm",
 ]

@@ -60,6 +60,12 @@ SIGNATURES = {
     "wdg_waveq_rk4_steps": ([_v, _v, _d, _v, _i], _i),
     "wdg_waveholtz_create_exact": ([_v, _d, _vp], _i),
     "wdg_mesh_partner_table": ([_v, _i, _v, _v, _v], _i),
+    "wdg_advect_create": ([_v, _i, _i, _v, _i, _vp], _i),
+    "wdg_advect_destroy": ([_v], None),
+    "wdg_advect_action": ([_v, _v, _v], _i),
+    "wdg_advect_bc_action": ([_v, _v, _v], _i),
+    "wdg_advect_rhs": ([_v, _v, _v], _i),
+    "wdg_advect_rk4_steps": ([_v, _v, _d, _v, _i], _i),
     "wdg_wave_create_halo": ([_v, _i, _v, _i, _i, _i, _v, _v, _vp], _i),
     "wdg_halo_info": ([_v, _v, _v], _i),
     "wdg_halo_gather": ([_v, _i, _v, _i, _v], _i),

@@ -760,6 +760,80 @@ class WaveHoltzBatch:
         return W, it, res, stt
 
 
+class AdvectionSystem:
+    """Linear advection with constant coefficients (wdg_advect_*): Advection<true>,
+    AdvectionHomogeneousBC<true> and MassMatrix<true> for n_var variables; a = (A_0, A_1) as
+    a(d, c, k) = a[d + n_var (c + n_var k)] (the reference's (n_var, n_var, 2) layout), both
+    symmetric.  FP64."""
+
+    def __init__(self, n_var: int, mesh: Mesh2D, basis, a, device: int = -1):
+        self.n_var, self.mesh, self.n = int(n_var), mesh, _gll_n(basis)
+        av = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+        if av.size != 2 * self.n_var ** 2:
+            raise WdgError(_lib.WDG_ERR_ARG, "a must hold 2 n_var^2 coefficients")
+        self._a = av
+        h = C.c_void_p()
+        check(lib().wdg_advect_create(mesh._h, self.n, self.n_var, C.c_void_p(av.ctypes.data), device, C.byref(h)),
+              "wdg_advect_create")
+        self._h = h
+        self.ndof = self.n_var * self.n * self.n * mesh.n_elem()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _destroy("wdg_advect_destroy", h)
+            self._h = None
+
+    def _call(self, fn, u, du, what):
+        pu, _ku = _ptr(u, name="u")
+        pd, _kd = _ptr(du, True, "du")
+        check(getattr(lib(), fn)(self._h, pu, pd), what)
+
+    def action(self, u, du) -> None:
+        self._call("wdg_advect_action", u, du, "Advection.action")
+
+    def bc_action(self, u, du) -> None:
+        self._call("wdg_advect_bc_action", u, du, "AdvectionHomogeneousBC.action")
+
+    def rhs(self, u, dudt) -> None:
+        self._call("wdg_advect_rhs", u, dudt, "rhs")
+
+    def rk4_steps(self, u, dt: float, t: float, nsteps: int) -> float:
+        pu, _ku = _ptr(u, True, "u")
+        tt = C.c_double(t)
+        check(lib().wdg_advect_rk4_steps(self._h, pu, float(dt), C.byref(tt), int(nsteps)), "rk4_steps")
+        return tt.value
+
+
+class Advection(Operator):
+    """Advection<true>(n_var, mesh, basis, a, constant_coefficient): du += (A u, grad v) + upwind
+    flux over interior edges (wavedg/Advection.hpp:17-142).  Constant symmetric coefficients."""
+
+    def __init__(self, n_var: int, mesh: Mesh2D, basis, a, constant_coefficient: bool = True, quad=None,
+                 approx_quad: bool = True):
+        _require_approx(approx_quad)
+        if not constant_coefficient or quad is not None:
+            raise WdgError(_lib.WDG_ERR_UNSUPPORTED, "advection is built for constant coefficients and the GLL rule")
+        self.sys = AdvectionSystem(n_var, mesh, basis, a)
+
+    def action(self, *args) -> None:
+        self.sys.action(args[-2], args[-1])
+
+
+class AdvectionHomogeneousBC(Operator):
+    """AdvectionHomogeneousBC<true>: du += boundary flux with u = 0 outside (wavedg/Advection.hpp:144-273)."""
+
+    def __init__(self, n_var: int, mesh: Mesh2D, basis, a, constant_coefficient: bool = True, quad=None,
+                 approx_quad: bool = True):
+        _require_approx(approx_quad)
+        if not constant_coefficient or quad is not None:
+            raise WdgError(_lib.WDG_ERR_UNSUPPORTED, "advection is built for constant coefficients and the GLL rule")
+        self.sys = AdvectionSystem(n_var, mesh, basis, a)
+
+    def action(self, *args) -> None:
+        self.sys.bc_action(args[-2], args[-1])
+
+
 def to_file(fname: str, u) -> None:
     """dg::to_file (examples/examples.hpp:14-19): a float64 array (numpy or CUDA tensor) as raw
     native-order bytes."""
