@@ -52,3 +52,23 @@ def test_decomposed_steps_match_undivided(gpu_lib, precision, world, kind):
     diff = np.abs(out - ref).max()
     print(f"{precision} {kind} x{world}: max |decomposed - undivided| = {diff:.3e}, rel {rel(out, ref):.3e}")
     assert diff == 0.0
+
+
+def test_whole_mesh_calls_are_refused(gpu_lib):
+    """A domain steps stage by stage with its halo filled; whole-step and operator calls, which
+    would take its cut sides for boundary sides, are refused with an error."""
+    import ctypes as C
+
+    import wavedg_b200 as W
+    from wavedg_b200 import decomp
+
+    _, mesh, basis, bc, whole, u0 = _setup("fp64")
+    d = decomp.Domain(mesh, basis, bc, decomp.partition(mesh.n_elem(), 2), 0)
+    u = np.zeros(d.ndof)
+    t = C.c_double(0.0)
+    rc = W.lib().wdg_rk4_steps(d._h, C.c_void_p(u.ctypes.data), 1e-3, C.byref(t), 1)
+    assert rc == W._lib.WDG_ERR_UNSUPPORTED
+    assert b"decomposed" in W.lib().wdg_last_error()
+    du = np.zeros(d.ndof)
+    rc = W.lib().wdg_rhs(d._h, C.c_void_p(u.ctypes.data), C.c_void_p(du.ctypes.data), None, 0.0)
+    assert rc == W._lib.WDG_ERR_UNSUPPORTED

@@ -2,6 +2,8 @@
 // the fused RHS / RK4 entry points.
 #include <cuda_runtime.h>
 
+#include <string>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -321,10 +323,22 @@ namespace
         return WDG_OK;
     }
 
+    // a domain of a decomposed mesh (halo traces) only steps stage by stage, with its halo
+    // filled by the caller; whole-operator and whole-step calls would treat its cut sides as
+    // boundary sides
+    int whole_mesh_only(const wdg_wave *w, const char *what)
+    {
+        if (w && w->halo)
+            return fail(WDG_ERR_UNSUPPORTED, std::string(what) +
+                                                 ": not available on a domain of a decomposed mesh (use wdg_rk4_stage)");
+        return WDG_OK;
+    }
+
     int op_entry(wdg_wave *w, const double *u, double *du, int flags)
     {
         if (!w)
             return fail(WDG_ERR_ARG, "null discretisation");
+        WDG_TRY(whole_mesh_only(w, "operator action"));
         DeviceGuard g(w->device);
         if (u == du)
             return fail(WDG_ERR_ARG, "input and output arrays must differ");
@@ -781,6 +795,7 @@ extern "C"
 
     int wdg_face_prolong(wdg_wave *w, int type, const double *u, double *uf)
     {
+        WDG_TRY(whole_mesh_only(w, "wdg_face_prolong"));
         if (!w || (type != 0 && type != 1))
             return fail(WDG_ERR_ARG, "wdg_face_prolong: bad arguments");
         DeviceGuard g(w->device);
@@ -793,6 +808,7 @@ extern "C"
 
     int wdg_face_prolong_t(wdg_wave *w, int type, const double *uf, double *u)
     {
+        WDG_TRY(whole_mesh_only(w, "wdg_face_prolong_t"));
         if (!w || (type != 0 && type != 1))
             return fail(WDG_ERR_ARG, "wdg_face_prolong_t: bad arguments");
         DeviceGuard g(w->device);
@@ -805,6 +821,7 @@ extern "C"
 
     int wdg_edge_flux(wdg_wave *w, int type, const double *ub, double *fb)
     {
+        WDG_TRY(whole_mesh_only(w, "wdg_edge_flux"));
         if (!w || (type != 0 && type != 1))
             return fail(WDG_ERR_ARG, "wdg_edge_flux: bad arguments");
         DeviceGuard g(w->device);
@@ -824,6 +841,7 @@ extern "C"
 
     int wdg_apply_bc(wdg_wave *w, double *uB)
     {
+        WDG_TRY(whole_mesh_only(w, "wdg_apply_bc"));
         if (!w)
             return fail(WDG_ERR_ARG, "null discretisation");
         DeviceGuard g(w->device);
@@ -860,6 +878,7 @@ extern "C"
 
     int wdg_rhs(wdg_wave *w, const double *u, double *dudt, const double *F, double s)
     {
+        WDG_TRY(whole_mesh_only(w, "wdg_rhs"));
         if (!w)
             return fail(WDG_ERR_ARG, "null discretisation");
         if (u == dudt)
@@ -880,6 +899,7 @@ extern "C"
 
     int wdg_rk4_steps(wdg_wave *w, double *u, double dt, double *t, int nsteps)
     {
+        WDG_TRY(whole_mesh_only(w, "wdg_rk4_steps"));
         if (!w || !u || !t || nsteps < 0)
             return fail(WDG_ERR_ARG, "wdg_rk4_steps: bad arguments");
         DeviceGuard g(w->device);
@@ -931,6 +951,7 @@ extern "C"
 
     int wdg_state_rk4_steps(wdg_wave *w, double dt, double *t, int nsteps)
     {
+        WDG_TRY(whole_mesh_only(w, "wdg_state_rk4_steps"));
         if (!w || !t || nsteps < 0)
             return fail(WDG_ERR_ARG, "wdg_state_rk4_steps: bad arguments");
         DeviceGuard g(w->device);

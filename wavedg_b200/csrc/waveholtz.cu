@@ -162,6 +162,8 @@ extern "C"
     {
         if (!w || !out || !(omega > 0.0))
             return fail(WDG_ERR_ARG, "wdg_waveholtz_create: need a discretisation and omega > 0");
+        if (w->halo)
+            return fail(WDG_ERR_UNSUPPORTED, "wdg_waveholtz_create: not available on a domain of a decomposed mesh");
         *out = nullptr;
         wdg_waveholtz *h = new wdg_waveholtz;
         h->w = w;
