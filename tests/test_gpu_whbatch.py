@@ -151,7 +151,7 @@ def test_device_inputs_written_just_before_the_solve(gpu_lib):
 
 def test_fp32_batch_and_fp64_finish(gpu_lib):
     """FP32 stepping stops on the stall rule or at tol; an FP64 batch warm-started from its
-    iterates then meets the FP64 tolerance (the plain iteration is the judge)."""
+    iterates then meets the FP64 tolerance (the plain iteration decides convergence)."""
     W, probs, systems32, Fs = _batch_problems("fp32")
     b32 = W.WaveHoltzBatch(systems32, [p[3] for p in probs])
     W32, it32, res32, st32 = b32.solve(Fs, 1e-6, 300, stall_limit=3)

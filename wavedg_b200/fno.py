@@ -3,8 +3,8 @@
 The network maps the forcing of a WaveHoltz problem (its normalised Gaussian, omega, and
 the grid coordinates) on a G x G cell-centred grid of [-1, 1]^2 to the solution's (p, u, v)
 on the same grid, which is interpolated to the DG nodes as the initial iterate W0.  The
-WaveHoltz iteration stays the judge: a warm-started solve stops at the same residual
-tolerance as a cold one, only the iteration count changes.
+WaveHoltz iteration still decides convergence: a warm-started solve stops at the same
+residual tolerance as a cold one, only the iteration count changes.
 
 Architecture: lift (4 -> width, pointwise), `layers` Fourier layers
 v <- act(K v + W v + b) with K the spectral convolution on the retained modes
