@@ -69,6 +69,25 @@ def test_plans_deliver_the_partner_traces(W, world, kind):
     assert sum(len(p.halo_elem) for p in plans.values()) == sum(len(v) for p in plans.values() for v in p.send.values()) // n
 
 
+def test_single_rank_and_uneven_partitions(W):
+    from wavedg_b200 import decomp
+
+    m, bc = _mesh(W)
+    nel = m.n_elem()
+    p = decomp.Plan(m, 3, bc, np.zeros(nel, dtype=np.int32), 0)
+    assert len(p.halo_elem) == 0 and p.send == {} and p.recv == {}
+    np.testing.assert_array_equal(p.local, np.arange(nel))
+    # blocks differ in size by at most one element and cover every element once
+    for world in (1, 2, 5, nel):
+        part = decomp.partition(nel, world)
+        counts = np.bincount(part, minlength=world)
+        assert counts.sum() == nel and counts.max() - counts.min() <= 1
+    # a rank that owns nothing sends and receives nothing
+    part = np.where(np.arange(nel) < nel // 2, 0, 2).astype(np.int32)
+    p1 = decomp.Plan(m, 3, bc, part, 1)
+    assert len(p1.local) == 0 and p1.send == {} and p1.recv == {}
+
+
 def test_local_boundary_codes(W):
     """Physical boundary sides keep their codes; cut sides become boundary sides of the local mesh."""
     from wavedg_b200 import decomp

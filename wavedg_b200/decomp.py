@@ -135,6 +135,8 @@ class Domain:
             raise WdgError(-1, "decomposition needs a mesh built from vertices")
         n = dg._gll_n(basis)
         self.plan = Plan(mesh, n, bc, part, rank)
+        if len(self.plan.local) == 0:
+            raise ValueError(f"rank {rank} owns no elements")
         self.rank, self.n = rank, n
         self.mesh = dg.Mesh2D.from_vertices(self.plan.verts, self.plan.quads)
         codes = self.plan.local_bc(self.mesh)
