@@ -281,39 +281,6 @@ namespace
         return F;
     }
 
-    template <typename T>
-    int dalloc(T **p, size_t count)
-    {
-        cudaError_t e = cudaMalloc((void **)p, sizeof(T) * std::max<size_t>(count, 1));
-        if (e != cudaSuccess)
-        {
-            *p = nullptr;
-            return cuda_fail(e, "cudaMalloc");
-        }
-        return WDG_OK;
-    }
-    template <typename T>
-    int put(T *d, const std::vector<T> &h)
-    {
-        if (!h.empty())
-            WDG_CUDA(cudaMemcpy(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
-        return WDG_OK;
-    }
-    struct Dev
-    {
-        int prev = -1;
-        explicit Dev(int d)
-        {
-            cudaGetDevice(&prev);
-            if (prev != d)
-                cudaSetDevice(d);
-        }
-        ~Dev()
-        {
-            if (prev >= 0)
-                cudaSetDevice(prev);
-        }
-    };
     unsigned blocks(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
     long long nvals(const wdg_advect *h) { return (long long)h->nv * h->n * h->n * h->w->nel; }
@@ -367,7 +334,7 @@ namespace
             return fail(WDG_ERR_ARG, "null advection argument");
         if (u == du)
             return fail(WDG_ERR_ARG, "input and output arrays must differ");
-        Dev g(h->w->device);
+        DeviceScope g(h->w->device);
         HostArg a[2];
         WDG_TRY(bind_arg(h->w, 0, u, (size_t)nvals(h), true, false, a[0]));
         WDG_TRY(bind_arg(h->w, 1, du, (size_t)nvals(h), accumulate, true, a[1]));
@@ -402,7 +369,7 @@ extern "C"
         h->w = w;
         h->n = n_colloc;
         h->nv = n_var;
-        Dev g(w->device);
+        DeviceScope g(w->device);
         const int n = n_colloc;
         std::vector<double> x(n), wt(n), D((size_t)n * n), av(a, a + 2 * v2);
         gauss_lobatto(n, x.data(), wt.data());
@@ -415,22 +382,22 @@ extern "C"
             if (st == WDG_OK)
                 st = r;
         };
-        chk(dalloc(&h->d_a, av.size()));
-        chk(dalloc(&h->d_x, x.size()));
-        chk(dalloc(&h->d_wt, wt.size()));
-        chk(dalloc(&h->d_D, D.size()));
-        chk(dalloc(&h->d_FI, FI.size()));
-        chk(dalloc(&h->d_FB, FB.size()));
-        chk(dalloc(&h->d_uf, (size_t)n * n_var * 2 * w->nI));
-        chk(dalloc(&h->d_uB, (size_t)n * n_var * 2 * w->nB));
+        chk(device_alloc(&h->d_a, av.size()));
+        chk(device_alloc(&h->d_x, x.size()));
+        chk(device_alloc(&h->d_wt, wt.size()));
+        chk(device_alloc(&h->d_D, D.size()));
+        chk(device_alloc(&h->d_FI, FI.size()));
+        chk(device_alloc(&h->d_FB, FB.size()));
+        chk(device_alloc(&h->d_uf, (size_t)n * n_var * 2 * w->nI));
+        chk(device_alloc(&h->d_uB, (size_t)n * n_var * 2 * w->nB));
         if (st == WDG_OK)
         {
-            chk(put(h->d_a, av));
-            chk(put(h->d_x, x));
-            chk(put(h->d_wt, wt));
-            chk(put(h->d_D, D));
-            chk(put(h->d_FI, FI));
-            chk(put(h->d_FB, FB));
+            chk(device_put(h->d_a, av));
+            chk(device_put(h->d_x, x));
+            chk(device_put(h->d_wt, wt));
+            chk(device_put(h->d_D, D));
+            chk(device_put(h->d_FI, FI));
+            chk(device_put(h->d_FB, FB));
         }
         if (st != WDG_OK)
         {
@@ -446,7 +413,7 @@ extern "C"
         if (!h)
             return;
         {
-            Dev g(h->w ? h->w->device : 0);
+            DeviceScope g(h->w ? h->w->device : 0);
             for (double *p : {h->d_a, h->d_x, h->d_wt, h->d_D, h->d_FI, h->d_FB, h->d_uf, h->d_uB, h->d_rk})
                 if (p)
                     cudaFree(p);
@@ -464,11 +431,11 @@ extern "C"
     {
         if (!h || !u || !t || nsteps < 0)
             return fail(WDG_ERR_ARG, "wdg_advect_rk4_steps: bad arguments");
-        Dev g(h->w->device);
+        DeviceScope g(h->w->device);
         wdg_wave *w = h->w;
         const long long nd = nvals(h);
         if (!h->d_rk)
-            WDG_TRY(dalloc(&h->d_rk, 2 * (size_t)nd));
+            WDG_TRY(device_alloc(&h->d_rk, 2 * (size_t)nd));
         double *k = h->d_rk, *p = h->d_rk + nd;
         HostArg a;
         WDG_TRY(bind_arg(w, 0, u, (size_t)nd, true, true, a));

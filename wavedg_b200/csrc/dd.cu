@@ -40,21 +40,6 @@ namespace
         }
     }
 
-    struct Dev
-    {
-        int prev = -1;
-        explicit Dev(int d)
-        {
-            cudaGetDevice(&prev);
-            if (prev != d)
-                cudaSetDevice(d);
-        }
-        ~Dev()
-        {
-            if (prev >= 0)
-                cudaSetDevice(prev);
-        }
-    };
 } // namespace
 
 extern "C"
@@ -101,7 +86,7 @@ extern "C"
         }
         wdg_wave *w = nullptr;
         WDG_TRY(wdg_wave_create(mesh, n_colloc, bc, precision, device, &w));
-        Dev g(w->device);
+        DeviceScope g(w->device);
         w->halo = 3LL * n_colloc * n_halo;
         cudaError_t e = cudaMemcpy(w->d_fbase, fb.data(), sizeof(int) * fb.size(), cudaMemcpyHostToDevice);
         if (e == cudaSuccess)
@@ -133,7 +118,7 @@ extern "C"
             return fail(WDG_ERR_ARG, "wdg_halo_gather: bad arguments");
         if (count == 0)
             return WDG_OK;
-        Dev g(w->device);
+        DeviceScope g(w->device);
         WDG_TRY(ensure_states(w));
         const unsigned grid = (unsigned)std::min(148 * 8, (count + 255) / 256);
         if (w->precision == WDG_FP32)
@@ -153,7 +138,7 @@ extern "C"
             return fail(WDG_ERR_ARG, "wdg_halo_put: bad arguments");
         if (count == 0)
             return WDG_OK;
-        Dev g(w->device);
+        DeviceScope g(w->device);
         WDG_TRY(ensure_states(w));
         char *dst = static_cast<char *>(w->d_state[buffer]) + w->real_size() * (size_t)(w->ndof + offset);
         WDG_CUDA(cudaMemcpyAsync(dst, src, w->real_size() * (size_t)count, cudaMemcpyDefault, w->stream));
@@ -164,7 +149,7 @@ extern "C"
     {
         if (!w || stage < 0 || stage > 4)
             return fail(WDG_ERR_ARG, "wdg_rk4_stage: stage must be 0..4");
-        Dev g(w->device);
+        DeviceScope g(w->device);
         return w->precision == WDG_FP32 ? rk4_stage<float>(w, stage, dt) : rk4_stage<double>(w, stage, dt);
     }
 }

@@ -286,40 +286,7 @@ namespace
 
     unsigned grid_for(long long n, int threads) { return (unsigned)std::min<long long>((n + threads - 1) / threads, 148LL * 32); }
 
-    template <typename T>
-    int dalloc(T **p, size_t count)
-    {
-        cudaError_t e = cudaMalloc((void **)p, sizeof(T) * std::max<size_t>(count, 1));
-        if (e != cudaSuccess)
-        {
-            *p = nullptr;
-            return cuda_fail(e, "cudaMalloc");
-        }
-        return WDG_OK;
-    }
-    template <typename T>
-    int put(T *d, const std::vector<T> &h)
-    {
-        if (!h.empty())
-            WDG_CUDA(cudaMemcpy(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
-        return WDG_OK;
-    }
 
-    struct Dev
-    {
-        int prev = -1;
-        explicit Dev(int d)
-        {
-            cudaGetDevice(&prev);
-            if (prev != d)
-                cudaSetDevice(d);
-        }
-        ~Dev()
-        {
-            if (prev >= 0)
-                cudaSetDevice(prev);
-        }
-    };
 
     size_t face_count(const wdg_waveq *h, int type)
     {
@@ -406,7 +373,7 @@ namespace
             return fail(WDG_ERR_ARG, "null exact-quadrature discretisation");
         if (u == du)
             return fail(WDG_ERR_ARG, "input and output arrays must differ");
-        Dev g(h->w->device);
+        DeviceScope g(h->w->device);
         HostArg a[2];
         WDG_TRY(bind_arg(h->w, 0, u, h->w->ndof, true, false, a[0]));
         WDG_TRY(bind_arg(h->w, 1, du, h->w->ndof, true, true, a[1]));
@@ -420,10 +387,10 @@ namespace wdg
     // RK buffers and the resident state exist before a period is captured into a graph
     int waveq_prepare(wdg_waveq *h)
     {
-        Dev g(h->w->device);
+        DeviceScope g(h->w->device);
         WDG_TRY(ensure_states(h->w));
         if (!h->d_rk)
-            WDG_TRY(dalloc(&h->d_rk, 2 * (size_t)h->w->ndof));
+            WDG_TRY(device_alloc(&h->d_rk, 2 * (size_t)h->w->ndof));
         return WDG_OK;
     }
 
@@ -475,7 +442,7 @@ extern "C"
         h->nqd = qdiv(n_colloc);
         h->nqf = qface(n_colloc);
         h->nqm = qface(n_colloc);
-        Dev g(w->device);
+        DeviceScope g(w->device);
         const int n = n_colloc, c = n * n;
         std::vector<double> x(n), wg(n);
         gauss_lobatto(n, x.data(), wg.data());
@@ -580,30 +547,30 @@ extern "C"
             if (st == WDG_OK)
                 st = r;
         };
-        chk(dalloc(&h->d_xd, xd.size()));
-        chk(dalloc(&h->d_wd, wd.size()));
-        chk(dalloc(&h->d_Pd, Pd.size()));
-        chk(dalloc(&h->d_Dd, Dd.size()));
-        chk(dalloc(&h->d_wf, wf.size()));
-        chk(dalloc(&h->d_Pf, Pf.size()));
-        chk(dalloc(&h->d_nI, nI.size()));
-        chk(dalloc(&h->d_nB, nB.size()));
-        chk(dalloc(&h->d_M, Mf.size()));
-        chk(dalloc(&h->d_Minv, Mi.size()));
-        chk(dalloc(&h->d_uf, face_count(h, 0)));
-        chk(dalloc(&h->d_uB, face_count(h, 1)));
+        chk(device_alloc(&h->d_xd, xd.size()));
+        chk(device_alloc(&h->d_wd, wd.size()));
+        chk(device_alloc(&h->d_Pd, Pd.size()));
+        chk(device_alloc(&h->d_Dd, Dd.size()));
+        chk(device_alloc(&h->d_wf, wf.size()));
+        chk(device_alloc(&h->d_Pf, Pf.size()));
+        chk(device_alloc(&h->d_nI, nI.size()));
+        chk(device_alloc(&h->d_nB, nB.size()));
+        chk(device_alloc(&h->d_M, Mf.size()));
+        chk(device_alloc(&h->d_Minv, Mi.size()));
+        chk(device_alloc(&h->d_uf, face_count(h, 0)));
+        chk(device_alloc(&h->d_uB, face_count(h, 1)));
         if (st == WDG_OK)
         {
-            chk(put(h->d_xd, xd));
-            chk(put(h->d_wd, wd));
-            chk(put(h->d_Pd, Pd));
-            chk(put(h->d_Dd, Dd));
-            chk(put(h->d_wf, wf));
-            chk(put(h->d_Pf, Pf));
-            chk(put(h->d_nI, nI));
-            chk(put(h->d_nB, nB));
-            chk(put(h->d_M, Mf));
-            chk(put(h->d_Minv, Mi));
+            chk(device_put(h->d_xd, xd));
+            chk(device_put(h->d_wd, wd));
+            chk(device_put(h->d_Pd, Pd));
+            chk(device_put(h->d_Dd, Dd));
+            chk(device_put(h->d_wf, wf));
+            chk(device_put(h->d_Pf, Pf));
+            chk(device_put(h->d_nI, nI));
+            chk(device_put(h->d_nB, nB));
+            chk(device_put(h->d_M, Mf));
+            chk(device_put(h->d_Minv, Mi));
         }
         if (st == WDG_OK)
         {
@@ -629,7 +596,7 @@ extern "C"
         if (!h)
             return;
         {
-            Dev g(h->w ? h->w->device : 0);
+            DeviceScope g(h->w ? h->w->device : 0);
             for (double *p : {h->d_xd, h->d_wd, h->d_Pd, h->d_Dd, h->d_wf, h->d_Pf, h->d_nI, h->d_nB, h->d_M, h->d_Minv, h->d_uf,
                               h->d_uB, h->d_rk})
                 if (p)
@@ -669,7 +636,7 @@ extern "C"
     {
         if (!h || (type != 0 && type != 1) || !ub || !fb)
             return fail(WDG_ERR_ARG, "wdg_waveq_edge_flux: bad arguments");
-        Dev g(h->w->device);
+        DeviceScope g(h->w->device);
         const size_t cnt = face_count(h, type);
         HostArg a[2];
         if (ub == fb)
@@ -688,7 +655,7 @@ extern "C"
     {
         if (!h || n_var < 1 || n_var > 16)
             return fail(WDG_ERR_ARG, "wdg_waveq_mass_inv: bad arguments");
-        Dev g(h->w->device);
+        DeviceScope g(h->w->device);
         HostArg a;
         WDG_TRY(bind_arg(h->w, 0, x, (size_t)n_var * h->n * h->n * h->w->nel, true, true, a));
         WDG_TRY(mass_dev(h, n_var, a.dev, true));
@@ -699,7 +666,7 @@ extern "C"
     {
         if (!h || n_var < 1 || n_var > 16 || !x || !y)
             return fail(WDG_ERR_ARG, "wdg_waveq_mass_action: bad arguments");
-        Dev g(h->w->device);
+        DeviceScope g(h->w->device);
         const size_t cnt = (size_t)n_var * h->n * h->n * h->w->nel;
         HostArg a[2];
         WDG_TRY(bind_arg(h->w, 0, x, cnt, true, false, a[0]));
@@ -716,7 +683,7 @@ extern "C"
             return fail(WDG_ERR_ARG, "wdg_waveq_rhs: bad arguments");
         if (u == dudt)
             return fail(WDG_ERR_ARG, "input and output arrays must differ");
-        Dev g(h->w->device);
+        DeviceScope g(h->w->device);
         HostArg a[3];
         int na = 2;
         WDG_TRY(bind_arg(h->w, 0, u, h->w->ndof, true, false, a[0]));
@@ -734,10 +701,10 @@ extern "C"
     {
         if (!h || !u || !t || nsteps < 0)
             return fail(WDG_ERR_ARG, "wdg_waveq_rk4_steps: bad arguments");
-        Dev g(h->w->device);
+        DeviceScope g(h->w->device);
         wdg_wave *w = h->w;
         if (!h->d_rk)
-            WDG_TRY(dalloc(&h->d_rk, 2 * (size_t)w->ndof));
+            WDG_TRY(device_alloc(&h->d_rk, 2 * (size_t)w->ndof));
         double *k = h->d_rk, *p = h->d_rk + w->ndof;
         HostArg a;
         WDG_TRY(bind_arg(w, 0, u, w->ndof, true, true, a));

@@ -87,6 +87,46 @@ namespace wdg
     // copy host outputs back, release temporaries, wait when any argument was host memory
     int finish_args(wdg_wave *w, HostArg *args, int nargs);
 
+    // host helpers shared by the C-ABI files: make `device` current for a scope; cudaMalloc of
+    // count elements (at least one) reported as a library error; upload a host vector
+    struct DeviceScope
+    {
+        int prev = -1;
+        explicit DeviceScope(int device)
+        {
+            cudaGetDevice(&prev);
+            if (prev != device)
+                cudaSetDevice(device);
+        }
+        ~DeviceScope()
+        {
+            if (prev >= 0)
+                cudaSetDevice(prev);
+        }
+    };
+    template <typename T>
+    int device_alloc(T **p, size_t count)
+    {
+        cudaError_t e = cudaMalloc((void **)p, sizeof(T) * (count ? count : 1));
+        if (e != cudaSuccess)
+        {
+            *p = nullptr;
+            return cuda_fail(e, "cudaMalloc");
+        }
+        return WDG_OK;
+    }
+    template <typename T>
+    int device_put(T *d, const std::vector<T> &h)
+    {
+        if (!h.empty())
+        {
+            cudaError_t e = cudaMemcpy(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess)
+                return cuda_fail(e, "cudaMemcpy");
+        }
+        return WDG_OK;
+    }
+
     // exact-quadrature periods for WaveHoltz (exactq.cu)
     int waveq_prepare(wdg_waveq *q);
     int waveq_period(wdg_waveq *q, double *u, double dt, int nt, const double *F, double omega, double *acc,
