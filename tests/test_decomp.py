@@ -119,9 +119,8 @@ def _worker(rank, world, port, q):
     import torch
     import torch.distributed as dist
 
-    from wavedg_b200 import decomp
-
     import wavedg_b200 as W
+    from wavedg_b200 import decomp
 
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
@@ -134,18 +133,24 @@ def _worker(rank, world, port, q):
         U = np.random.default_rng(1).standard_normal((m.n_elem(), 3 * n * n))
         local = torch.from_numpy(U[p.local].ravel().copy())
         halo = torch.zeros(3 * n * len(p.halo_elem), dtype=torch.float64)
-        ops = []
-        for r in sorted(p.send):
-            idx = torch.from_numpy(p.send[r].astype(np.int64))
-            buf = torch.stack([local[idx + f] for f in range(3)], dim=1).reshape(-1).contiguous()
-            ops.append(dist.P2POp(dist.isend, buf, r))
-        recv = {s: torch.zeros(3 * n * cnt, dtype=torch.float64) for s, (_, cnt) in p.recv.items()}
-        for s in sorted(p.recv):
-            ops.append(dist.P2POp(dist.irecv, recv[s], s))
-        for req in dist.batch_isend_irecv(ops):
-            req.wait()
-        for s, (first, cnt) in p.recv.items():
-            halo[3 * n * first: 3 * n * (first + cnt)] = recv[s]
+
+        class HostDomain:
+            """The exchange-facing side of decomp.Domain over host tensors (gloo)."""
+            plan = p
+            _recv_buf = {s: torch.zeros(3 * n * cnt, dtype=torch.float64) for s, (_, cnt) in p.recv.items()}
+
+            def gather(self, stage, r):
+                idx = torch.from_numpy(p.send[r].astype(np.int64))
+                return torch.stack([local[idx + f] for f in range(3)], dim=1).reshape(-1).contiguous()
+
+            def put(self, stage, s, values):
+                first, cnt = p.recv[s]
+                halo[3 * n * first: 3 * n * (first + cnt)] = values
+
+            def sync(self):
+                pass
+
+        decomp.dist_exchange(HostDomain())(0)  # the exchange Domain.rk4_steps uses with NCCL
         fb, fc = decomp.partner_table(m, n, bc)
         stride = {0: 3, 1: -3, 2: 3 * n, 3: -3 * n}
         bad = 0
