@@ -266,6 +266,7 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_extras and args.precision == "fp64" and world == 1:
         extra["exact_quadrature"] = exact_quadrature(local_rank, cpu_leg=not args.no_cpu_baseline)
         extra["advection"] = advection(local_rank, cpu_leg=not args.no_cpu_baseline)
+        extra["decomposition"] = decomposition(local_rank)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -509,6 +510,54 @@ def advection(device: int, n_el: int = 256, P: int = 4, nv: int = 2, reps: int =
             out["cpu_reference_ms_per_rhs"] = (time.perf_counter() - t0) * 1e3
             out["cpu_reference"] = "the reference's Advection / AdvectionHomogeneousBC / MassMatrix<true>, 1 thread"
     return out
+
+
+def decomposition(device: int, n_el: int = 512, P: int = 4, ranks: int = 2, steps: int = 10) -> dict:
+    """One mesh split into `ranks` domains (contiguous element blocks), emulated on one GPU: the
+    domains step one after another with their halo exchanged by device copies before every
+    RK stage.  Against the undivided mesh on the same GPU this measures what the
+    decomposition itself adds (halo gather, copies, the extra launches and host syncs), not
+    multi-GPU speed; the states must agree bit for bit."""
+    import torch
+
+    import wavedg_b200 as W
+    from wavedg_b200 import decomp
+    from wavedg_b200 import meshgen as mg
+
+    v, q = mg.perturbed_rect(n_el, 0.2, seed=1)
+    mesh = W.Mesh2D.from_vertices(v, q)
+    basis = W.QuadratureRule.quadrature_rule(P + 1, W.QuadratureRule.GaussLobatto)
+    bc = np.zeros(mesh.n_edges(1), dtype=np.int32)
+    whole = W.WaveSystem(mesh, basis, bc, device=device)
+    u0 = np.random.default_rng(3).standard_normal(whole.ndof)
+    dt = 0.1 * mesh.min_h() / (P + 1) ** 2
+    part = decomp.partition(mesh.n_elem(), ranks)
+    doms = [decomp.Domain(mesh, basis, bc, part, r, device=device) for r in range(ranks)]
+    for d in doms:
+        d.upload(u0)
+    decomp.step_all(doms, dt, 1)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    decomp.step_all(doms, dt, steps)
+    for d in doms:
+        d.sync()
+    t_dd = (time.perf_counter() - t0) / steps
+    ud = np.zeros_like(u0)
+    for d in doms:
+        d.download(ud)
+    uw = torch.from_numpy(u0.copy()).cuda()  # device array: no transfers in the timed loop
+    whole.rk4_steps(uw, dt, 0.0, 1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    whole.rk4_steps(uw, dt, 0.0, steps)
+    torch.cuda.synchronize()
+    t_whole = (time.perf_counter() - t0) / steps
+    uw = uw.cpu().numpy()
+    halo = sum(d.halo for d in doms)
+    return {"workload": f"rk4_fp64_{n_el}x{n_el}_P{P}_{ranks}_domains_one_gpu", "ms_per_step_domains": t_dd * 1e3,
+            "ms_per_step_undivided": t_whole * 1e3, "halo_values": halo,
+            "halo_bytes_per_stage": 8 * halo, "identical_to_undivided": bool(np.array_equal(ud, uw)),
+            "note": "domains run one after another on one GPU: the difference is the decomposition's own cost"}
 
 
 def cpu_baseline(v, q, bc, n, dt, u0, budget=30.0):
