@@ -208,20 +208,15 @@ class Domain:
 
 
 def local_exchange(domains):
-    """Exchange among Domains of one process (one GPU): device copies, in stream order."""
+    """Exchange among Domains of one process (one GPU): device copies.  Every Domain issues its
+    work on its handle's stream, the legacy default stream, so gathers, copies and stages of
+    all domains run in issue order without host synchronisation; a gather buffer is rewritten
+    only by a later gather, issued after the copy that read it."""
 
     def run(stage):
-        # gathers on each sender's stream, then (after they finish) the receivers' copies on
-        # theirs; the gather buffers are reused next stage, so every copy ends before returning
         for d in domains:
             for r in d.plan.send:
-                d.gather(stage, r)
-            d.sync()
-        for d in domains:
-            for r in d.plan.send:
-                domains[r].put(stage, d.rank, d._send_buf[r])
-        for d in domains:
-            d.sync()
+                domains[r].put(stage, d.rank, d.gather(stage, r))
 
     return run
 
