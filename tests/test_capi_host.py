@@ -121,3 +121,29 @@ def test_meshgen_properties():
     p = vs[qs]
     area = 0.5 * np.sum(p[:, :, 0] * np.roll(p[:, :, 1], -1, 1) - np.roll(p[:, :, 0], -1, 1) * p[:, :, 1], axis=1)
     assert (area > 0).all()
+
+
+def test_argument_errors_before_any_device_work(L):
+    """Argument checks of the exact-quadrature, advection and decomposition front ends raise
+    before anything touches a GPU."""
+    import wavedg_b200 as W
+    from wavedg_b200 import decomp
+
+    mesh = W.Mesh2D.uniform_rect(3, -1, 1, 3, -1, 1)
+    basis = W.QuadratureRule.quadrature_rule(4, W.QuadratureRule.GaussLobatto)
+    with pytest.raises(W.WdgError, match="default rules"):
+        W.ExactDiscretisation(mesh, 4, quad=W.QuadratureRule.quadrature_rule(6, 0))
+    with pytest.raises(W.WdgError, match="2 n_var"):
+        W.AdvectionSystem(2, mesh, basis, np.zeros(5))
+    with pytest.raises(W.WdgError, match="constant coefficients"):
+        W.Advection(1, mesh, basis, [1.0, 0.0], constant_coefficient=False)
+    with pytest.raises(ValueError, match="one rank per element"):
+        decomp.Plan(mesh, 4, None, np.zeros(5, dtype=np.int32), 0)
+    with pytest.raises(ValueError):
+        decomp.partition(10, 0)
+    # the C entry points reject bad arguments with a status, not a crash
+    h = C.c_void_p()
+    assert L.wdg_waveq_create(None, 4, None, 0, C.byref(h)) == W._lib.WDG_ERR_ARG
+    assert L.wdg_advect_create(mesh._h, 4, 9, C.c_void_p(np.zeros(162).ctypes.data), 0, C.byref(h)) == \
+        W._lib.WDG_ERR_UNSUPPORTED
+    assert L.wdg_mesh_partner_table(mesh._h, 1, None, None, None) == W._lib.WDG_ERR_ARG
