@@ -169,3 +169,45 @@ def test_oracle_catches_planted_error():
     bc[0] = (bc[0] + 1) % 3  # wrong boundary code on one edge
     op = cpu.Op(m, int(g["n"]), bc)
     assert rel(op.rhs(g["u"]), g["rhs"]) > 1e-6
+
+
+@pytest.mark.skipif(not cpu.available("reference"), reason="the reference library is built where its sources are")
+@pytest.mark.parametrize("n", range(2, 10))
+def test_exact_quadrature_every_degree_against_the_reference(n):
+    """The oracle's exact-quadrature restatement against the compiled reference for every
+    degree the GPU path builds (n = 2..9), all operators, one seeded state."""
+    from wavedg_b200 import meshgen as mg
+
+    v, q = mg.perturbed_rect(4, 0.2, seed=n)
+    v, q = mg.scrambled(v, q, seed=n + 1)
+    rng = np.random.default_rng(n)
+    mo, mr = cpu.Mesh(v, q, "oracle"), cpu.Mesh(v, q, "reference")
+    bc = rng.integers(0, 3, size=mo.n_edges(1)).astype(np.int32)
+    o, r = cpu.OpQ(mo, n, bc), cpu.OpQ(mr, n, bc)
+    u = rng.standard_normal(o.ndof)
+    assert rel(o.rhs(u), r.rhs(u)) < 1e-12
+    for k in (0, 1):
+        uf = rng.standard_normal(n * 6 * mo.n_edges(k))
+        assert rel(o.flux(k, uf), r.flux(k, uf)) < 1e-12
+    x1, x2 = u.copy(), u.copy()
+    o.mass_inv(3, x1)
+    r.mass_inv(3, x2)
+    assert rel(x1, x2) < 1e-12
+
+
+@pytest.mark.skipif(not cpu.available("reference"), reason="the reference library is built where its sources are")
+@pytest.mark.parametrize("nv", range(1, 9))
+def test_advection_every_variable_count_against_the_reference(nv):
+    """The oracle's constant-coefficient advection against the compiled reference for every
+    n_var the GPU path builds (1..8), random symmetric coefficients."""
+    from wavedg_b200 import meshgen as mg
+
+    v, q = mg.perturbed_rect(4, 0.2, seed=nv)
+    rng = np.random.default_rng(100 + nv)
+    A = rng.standard_normal((2, nv, nv))
+    A = A + A.transpose(0, 2, 1)
+    a = np.concatenate([A[0].reshape(-1, order="F"), A[1].reshape(-1, order="F")])
+    o = cpu.OpA(cpu.Mesh(v, q, "oracle"), 4, nv, a)
+    r = cpu.OpA(cpu.Mesh(v, q, "reference"), 4, nv, a)
+    u = rng.standard_normal(o.ndof)
+    assert rel(o.rhs(u), r.rhs(u)) < 1e-12
