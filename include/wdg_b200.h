@@ -238,15 +238,21 @@ int wdg_load_gaussians(wdg_wave *wave, int n_src, const double *cx, const double
                        const double *amp, double scale, int comp, int mass_inv, double *F);
 
 /* wdg_load_gaussians for callers that cannot allocate device memory (no counterpart in the
- * reference) -- code that issues its work while a CUDA graph is being captured, where cudaMalloc
- * is not allowed; loops whose memory is fixed before they start; hosts whose own allocator owns
- * the GPU's memory.  The same load vector, but the source table is staged in a fixed 32 KiB array that
- * belongs to the library image (held on every GPU that loads the library until the process exits)
- * instead of a buffer allocated on first use.  Nothing is allocated: at most 1024 sources per call
- * (more return WDG_ERR_ARG), and F must be device memory.  The first call on a device looks up the
- * array's device address; make it before any stream capture.  All calls share the one table, so
- * calls that overlap on the GPU (different streams or threads) race.  Asynchronous on the handle's
- * stream; cx..amp may be host or device arrays. */
+ * reference).  wdg_load_gaussians grows a device buffer for its source table on first use; some
+ * callers cannot let a library do that once they run: loops whose memory is fixed before they start
+ * (a cudaMalloc there could fail, and it synchronises the device, stalling a real-time loop), and
+ * hosts whose own allocator has reserved the GPU's memory.  This entry point gives the same load
+ * vector but stages the table in a fixed 32 KiB array that belongs to the library image (held on
+ * every GPU that loads the library until the process exits).  Nothing is allocated: at most 1024
+ * sources per call (more return WDG_ERR_ARG), and F must be device memory.
+ * The first call on a device looks up the array's device address (once per device, cached for the
+ * life of the process); make that first call before any stream capture.  The cached address dies
+ * with the device's context: after cudaDeviceReset this entry point must not be called again in
+ * the process.  All calls share the one table and it keeps the last call's sources, so calls that
+ * overlap on the GPU (different streams or threads) race.  Asynchronous on the handle's stream:
+ * cx..amp in pageable host memory are copied before the call returns; in pinned host or device
+ * memory they are read when the stream reaches the copy and must stay valid and unchanged until
+ * then. */
 int wdg_load_gaussians_noalloc(wdg_wave *wave, int n_src, const double *cx, const double *cy,
                                const double *sigma, const double *amp, double scale, int comp, int mass_inv,
                                double *F);

@@ -14,6 +14,21 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
 
 
+def require_reference_build(path=None):
+    """The reference library compiled from its sources (oracle/_ref) is part of the test
+    set-up: a missing build fails the parity tests that compare against it instead of
+    turning them off.  WDG_ALLOW_NO_REFERENCE=1 lets them skip (a checkout without the
+    reference sources)."""
+    from oracle import cpu
+
+    ok = cpu.available("reference") if path is None else os.path.exists(path)
+    if not ok:
+        what = path or "oracle/_ref/libwdgref.so"
+        if os.environ.get("WDG_ALLOW_NO_REFERENCE") == "1":
+            pytest.skip(f"{what} not built (WDG_ALLOW_NO_REFERENCE=1)")
+        pytest.fail(f"{what} is missing: build it with `make -C oracle ref` (needs the reference sources)")
+
+
 def golden(name):
     return dict(np.load(os.path.join(GOLDEN, name), allow_pickle=False))
 

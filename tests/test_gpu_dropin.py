@@ -11,14 +11,15 @@ import subprocess
 
 import pytest
 
+from conftest import require_reference_build
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 BIN = os.path.join(HERE, "..", "oracle", "_ref", "dropin_test")
 
 
 @pytest.mark.gpu
 def test_reference_driver_with_dropins():
-    if not os.path.exists(BIN):
-        pytest.skip("oracle/_ref/dropin_test not built (needs the reference sources)")
+    require_reference_build(BIN)
     out = subprocess.run([BIN], capture_output=True, text=True, timeout=300)
     print(out.stdout)
     assert out.returncode == 0, out.stdout + out.stderr

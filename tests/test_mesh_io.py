@@ -11,6 +11,7 @@ import os
 import numpy as np
 import pytest
 
+from conftest import require_reference_build
 from oracle import cpu
 
 
@@ -49,13 +50,13 @@ def test_from_file_matches_the_reference_reader(W, tmp_path, name):
         np.testing.assert_array_equal(m.edges(t), r.edges(t))
     assert m.min_h() == r.min_h()
     np.testing.assert_array_equal(m.boundary_midpoints(), r.boundary_midpoints())
-    if cpu.available("reference"):
-        g = cpu.reference_mesh_from_file(d)
-        assert g is not None and g["n_elem"] == len(q)
-        np.testing.assert_array_equal(m.edges(0), g["edges_interior"])
-        np.testing.assert_array_equal(m.edges(1), g["edges_boundary"])
-        assert m.min_h() == g["min_h"]
-        np.testing.assert_array_equal(m.boundary_midpoints(), g["midpoints"])
+    require_reference_build()
+    g = cpu.reference_mesh_from_file(d)
+    assert g is not None and g["n_elem"] == len(q)
+    np.testing.assert_array_equal(m.edges(0), g["edges_interior"])
+    np.testing.assert_array_equal(m.edges(1), g["edges_boundary"])
+    assert m.min_h() == g["min_h"]
+    np.testing.assert_array_equal(m.boundary_midpoints(), g["midpoints"])
 
 
 def test_file_text_is_read_as_the_reference_reads_it(W, tmp_path):
@@ -70,10 +71,10 @@ def test_file_text_is_read_as_the_reference_reads_it(W, tmp_path):
     r = cpu.Mesh.from_file(str(d), "oracle")
     for t in (0, 1):
         np.testing.assert_array_equal(m.edges(t), r.edges(t))
-    if cpu.available("reference"):
-        g = cpu.reference_mesh_from_file(str(d))
-        np.testing.assert_array_equal(m.edges(0), g["edges_interior"])
-        np.testing.assert_array_equal(m.edges(1), g["edges_boundary"])
+    require_reference_build()
+    g = cpu.reference_mesh_from_file(str(d))
+    np.testing.assert_array_equal(m.edges(0), g["edges_interior"])
+    np.testing.assert_array_equal(m.edges(1), g["edges_boundary"])
 
 
 def test_bad_mesh_files_are_errors(W, tmp_path):

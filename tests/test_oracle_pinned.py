@@ -8,7 +8,7 @@ eigen-decomposition for the flux matrices), so agreement here pins it.
 import numpy as np
 import pytest
 
-from conftest import golden, golden_files, rel
+from conftest import golden, golden_files, rel, require_reference_build
 from oracle import cpu
 
 TOL = 1e-13  # FP64 restatement vs reference: only rounding order differs
@@ -171,13 +171,13 @@ def test_oracle_catches_planted_error():
     assert rel(op.rhs(g["u"]), g["rhs"]) > 1e-6
 
 
-@pytest.mark.skipif(not cpu.available("reference"), reason="the reference library is built where its sources are")
 @pytest.mark.parametrize("n", range(2, 10))
 def test_exact_quadrature_every_degree_against_the_reference(n):
     """The oracle's exact-quadrature restatement against the compiled reference for every
     degree the GPU path builds (n = 2..9), all operators, one seeded state."""
     from wavedg_b200 import meshgen as mg
 
+    require_reference_build()
     v, q = mg.perturbed_rect(4, 0.2, seed=n)
     v, q = mg.scrambled(v, q, seed=n + 1)
     rng = np.random.default_rng(n)
@@ -195,13 +195,13 @@ def test_exact_quadrature_every_degree_against_the_reference(n):
     assert rel(x1, x2) < 1e-12
 
 
-@pytest.mark.skipif(not cpu.available("reference"), reason="the reference library is built where its sources are")
 @pytest.mark.parametrize("nv", range(1, 9))
 def test_advection_every_variable_count_against_the_reference(nv):
     """The oracle's constant-coefficient advection against the compiled reference for every
     n_var the GPU path builds (1..8), random symmetric coefficients."""
     from wavedg_b200 import meshgen as mg
 
+    require_reference_build()
     v, q = mg.perturbed_rect(4, 0.2, seed=nv)
     rng = np.random.default_rng(100 + nv)
     A = rng.standard_normal((2, nv, nv))

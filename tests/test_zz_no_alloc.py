@@ -1,8 +1,8 @@
 """wdg_load_gaussians_noalloc: the load-vector entry point for callers that cannot
-allocate device memory (work issued under CUDA graph capture, fixed-memory
-real-time loops, hosts whose allocator owns the GPU).  It must give the same
-load vector as wdg_load_gaussians, call after call, while keeping its source
-table in the library's fixed-size array.  Collected last on purpose."""
+allocate device memory (real-time loops whose memory is fixed before they start,
+hosts whose own allocator has reserved the GPU).  It must give the same load
+vector as wdg_load_gaussians, call after call, while keeping its source table in
+the library's fixed-size array.  Collected last on purpose."""
 import ctypes as C
 
 import numpy as np

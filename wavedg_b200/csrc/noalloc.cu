@@ -3,11 +3,15 @@
 // wdg_load_gaussians stages the Gaussian source table (cx, cy, sigma, amp per
 // source) in a device buffer it allocates on first use and regrows when a call
 // brings more sources.  Some callers cannot let a library allocate device
-// memory once they are running: code that issues its work while a CUDA graph is
-// being captured (cudaMalloc is not allowed there), real-time loops whose memory
-// is fixed when they start, or hosts whose own allocator owns all of the GPU's
-// memory.  For them wdg_load_gaussians_noalloc keeps the table in a fixed-size
-// array that is part of the library image instead.
+// memory once they are running: real-time loops whose memory is fixed when they
+// start (a cudaMalloc can fail there and synchronises the device), or hosts
+// whose own allocator has reserved the GPU's memory.  For them
+// wdg_load_gaussians_noalloc keeps the table in a fixed-size array that is part
+// of the library image instead.
+//
+// The array's device address is looked up once per device and cached for the
+// life of the process; it does not survive cudaDeviceReset, after which this
+// entry point must not be called again.
 #include <cuda_runtime.h>
 
 #include <mutex>

@@ -26,11 +26,52 @@ from __future__ import annotations
 import argparse
 import json
 import math
+import os
 import time
 
 import numpy as np
 
 OMEGA, SIGMA, NE, NCOLLOC = 20.0, 0.05, 128, 5
+
+# the trained network shipped with the package (FNO(grid=512, width=32, modes=16, layers=4,
+# hidden=64)); written by `--save` in the compact format below
+PACKAGED_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "fno_waveholtz_c5.npz")
+
+
+def save_weights(path: str, net, scale: float, meta: dict | None = None) -> None:
+    """Compact weight file: the spectral tensors R* as float16 times a per-tensor power-of-two
+    scale (their entries span a few decades below 1; 11 significant bits are far below what a
+    warm start can resolve), every other parameter as float32, plus the output scale and a
+    JSON record of how the network was trained."""
+    out = {"__scale__": np.array(scale, dtype=np.float64)}
+    for k, v in net.state_dict().items():
+        if k.startswith("R"):
+            e = int(np.ceil(np.log2(max(float(np.abs(v).max()), 1e-30)))) - 14  # max |v| / 2^e < 2^14
+            out[k] = (v / np.float32(2.0 ** e)).astype(np.float16)
+            out[k + ".exp2"] = np.array(e, dtype=np.int32)
+        else:
+            out[k] = v.astype(np.float32)
+    if meta is not None:
+        out["__meta__"] = np.array(json.dumps(meta))
+    np.savez(path, **out)
+
+
+def load_weights(path: str, net) -> float:
+    """Load a file written by save_weights (or a plain float32 state dict with __scale__) into
+    `net`; returns the output scale."""
+    sd = dict(np.load(path))
+    scale = float(sd.pop("__scale__"))
+    sd.pop("__meta__", None)
+    exps = {k[:-5]: int(sd.pop(k)) for k in [k for k in sd if k.endswith(".exp2")]}
+    for k, e in exps.items():
+        sd[k] = sd[k].astype(np.float32) * np.float32(2.0 ** e)
+    net.load_state_dict(sd)
+    return scale
+
+
+def weights_meta(path: str) -> dict:
+    sd = np.load(path)
+    return json.loads(str(sd["__meta__"])) if "__meta__" in sd.files else {}
 
 
 def centers(count: int, seed: int) -> np.ndarray:
@@ -219,19 +260,21 @@ def evaluate(net, fam: Family, count: int, seed: int, scale: float, n_plain: int
     Fp = fam.forcing(cs[:n_plain])
     t.cuda.synchronize()
     t0 = time.perf_counter()
-    plain_W, plain_it = [], []
+    plain_W, plain_it, plain_r = [], [], []
     for F in Fp:
         Wp = t.zeros(fam.ndof, dtype=t.float64, device="cuda")
-        _, it, _ = wh.solve(F, 1e-6, 1000, W=Wp)
+        _, it, r = wh.solve(F, 1e-6, 1000, W=Wp)
         plain_W.append(Wp)
         plain_it.append(it)
+        plain_r.append(float(r))
     t.cuda.synchronize()
     tp = time.perf_counter() - t0
     res["plain_fp64"] = {"solves": n_plain, "seconds": tp, "solves_per_s": n_plain / tp,
-                         "iterations_mean": float(np.mean(plain_it))}
+                         "iterations": [int(i) for i in plain_it], "iterations_mean": float(np.mean(plain_it)),
+                         "residuals": plain_r}
     log(f"  plain FP64: {n_plain} solves in {tp:.1f} s, iterations {plain_it}")
     for arm in arms:
-        secs, it32s, it64s, errs = 0.0, [], [], []
+        secs, it32s, it64s, errs, r64s = 0.0, [], [], [], []
         for b0 in range(0, count, fam.nb):
             blk = cs[b0:b0 + fam.nb]
             if len(blk) < fam.nb:
@@ -246,6 +289,7 @@ def evaluate(net, fam: Family, count: int, seed: int, scale: float, n_plain: int
             assert (st == 0).all() and (r64 < 1e-6).all(), (st, r64)
             it32s += it32.tolist()
             it64s += it64.tolist()
+            r64s += [float(r) for r in r64]
             if b0 == 0:
                 for i in range(n_plain):
                     errs.append((W[i] - plain_W[i]).norm().item() / plain_W[i].norm().item())
@@ -253,6 +297,8 @@ def evaluate(net, fam: Family, count: int, seed: int, scale: float, n_plain: int
         res[f"batched_{arm}"] = {"solves": done, "seconds": secs, "solves_per_s": done / secs,
                                  "fp32_iterations_mean": float(np.mean(it32s)),
                                  "fp64_iterations_mean": float(np.mean(it64s)),
+                                 "fp64_residual_max": float(max(r64s)), "fp64_residuals": r64s,
+                                 "all_converged": bool(max(r64s) < 1e-6),
                                  "rel_diff_vs_plain_fp64": float(max(errs)) if errs else None}
         log(f"  batched {arm}: {done} solves in {secs:.1f} s, FP32 iterations {np.mean(it32s):.1f}, "
             f"FP64 finish {np.mean(it64s):.1f}")
@@ -317,13 +363,14 @@ def main(argv=None):
     ap.add_argument("--data-seed", type=int, default=None, help="seed of the training sources (default 1000 + seed)")
     ap.add_argument("--lr", type=float, default=2e-3, help="peak learning rate")
     ap.add_argument("--save", default=None, help="save the trained network here (default: --weights)")
+    ap.add_argument("--data-net", default=None,
+                    help="weights of a network whose predictions start the training-data solves")
     ap.add_argument("--arms", default="cold,warm", help="batched arms evaluated (cold, warm)")
     ap.add_argument("--time-batch", type=int, default=0, help="only time whole periods of a batch of this many solves")
     ap.add_argument("--periods", type=int, default=3, help="--time-batch: periods timed")
     ap.add_argument("--precision", choices=["fp32", "fp64", "both"], default="both", help="--time-batch precision")
     ap.add_argument("--no-autotune", action="store_true", help="--time-batch: default launch shape")
     a = ap.parse_args(argv)
-    import os
 
     if a.time_batch:
         prec = ("fp32", "fp64") if a.precision == "both" else (a.precision,)
@@ -339,30 +386,35 @@ def main(argv=None):
            "fno": {"layers": 4, "width": 32, "modes": 16, "hidden": 64}}
     loaded = bool(a.weights and os.path.exists(a.weights))
     if loaded:
-        sd = dict(np.load(a.weights))
-        scale = float(sd.pop("__scale__"))
-        net.load_state_dict(sd)
+        scale = load_weights(a.weights, net)
         out["trained"] = "loaded"
     if not loaded or a.finetune:
         t0 = time.perf_counter()
         dseed = 1000 + a.seed if a.data_seed is None else a.data_seed
-        cs, grids = make_dataset(fam, a.train, dseed, a.train_tol, a.grid, net if loaded else None,
-                                 scale if loaded else 1.0)
+        # the network whose predictions start the data solves (they only save iterations:
+        # every solve still runs to the training tolerance)
+        dnet, dscale = (net, scale) if loaded else (None, 1.0)
+        if a.data_net:
+            dnet = FNO(grid=a.grid, width=32, modes=16, layers=4, hidden=64, seed=a.seed)
+            dscale = load_weights(a.data_net, dnet)
+        cs, grids = make_dataset(fam, a.train, dseed, a.train_tol, a.grid, dnet, dscale)
+        del dnet
         if not loaded:
             scale = math.sqrt(grids.square().mean().item())
         grids /= scale
         gen = time.perf_counter() - t0
         hist, ttrain = train(net, cs, grids, a.epochs, lr=a.lr, seed=a.seed, symmetries=not a.no_symmetries)
         out["data"] = {"solutions": a.train, "seed": dseed, "tol": a.train_tol, "seconds": gen,
-                       "symmetries": 1 if a.no_symmetries else 8, "warm_started": loaded}
+                       "symmetries": 1 if a.no_symmetries else 8, "warm_started": loaded or bool(a.data_net)}
         out["training"] = {"epochs": a.epochs, "lr": a.lr, "seconds": ttrain, "rel_rms_error": hist,
-                           "finetune": loaded}
+                           "finetune": loaded, "from_scratch": not loaded}
         del grids
         dst = a.save or a.weights
         if dst:
-            sd = net.state_dict()
-            sd["__scale__"] = np.array(scale)
-            np.savez(dst, **sd)
+            meta = {"fno": out["fno"], "grid": a.grid, "family": out["family"], "data": out["data"],
+                    "training": {k: v for k, v in out["training"].items() if k != "rel_rms_error"},
+                    "final_rel_rms_error": hist[-1], "seed": a.seed}
+            save_weights(dst, net, scale, meta)
     if a.eval:
         out["eval"] = evaluate(net, fam, a.eval, 5000 + a.seed, scale, a.plain, arms=tuple(a.arms.split(",")))
     print(json.dumps(out), flush=True)
