@@ -1,7 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the reference library.
 
     make -C oracle ref          # compiles the reference (needs its sources)
-    python tests/golden/make_golden.py [--exact-quadrature-only | --advection-only]
+    python tests/golden/make_golden.py [--exact-quadrature-only | --advection-only | --reference-meshes]
 
 Every output array is produced by the reference waveDG code compiled from its
 own sources (oracle/_ref/libwdgref.so, driven through oracle/ref_harness.cpp).
@@ -15,6 +15,7 @@ and all interior operators are the reference classes themselves.
 from __future__ import annotations
 
 import os
+import shutil
 import sys
 
 import numpy as np
@@ -27,6 +28,9 @@ from oracle import cpu  # noqa: E402
 from wavedg_b200 import meshgen as mg  # noqa: E402
 
 KIND = "reference"
+# the reference's own mesh files (meshes/<name>/{info,coordinates,elements}.txt)
+REF_DIR = os.environ.get("WDG_REFERENCE_DIR", "/root/reference")
+REF_MESHES = ("Square", "L", "skew")
 
 
 def meshes():
@@ -200,9 +204,35 @@ def opq_fixture(name, v, q, m, n, seed):
     np.savez_compressed(os.path.join(HERE, f"opq_{name}_n{n}.npz"), **out)
 
 
+def reference_meshes():
+    """The reference's mesh files, copied unchanged into tests/golden/meshes/<name>/ (data, read
+    by Mesh2D::from_file, source/Mesh2D.cpp:94-128); per mesh the connectivity the reference's
+    own reader builds from them (mesh_file_<name>.npz), and operator fixtures on all three
+    (their sides meet with every relative orientation, delta = -1 included)."""
+    cases = {"Square": [6], "L": [5], "skew": [4]}
+    for k, name in enumerate(REF_MESHES):
+        src, dst = os.path.join(REF_DIR, "meshes", name), os.path.join(HERE, "meshes", name)
+        os.makedirs(dst, exist_ok=True)
+        for f in ("info.txt", "coordinates.txt", "elements.txt"):
+            shutil.copyfile(os.path.join(src, f), os.path.join(dst, f))
+        g = cpu.reference_mesh_from_file(dst)
+        v = np.loadtxt(os.path.join(dst, "coordinates.txt"), dtype=np.float64).reshape(-1, 2)
+        q = np.loadtxt(os.path.join(dst, "elements.txt"), dtype=np.int32).reshape(-1, 4)
+        np.savez_compressed(os.path.join(HERE, f"mesh_file_{name}.npz"), verts=v, quads=q,
+                            edges_interior=g["edges_interior"], edges_boundary=g["edges_boundary"], min_h=g["min_h"],
+                            midpoints=g["midpoints"])
+        m = cpu.Mesh(v, q, KIND)
+        for n in cases[name]:
+            op_fixture(f"file{name}", v, q, m, n, 3000 + 100 * k + n)
+
+
 def main():
     if not cpu.available("reference"):
         raise SystemExit("build the reference first: make -C oracle ref")
+    if "--reference-meshes" in sys.argv:
+        reference_meshes()
+        print("reference-mesh fixtures written to", HERE)
+        return
     qcases = {"scrambled6": [3, 5], "lshape3": [4]}
     acases = {"scrambled6": [(5, 1), (4, 2)], "lshape3": [(3, 4)]}
     if "--advection-only" in sys.argv:

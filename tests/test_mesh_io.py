@@ -109,3 +109,25 @@ def test_snapshot_bytes_and_round_trip(W, tmp_path):
         W.read_file(f, np.zeros(1233))
     W.to_file(str(tmp_path / "empty"), np.zeros(0))
     assert os.path.getsize(tmp_path / "empty") == 0
+
+
+@pytest.mark.parametrize("name", ["Square", "L", "skew"])
+def test_reference_mesh_files(W, name):
+    """The reference's own mesh files (copied into tests/golden/meshes/ by make_golden.py
+    --reference-meshes): the library's reader must build exactly the connectivity, min_h and
+    boundary midpoints that the reference's Mesh2D::from_file built from the same files
+    (fixture), and the oracle's reader the same."""
+    from conftest import GOLDEN, golden
+
+    d = os.path.join(GOLDEN, "meshes", name)
+    g = golden(f"mesh_file_{name}.npz")
+    m = W.Mesh2D.from_file(d)
+    assert m.n_elem() == len(g["quads"])
+    np.testing.assert_array_equal(m.edges(0), g["edges_interior"])
+    np.testing.assert_array_equal(m.edges(1), g["edges_boundary"])
+    assert m.min_h() == float(g["min_h"])
+    np.testing.assert_array_equal(m.boundary_midpoints(), g["midpoints"])
+    np.testing.assert_array_equal(W.Mesh2D.from_vertices(g["verts"], g["quads"]).edges(0), g["edges_interior"])
+    r = cpu.Mesh.from_file(d, "oracle")
+    for t in (0, 1):
+        np.testing.assert_array_equal(r.edges(t), m.edges(t))
