@@ -34,6 +34,8 @@ UNIT = "DOF-stage/s"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM = 6650.0  # GB/s, used only when MEASURED_PEAKS.json is absent
 REF_TIME_BUDGET = 150.0  # seconds of reference CPU work in --impl reference
+LEGS = ("waveholtz_c3", "learned_warm_start", "exact_quadrature", "advection", "decomposition", "waveholtz_config4")
+T_START = time.perf_counter()
 
 
 def parse():
@@ -52,6 +54,11 @@ def parse():
     ap.add_argument("--ref-procs", type=int, default=0, help="--impl reference: host processes (0: one per core)")
     ap.add_argument("--tile", type=int, default=0, help="elements per block (0: autotune)")
     ap.add_argument("--stages", type=int, default=0, help="pipeline depth with --tile (0: default)")
+    ap.add_argument("--legs", default="", help=f"companion measurements to run (comma list of {','.join(LEGS)}; "
+                    "default: all)")
+    ap.add_argument("--budget", type=float, default=1200.0,
+                    help="seconds the whole run should take; the batched-solve leg stops its FP32 phase in time "
+                         "(0: no limit)")
     ap.add_argument("--kernel", choices=["auto", "warp", "tiled", "ws"], default="auto",
                     help="fused-kernel family (auto: the autotuner picks)")
     return ap.parse_args()
@@ -258,6 +265,10 @@ def run_ours(args, rank, world, local_rank):
                          "frac": b32 / (ms32 / args.steps / 1e3) / 1e9 / peak}
         del s32
 
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(v, q, bc, args.P + 1, dt, sys_.download())
+
     # single-GPU companion measurements: skipped under torchrun so that a multi-GPU run holds
     # its GPUs only for the replicated RK4 measurement
     def companion(name, fn, *a, **kw):
@@ -267,17 +278,25 @@ def run_ours(args, rank, world, local_rank):
         except Exception as e:  # noqa: BLE001
             extra[name] = {"error": f"{type(e).__name__}: {e}"}
 
-    if not args.no_extras and not args.no_waveholtz and args.precision == "fp64" and world == 1:
+    legs = set(args.legs.split(",")) if args.legs else set(LEGS)
+    want = lambda name: name in legs and not args.no_extras and args.precision == "fp64" and world == 1  # noqa: E731
+    wh_ok = not args.no_waveholtz
+    if want("waveholtz_c3") and wh_ok:
         companion("waveholtz_c3", waveholtz_c3, local_rank)
-        companion("waveholtz_batched", waveholtz_batched, local_rank)
-    if not args.no_extras and args.precision == "fp64" and world == 1:
+    if want("learned_warm_start") and wh_ok:
+        companion("learned_warm_start", learned_warm_start, local_rank)
+    if want("exact_quadrature"):
         companion("exact_quadrature", exact_quadrature, local_rank, cpu_leg=not args.no_cpu_baseline)
+    if want("advection"):
         companion("advection", advection, local_rank, cpu_leg=not args.no_cpu_baseline)
+    if want("decomposition"):
         companion("decomposition", decomposition, local_rank)
+    if want("waveholtz_config4") and wh_ok:
+        # last: its FP32 phase gets what is left of the run's time budget (0: no limit), keeping
+        # about three minutes for its FP64 finish and the plain-FP64 periods
+        left = args.budget - (time.perf_counter() - T_START) - 180.0 if args.budget > 0 else 1e9
+        companion("waveholtz_config4", waveholtz_config4, local_rank, deadline=max(60.0, left))
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(v, q, bc, args.P + 1, dt, sys_.download())
 
     if dist is not None:
         dist.barrier(device_ids=[local_rank])
@@ -355,26 +374,67 @@ def waveholtz_c3(device: int, seed: int = 3) -> dict:
     return out
 
 
-def waveholtz_batched(device: int, count: int = 16, seed: int = 4) -> dict:
-    """Batched WaveHoltz on a draw from the batched-solve distribution at a quarter of its mesh
-    sizes (n in {16, 24, 32, 48, 64} elements per side instead of {64, ..., 256}): omega uniform in
-    [10, 40], P in {3, 4, 6}, 1-4 Gaussian sources (sigma 0.05, centres in [-0.8, 0.8]^2, N(0, 1)
-    amplitudes), outflow, tolerance 1e-6.  The same problems solved (a) one at a time with plain
-    FP64 WaveHoltz and (b) as one batch: FP32 stepping with FP64 filter / residual until the
-    FP32 floor (3e-6 or a 3-iteration stall), then an FP64 batch from those iterates to 1e-6."""
-    import torch
+def learned_warm_start(device: int, count: int = 32, seed: int = 7000, n_plain: int = 4) -> dict:
+    """Learned warm start on the single-solve Helmholtz family (128 x 128 uniform quads, P = 4,
+    omega = 20, one Gaussian source with x0 ~ U[-0.5, 0.5]^2, outflow) with the network shipped
+    in wavedg_b200/weights/ (trained on the family's own solutions; its training record is
+    stored in the file).  `count` fresh seeded problems (seeds disjoint from the training
+    data's) solved three ways to FP64 residual 1e-6: plain FP64 WaveHoltz one solve at a time
+    (n_plain of them), batched FP32 + FP64 finish from zero, and the same from the network's
+    prediction (prediction time included).  The plain iteration decides convergence in all."""
+    from wavedg_b200 import warmstart as ws
+    from wavedg_b200.fno import FNO
 
-    import wavedg_b200 as W
+    path = ws.PACKAGED_WEIGHTS
+    net = FNO(grid=512, width=32, modes=16, layers=4, hidden=64, device=device)
+    scale = ws.load_weights(path, net)
+    fam = ws.Family(count, device=device)
+    res = ws.evaluate(net, fam, count, seed, scale, n_plain=n_plain, arms=("cold", "warm"), log=lambda *_: None)
+    meta = ws.weights_meta(path)
+    res["workload"] = f"waveholtz_128x128_P4_omega20_outflow_{count}_fresh_problems_tol1e-6"
+    res["weights"] = {"file": os.path.relpath(path, ROOT), "training": meta}
+    res["speedup"] = res["speedup_batched_warm_vs_plain"]
+    return res
 
+
+def config4_problems(count: int = 64, seed: int = 4):
+    """The batched-solve distribution: per solve omega ~ U[10, 40], an n x n uniform quad mesh of
+    [-1, 1]^2 with n ~ U{64, 96, 128, 192, 256}, P ~ U{3, 4, 6}, 1-4 Gaussian sources (sigma 0.05,
+    centres ~ U[-0.8, 0.8]^2, amplitudes ~ N(0, 1)), outflow boundary."""
     rng = np.random.default_rng(seed)
     probs = []
     for _ in range(count):
-        n = int(rng.choice([16, 24, 32, 48, 64]))
+        n = int(rng.choice([64, 96, 128, 192, 256]))
         P = int(rng.choice([3, 4, 6]))
         om = float(rng.uniform(10.0, 40.0))
         k = int(rng.integers(1, 5))
         probs.append((n, P, om, rng.uniform(-0.8, 0.8, size=(k, 2)), rng.standard_normal(k)))
-    s64, s32, Fs, whs = [], [], [], []
+    return probs
+
+
+def waveholtz_config4(device: int, count: int = 64, seed: int = 4, deadline: float = 720.0,
+                      chunk_iters: int = 30) -> dict:
+    """Batched WaveHoltz on 64 solves of the batched-solve distribution (config4_problems), to
+    relative residual 1e-6.
+
+    batched   FP32 stepping with FP64 filter / residual in one batch until each solve reaches
+              3e-6 (or stalls 3 iterations on the FP32 floor), then an FP64 batch from those
+              iterates to 1e-6.  The FP32 phase runs in calls of at most `chunk_iters`
+              iterations, each on a batch of the solves still running (every later call starts
+              from the iterate with the |pi0| measured before, so nothing is repeated); it stops
+              at `deadline` seconds, and the record then says which solves were unfinished.
+    plain     plain FP64 WaveHoltz, one solve at a time, is timed as one period of every solve
+              (WaveHoltz::S after a warm-up period) times the periods a plain solve of it runs:
+              its iterations + 1 (the pi0 period), the iterations being those the batch needed
+              (FP32 + FP64 iterations; the same fixed-point map).  The rule is checked on the two
+              solves with the fewest DOF-steps per period, solved in full.
+    Wall times on the host around synchronous calls."""
+    import torch
+
+    import wavedg_b200 as W
+
+    probs = config4_problems(count, seed)
+    s64, s32, Fs, meshes, bases, bcs = [], [], [], [], [], []
     for (n, P, om, cs, amps) in probs:
         mesh = W.Mesh2D.uniform_rect(n, -1.0, 1.0, n, -1.0, 1.0)
         basis = W.QuadratureRule.quadrature_rule(P + 1, W.QuadratureRule.GaussLobatto)
@@ -383,42 +443,111 @@ def waveholtz_batched(device: int, count: int = 16, seed: int = 4) -> dict:
         s64.append(a)
         s32.append(W.WaveSystem(mesh, basis, bc, precision="fp32", device=device))
         F = torch.zeros(a.ndof, dtype=torch.float64, device="cuda")
-        a.load_gaussians(cs, [0.05] * len(amps), amps * om ** 2, 1.0, 0, False, out=F)
+        a.load_gaussians(cs, [0.05] * len(amps), amps, 1.0, 0, False, out=F)
         Fs.append(F)
-        whs.append(W.WaveHoltz(om, mesh, basis, bc, True, system=a))
+        meshes.append(mesh)
+        bases.append(basis)
+        bcs.append(bc)
     oms = [p[2] for p in probs]
-    ndof = sum(a.ndof for a in s64)
-    # (a) plain FP64, one solve at a time
-    Wp, itp = [], []
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for F, wh in zip(Fs, whs):
-        Wx = torch.zeros_like(F)
-        _, it, _ = wh.solve(F, 1e-6, 2000, W=Wx)
-        Wp.append(Wx)
-        itp.append(it)
-    torch.cuda.synchronize()
-    t_plain = time.perf_counter() - t0
-    # (b) batched FP32 then FP64 finish
+    ndof = np.array([a.ndof for a in s64], dtype=np.int64)
+
+    # ---- batched: FP32 phase in chunks, then the FP64 finish
     b32 = W.WaveHoltzBatch(s32, oms)
-    b64 = W.WaveHoltzBatch(s64, oms)
-    b32.autotune(64)
+    tune_ms = b32.autotune(32)
+    launch = b32.launch_config()
+    nt = np.array([b32.params(i)[2] for i in range(count)], dtype=np.int64)
     Wb = [torch.zeros_like(F) for F in Fs]
+    it32 = np.zeros(count, dtype=np.int64)
+    pi0n = np.zeros(count)
+    started = np.zeros(count, dtype=bool)
+    st32 = np.full(count, -1)
+    active = list(range(count))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    _, it32, _, _ = b32.solve(Fs, 3e-6, 2000, W=Wb, stall_limit=3)
-    _, it64, r64, st = b64.solve(Fs, 1e-6, 2000, W=Wb, warm=[1] * count, pi0_norm=b32.pi0_norm)
+    calls = 0
+    while active and time.perf_counter() - t0 < deadline:
+        b = b32 if calls == 0 else W.WaveHoltzBatch([s32[i] for i in active], [oms[i] for i in active])
+        if calls > 0:
+            b.set_launch(launch["rounds"], launch["ring"])
+        Wl = [Wb[i] for i in active]
+        _, it, _, st = b.solve([Fs[i] for i in active], 3e-6, chunk_iters, W=Wl, warm=started[active].astype(np.int32),
+                               stall_limit=3, pi0_norm=pi0n[active])
+        for k, i in enumerate(active):
+            it32[i] += it[k]
+            pi0n[i] = b.pi0_norm[k]
+            st32[i] = st[k]
+        started[active] = True
+        active = [i for k, i in enumerate(active) if st[k] == 1]
+        calls += 1
+        del b
     torch.cuda.synchronize()
-    t_batch = time.perf_counter() - t0
-    err = max((Wb[i] - Wp[i]).norm().item() / Wp[i].norm().item() for i in range(count))
-    return {"workload": f"waveholtz_batch_{count}_solves_n16-64_P3-6_omega10-40_tol1e-6",
-            "solves": count, "total_dof": ndof,
-            "plain_fp64": {"seconds": t_plain, "solves_per_s": count / t_plain, "iterations_mean": float(np.mean(itp))},
-            "batched_fp32_fp64": {"seconds": t_batch, "solves_per_s": count / t_batch,
-                                  "fp32_iterations_mean": float(np.mean(it32)),
-                                  "fp64_iterations_mean": float(np.mean(it64)),
-                                  "all_converged": bool((st == 0).all() and (r64 < 1e-6).all()),
-                                  "max_rel_diff_vs_plain": err, "launch": b32.launch_config()},
+    t_fp32 = time.perf_counter() - t0
+    finished = not active
+    del b32
+    b64 = W.WaveHoltzBatch(s64, oms)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    _, it64, r64, st64 = b64.solve(Fs, 1e-6, 200, W=Wb, warm=[1] * count, pi0_norm=pi0n)
+    torch.cuda.synchronize()
+    t_fp64 = time.perf_counter() - t1
+    t_batch = t_fp32 + t_fp64
+    del b64
+    # DOF-stage updates the FP32 phase ran: every iteration is one forced period (a zero start's
+    # first period yields pi0 and counts as iteration 1; later calls start from W with |pi0| known)
+    dofstage32 = float(np.sum(ndof * 5 * nt * it32))
+    # algorithmic bytes per DOF-stage of the FP32 batched stage kernel: u, k in and u', k' out
+    # (4 B each; stage 1 reads no k), FP32 forcing in, FP64 filter in and out on the fifth stage:
+    # (16 + 3 x 20 + 36) / 5 = 22.4 B
+    peak, _ = peak_hbm()
+    achieved = 22.4 * dofstage32 / t_fp32 / 1e9
+
+    # ---- plain FP64: one period per solve, then the iteration rule
+    per = np.zeros(count)
+    for i in range(count):
+        wh = W.WaveHoltz(oms[i], meshes[i], bases[i], bcs[i], True, system=s64[i])
+        w = torch.zeros_like(Fs[i])
+        wh.pi0(w, Fs[i])  # warm-up: records the period's graph
+        torch.cuda.synchronize()
+        ts = time.perf_counter()
+        wh.S(w)
+        torch.cuda.synchronize()
+        per[i] = time.perf_counter() - ts
+        del wh, w
+    plain_iters = it32 + it64
+    t_plain_est = per * (plain_iters + 1)
+    check = []
+    for i in np.argsort(ndof * nt)[:2]:
+        wh = W.WaveHoltz(oms[i], meshes[i], bases[i], bcs[i], True, system=s64[i])
+        w = torch.zeros_like(Fs[i])
+        torch.cuda.synchronize()
+        ts = time.perf_counter()
+        _, itp, _ = wh.solve(Fs[i], 1e-6, 2000, W=w)
+        torch.cuda.synchronize()
+        tm = time.perf_counter() - ts
+        check.append({"solve": int(i), "iterations": int(itp), "batch_iterations": int(plain_iters[i]),
+                      "seconds": tm, "estimated_seconds": float(t_plain_est[i]),
+                      "rel_diff_vs_batched": (Wb[i] - w).norm().item() / w.norm().item()})
+        del wh, w
+    t_plain = float(np.sum(t_plain_est))
+    done = int(np.sum((st64 == 0) & (r64 < 1e-6)))
+    return {"workload": f"waveholtz_batch_{count}_solves_n64-256_P3-6_omega10-40_1-4src_tol1e-6",
+            "solves": count, "total_dof": int(ndof.sum()), "seed": seed,
+            "per_solve": [{"n": p[0], "P": p[1], "omega": round(p[2], 4), "sources": len(p[4]), "ndof": int(ndof[i]),
+                           "nt": int(nt[i]), "fp32_iterations": int(it32[i]), "fp64_iterations": int(it64[i]),
+                           "residual": float(r64[i]), "plain_period_s": float(per[i])}
+                          for i, p in enumerate(probs)],
+            "batched_fp32_fp64": {"seconds": t_batch, "fp32_seconds": t_fp32, "fp64_seconds": t_fp64,
+                                  "solves_per_s": count / t_batch, "fp32_calls": calls,
+                                  "fp32_phase_finished": finished, "converged": done,
+                                  "all_converged": bool(finished and done == count),
+                                  "max_residual": float(np.max(r64)), "launch": launch,
+                                  "autotune_ms_per_step": tune_ms,
+                                  "fp32_dof_stage_per_s": dofstage32 / t_fp32,
+                                  "fp32_stage_kernel_hbm": {"bytes_per_dof_stage": 22.4, "achieved_gbs": achieved,
+                                                            "peak_gbs": peak, "frac": achieved / peak}},
+            "plain_fp64": {"seconds_estimated": t_plain, "solves_per_s": count / t_plain,
+                           "rule": "per solve: one timed period x (batch FP32 + FP64 iterations + 1)",
+                           "period_seconds_total": float(per.sum()), "checked_in_full": check},
             "speedup": t_plain / t_batch}
 
 

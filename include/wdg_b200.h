@@ -128,6 +128,20 @@ int wdg_wave_get_launch(const wdg_wave *wave, int *family, int *elems_per_block,
 int wdg_wave_autotune(wdg_wave *wave, int steps, float *best_ms_per_step);
 /* Mesh2D::element_metrics(basis).physical_coordinates(): xy (2, n, n, n_elem) */
 int wdg_wave_node_coords(wdg_wave *wave, double *xy);
+/* Failure detection (no counterpart in the reference, which has no device-side waits): every
+ * wait of the fused stage kernels on a copy completion gives up after `seconds` (default 2),
+ * records it in the handle's device error word and lets the kernel finish; the next
+ * synchronising call returns WDG_ERR_TIMEOUT and clears the word, and the handle stays usable. */
+int wdg_wave_set_wait_limit(wdg_wave *wave, double seconds);
+/* Test hooks (no counterpart in the reference) that exercise that failure detection without
+ * faulting the GPU.  wdg_test_skip_chunk: in the first stage launch of the next RK4 call that
+ * takes the warp-specialised kernel, every CTA leaves its chunk number `chunk` unloaded (-1:
+ * none), so the waits on that chunk run out.  wdg_test_set_partner: overwrites the fused
+ * kernels' partner offset of (elem, side) (returns the previous value in *previous); an offset
+ * outside the state makes the kernels skip that trace and report WDG_ERR_ARG ("neighbour
+ * index outside the mesh") instead of reading out of bounds. */
+int wdg_test_skip_chunk(wdg_wave *wave, int chunk);
+int wdg_test_set_partner(wdg_wave *wave, int elem, int side, int offset, int *previous);
 
 /* ---- Operator::action drop-ins, FP64, accumulate (y += A x) ---- */
 int wdg_div_action(wdg_wave *wave, const double *u, double *du);   /* Div<true>::action (source/Div.cpp:131-196) */
@@ -192,6 +206,18 @@ int wdg_halo_put(wdg_wave *wave, int buffer, long long offset, const void *src, 
 /* RK4 stage `stage` (0..4) of ode::RungeKutta4::step on the resident state: reads buffer
  * 0, 1, 2, 1, 2 and writes 1, 2, 1, 2, 0; the stage's input halo must be filled first */
 int wdg_rk4_stage(wdg_wave *wave, int stage, double dt);
+/* wdg_rk4_stage of the step that starts at time t, with the terms WaveHoltz adds
+ * (source/WaveHoltz.cpp:55-121): F (device, the handle's precision, NULL for none) enters the
+ * RHS as F * (-sin(omega (t + c_stage dt)) / omega); at stage 4, acc (device FP64, NULL for
+ * none) accumulates acc_c * (the new state), the period filter's term of this step. */
+int wdg_rk4_stage_forced(wdg_wave *wave, int stage, double dt, double t, const void *F, double omega, double *acc,
+                         double acc_c);
+/* Mesh2D::distribute's element -> rank maps, computed on the host without MPI
+ * (source/Mesh2D.cpp:233-382): method 0 recursive coordinate bisection (rcb), 1 reverse
+ * Cuthill-McKee blocks (rcm).  e2p: n_elem ranks in [0, n_parts).  The rcb principal axis takes
+ * the mean of y from y and cuts a part with zero covariance across its axis of larger
+ * variance (the reference averages x for both means and divides by the covariance). */
+int wdg_mesh_partition(const wdg_mesh *mesh, int n_parts, int method, int *e2p);
 
 /* ---- exact quadrature (approx_quad = false), FP64 ---- */
 /* WaveEquation(mesh, basis, false) (source/WaveEquation.cpp:5-30: Div<false>, EdgeFlux<false>),

@@ -180,3 +180,116 @@ def test_two_gloo_ranks_exchange_halos(W):
         assert pr.exitcode == 0
     for rank, nhalo, bad in res:
         assert nhalo > 0 and bad == 0, (rank, nhalo, bad)
+
+
+def _rcb_restated(centres, nparts):
+    """Recursive coordinate bisection as source/Mesh2D.cpp:233-294 describes it (principal axis
+    of the part's centres, smallest-prime-divisor equal-count cuts, new ranks in breadth-first
+    order), with the y mean taken from y; for centres whose projections are all distinct."""
+    e2p = np.zeros(len(centres), dtype=np.int32)
+    queue = [np.arange(len(centres))]
+    parts = [nparts]
+    rank = 1
+    while queue:
+        ids, p = queue.pop(0), parts.pop(0)
+        x = centres[ids]
+        m = x.mean(axis=0)
+        c = np.cov(x.T)
+        vx, vy, cv = c[0, 0], c[1, 1], c[0, 1]
+        if cv != 0.0:
+            ex, ey = (np.sqrt((vx - vy) ** 2 + 4 * cv * cv) + vx - vy) / (2 * cv), 1.0
+        else:
+            ex, ey = (1.0, 0.0) if vx >= vy else (0.0, 1.0)
+        pc = ex * (x[:, 0] - m[0]) + ey * (x[:, 1] - m[1])
+        d = next(k for k in range(2, p + 1) if p % k == 0 and all(k % j for j in range(2, int(k ** 0.5) + 1)))
+        order = ids[np.argsort(pc, kind="stable")]
+        pos = [k * len(ids) // d for k in range(d + 1)]
+        for k in range(1, d):  # the first piece keeps the part's rank
+            e2p[order[pos[k]:pos[k + 1]]] = rank
+            rank += 1
+        if p // d > 1:
+            for k in range(d):
+                queue.append(order[pos[k]:pos[k + 1]])
+                parts.append(p // d)
+    return e2p
+
+
+@pytest.mark.parametrize("world", [2, 3, 4, 6, 8, 9])
+def test_rcb_partition_matches_its_restatement(W, world):
+    from wavedg_b200 import decomp
+    from wavedg_b200 import meshgen as mg
+
+    v, q = mg.perturbed_rect(12, 0.2, seed=world)
+    v, q = mg.scrambled(v, q, seed=world + 1)
+    m = W.Mesh2D.from_vertices(v, q)
+    e2p = decomp.partition_mesh(m, world, "rcb")
+    centres = v[q].mean(axis=1)
+    want = _rcb_restated(centres, world)
+    # ranks are equal as sets of elements (the restatement numbers them the same way)
+    np.testing.assert_array_equal(e2p, want)
+    sizes = np.bincount(e2p, minlength=world)
+    assert sizes.min() > 0 and sizes.max() - sizes.min() <= 2
+    np.testing.assert_array_equal(decomp.partition_mesh(m, world, "rcb"), e2p)
+
+
+def test_rcb_cuts_a_square_into_quadrants_and_rcm_into_blocks(W):
+    from wavedg_b200 import decomp
+
+    m = W.Mesh2D.uniform_rect(16, -1.0, 1.0, 16, -1.0, 1.0)
+    e2p = decomp.partition_mesh(m, 4, "rcb").reshape(16, 16)  # [row (y), column (x)]
+    for r in range(4):
+        rows, cols = np.nonzero(e2p == r)
+        assert len(rows) == 64 and np.ptp(rows) == 7 and np.ptp(cols) == 7
+    for world in (1, 3, 5, 16):
+        e = decomp.partition_mesh(m, world, "rcm")
+        sizes = np.bincount(e, minlength=world)
+        assert sizes.min() > 0 and sizes.max() - sizes.min() <= 1
+
+
+def test_partition_errors(W):
+    from wavedg_b200 import decomp
+    from wavedg_b200 import meshgen as mg
+
+    m = W.Mesh2D.uniform_rect(4, -1.0, 1.0, 4, -1.0, 1.0)
+    for bad in (0, 17):
+        with pytest.raises(W.WdgError):
+            decomp.partition_mesh(m, bad)
+    # two squares with no shared edge: rcm cannot order a disconnected mesh
+    v1, q1 = mg.uniform_rect(2, 0.0, 1.0, 2, 0.0, 1.0)
+    v2, q2 = mg.uniform_rect(2, 2.0, 3.0, 2, 0.0, 1.0)
+    m2 = W.Mesh2D.from_vertices(np.vstack([v1, v2]), np.vstack([q1, q2 + len(v1)]))
+    with pytest.raises(W.WdgError, match="not connected"):
+        decomp.partition_mesh(m2, 2, "rcm")
+    assert len(np.unique(decomp.partition_mesh(m2, 2, "rcb"))) == 2
+
+
+def _allreduce_worker(rank, world, port, q):
+    import torch.distributed as dist
+
+    from wavedg_b200 import decomp
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        q.put((rank, decomp.dist_allreduce()([rank + 1.0, 0.5 * rank])))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_sum_the_norms(W):
+    """The WaveHoltz norm / error sums (source/linalg.cpp:102-131) over two gloo ranks."""
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_allreduce_worker, args=(r, 2, port, q)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    res = [q.get(timeout=180) for _ in procs]
+    for pr in procs:
+        pr.join(timeout=60)
+        assert pr.exitcode == 0
+    for _, sums in res:
+        assert sums == [3.0, 0.5]

@@ -71,6 +71,8 @@ SIGNATURES = {
     "wdg_halo_gather": ([_v, _i, _v, _i, _v], _i),
     "wdg_halo_put": ([_v, _i, _ll, _v, _ll], _i),
     "wdg_rk4_stage": ([_v, _i, _d], _i),
+    "wdg_rk4_stage_forced": ([_v, _i, _d, _d, _v, _d, _v, _d], _i),
+    "wdg_mesh_partition": ([_v, _i, _i, _v], _i),
     "wdg_write_raw": ([C.c_char_p, _ll, _v], _i),
     "wdg_read_raw": ([C.c_char_p, _ll, _v], _i),
     "wdg_mesh_from_tables": ([_i, _v, _i, _v, _i, _v, _vp], _i),
@@ -94,6 +96,9 @@ SIGNATURES = {
     "wdg_wave_get_launch": ([_v, _ip, _ip, _ip, _ip], _i),
     "wdg_wave_autotune": ([_v, _i, C.POINTER(C.c_float)], _i),
     "wdg_wave_node_coords": ([_v, _v], _i),
+    "wdg_wave_set_wait_limit": ([_v, _d], _i),
+    "wdg_test_skip_chunk": ([_v, _i], _i),
+    "wdg_test_set_partner": ([_v, _i, _i, _i, _ip], _i),
     "wdg_div_action": ([_v, _v, _v], _i),
     "wdg_wave_action": ([_v, _v, _v], _i),
     "wdg_wavebc_action": ([_v, _v, _v], _i),

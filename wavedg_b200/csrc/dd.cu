@@ -152,4 +152,21 @@ extern "C"
         DeviceScope g(w->device);
         return w->precision == WDG_FP32 ? rk4_stage<float>(w, stage, dt) : rk4_stage<double>(w, stage, dt);
     }
+
+    int wdg_rk4_stage_forced(wdg_wave *w, int stage, double dt, double t, const void *F, double omega, double *acc,
+                             double acc_c)
+    {
+        if (!w || stage < 0 || stage > 4 || (F && !(omega != 0.0)))
+            return fail(WDG_ERR_ARG, "wdg_rk4_stage_forced: stage must be 0..4 and omega nonzero with a forcing");
+        DeviceScope g(w->device);
+        bool dev = true;
+        if (F)
+            WDG_TRY(is_device_ptr(w, F, dev));
+        if (dev && acc)
+            WDG_TRY(is_device_ptr(w, acc, dev));
+        if (!dev)
+            return fail(WDG_ERR_ARG, "wdg_rk4_stage_forced: F and acc must be device arrays");
+        return w->precision == WDG_FP32 ? rk4_stage<float>(w, stage, dt, t, F, omega, acc, acc_c)
+                                        : rk4_stage<double>(w, stage, dt, t, F, omega, acc, acc_c);
+    }
 }

@@ -183,10 +183,11 @@ namespace wdg
         asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
         return t;
     }
-    // bounded wait: gives up after kWaitLimitNs of wall time (the copies it waits
-    // for take microseconds; the limit only guards against a lost completion)
-    constexpr uint64_t kWaitLimitNs = 2000000000ull;
-    __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+    // bounded wait: gives up after limit_ns of wall time (the copies it waits for take
+    // microseconds; the limit only guards against a lost completion).  Stage launches pass the
+    // handle's limit (StageArgs::wait_ns, 2 s unless set); other kernels use the default.
+    __device__ __forceinline__ uint64_t wait_limit(unsigned long long ns) { return ns ? ns : kWaitLimitNs; }
+    __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64_t limit_ns = kWaitLimitNs)
     {
         if (mbar_try_wait(bar, parity))
             return true;
@@ -195,7 +196,7 @@ namespace wdg
         {
             if (mbar_try_wait_sleep(bar, parity))
                 return true;
-            if (globaltimer_ns() - t0 > kWaitLimitNs)
+            if (globaltimer_ns() - t0 > limit_ns)
                 return false;
         }
     }
@@ -464,7 +465,7 @@ namespace wdg
             const bool tout = RK && a.tma_out && (k + 1) * E <= a.nel;
 
             // every thread waits (sleeping) on this tile's bulk loads
-            if (tin && !mbar_wait(&bars[b], (it / S) & 1))
+            if (tin && !mbar_wait(&bars[b], (it / S) & 1, wait_limit(a.wait_ns)))
                 bad = 1;
             if (!tin)
             {
@@ -617,7 +618,7 @@ namespace wdg
                     {
                         const int kq = k + q * G;
                         if (kq < ntiles && tma_tile(kq))
-                            mbar_wait(&bars[(it + q) % S], ((it + q) / S) & 1);
+                            mbar_wait(&bars[(it + q) % S], ((it + q) / S) & 1, wait_limit(a.wait_ns));
                     }
                     bulk_wait_all();
                 }

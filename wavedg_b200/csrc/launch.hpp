@@ -49,6 +49,9 @@ namespace wdg
         unsigned *err;        // device error word (bit 0: wait timeout, bit 1: bad neighbour index)
         int nread;            // values of u neighbour traces may come from (0: nel * 3 n^2; a domain
                               // of a decomposed mesh appends its halo traces after its elements)
+        unsigned long long wait_ns; // limit of every bounded device-side wait (0: kWaitLimitNs)
+        int test_skip;        // test hook (family 2): 1 + the number of the chunk every CTA leaves
+                              // unloaded, so the waits on it run out; 0 (none) in every other launch
     };
 
     struct Geometry
@@ -77,6 +80,9 @@ namespace wdg
     size_t ws_smem_bytes(int n, bool fp32, int chunk, int ring);
     constexpr int kWsDefaultRing = 2;
     int ws_default_chunk(int n, bool fp32);   // most rounds (<= 4) whose default ring fits 3 CTAs per SM
+
+    // default limit of a bounded device-side wait (a lost copy completion; never reached otherwise)
+    constexpr unsigned long long kWaitLimitNs = 2000000000ull;
 
     // warp-specialised stage kernels: one producer warp + kWsConsumers consumer warps per CTA
     constexpr int kWsConsumers = 4;

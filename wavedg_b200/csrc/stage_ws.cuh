@@ -613,21 +613,24 @@ namespace wdg
             c.el0 = ((int)blockIdx.x + m * G) * C;
             c.ne = min(C, a.nel - c.el0);
         };
+        const uint64_t wlim = wait_limit(a.wait_ns);
 
         if (warp == kWsConsumers)
         {
             // ------------------------------------------------------------ producer
+            // test hook: chunk test_skip - 1 is never loaded, so every wait on it runs out
             for (int m = 0; m < min(S, M); ++m)
             {
                 at(m);
-                ws_load<N, Real, EXTRA>(c, slots + (m % S) * L.slot, &full[m % S], lane);
+                if (m + 1 != a.test_skip)
+                    ws_load<N, Real, EXTRA>(c, slots + (m % S) * L.slot, &full[m % S], lane);
             }
             int m = 0;
             for (; m < M; ++m)
             {
                 const int q = m % S;
                 // a warp-uniform verdict, so no lane leaves while others go on
-                if (!__all_sync(0xffffffffu, mbar_wait(&done[q], (m / S) & 1)))
+                if (!__all_sync(0xffffffffu, mbar_wait(&done[q], (m / S) & 1, wlim)))
                     break;
                 at(m);
                 ws_store<N, Real, EXTRA>(c, slots + q * L.slot, lane);
@@ -637,7 +640,8 @@ namespace wdg
                         bulk_wait_read(); // the store above has read the slot
                     __syncwarp();
                     at(m + S);
-                    ws_load<N, Real, EXTRA>(c, slots + q * L.slot, &full[q], lane);
+                    if (m + S + 1 != a.test_skip)
+                        ws_load<N, Real, EXTRA>(c, slots + q * L.slot, &full[q], lane);
                 }
             }
             if (m < M)
@@ -647,7 +651,7 @@ namespace wdg
                 {
                     atomicOr(a.err, 1u);
                     for (int r = m; r < min(m + S, M); ++r)
-                        mbar_wait(&full[r % S], (r / S) & 1);
+                        mbar_wait(&full[r % S], (r / S) & 1, wlim);
                 }
             }
             if (lane == 0)
@@ -660,7 +664,7 @@ namespace wdg
         for (int m = 0; m < M; ++m)
         {
             const int q = m % S;
-            if (!__all_sync(0xffffffffu, mbar_wait(&full[q], (m / S) & 1)))
+            if (!__all_sync(0xffffffffu, mbar_wait(&full[q], (m / S) & 1, wlim)))
             {
                 if (lane == 0)
                     atomicOr(a.err, 1u);

@@ -123,6 +123,7 @@ namespace wdg
         a.ring = w->ws_ring;
         a.err = w->d_err;
         a.nread = w->halo ? (int)(w->ndof + w->halo) : 0;
+        a.wait_ns = w->wait_ns;
         return a;
     }
 
@@ -138,6 +139,9 @@ namespace wdg
         StageArgs<Real> a = base_args<Real>(w);
         a.du = du;
         a.dt = (Real)dt;
+        // test hook (wdg_test_skip_chunk): the first stage launch of this call only
+        a.test_skip = w->test_skip;
+        w->test_skip = 0;
         for (int s = 0; s < nsteps; ++s)
         {
             const Real *src = A;
@@ -167,6 +171,7 @@ namespace wdg
                 cudaError_t e = launch_stage<Real>(w->n, true, a, w->max_ctas, w->stream);
                 if (e != cudaSuccess)
                     return cuda_fail(e, "stage kernel launch");
+                a.test_skip = 0;
                 src = dst;
             }
             t += dt;
@@ -179,7 +184,7 @@ namespace wdg
     // stage st (0..4) of one RK4 step on the resident buffers, the rotation of rk4_run:
     // reads A, B, C, B, C and writes B, C, B, C, A (A = the resident state)
     template <typename Real>
-    int rk4_stage(wdg_wave *w, int st, double dt)
+    int rk4_stage(wdg_wave *w, int st, double dt, double t, const void *F, double omega, double *acc, double acc_c)
     {
         WDG_TRY(ensure_states(w));
         Real *buf[3] = {static_cast<Real *>(w->d_state[0]), static_cast<Real *>(w->d_state[1]),
@@ -195,13 +200,25 @@ namespace wdg
         a.rk_b = (Real)rk4b[st];
         a.use_tma = aligned16(a.u) ? 1 : 0;
         a.tma_out = aligned16(a.out) ? 1 : 0;
+        if (F)
+        {
+            a.flags |= F_FORCE;
+            a.F = static_cast<const Real *>(F);
+            a.fscale = (Real)(-1.0 / omega * std::sin(omega * (t + rk4c[st] * dt)));
+        }
+        if (st == 4 && acc)
+        {
+            a.flags |= F_FILTER;
+            a.acc = acc;
+            a.acc_c = acc_c;
+        }
         cudaError_t e = launch_stage<Real>(w->n, true, a, w->max_ctas, w->stream);
         if (e != cudaSuccess)
             return cuda_fail(e, "stage kernel launch");
         return WDG_OK;
     }
-    template int rk4_stage<double>(wdg_wave *, int, double);
-    template int rk4_stage<float>(wdg_wave *, int, double);
+    template int rk4_stage<double>(wdg_wave *, int, double, double, const void *, double, double *, double);
+    template int rk4_stage<float>(wdg_wave *, int, double, double, const void *, double, double *, double);
 } // namespace wdg
 
 namespace
@@ -639,6 +656,38 @@ extern "C"
             return fail(WDG_ERR_ARG, "wdg_wave_set_stages: no tile fits shared memory at this depth");
         w->stages = stages;
         w->tile = tile;
+        return WDG_OK;
+    }
+
+    int wdg_wave_set_wait_limit(wdg_wave *w, double seconds)
+    {
+        if (!w || !(seconds > 0.0) || seconds > 60.0)
+            return fail(WDG_ERR_ARG, "wdg_wave_set_wait_limit: the limit must be in (0, 60] seconds");
+        w->wait_ns = std::max(1ull, (unsigned long long)(seconds * 1e9));
+        return WDG_OK;
+    }
+
+    int wdg_test_skip_chunk(wdg_wave *w, int chunk)
+    {
+        if (!w || chunk < -1)
+            return fail(WDG_ERR_ARG, "wdg_test_skip_chunk: chunk must be >= 0 (or -1: none)");
+        w->test_skip = chunk + 1;
+        return WDG_OK;
+    }
+
+    int wdg_test_set_partner(wdg_wave *w, int elem, int side, int offset, int *previous)
+    {
+        if (!w || elem < 0 || elem >= w->nel || side < 0 || side > 3)
+            return fail(WDG_ERR_ARG, "wdg_test_set_partner: element or side out of range");
+        DeviceGuard g(w->device);
+        int *p = reinterpret_cast<int *>(w->d_fbase + elem) + side;
+        int old = 0;
+        WDG_CUDA(cudaMemcpyAsync(&old, p, sizeof(int), cudaMemcpyDeviceToHost, w->stream));
+        WDG_CUDA(cudaStreamSynchronize(w->stream));
+        WDG_CUDA(cudaMemcpyAsync(p, &offset, sizeof(int), cudaMemcpyHostToDevice, w->stream));
+        WDG_CUDA(cudaStreamSynchronize(w->stream));
+        if (previous)
+            *previous = old;
         return WDG_OK;
     }
 

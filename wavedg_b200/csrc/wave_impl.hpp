@@ -41,6 +41,8 @@ struct wdg_wave
     double *d_result = nullptr; // 8 doubles
     double *h_result = nullptr; // pinned, 8 doubles
     unsigned *d_err = nullptr;
+    unsigned long long wait_ns = 0; // limit of the stage kernels' bounded waits (0: kWaitLimitNs)
+    int test_skip = 0;              // test hook: 1 + chunk the next RK launch leaves unloaded
     double *d_src = nullptr;    // gaussian source table
     int src_cap = 0;
 
@@ -68,8 +70,11 @@ namespace wdg
     };
     template <typename Real>
     int rk4_run(wdg_wave *w, Real *A, double dt, double &t, int nsteps, const RKExtras &x);
+    // stage st of the RK4 step that starts at time t; with F, forcing F * s(t + c_st dt),
+    // s(t) = -sin(omega t) / omega; with acc (stage 4 only), the filter acc += acc_c * u_new
     template <typename Real>
-    int rk4_stage(wdg_wave *w, int st, double dt);
+    int rk4_stage(wdg_wave *w, int st, double dt, double t = 0.0, const void *F = nullptr, double omega = 0.0,
+                  double *acc = nullptr, double acc_c = 0.0);
 
     extern const double rk4a[5], rk4b[5], rk4c[5];
 

@@ -41,6 +41,16 @@ def partition(n_elem: int, world: int) -> np.ndarray:
     return (np.arange(n_elem, dtype=np.int64) * world // max(n_elem, 1)).astype(np.int32)
 
 
+def partition_mesh(mesh, world: int, method: str = "rcb") -> np.ndarray:
+    """Element -> rank by Mesh2D::distribute's methods (wdg_mesh_partition,
+    source/Mesh2D.cpp:233-382): "rcb" recursive coordinate bisection, "rcm" reverse
+    Cuthill-McKee blocks.  Deterministic, so every rank computes the same map."""
+    e2p = np.zeros(mesh.n_elem(), dtype=np.int32)
+    check(lib().wdg_mesh_partition(mesh._h, int(world), {"rcb": 0, "rcm": 1}[method], C.c_void_p(e2p.ctypes.data)),
+          "partition_mesh")
+    return e2p
+
+
 def partner_table(mesh, n: int, bc=None):
     """(fbase (nel, 4), fcode (nel,)) of the fused kernels for `mesh` (wdg_mesh_partner_table)."""
     nel = mesh.n_elem()
@@ -154,6 +164,11 @@ class Domain:
         self.dtype = torch.float32 if precision == "fp32" else torch.float64
         dev = torch.device("cuda", torch.cuda.current_device() if device < 0 else device)
         self.device = dev
+        # every launch of this domain goes to torch's current stream, so collectives issued
+        # through torch.distributed are ordered after the gathers and before the puts on the
+        # device, with no host synchronisation
+        self.stream = torch.cuda.current_stream(dev)
+        check(lib().wdg_wave_set_stream(h, C.c_void_p(self.stream.cuda_stream)), "Domain stream")
         self._send_idx = {r: torch.from_numpy(v).to(dev) for r, v in p.send.items()}
         self._send_buf = {r: torch.empty(3 * len(v), dtype=self.dtype, device=dev) for r, v in p.send.items()}
         self._recv_buf = {s: torch.empty(3 * n * cnt, dtype=self.dtype, device=dev) for s, (_, cnt) in p.recv.items()}
@@ -193,8 +208,25 @@ class Domain:
         check(lib().wdg_halo_put(self._h, _STAGE_BUFFER[stage], 3 * self.n * first, C.c_void_p(values.data_ptr()),
                                  3 * self.n * cnt), "halo put")
 
-    def stage(self, stage: int, dt: float) -> None:
-        check(lib().wdg_rk4_stage(self._h, int(stage), float(dt)), "rk4 stage")
+    def stage(self, stage: int, dt: float, t: float = 0.0, F=None, omega: float = 0.0, acc=None,
+              acc_c: float = 0.0) -> None:
+        """RK stage `stage` of the step starting at t; optionally the WaveHoltz forcing F (device,
+        the domain's precision) and, at stage 4, the filter acc += acc_c u (device FP64)."""
+        if F is None and acc is None:
+            check(lib().wdg_rk4_stage(self._h, int(stage), float(dt)), "rk4 stage")
+            return
+        check(lib().wdg_rk4_stage_forced(self._h, int(stage), float(dt), float(t),
+                                         None if F is None else C.c_void_p(F.data_ptr()), float(omega),
+                                         None if acc is None else C.c_void_p(acc.data_ptr()), float(acc_c)),
+              "rk4 stage")
+
+    def set_state(self, u_local) -> None:
+        """The resident state from this domain's own values (device FP64 tensor, local order)."""
+        check(lib().wdg_state_upload(self._h, C.c_void_p(u_local.data_ptr())), "Domain.set_state")
+
+    def local(self, u_global):
+        """This domain's values of a global array (numpy), local element order."""
+        return np.ascontiguousarray(np.asarray(u_global).reshape(-1, self.plan.nd)[self.plan.local]).reshape(-1)
 
     def sync(self) -> None:
         check(lib().wdg_wave_sync(self._h))
@@ -232,21 +264,118 @@ def step_all(domains, dt: float, nsteps: int) -> None:
 
 
 def dist_exchange(domain, group=None):
-    """Exchange over torch.distributed (NCCL between GPUs): one send and one receive per
-    neighbouring rank per stage, posted together."""
+    """Exchange over torch.distributed: one send and one receive per neighbouring rank per stage,
+    posted together.  With NCCL everything stays on the device and in stream order: the gathers
+    run on torch's current stream, NCCL's sends wait for them there, req.wait() makes the
+    current stream wait for the receives, and the puts and the stage follow; the host never
+    waits.  Backends without CUDA tensors (gloo) move the traces through host buffers."""
+    import torch
     import torch.distributed as dist
+
+    on_device = dist.get_backend(group) == "nccl"
+    host = {}
+    if not on_device:
+        host = {s: torch.empty(b.numel(), dtype=b.dtype) for s, b in domain._recv_buf.items()}
 
     def run(stage):
         ops = []
         for r in sorted(domain.plan.send):
-            ops.append(dist.P2POp(dist.isend, domain.gather(stage, r), r, group))
+            buf = domain.gather(stage, r)
+            ops.append(dist.P2POp(dist.isend, buf if on_device else buf.cpu(), r, group))
         for s in sorted(domain.plan.recv):
-            ops.append(dist.P2POp(dist.irecv, domain._recv_buf[s], s, group))
-        domain.sync()
+            ops.append(dist.P2POp(dist.irecv, domain._recv_buf[s] if on_device else host[s], s, group))
         if ops:
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
         for s in sorted(domain.plan.recv):
-            domain.put(stage, s, domain._recv_buf[s])
+            domain.put(stage, s, domain._recv_buf[s] if on_device else host[s])
 
     return run
+
+
+def dist_allreduce(group=None, device=None):
+    """Global sums over torch.distributed (the two FP64 sums of WaveHoltz's norm and error,
+    source/linalg.cpp:102-131): a list of floats -> the list of their sums over all ranks."""
+    import torch
+    import torch.distributed as dist
+
+    dev = device if dist.get_backend(group) == "nccl" else "cpu"
+
+    def run(values):
+        t = torch.tensor(values, dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        return t.cpu().tolist()
+
+    return run
+
+
+class DomainWaveHoltz:
+    """WaveHoltz (source/WaveHoltz.cpp:5-145) on one domain of a decomposed mesh.  T, dt and nt
+    follow WaveHoltz::WaveHoltz (:5-30) with min_h of the whole mesh, so every rank steps alike.
+    One forced period from W, with the filter started at 0.5 dt K(0) W, yields S W + pi0 by
+    linearity (the first period from zero is pi0 itself); the filter's weights and the
+    stage times are those of WaveHoltz::pi0 / S (:55-121)."""
+
+    def __init__(self, domain: Domain, omega: float, mesh_min_h: float):
+        import math
+
+        self.d, self.omega = domain, float(omega)
+        n = domain.n
+        self.T = 2.0 * math.pi / self.omega
+        dt0 = 0.5 * mesh_min_h / (n * n)
+        self.nt = int(math.ceil(self.T / dt0))
+        self.dt = self.T / self.nt
+        self.ndof = domain.ndof
+
+    def K(self, t: float) -> float:
+        import math
+
+        return self.omega / math.pi * (math.cos(self.omega * t) - 0.25)
+
+
+def waveholtz_solve(whs, Fs, tol: float, maxit: int, exchange, allreduce, W=None):
+    """The fixed-point loop of examples/waveholtz2d.cpp:165-185 on a decomposed mesh:
+    W <- S W + pi0 until |W - W_prev| / |pi0| < tol (norms over the whole mesh, by `allreduce`).
+
+    whs: this process's DomainWaveHoltz objects (one per rank under torch.distributed; every
+    rank's when they share a process); Fs: their local load vectors (device, FP64); exchange(st)
+    fills the input halo of RK stage st of all of them (dist_exchange, local_exchange);
+    allreduce(list) -> global sums.  W: initial local iterates (default zero), overwritten.
+    Returns (W list, iterations, residual)."""
+    torch = whs[0].d.torch
+    W = [torch.zeros(wh.ndof, dtype=torch.float64, device=wh.d.device) if W is None else W[i]
+         for i, wh in enumerate(whs)]
+    F = [f if wh.d.dtype == torch.float64 else f.to(wh.d.dtype) for f, wh in zip(Fs, whs)]
+    acc = [torch.empty_like(w) for w in W]
+    wh0 = whs[0]
+    pz, res, it = None, float("inf"), 0
+    zero = all(float(w.abs().max()) == 0.0 for w in W) if W else True
+    for it in range(1, maxit + 1):
+        for wh, w, a in zip(whs, W, acc):
+            wh.d.set_state(w)
+            torch.mul(w, 0.5 * wh0.dt * wh0.K(0.0), out=a)
+        t = 0.0
+        for k in range(1, wh0.nt + 1):
+            t1 = t + wh0.dt  # the step's end time, accumulated as ode::RungeKutta4::step does
+            c = (0.5 if k == wh0.nt else 1.0) * wh0.dt * wh0.K(t1)
+            for st in range(5):
+                exchange(st)
+                for wh, f, a in zip(whs, F, acc):
+                    wh.d.stage(st, wh0.dt, t, f, wh0.omega, a, c)
+            t = t1
+        sums = [0.0, 0.0]
+        for w, a in zip(W, acc):
+            sums[0] += float(torch.sum((a - w) ** 2))
+            sums[1] += float(torch.sum(a * a))
+        dsum, nsum = allreduce(sums)
+        if pz is None:
+            # a zero start's first period is pi0; a warm start would need it separately
+            if not zero:
+                raise ValueError("waveholtz_solve starts from zero")
+            pz = nsum ** 0.5
+        for w, a in zip(W, acc):
+            w.copy_(a)
+        res = dsum ** 0.5 / pz
+        if res < tol:
+            break
+    return W, it, res
