@@ -34,7 +34,8 @@ UNIT = "DOF-stage/s"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM = 6650.0  # GB/s, used only when MEASURED_PEAKS.json is absent
 REF_TIME_BUDGET = 150.0  # seconds of reference CPU work in --impl reference
-LEGS = ("waveholtz_c3", "learned_warm_start", "exact_quadrature", "advection", "decomposition", "waveholtz_config4")
+LEGS = ("waveholtz_c3", "learned_warm_start", "exact_quadrature", "advection", "euler", "decomposition",
+        "waveholtz_config4")
 T_START = time.perf_counter()
 
 
@@ -289,6 +290,8 @@ def run_ours(args, rank, world, local_rank):
         companion("exact_quadrature", exact_quadrature, local_rank, cpu_leg=not args.no_cpu_baseline)
     if want("advection"):
         companion("advection", advection, local_rank, cpu_leg=not args.no_cpu_baseline)
+    if want("euler"):
+        companion("euler", euler, local_rank, cpu_leg=not args.no_cpu_baseline)
     if want("decomposition"):
         companion("decomposition", decomposition, local_rank)
     if want("waveholtz_config4") and wh_ok:
@@ -632,10 +635,15 @@ def advection(device: int, n_el: int = 256, P: int = 4, nv: int = 2, reps: int =
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / reps
+    nel = mesh.n_elem()
+    # algorithmic bytes of the fused RHS: u in, dudt out, the per-side |n.A| tables (4 nv^2
+    # doubles per element) and the 64-byte corner block of every element
+    byts = 16 * s.ndof + 8 * 4 * nv * nv * nel + 64 * nel
+    peak, _ = peak_hbm()
     out = {"workload": f"rhs_advection_nvar{nv}_{n_el}x{n_el}_P{P}_perturbed", "values": s.ndof,
-           "ms_per_rhs": ms, "values_per_s": s.ndof / (ms / 1e3),
-           # algorithmic bytes: u in, dudt out (the corners and edge tables are small)
-           "achieved_gbs": 16 * s.ndof / (ms / 1e3) / 1e9}
+           "ms_per_rhs": ms, "values_per_s": s.ndof / (ms / 1e3), "bytes_per_rhs": byts,
+           "achieved_gbs": byts / (ms / 1e3) / 1e9, "frac": byts / (ms / 1e3) / 1e9 / peak,
+           "kernel": "claw_kernel (one fused launch per RHS)"}
     if cpu_leg:
         kind, cpu = _ref_lib()
         if kind == "reference":
@@ -645,6 +653,66 @@ def advection(device: int, n_el: int = 256, P: int = 4, nv: int = 2, reps: int =
             op.rhs(uh)
             out["cpu_reference_ms_per_rhs"] = (time.perf_counter() - t0) * 1e3
             out["cpu_reference"] = "the reference's Advection / AdvectionHomogeneousBC / MassMatrix<true>, 1 thread"
+    return out
+
+
+def euler(device: int, n_el: int = 256, P: int = 4, reps: int = 20, cpu_leg: bool = True) -> dict:
+    """The compressible Euler system of the reference's nonlinear example (DivF2D<true>,
+    EdgeFluxF2D<true> with the local Lax-Friedrichs flux, MassMatrix<true>) on a perturbed
+    n_el x n_el mesh, P = 4, a smooth positive state: one fused RHS launch and one SSPRK3 step
+    on device arrays (CUDA events over `reps`), with the HBM fraction of the RHS; beside it the
+    reference's own CPU time derivative on the same mesh (1 thread), when present."""
+    import torch
+
+    import wavedg_b200 as W
+    from wavedg_b200 import meshgen as mg
+
+    v, q = mg.perturbed_rect(n_el, 0.2, seed=1, lo=0.0, hi=10.0)
+    mesh = W.Mesh2D.from_vertices(v, q)
+    basis = W.QuadratureRule.quadrature_rule(P + 1, W.QuadratureRule.GaussLobatto)
+    s = W.EulerSystem(mesh, basis, device=device)
+    n = P + 1
+    rng = np.random.default_rng(2)
+    nn = s.ndof // 4
+    rho, p = 1.0 + 0.2 * rng.random(nn), 1.0 + 0.2 * rng.random(nn)
+    uu, vv = 0.3 * rng.standard_normal(nn), 0.3 * rng.standard_normal(nn)
+    U = np.stack([rho, rho * uu, rho * vv, p / 0.4 + 0.5 * rho * (uu * uu + vv * vv)], axis=1).ravel()
+    u = torch.from_numpy(U).cuda()
+    du = torch.empty_like(u)
+    for _ in range(3):
+        s.rhs(u, du)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        s.rhs(u, du)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    dt = 0.2 * mesh.min_h() / (6.0 * n * n)
+    w = u.clone()
+    s.steps(w, dt, 0.0, 2, "ssprk3")
+    torch.cuda.synchronize()
+    e0.record()
+    s.steps(w, dt, 0.0, reps, "ssprk3")
+    e1.record()
+    torch.cuda.synchronize()
+    ms_step = e0.elapsed_time(e1) / reps
+    nel = mesh.n_elem()
+    byts = 16 * s.ndof + 64 * nel  # u in, dudt out, corners
+    peak, _ = peak_hbm()
+    out = {"workload": f"rhs_euler_{n_el}x{n_el}_P{P}_perturbed", "values": s.ndof, "ms_per_rhs": ms,
+           "values_per_s": s.ndof / (ms / 1e3), "bytes_per_rhs": byts, "achieved_gbs": byts / (ms / 1e3) / 1e9,
+           "frac": byts / (ms / 1e3) / 1e9 / peak, "ms_per_ssprk3_step": ms_step,
+           "kernel": "claw_kernel (one fused launch per RHS / stage)"}
+    if cpu_leg:
+        kind, cpu = _ref_lib()
+        if kind == "reference":
+            op = cpu.OpE(cpu.Mesh(v, q, "reference"), n)
+            t0 = time.perf_counter()
+            op.rhs(U)
+            out["cpu_reference_ms_per_rhs"] = (time.perf_counter() - t0) * 1e3
+            out["cpu_reference"] = "the reference's DivF2D / EdgeFluxF2D / MassMatrix<true> with the example's fluxes, 1 thread"
     return out
 
 

@@ -183,6 +183,30 @@ int wdg_advect_bc_action(wdg_advect *adv, const double *u, double *du); /* Advec
 int wdg_advect_rhs(wdg_advect *adv, const double *u, double *dudt);
 int wdg_advect_rk4_steps(wdg_advect *adv, double *u, double dt, double *t, int nsteps);
 
+/* ---- nonlinear conservation law: the compressible Euler system of examples/cl2d.cpp ---- */
+/* State u(d, i, j, el), d = density, x-momentum, y-momentum, energy; gamma = 1.4; FP64.
+ * The operators of the example with approx_quad = true on GLL nodes: DivF2D<true>
+ * (wavedg/DivF.hpp:74-260) with its physical flux F(u) (cl2d.cpp:67-90), EdgeFluxF2D<true>
+ * (wavedg/EdgeFluxF.hpp:65-180) with its local Lax-Friedrichs numerical flux
+ * 1/2 n.(F(uL) + F(uR)) + 1/2 max(|v| + c) (uL - uR) (cl2d.cpp:92-120), MassMatrix<true>. */
+typedef struct wdg_claw wdg_claw;
+int wdg_euler_create(const wdg_mesh *mesh, int n_colloc, int device, wdg_claw **out);
+void wdg_claw_destroy(wdg_claw *claw);
+int wdg_claw_set_stream(wdg_claw *claw, void *cuda_stream);
+int wdg_claw_sync(wdg_claw *claw);
+/* DivF2D<true>::action: divF += (F(u), grad v) */
+int wdg_claw_div(wdg_claw *claw, const double *u, double *divF);
+/* EdgeFluxF2D<true>::action on face traces uB (n, 4, 2, n_edges(face_type)): fB(side 0) =
+ * w_i |E|/2 fh(n, side 0, side 1), fB(side 1) = -fB(side 0), n the outward normal of the
+ * edge's first element; fB may be uB */
+int wdg_claw_flux(wdg_claw *claw, int face_type, const double *uB, double *fB);
+/* the time derivative of examples/cl2d.cpp:171-220: dudt = M^{-1} (DivF(u) - interior faces -
+ * boundary faces with exterior state = interior state), one fused launch */
+int wdg_claw_rhs(wdg_claw *claw, const double *u, double *dudt);
+/* nsteps of ode::RungeKutta4 (method 0, wavedg/ode.hpp:66-93) or ode::SSPRK3 (method 1,
+ * wavedg/ode.hpp:145-186, the stepper of cl2d.cpp) on u in place, one fused launch per stage */
+int wdg_claw_steps(wdg_claw *claw, int method, double *u, double dt, double *t, int nsteps);
+
 /* ---- domain decomposition (one rank's share of a mesh) ---- */
 /* The fused kernels' partner table of `mesh` (what Mesh2D::distribute and FaceVector need to
  * know, source/Mesh2D.cpp:384-592): per element side the DOF offset of the neighbour node that

@@ -60,6 +60,13 @@ _SIGS = {
     "opa_bc_action": ([_v, _dp, _dp], None),
     "opa_rhs": ([_v, _dp, _dp], None),
     "opa_rk4": ([_v, _d, _i, C.POINTER(C.c_double), _dp], None),
+    "ope_create": ([_v, _i], _v),
+    "ope_destroy": ([_v], None),
+    "ope_div": ([_v, _dp, _dp], None),
+    "ope_flux": ([_v, _i, _dp, _dp], None),
+    "ope_prolong": ([_v, _i, _dp, _dp], None),
+    "ope_rhs": ([_v, _dp, _dp], None),
+    "ope_steps": ([_v, _i, _d, _i, C.POINTER(C.c_double), _dp], None),
     "opq_create": ([_v, _i, _ip], _v),
     "opq_destroy": ([_v], None),
     "opq_div": ([_v, _dp, _dp], None),
@@ -334,6 +341,50 @@ class WaveHoltz:
         err = C.c_double()
         it = self.L.wh_solve(self.h, _f64(pi0), tol, maxit, W, C.byref(err))
         return W, it, err.value
+
+
+class OpE:
+    """The compressible Euler system of examples/cl2d.cpp (gamma = 1.4, local Lax-Friedrichs
+    flux) with DivF2D<true>, EdgeFluxF2D<true> (interior and boundary; exterior boundary state =
+    interior state), the Lobatto prolongators and MassMatrix<true>, on the CPU checker.  State
+    (4, n, n, n_elem): density, x- and y-momentum, energy."""
+
+    nv = 4
+
+    def __init__(self, mesh: Mesh, n: int):
+        self.L, self.mesh, self.n = mesh.L, mesh, n
+        self.h = self.L.ope_create(mesh.h, n)
+        self.ndof = 4 * n * n * mesh.n_elem
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.ope_destroy(self.h)
+            self.h = None
+
+    def div(self, u, du):
+        self.L.ope_div(self.h, _f64(u), du)
+
+    def prolong(self, kind, u):
+        ub = np.zeros(self.n * 4 * 2 * self.mesh.n_edges(kind))
+        self.L.ope_prolong(self.h, kind, _f64(u), ub)
+        return ub
+
+    def flux(self, kind, ub):
+        fb = np.zeros_like(_f64(ub))
+        self.L.ope_flux(self.h, kind, _f64(ub), fb)
+        return fb
+
+    def rhs(self, u):
+        du = np.zeros(self.ndof)
+        self.L.ope_rhs(self.h, _f64(u), du)
+        return du
+
+    def steps(self, u, dt, nsteps, method="rk4", t=0.0):
+        """ode::RungeKutta4 ("rk4") or ode::SSPRK3 ("ssprk3") steps of the time derivative."""
+        u = _f64(u).copy()
+        tt = C.c_double(t)
+        self.L.ope_steps(self.h, {"rk4": 0, "ssprk3": 1}[method], dt, nsteps, C.byref(tt), u)
+        return u, tt.value
 
 
 class OpQ:

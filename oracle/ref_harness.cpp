@@ -265,6 +265,90 @@ namespace
         }
     };
 
+    // The compressible Euler system of examples/cl2d.cpp (gamma = 1.4): its physical flux,
+    // wave speed and local Lax-Friedrichs numerical flux, as that example defines them
+    // (cl2d.cpp:67-126), for the reference's nonlinear operators below.
+    constexpr double kGamma = 1.4;
+    void euler_flux(const double *, const double q[4], double fg[8])
+    {
+        const double rho = q[0], u = q[1] / q[0], v = q[2] / q[0], E = q[3];
+        const double p = (kGamma - 1.0) * (E - 0.5 * rho * (u * u + v * v));
+        fg[0] = rho * u;
+        fg[1] = rho * u * u + p;
+        fg[2] = rho * u * v;
+        fg[3] = u * (E + p);
+        fg[4] = rho * v;
+        fg[5] = rho * u * v;
+        fg[6] = rho * v * v + p;
+        fg[7] = v * (E + p);
+    }
+    double euler_speed(const double q[4])
+    {
+        const double rho = q[0], u = q[1] / q[0], v = q[2] / q[0], E = q[3];
+        const double p = (kGamma - 1.0) * (E - 0.5 * rho * (u * u + v * v));
+        return std::hypot(u, v) + std::sqrt(kGamma * p / rho);
+    }
+    void euler_llf(const double *x, const double nrm[2], const double qL[4], const double qR[4], double fh[4])
+    {
+        double fL[8], fR[8];
+        euler_flux(x, qL, fL);
+        euler_flux(x, qR, fR);
+        const double c = std::max(euler_speed(qL), euler_speed(qR));
+        for (int d = 0; d < 4; ++d)
+            fh[d] = 0.5 * nrm[0] * (fL[d] + fR[d]) + 0.5 * nrm[1] * (fL[4 + d] + fR[4 + d]) + 0.5 * c * (qL[d] - qR[d]);
+    }
+
+    // DivF2D<true>, EdgeFluxF2D<true> (interior and boundary), the Lobatto prolongators and
+    // MassMatrix<true>, composed into the time derivative of examples/cl2d.cpp:171-220 with
+    // approx_quad = true: exterior boundary state = interior state.
+    struct RefOpE
+    {
+        static constexpr int nv = 4;
+        const Mesh2D &mesh;
+        const QuadratureRule *basis;
+        const int n, ndof, nI, nB;
+        DivF2D<true> div;
+        EdgeFluxF2D<true> flxI, flxB;
+        std::unique_ptr<FaceProlongator> prolI, prolB;
+        MassMatrix<true> m;
+        mutable std::vector<double> uI, uB;
+
+        RefOpE(const Mesh2D &mesh_, int n_colloc)
+            : mesh(mesh_), basis(QuadratureRule::quadrature_rule(n_colloc, QuadratureRule::GaussLobatto)), n(n_colloc),
+              ndof(nv * n_colloc * n_colloc * mesh_.n_elem()), nI(mesh_.n_edges(FaceType::INTERIOR)),
+              nB(mesh_.n_edges(FaceType::BOUNDARY)), div(mesh_, basis), flxI(mesh_, FaceType::INTERIOR, basis),
+              flxB(mesh_, FaceType::BOUNDARY, basis), prolI(make_face_prolongator(mesh_, basis, FaceType::INTERIOR)),
+              prolB(make_face_prolongator(mesh_, basis, FaceType::BOUNDARY)), m(mesh_, basis),
+              uI((size_t)n_colloc * nv * 2 * nI), uB((size_t)n_colloc * nv * 2 * nB)
+        {
+        }
+        void flux(int type, const double *ub, double *fb) const
+        {
+            (type == 0 ? flxI : flxB).action(nv, euler_llf, ub, fb);
+        }
+        void rhs(const double *u, double *dudt) const
+        {
+            for (int i = 0; i < ndof; ++i)
+                dudt[i] = 0.0;
+            div.action(nv, euler_flux, u, dudt);
+            prolI->action(nv, u, uI.data());
+            flxI.action(nv, euler_llf, uI.data(), uI.data());
+            for (double &x : uI)
+                x *= -1;
+            prolI->t(nv, uI.data(), dudt);
+            prolB->action(nv, u, uB.data());
+            for (int e = 0; e < nB; ++e)
+                for (int d = 0; d < nv; ++d)
+                    for (int i = 0; i < n; ++i)
+                        uB[i + n * (d + nv * (1 + 2 * (size_t)e))] = uB[i + n * (d + nv * (0 + 2 * (size_t)e))];
+            flxB.action(nv, euler_llf, uB.data(), uB.data());
+            for (double &x : uB)
+                x *= -1;
+            prolB->t(nv, uB.data(), dudt);
+            m.inv(nv, dudt);
+        }
+    };
+
     // WaveHoltz restated over RefOp so that the composed boundary operator can
     // be used (the reference class hard-wires WaveBC).  Loop structure, time
     // accumulation and filter weights follow source/WaveHoltz.cpp:5-145; with
@@ -514,6 +598,39 @@ extern "C"
         auto f = [op](double *dudt, const double, const double *v) { op->rhs(v, dudt); };
         for (int s = 0; s < nsteps; ++s)
             rk.step(dt, f, *t, u);
+    }
+
+    // ---- compressible Euler (examples/cl2d.cpp), DivF2D<true> / EdgeFluxF2D<true> ----
+    void *ref_ope_create(void *m, int n_colloc) { return new RefOpE(static_cast<RefMesh *>(m)->mesh, n_colloc); }
+    void ref_ope_destroy(void *o) { delete static_cast<RefOpE *>(o); }
+    void ref_ope_div(void *o, const double *u, double *du)
+    {
+        static_cast<RefOpE *>(o)->div.action(RefOpE::nv, euler_flux, u, du);
+    }
+    void ref_ope_flux(void *o, int type, const double *ub, double *fb) { static_cast<RefOpE *>(o)->flux(type, ub, fb); }
+    void ref_ope_prolong(void *o, int type, const double *u, double *ub)
+    {
+        RefOpE *op = static_cast<RefOpE *>(o);
+        (type == 0 ? op->prolI : op->prolB)->action(RefOpE::nv, u, ub);
+    }
+    void ref_ope_rhs(void *o, const double *u, double *du) { static_cast<RefOpE *>(o)->rhs(u, du); }
+    // method 0: ode::RungeKutta4, 1: ode::SSPRK3 (the stepper examples/cl2d.cpp uses)
+    void ref_ope_steps(void *o, int method, double dt, int nsteps, double *t, double *u)
+    {
+        RefOpE *op = static_cast<RefOpE *>(o);
+        auto f = [op](double *dudt, const double, const double *v) { op->rhs(v, dudt); };
+        if (method == 0)
+        {
+            ode::RungeKutta4 rk(op->ndof);
+            for (int s = 0; s < nsteps; ++s)
+                rk.step(dt, f, *t, u);
+        }
+        else
+        {
+            ode::SSPRK3 rk(op->ndof);
+            for (int s = 0; s < nsteps; ++s)
+                rk.step(dt, f, *t, u);
+        }
     }
 
     // ---- exact quadrature (approx_quad = false) ----

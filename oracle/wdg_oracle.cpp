@@ -840,6 +840,157 @@ namespace
         }
     };
 
+    // The compressible Euler system of examples/cl2d.cpp:67-126 (gamma = 1.4): physical flux
+    // (f in fg[0..3], g in fg[4..7]), wave speed |v| + sqrt(gamma p / rho), and the local
+    // Lax-Friedrichs flux 1/2 n.(F(qL) + F(qR)) + 1/2 max(speed) (qL - qR).
+    constexpr double kGammaE = 1.4;
+    void euler_flux(const double q[4], double fg[8])
+    {
+        const double rho = q[0], u = q[1] / q[0], v = q[2] / q[0], E = q[3];
+        const double p = (kGammaE - 1.0) * (E - 0.5 * rho * (u * u + v * v));
+        fg[0] = rho * u;
+        fg[1] = rho * u * u + p;
+        fg[2] = rho * u * v;
+        fg[3] = u * (E + p);
+        fg[4] = rho * v;
+        fg[5] = rho * u * v;
+        fg[6] = rho * v * v + p;
+        fg[7] = v * (E + p);
+    }
+    double euler_speed(const double q[4])
+    {
+        const double rho = q[0], u = q[1] / q[0], v = q[2] / q[0], E = q[3];
+        const double p = (kGammaE - 1.0) * (E - 0.5 * rho * (u * u + v * v));
+        return std::hypot(u, v) + std::sqrt(kGammaE * p / rho);
+    }
+    void euler_llf(const double nrm[2], const double qL[4], const double qR[4], double fh[4])
+    {
+        double fL[8], fR[8];
+        euler_flux(qL, fL);
+        euler_flux(qR, fR);
+        const double c = std::max(euler_speed(qL), euler_speed(qR));
+        for (int d = 0; d < 4; ++d)
+            fh[d] = 0.5 * nrm[0] * (fL[d] + fR[d]) + 0.5 * nrm[1] * (fL[4 + d] + fR[4 + d]) + 0.5 * c * (qL[d] - qR[d]);
+    }
+
+    // The nonlinear conservation-law operators with approximate quadrature on GLL nodes for the
+    // Euler system: DivF2D<true>::action (wavedg/DivF.hpp:203-260), EdgeFluxF2D<true>::action
+    // (wavedg/EdgeFluxF.hpp:138-180), and the time derivative of examples/cl2d.cpp:171-220
+    // (exterior boundary state = interior state), with the Lobatto prolongation and mass of Op.
+    struct OpE
+    {
+        static constexpr int nv = 4;
+        const Op base;
+        const Mesh &m;
+        int n, nel, ndof;
+
+        OpE(const Mesh &m_, int n_)
+            : base(m_, n_, std::vector<int>(m_.boundary.size(), 0).data()), m(m_), n(n_), nel(m_.nel),
+              ndof(nv * n_ * n_ * m_.nel)
+        {
+        }
+        void div(const double *u, double *du) const
+        {
+            const int nn = n * n;
+            vec F0((size_t)nv * nn), F1((size_t)nv * nn); // F0(l, d, j) at l + n (d + nv j); F1(l, d, i) likewise
+            for (int el = 0; el < nel; ++el)
+            {
+                const double *ue = u + (size_t)nv * nn * el;
+                for (int j = 0; j < n; ++j)
+                    for (int i = 0; i < n; ++i)
+                    {
+                        double J[4], fg[8];
+                        jacobian(&m.corners[8 * (size_t)el], base.x[i], base.x[j], J);
+                        const double W = base.w[i] * base.w[j];
+                        const double Ye = J[3] * W, Xe = J[2] * W, Yx = J[1] * W, Xx = J[0] * W;
+                        euler_flux(ue + nv * (i + n * j), fg);
+                        for (int d = 0; d < nv; ++d)
+                        {
+                            F0[i + n * (d + nv * j)] = Ye * fg[d] - Xe * fg[4 + d];
+                            F1[j + n * (d + nv * i)] = -Yx * fg[d] + Xx * fg[4 + d];
+                        }
+                    }
+                for (int j = 0; j < n; ++j)
+                    for (int i = 0; i < n; ++i)
+                        for (int d = 0; d < nv; ++d)
+                        {
+                            double s = 0.0;
+                            for (int l = 0; l < n; ++l)
+                                s += base.D[l + n * i] * F0[l + n * (d + nv * j)] + base.D[l + n * j] * F1[l + n * (d + nv * i)];
+                            du[d + nv * (i + n * (j + (size_t)n * el))] += s;
+                        }
+            }
+        }
+        void prolong(bool interior, const double *u, double *uf) const
+        {
+            const auto &v2e = interior ? base.v2eI : base.v2eB;
+            const int N = (int)(interior ? m.interior.size() : m.boundary.size());
+            std::fill(uf, uf + (size_t)n * nv * 2 * N, 0.0);
+            for (int e = 0; e < N; ++e)
+                for (int s = 0; s < (interior ? 2 : 1); ++s)
+                    for (int i = 0; i < n; ++i)
+                        for (int d = 0; d < nv; ++d)
+                            uf[i + n * (d + nv * (s + 2 * (size_t)e))] = u[d + nv * (size_t)v2e[i + n * (s + 2 * (size_t)e)]];
+        }
+        void prolong_t(bool interior, const double *uf, double *u) const
+        {
+            const auto &v2e = interior ? base.v2eI : base.v2eB;
+            const int N = (int)(interior ? m.interior.size() : m.boundary.size());
+            for (int e = 0; e < N; ++e)
+                for (int s = 0; s < (interior ? 2 : 1); ++s)
+                    for (int i = 0; i < n; ++i)
+                        for (int d = 0; d < nv; ++d)
+                            u[d + nv * (size_t)v2e[i + n * (s + 2 * (size_t)e)]] += uf[i + n * (d + nv * (s + 2 * (size_t)e))];
+        }
+        // fB(i, d, 0) = W_i |E|/2 fh(n, u0, u1), fB(i, d, 1) = -fB(i, d, 0); n = outward normal of elements[0]
+        void flux(bool interior, const double *ub, double *fb) const
+        {
+            const auto &list = interior ? m.interior : m.boundary;
+            const int N = (int)list.size();
+            double qL[4], qR[4], fh[4];
+            for (int e = 0; e < N; ++e)
+            {
+                const Edge &E = m.edges[list[e]];
+                for (int i = 0; i < n; ++i)
+                {
+                    for (int d = 0; d < nv; ++d)
+                    {
+                        qL[d] = ub[i + n * (d + nv * (0 + 2 * (size_t)e))];
+                        qR[d] = ub[i + n * (d + nv * (1 + 2 * (size_t)e))];
+                    }
+                    euler_llf(E.n, qL, qR, fh);
+                    for (int d = 0; d < nv; ++d)
+                    {
+                        const double fl = fh[d] * base.w[i] * E.meas;
+                        fb[i + n * (d + nv * (0 + 2 * (size_t)e))] = fl;
+                        fb[i + n * (d + nv * (1 + 2 * (size_t)e))] = -fl;
+                    }
+                }
+            }
+        }
+        void rhs(const double *u, double *du) const
+        {
+            std::fill(du, du + ndof, 0.0);
+            div(u, du);
+            vec uI((size_t)n * nv * 2 * m.interior.size()), uB((size_t)n * nv * 2 * m.boundary.size());
+            prolong(true, u, uI.data());
+            flux(true, uI.data(), uI.data());
+            for (double &x : uI)
+                x = -x;
+            prolong_t(true, uI.data(), du);
+            prolong(false, u, uB.data());
+            for (size_t e = 0; e < m.boundary.size(); ++e)
+                for (int d = 0; d < nv; ++d)
+                    for (int i = 0; i < n; ++i)
+                        uB[i + n * (d + nv * (1 + 2 * e))] = uB[i + n * (d + nv * (0 + 2 * e))];
+            flux(false, uB.data(), uB.data());
+            for (double &x : uB)
+                x = -x;
+            prolong_t(false, uB.data(), du);
+            base.mass_inv(nv, du);
+        }
+    };
+
     // D(i, j) = phi_j'(xq_i) at points off (or on) the nodes: lagrange_basis_deriv with the
     // two branches of lagrange_derivative (lagrange_interpolation.cpp:33-50, 96-139)
     void deriv_at(int n, const double *x, int nq, const double *xq, double *D)
@@ -1429,6 +1580,38 @@ extern "C"
         auto f = [op](double *dudt, double, const double *v) { op->rhs(v, dudt); };
         for (int s = 0; s < nsteps; ++s)
             rk4_step(op->ndof, dt, f, *t, u, p, du);
+    }
+    void *orc_ope_create(void *m, int n) { return new OpE(*static_cast<Mesh *>(m), n); }
+    void orc_ope_destroy(void *o) { delete static_cast<OpE *>(o); }
+    void orc_ope_div(void *o, const double *u, double *du) { static_cast<OpE *>(o)->div(u, du); }
+    void orc_ope_flux(void *o, int type, const double *ub, double *fb) { static_cast<OpE *>(o)->flux(type == 0, ub, fb); }
+    void orc_ope_prolong(void *o, int type, const double *u, double *ub) { static_cast<OpE *>(o)->prolong(type == 0, u, ub); }
+    void orc_ope_rhs(void *o, const double *u, double *du) { static_cast<OpE *>(o)->rhs(u, du); }
+    // method 0: ode::RungeKutta4; 1: ode::SSPRK3 (wavedg/ode.hpp:145-186), step for step
+    void orc_ope_steps(void *o, int method, double dt, int nsteps, double *t, double *u)
+    {
+        OpE *op = static_cast<OpE *>(o);
+        const int nd = op->ndof;
+        vec p(nd), du(nd), y(nd);
+        auto f = [op](double *dudt, double, const double *v) { op->rhs(v, dudt); };
+        for (int s = 0; s < nsteps; ++s)
+        {
+            if (method == 0)
+            {
+                rk4_step(nd, dt, f, *t, u, p, du);
+                continue;
+            }
+            f(p.data(), *t, u);
+            for (int i = 0; i < nd; ++i)
+                y[i] = u[i] + dt * p[i];
+            f(p.data(), *t + dt, y.data());
+            for (int i = 0; i < nd; ++i)
+                y[i] = 0.25 * (y[i] + 3.0 * u[i] + dt * p[i]);
+            f(p.data(), *t + 0.5 * dt, y.data());
+            for (int i = 0; i < nd; ++i)
+                u[i] = (u[i] + 2.0 * y[i] + 2.0 * dt * p[i]) / 3.0;
+            *t += dt;
+        }
     }
     void *orc_opq_create(void *m, int n, const int *bc) { return new OpQ(*static_cast<Mesh *>(m), n, bc); }
     void orc_opq_destroy(void *o) { delete static_cast<OpQ *>(o); }

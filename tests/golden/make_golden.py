@@ -1,7 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the reference library.
 
     make -C oracle ref          # compiles the reference (needs its sources)
-    python tests/golden/make_golden.py [--exact-quadrature-only | --advection-only | --reference-meshes]
+    python tests/golden/make_golden.py [--exact-quadrature-only | --advection-only | --reference-meshes | --euler]
 
 Every output array is produced by the reference waveDG code compiled from its
 own sources (oracle/_ref/libwdgref.so, driven through oracle/ref_harness.cpp).
@@ -204,6 +204,46 @@ def opq_fixture(name, v, q, m, n, seed):
     np.savez_compressed(os.path.join(HERE, f"opq_{name}_n{n}.npz"), **out)
 
 
+def euler_state(ndof, rng):
+    """A positive Euler state per node: density 1 + 0.2 U, velocities 0.3 N, pressure 1 + 0.2 U
+    (total energy p / (gamma - 1) + rho |v|^2 / 2)."""
+    nn = ndof // 4
+    rho = 1.0 + 0.2 * rng.random(nn)
+    u, v = 0.3 * rng.standard_normal(nn), 0.3 * rng.standard_normal(nn)
+    p = 1.0 + 0.2 * rng.random(nn)
+    return np.stack([rho, rho * u, rho * v, p / 0.4 + 0.5 * rho * (u * u + v * v)], axis=1).ravel()
+
+
+def euler_fixture(name, v, q, m, n, seed):
+    """The compressible Euler operators of examples/cl2d.cpp with approx_quad = true:
+    DivF2D<true> (accumulating), the prolongators, EdgeFluxF2D<true> with the local
+    Lax-Friedrichs flux (interior traces; boundary traces with exterior = interior), the time
+    derivative, 3 steps of ode::RungeKutta4 and of ode::SSPRK3."""
+    rng = np.random.default_rng(seed)
+    op = cpu.OpE(m, n)
+    u = euler_state(op.ndof, rng)
+    out = dict(verts=v, quads=q, n=n, u=u)
+    r = rng.standard_normal(op.ndof)
+    out["div_in"] = r.copy()
+    op.div(u, r)
+    out["div"] = r
+    for k in (0, 1):
+        ub = op.prolong(k, u)
+        out[f"prolong{k}"] = ub.copy()
+        if k == 1:  # exterior boundary state = interior state, as the example sets it
+            ub = ub.reshape(-1, 2, 4 * n)
+            ub[:, 1] = ub[:, 0]
+            ub = ub.reshape(-1)
+        out[f"flux{k}_in"] = ub
+        out[f"flux{k}"] = op.flux(k, ub)
+    out["rhs"] = op.rhs(u)
+    dt = 0.1 * m.min_h() / (n * n)
+    out["dt"] = dt
+    out["rk4_3"], _ = op.steps(u, dt, 3, "rk4")
+    out["ssprk3_3"], _ = op.steps(u, dt, 3, "ssprk3")
+    np.savez_compressed(os.path.join(HERE, f"euler_{name}_n{n}.npz"), **out)
+
+
 def reference_meshes():
     """The reference's mesh files, copied unchanged into tests/golden/meshes/<name>/ (data, read
     by Mesh2D::from_file, source/Mesh2D.cpp:94-128); per mesh the connectivity the reference's
@@ -229,6 +269,17 @@ def reference_meshes():
 def main():
     if not cpu.available("reference"):
         raise SystemExit("build the reference first: make -C oracle ref")
+    if "--euler" in sys.argv:
+        ecases = {"scrambled6": [4], "lshape3": [5]}
+        for seed, (name, v, q) in enumerate(meshes()):
+            for n in ecases.get(name, []):
+                euler_fixture(name, v, q, cpu.Mesh(v, q, KIND), n, 4000 + 100 * seed + n)
+        g = os.path.join(HERE, "meshes", "Square")
+        v = np.loadtxt(os.path.join(g, "coordinates.txt")).reshape(-1, 2)
+        q = np.loadtxt(os.path.join(g, "elements.txt"), dtype=np.int32).reshape(-1, 4)
+        euler_fixture("fileSquare", v, q, cpu.Mesh(v, q, KIND), 3, 4999)
+        print("Euler fixtures written to", HERE)
+        return
     if "--reference-meshes" in sys.argv:
         reference_meshes()
         print("reference-mesh fixtures written to", HERE)

@@ -3,8 +3,9 @@
 * the BF16 tensor-core GEMM, every transpose / batch / split-K form the network uses,
   against an FP64 product of the same BF16-rounded operands (FP32 accumulation: 1e-5);
 * forward pass and every parameter gradient of a small FNO (grid 32, width 8, 4 modes,
-  4 layers) against torch FP64 autograd on the CPU with torch.fft, from the same FP32
-  parameters.  BF16 activations and weights bound the agreement: 2e-2 on the output, 4e-2
+  4 layers) and of one with the learned warm start's channel and mode counts (grid 64,
+  width 32, 16 modes, hidden 64) against torch FP64 autograd on the CPU with torch.fft,
+  from the same FP32 parameters.  BF16 activations and weights bound the agreement: 2e-2 on the output, 4e-2
   on each gradient tensor (relative 2-norm);
 * resampling between DG nodes and the grid: exact for a bilinear field both ways.
 """
@@ -72,12 +73,15 @@ def _torch_reference(params, inp, L, modes):
     return P, y
 
 
-def test_fno_forward_and_gradients(gpu_lib):
+@pytest.mark.parametrize("G,width,modes,H", [(32, 8, 4, 16), (64, 32, 16, 64)])
+def test_fno_forward_and_gradients(gpu_lib, G, width, modes, H):
+    """A toy network, and the shipped network's channel, mode and hidden counts (32, 16, 64)
+    on a 64 x 64 grid."""
     import torch
 
     from wavedg_b200 import fno
 
-    G, width, modes, L, H, B = 32, 8, 4, 4, 16, 2
+    L, B = 4, 2
     net = fno.FNO(grid=G, width=width, modes=modes, layers=L, hidden=H, seed=3)
     # larger spectral weights than the default initialisation so the Fourier branch matters
     for l in range(L):
@@ -98,7 +102,8 @@ def test_fno_forward_and_gradients(gpu_lib):
     worst = {}
     for k in net.params:
         worst[k] = _rel(net.grads[k].cpu().numpy(), P[k].grad.numpy())
-    print({k: f"{v:.1e}" for k, v in worst.items()})
+    print(f"G {G} width {width} modes {modes}: output {_rel(y.cpu().numpy(), yr.detach().numpy()):.1e}, gradients",
+          {k: f"{v:.1e}" for k, v in worst.items()})
     assert max(worst.values()) < 4e-2, worst
 
 

@@ -211,3 +211,22 @@ def test_advection_every_variable_count_against_the_reference(nv):
     r = cpu.OpA(cpu.Mesh(v, q, "reference"), 4, nv, a)
     u = rng.standard_normal(o.ndof)
     assert rel(o.rhs(u), r.rhs(u)) < 1e-12
+
+
+@pytest.mark.parametrize("fname", golden_files("euler_"))
+def test_oracle_euler_against_reference_fixtures(fname):
+    """The oracle's restatement of DivF2D<true>, EdgeFluxF2D<true> with the local
+    Lax-Friedrichs flux, the cl2d time derivative, RK4 and SSPRK3 against the reference's
+    own outputs."""
+    g = golden(fname)
+    m = cpu.Mesh(g["verts"], g["quads"], "oracle")
+    op = cpu.OpE(m, int(g["n"]))
+    d = g["div_in"].copy()
+    op.div(g["u"], d)
+    assert rel(d, g["div"]) < 1e-13
+    for k in (0, 1):
+        np.testing.assert_array_equal(op.prolong(k, g["u"]), g[f"prolong{k}"])
+        assert rel(op.flux(k, g[f"flux{k}_in"]), g[f"flux{k}"]) < 1e-13
+    assert rel(op.rhs(g["u"]), g["rhs"]) < 1e-13
+    assert rel(op.steps(g["u"], float(g["dt"]), 3, "rk4")[0], g["rk4_3"]) < 1e-13
+    assert rel(op.steps(g["u"], float(g["dt"]), 3, "ssprk3")[0], g["ssprk3_3"]) < 1e-13

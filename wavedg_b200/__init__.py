@@ -12,6 +12,7 @@ from .dg import (  # noqa: F401
     Div,
     ExactDiscretisation,
     EdgeFlux,
+    EulerSystem,
     FaceProlongator,
     FaceType,
     LinearFunctional2D,
@@ -33,7 +34,8 @@ from .dg import (  # noqa: F401
 )
 
 __all__ = [
-    "Advection", "AdvectionHomogeneousBC", "AdvectionSystem", "read_file", "to_file", "Discretisation", "Div", "ExactDiscretisation", "EdgeFlux", "FaceProlongator", "FaceType", "LinearFunctional2D", "MassMatrix",
+    "Advection", "AdvectionHomogeneousBC", "AdvectionSystem", "read_file", "to_file", "Discretisation", "Div", "ExactDiscretisation", "EdgeFlux", "EulerSystem",
+    "FaceProlongator", "FaceType", "LinearFunctional2D", "MassMatrix",
     "Mesh2D", "Operator", "QuadratureRule", "RungeKutta4", "WaveBC", "WaveEquation", "WaveHoltz", "WaveHoltzBatch", "WaveSystem",
     "WdgError", "WDG_FP32", "WDG_FP64", "error", "lib", "make_face_prolongator", "norm",
 ]

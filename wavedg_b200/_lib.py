@@ -66,6 +66,14 @@ SIGNATURES = {
     "wdg_advect_bc_action": ([_v, _v, _v], _i),
     "wdg_advect_rhs": ([_v, _v, _v], _i),
     "wdg_advect_rk4_steps": ([_v, _v, _d, _v, _i], _i),
+    "wdg_euler_create": ([_v, _i, _i, _vp], _i),
+    "wdg_claw_destroy": ([_v], None),
+    "wdg_claw_set_stream": ([_v, _v], _i),
+    "wdg_claw_sync": ([_v], _i),
+    "wdg_claw_div": ([_v, _v, _v], _i),
+    "wdg_claw_flux": ([_v, _i, _v, _v], _i),
+    "wdg_claw_rhs": ([_v, _v, _v], _i),
+    "wdg_claw_steps": ([_v, _i, _v, _d, _dp, _i], _i),
     "wdg_wave_create_halo": ([_v, _i, _v, _i, _i, _i, _v, _v, _vp], _i),
     "wdg_halo_info": ([_v, _v, _v], _i),
     "wdg_halo_gather": ([_v, _i, _v, _i, _v], _i),

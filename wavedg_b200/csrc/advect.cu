@@ -10,9 +10,11 @@
 // a holds A_0 and A_1 as a(d, c, k) = a[d + nv (c + nv k)].  The upwind flux needs |n . A|;
 // it is formed per edge on the host from a Jacobi eigen-decomposition, so A_0 and A_1 must
 // be symmetric (the reference's general eigen-solver path for non-symmetric A is not built).
-// FP64; component kernels in the reference layouts (u(d, i, j, el), face traces (i, d, side,
-// edge)); geometry, edge tables, mass and argument staging are those of an internal
-// collocation handle.
+// FP64.  The RHS and RK4 run as one fused launch per evaluation or stage (claw_kernels.cuh:
+// volume, both face terms with the upwind flux 1/2 (n.A)(a + b) + 1/2 |n.A| (a - b), mass
+// inverse, RK update); the operator entry points (action, bc_action) keep component kernels in
+// the reference layouts (u(d, i, j, el), face traces (i, d, side, edge)).  Geometry, edge and
+// partner tables and argument staging are those of an internal collocation handle.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -32,7 +34,8 @@ struct wdg_advect
     double *d_x = nullptr, *d_wt = nullptr, *d_D = nullptr; // GLL nodes, weights, D(l, j)
     double *d_FI = nullptr, *d_FB = nullptr; // per edge and side: |E|/2 Fs(c, d), (nv, nv, 2, edges)
     double *d_uf = nullptr, *d_uB = nullptr;
-    double *d_rk = nullptr; // RK4: k and the stage derivative
+    double *d_absA = nullptr;           // |n.A| per element side for the fused kernel, (nv, nv, 4, nel)
+    double *d_rk = nullptr;             // RK4: the two rotation buffers and the register
 };
 
 namespace
@@ -187,17 +190,6 @@ namespace
         }
     }
 
-    __global__ void adv_rk_stage_kernel(double *u, double *k, const double *p, double a, double b, double dt, bool first,
-                                        long long n)
-    {
-        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        {
-            const double ki = first ? dt * p[i] : a * k[i] + dt * p[i];
-            k[i] = ki;
-            u[i] += b * ki;
-        }
-    }
-
     // symmetric m x m eigen-decomposition, cyclic Jacobi: A = R diag(e) R^T (column-major)
     void jacobi_eig(int m, const double *A_, double *R, double *e)
     {
@@ -281,6 +273,39 @@ namespace
         return F;
     }
 
+    // |n.A| = R |diag(lambda)| R^T of n.A per element side, n the side's outward normal (the same
+    // arithmetic as the fused kernel's claw_side), for the upwind flux of the fused kernel
+    std::vector<double> abs_tables(const wdg_mesh &mesh, int nv, const double *a)
+    {
+        const int v2 = nv * nv;
+        std::vector<double> T((size_t)v2 * 4 * mesh.nel);
+        for (int el = 0; el < mesh.nel; ++el)
+        {
+            const double *c = &mesh.corners[8 * (size_t)el];
+            for (int s = 0; s < 4; ++s)
+            {
+                const int p0 = (s == 0 || s == 3) ? 0 : (s == 1 ? 1 : 3), p1 = (s == 0) ? 1 : (s == 3 ? 3 : 2);
+                const double dx = c[2 * p1] - c[2 * p0], dy = c[2 * p1 + 1] - c[2 * p0 + 1];
+                const double len = std::sqrt(dx * dx + dy * dy), sgn = (s >= 2) ? -1.0 : 1.0;
+                const double nx = sgn * dy / len, ny = -sgn * dx / len;
+                double nA[kMaxVar * kMaxVar], R[kMaxVar * kMaxVar], ev[kMaxVar];
+                for (int d = 0; d < v2; ++d)
+                    nA[d] = nx * a[d] + ny * a[d + v2];
+                jacobi_eig(nv, nA, R, ev);
+                double *t = &T[(size_t)v2 * (4 * (size_t)el + s)];
+                for (int d = 0; d < nv; ++d)
+                    for (int k = 0; k < nv; ++k)
+                    {
+                        double acc = 0.0;
+                        for (int m = 0; m < nv; ++m)
+                            acc += R[d + nv * m] * std::abs(ev[m]) * R[k + nv * m];
+                        t[d + nv * k] = acc;
+                    }
+            }
+        }
+        return T;
+    }
+
     unsigned blocks(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
     long long nvals(const wdg_advect *h) { return (long long)h->nv * h->n * h->n * h->w->nel; }
@@ -317,13 +342,16 @@ namespace
         return faces_dev(h, 0, u, du);
     }
     int bc_dev(wdg_advect *h, const double *u, double *du) { return faces_dev(h, 1, u, du); }
+    // dudt = M^{-1} (A u + B u): one fused launch (volume, both face terms with the upwind flux,
+    // mass inverse; claw_kernels.cuh)
     int rhs_dev(wdg_advect *h, const double *u, double *dudt)
     {
         wdg_wave *w = h->w;
-        WDG_CUDA(cudaMemsetAsync(dudt, 0, sizeof(double) * nvals(h), w->stream));
-        WDG_TRY(action_dev(h, u, dudt));
-        WDG_TRY(bc_dev(h, u, dudt));
-        WDG_CUDA(launch_mass(w->geo, h->nv, dudt, dudt, true, w->stream));
+        ClawArgs c = claw_args(w, u, dudt);
+        c.A = h->d_a;
+        c.absA = h->d_absA;
+        c.mode = CLAW_RHS;
+        WDG_CUDA(launch_claw(1, h->n, h->nv, c, w->stream));
         return WDG_OK;
     }
 
@@ -376,6 +404,7 @@ extern "C"
         deriv_matrix(n, x.data(), D.data());
         const std::vector<double> FI = flux_tables(*mesh, mesh->interior, n_var, a);
         const std::vector<double> FB = flux_tables(*mesh, mesh->boundary, n_var, a);
+        const std::vector<double> AB = abs_tables(*mesh, n_var, a);
         int st = WDG_OK;
         auto chk = [&](int r)
         {
@@ -388,6 +417,7 @@ extern "C"
         chk(device_alloc(&h->d_D, D.size()));
         chk(device_alloc(&h->d_FI, FI.size()));
         chk(device_alloc(&h->d_FB, FB.size()));
+        chk(device_alloc(&h->d_absA, AB.size()));
         chk(device_alloc(&h->d_uf, (size_t)n * n_var * 2 * w->nI));
         chk(device_alloc(&h->d_uB, (size_t)n * n_var * 2 * w->nB));
         if (st == WDG_OK)
@@ -398,6 +428,7 @@ extern "C"
             chk(device_put(h->d_D, D));
             chk(device_put(h->d_FI, FI));
             chk(device_put(h->d_FB, FB));
+            chk(device_put(h->d_absA, AB));
         }
         if (st != WDG_OK)
         {
@@ -414,7 +445,7 @@ extern "C"
             return;
         {
             DeviceScope g(h->w ? h->w->device : 0);
-            for (double *p : {h->d_a, h->d_x, h->d_wt, h->d_D, h->d_FI, h->d_FB, h->d_uf, h->d_uB, h->d_rk})
+            for (double *p : {h->d_a, h->d_x, h->d_wt, h->d_D, h->d_FI, h->d_FB, h->d_uf, h->d_uB, h->d_absA, h->d_rk})
                 if (p)
                     cudaFree(p);
         }
@@ -435,21 +466,12 @@ extern "C"
         wdg_wave *w = h->w;
         const long long nd = nvals(h);
         if (!h->d_rk)
-            WDG_TRY(device_alloc(&h->d_rk, 2 * (size_t)nd));
-        double *k = h->d_rk, *p = h->d_rk + nd;
+            WDG_TRY(device_alloc(&h->d_rk, 3 * (size_t)nd));
+        double *bufs[3] = {h->d_rk, h->d_rk + nd, h->d_rk + 2 * nd};
         HostArg a;
         WDG_TRY(bind_arg(w, 0, u, (size_t)nd, true, true, a));
-        const unsigned gr = (unsigned)std::min<long long>(blocks(nd, 256), 148 * 32);
-        for (int step = 0; step < nsteps; ++step)
-        {
-            for (int st = 0; st < 5; ++st)
-            {
-                WDG_TRY(rhs_dev(h, a.dev, p));
-                adv_rk_stage_kernel<<<gr, 256, 0, w->stream>>>(a.dev, k, p, rk4a[st], rk4b[st], dt, st == 0, nd);
-                WDG_CUDA(cudaGetLastError());
-            }
-            *t += dt;
-        }
+        // fused stage kernels (claw_kernels.cuh), the buffer rotation of the wave path
+        WDG_TRY(claw_steps(w, 1, h->nv, h->d_a, h->d_absA, bufs, 0, a.dev, dt, t, nsteps));
         return finish_args(w, &a, 1);
     }
 }

@@ -1,0 +1,395 @@
+// Fused element kernels of the conservation-law path (included by kernels.cu, which owns the
+// basis tables): u_t + div F(u) = 0 with nodal DG on GLL nodes, approximate quadrature.
+//
+// One warp per element, the element's values staged in shared memory:
+//   volume   per node the physical flux (f, g) = F(u), its contravariant form
+//            (W (y_eta f - x_eta g), W (-y_xi f + x_xi g)), and the D contraction
+//            (DivF2D<true>::action, wavedg/DivF.hpp:203-260; Div<true> for a linear flux);
+//   faces    per face node the numerical flux fh(n, u_own, u_nbr) with n the element's own
+//            outward normal, subtracted times w_k |E| / 2 (EdgeFluxF2D<true>::action,
+//            wavedg/EdgeFluxF.hpp:138-180, with the sign flip and transpose prolongation of
+//            examples/cl2d.cpp:175-219); the neighbour's trace is read from the stage's input
+//            through the partner table of the fused wave kernels;
+//   mass     M^{-1} = 1 / (w_i w_j det J) (MassMatrix<true>);
+//   output   the RHS, or one stage of ode::RungeKutta4 or ode::SSPRK3 (wavedg/ode.hpp:66-93,
+//            145-186) applied in the same pass.
+// Each face contribution uses the element's own normal and the numerical flux's antisymmetry
+// fh(-n, b, a) = -fh(n, a, b), which holds exactly in floating point for both fluxes below, so
+// the two elements of an edge add exactly opposite terms, as the reference's edge loop does.
+//
+// Flux models:
+//   ClawEuler    the compressible Euler system of examples/cl2d.cpp:67-126 (gamma 1.4) with its
+//                local Lax-Friedrichs flux; exterior boundary state = interior state.
+//   ClawLinear   f = A_0 u, g = A_1 u (Advection<true>), upwind flux
+//                fh = 1/2 (n.A)(a + b) + 1/2 |n.A| (a - b), |n.A| per element side from a table
+//                formed at set-up; exterior boundary state 0 (AdvectionHomogeneousBC<true>).
+
+namespace wdg
+{
+    struct ClawEuler
+    {
+        static constexpr double gamma = 1.4;
+        __device__ static void flux(const ClawArgs &, const double *q, double *f, double *g)
+        {
+            const double rho = q[0], u = q[1] / q[0], v = q[2] / q[0], E = q[3];
+            const double p = (gamma - 1.0) * (E - 0.5 * rho * (u * u + v * v));
+            f[0] = rho * u;
+            f[1] = rho * u * u + p;
+            f[2] = rho * u * v;
+            f[3] = u * (E + p);
+            g[0] = rho * v;
+            g[1] = rho * u * v;
+            g[2] = rho * v * v + p;
+            g[3] = v * (E + p);
+        }
+        __device__ static double speed(const double *q)
+        {
+            const double rho = q[0], u = q[1] / q[0], v = q[2] / q[0], E = q[3];
+            const double p = (gamma - 1.0) * (E - 0.5 * rho * (u * u + v * v));
+            return hypot(u, v) + sqrt(gamma * p / rho);
+        }
+        template <int NV>
+        __device__ static void exterior(const double *q, double *x)
+        {
+#pragma unroll
+            for (int d = 0; d < NV; ++d)
+                x[d] = q[d];
+        }
+        template <int NV>
+        __device__ static void numflux(const ClawArgs &a, int, int, double nx, double ny, const double *qL,
+                                       const double *qR, double *fh)
+        {
+            double fL[4], gL[4], fR[4], gR[4];
+            flux(a, qL, fL, gL);
+            flux(a, qR, fR, gR);
+            const double c = fmax(speed(qL), speed(qR));
+#pragma unroll
+            for (int d = 0; d < 4; ++d)
+                fh[d] = 0.5 * nx * (fL[d] + fR[d]) + 0.5 * ny * (gL[d] + gR[d]) + 0.5 * c * (qL[d] - qR[d]);
+        }
+    };
+
+    struct ClawLinear
+    {
+        template <int NV>
+        __device__ static void flux_n(const ClawArgs &a, const double *q, double *f, double *g)
+        {
+#pragma unroll
+            for (int d = 0; d < NV; ++d)
+            {
+                double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+                for (int c = 0; c < NV; ++c)
+                {
+                    s0 += a.A[d + NV * c] * q[c];
+                    s1 += a.A[d + NV * c + NV * NV] * q[c];
+                }
+                f[d] = s0;
+                g[d] = s1;
+            }
+        }
+        template <int NV>
+        __device__ static void exterior(const double *, double *x)
+        {
+#pragma unroll
+            for (int d = 0; d < NV; ++d)
+                x[d] = 0.0;
+        }
+        template <int NV>
+        __device__ static void numflux(const ClawArgs &a, int el, int side, double nx, double ny, const double *qL,
+                                       const double *qR, double *fh)
+        {
+            const double *T = a.absA + (size_t)NV * NV * (4 * (size_t)el + side);
+#pragma unroll
+            for (int d = 0; d < NV; ++d)
+            {
+                double c = 0.0, u = 0.0;
+#pragma unroll
+                for (int k = 0; k < NV; ++k)
+                {
+                    const double nA = nx * a.A[d + NV * k] + ny * a.A[d + NV * k + NV * NV];
+                    c += nA * (qL[k] + qR[k]);
+                    u += T[d + NV * k] * (qL[k] - qR[k]);
+                }
+                fh[d] = 0.5 * c + 0.5 * u;
+            }
+        }
+    };
+
+    template <class M, int NV>
+    __device__ __forceinline__ void claw_flux(const ClawArgs &a, const double *q, double *f, double *g)
+    {
+        if constexpr (std::is_same<M, ClawLinear>::value)
+            ClawLinear::flux_n<NV>(a, q, f, g);
+        else
+            M::flux(a, q, f, g);
+    }
+
+    // outward unit normal and measure (length / 2) of side s of an element with corners c
+    // (StraightEdge, wavedg/Edge.hpp:107-122); side s runs from corner p0 to p1: 0: 0 -> 1,
+    // 1: 1 -> 2, 2: 3 -> 2, 3: 0 -> 3 (sides 2 and 3 against the counter-clockwise order)
+    __device__ __forceinline__ void claw_side(const double *c, int s, double &nx, double &ny, double &meas)
+    {
+        const int p0 = (s == 0 || s == 3) ? 0 : (s == 1 ? 1 : 3), p1 = (s == 0) ? 1 : (s == 3 ? 3 : 2);
+        const double dx = c[2 * p1] - c[2 * p0], dy = c[2 * p1 + 1] - c[2 * p0 + 1];
+        const double len = sqrt(dx * dx + dy * dy), sgn = (s >= 2) ? -1.0 : 1.0;
+        nx = sgn * dy / len;
+        ny = -sgn * dx / len;
+        meas = 0.5 * len;
+    }
+
+    constexpr int kClawWarps = 4;
+
+    template <int N, int NV, class M>
+    __global__ void __launch_bounds__(32 * kClawWarps) claw_kernel(const ClawArgs a)
+    {
+        constexpr int NN = N * N, ND = NV * NN;
+        extern __shared__ double csm[];
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        double *q = csm + (size_t)warp * 3 * ND, *Fs = q + ND, *Gs = Fs + ND;
+        const long long limit = (long long)a.nel * NN; // nodes a neighbour index may name
+        for (int el = blockIdx.x * kClawWarps + warp; el < a.nel; el += gridDim.x * kClawWarps)
+        {
+            const double *xe = a.x + (size_t)el * ND;
+            for (int k = lane; k < ND; k += 32)
+                q[k] = xe[k];
+            double c[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                c[k] = __ldg(a.corners + 8 * (size_t)el + k);
+            const uint32_t codes = __ldg(a.fcode + el);
+            const int4 fb = __ldg(a.fbase + el);
+            __syncwarp();
+            // volume: contravariant fluxes per node
+            for (int node = lane; node < NN; node += 32)
+            {
+                const int i = node % N, j = node / N;
+                const double xi = Tab<double>::x(N, i), eta = Tab<double>::x(N, j);
+                const double Xx = 0.25 * ((1.0 - eta) * (c[2] - c[0]) + (1.0 + eta) * (c[4] - c[6]));
+                const double Yx = 0.25 * ((1.0 - eta) * (c[3] - c[1]) + (1.0 + eta) * (c[5] - c[7]));
+                const double Xe = 0.25 * ((1.0 - xi) * (c[6] - c[0]) + (1.0 + xi) * (c[4] - c[2]));
+                const double Ye = 0.25 * ((1.0 - xi) * (c[7] - c[1]) + (1.0 + xi) * (c[5] - c[3]));
+                const double W = Tab<double>::w(N, i) * Tab<double>::w(N, j);
+                double qq[NV], f[NV], g[NV];
+#pragma unroll
+                for (int d = 0; d < NV; ++d)
+                    qq[d] = q[NV * node + d];
+                claw_flux<M, NV>(a, qq, f, g);
+#pragma unroll
+                for (int d = 0; d < NV; ++d)
+                {
+                    Fs[NV * node + d] = (Ye * W) * f[d] - (Xe * W) * g[d];
+                    Gs[NV * node + d] = -(Yx * W) * f[d] + (Xx * W) * g[d];
+                }
+            }
+            __syncwarp();
+            for (int node = lane; node < NN; node += 32)
+            {
+                const int i = node % N, j = node / N;
+                double r[NV];
+#pragma unroll
+                for (int d = 0; d < NV; ++d)
+                {
+                    double s = 0.0;
+#pragma unroll
+                    for (int l = 0; l < N; ++l)
+                        s += Tab<double>::D(N, l + N * i) * Fs[NV * (l + N * j) + d] +
+                             Tab<double>::D(N, l + N * j) * Gs[NV * (i + N * l) + d];
+                    r[d] = s;
+                }
+                const size_t g0 = (size_t)el * ND + (size_t)NV * node;
+                if (a.mode == CLAW_DIV)
+                {
+#pragma unroll
+                    for (int d = 0; d < NV; ++d)
+                        a.out[g0 + d] += r[d];
+                    continue;
+                }
+                double qq[NV];
+#pragma unroll
+                for (int d = 0; d < NV; ++d)
+                    qq[d] = q[NV * node + d];
+                // faces through this node: side 0 (j = 0, k = i), 1 (i = n-1, k = j),
+                // 2 (j = n-1, k = i), 3 (i = 0, k = j)
+#pragma unroll
+                for (int s = 0; s < 4; ++s)
+                {
+                    const bool on = (s == 0) ? (j == 0) : (s == 1) ? (i == N - 1) : (s == 2) ? (j == N - 1) : (i == 0);
+                    if (!on)
+                        continue;
+                    const int k = (s == 0 || s == 2) ? i : j;
+                    const uint32_t byte = (codes >> (8 * s)) & 0xffu;
+                    double ext[NV];
+                    if (byte & 0x80u)
+                        M::template exterior<NV>(qq, ext);
+                    else
+                    {
+                        const int off = (s == 0) ? fb.x : (s == 1) ? fb.y : (s == 2) ? fb.z : fb.w;
+                        const long long pn = (long long)(off / 3) + (long long)k * (partner_stride<N>(byte) / 3);
+                        if (off < 0 || pn < 0 || pn >= limit)
+                        {
+                            atomicOr(a.err, 2u);
+#pragma unroll
+                            for (int d = 0; d < NV; ++d)
+                                ext[d] = qq[d];
+                        }
+                        else
+                        {
+#pragma unroll
+                            for (int d = 0; d < NV; ++d)
+                                ext[d] = __ldg(a.x + (size_t)NV * pn + d);
+                        }
+                    }
+                    double nx, ny, meas, fh[NV];
+                    claw_side(c, s, nx, ny, meas);
+                    M::template numflux<NV>(a, el, s, nx, ny, qq, ext, fh);
+                    const double wk = Tab<double>::w(N, k) * meas;
+#pragma unroll
+                    for (int d = 0; d < NV; ++d)
+                        r[d] -= wk * fh[d];
+                }
+                // M^{-1}: w_i w_j det J (MassMatrix<true>)
+                {
+                    const double xi = Tab<double>::x(N, i), eta = Tab<double>::x(N, j);
+                    const double Xx = 0.25 * ((1.0 - eta) * (c[2] - c[0]) + (1.0 + eta) * (c[4] - c[6]));
+                    const double Yx = 0.25 * ((1.0 - eta) * (c[3] - c[1]) + (1.0 + eta) * (c[5] - c[7]));
+                    const double Xe = 0.25 * ((1.0 - xi) * (c[6] - c[0]) + (1.0 + xi) * (c[4] - c[2]));
+                    const double Ye = 0.25 * ((1.0 - xi) * (c[7] - c[1]) + (1.0 + xi) * (c[5] - c[3]));
+                    const double m = Tab<double>::w(N, i) * Tab<double>::w(N, j) * (Xx * Ye - Yx * Xe);
+#pragma unroll
+                    for (int d = 0; d < NV; ++d)
+                        r[d] /= m;
+                }
+                switch (a.mode)
+                {
+                case CLAW_RHS:
+#pragma unroll
+                    for (int d = 0; d < NV; ++d)
+                        a.out[g0 + d] = r[d];
+                    break;
+                case CLAW_RK4:
+#pragma unroll
+                    for (int d = 0; d < NV; ++d)
+                    {
+                        const double kd = (a.rk_a == 0.0) ? a.dt * r[d] : a.rk_a * a.du[g0 + d] + a.dt * r[d];
+                        a.du[g0 + d] = kd;
+                        a.out[g0 + d] = qq[d] + a.rk_b * kd;
+                    }
+                    break;
+                case CLAW_SSP0:
+#pragma unroll
+                    for (int d = 0; d < NV; ++d)
+                        a.out[g0 + d] = qq[d] + a.dt * r[d];
+                    break;
+                case CLAW_SSP1:
+#pragma unroll
+                    for (int d = 0; d < NV; ++d)
+                        a.out[g0 + d] = 0.25 * (qq[d] + 3.0 * a.base[g0 + d] + a.dt * r[d]);
+                    break;
+                default: // CLAW_SSP2
+#pragma unroll
+                    for (int d = 0; d < NV; ++d)
+                        a.out[g0 + d] = (a.base[g0 + d] + 2.0 * qq[d] + 2.0 * a.dt * r[d]) / 3.0;
+                    break;
+                }
+            }
+            __syncwarp(); // the element's staging is reused for the next one
+        }
+    }
+
+    // EdgeFluxF2D<true>::action for the Euler system on face traces (n, 4, 2, edges): thread per
+    // (face node, edge); fB = +- w_i |E| / 2 fh(n, side 0, side 1), n the outward normal of the
+    // edge's first element (in place allowed: a thread reads its node's traces before writing)
+    __global__ void euler_face_flux_kernel(int n, int ne, const int *__restrict__ edges, const double *__restrict__ corners,
+                                           const double *ub, double *fb)
+    {
+        const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+        if (q >= (long long)n * ne)
+            return;
+        const int i = (int)(q % n), e = (int)(q / n);
+        const int el = edges[5 * (size_t)e], s = edges[5 * (size_t)e + 1];
+        double c[8];
+        for (int k = 0; k < 8; ++k)
+            c[k] = corners[8 * (size_t)el + k];
+        double nx, ny, meas, qL[4], qR[4], fh[4];
+        claw_side(c, s, nx, ny, meas);
+        for (int d = 0; d < 4; ++d)
+        {
+            qL[d] = ub[i + n * (d + 4 * (0 + 2 * (size_t)e))];
+            qR[d] = ub[i + n * (d + 4 * (1 + 2 * (size_t)e))];
+        }
+        ClawArgs none{};
+        ClawEuler::numflux<4>(none, 0, 0, nx, ny, qL, qR, fh);
+        const double wm = c_tab[n].w[i] * meas;
+        for (int d = 0; d < 4; ++d)
+        {
+            fb[i + n * (d + 4 * (0 + 2 * (size_t)e))] = fh[d] * wm;
+            fb[i + n * (d + 4 * (1 + 2 * (size_t)e))] = -fh[d] * wm;
+        }
+    }
+
+    // shared memory of one CTA of claw_kernel
+    inline size_t claw_smem(int n, int nv) { return sizeof(double) * 3 * (size_t)nv * n * n * kClawWarps; }
+
+    template <int N, int NV, class M>
+    cudaError_t launch_claw_nv(const ClawArgs &a, cudaStream_t s)
+    {
+        const size_t smem = claw_smem(N, NV);
+        auto kern = claw_kernel<N, NV, M>;
+        if (smem > 48 * 1024)
+        {
+            static uint64_t set = 0; // devices whose attribute is set
+            int dev = 0;
+            cudaGetDevice(&dev);
+            if (!(set & (1ull << (dev & 63))))
+            {
+                cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                if (e != cudaSuccess)
+                    return e;
+                set |= 1ull << (dev & 63);
+            }
+        }
+        const int blocks = std::max(1, std::min((a.nel + kClawWarps - 1) / kClawWarps, 148 * 16));
+        kern<<<blocks, 32 * kClawWarps, smem, s>>>(a);
+        return cudaGetLastError();
+    }
+
+    template <int N, class M>
+    cudaError_t launch_claw_n(int nv, const ClawArgs &a, cudaStream_t s)
+    {
+        if constexpr (std::is_same<M, ClawEuler>::value)
+            return nv == 4 ? launch_claw_nv<N, 4, M>(a, s) : cudaErrorInvalidValue;
+        else
+        {
+            switch (nv)
+            {
+            case 1: return launch_claw_nv<N, 1, M>(a, s);
+            case 2: return launch_claw_nv<N, 2, M>(a, s);
+            case 3: return launch_claw_nv<N, 3, M>(a, s);
+            case 4: return launch_claw_nv<N, 4, M>(a, s);
+            case 5: return launch_claw_nv<N, 5, M>(a, s);
+            case 6: return launch_claw_nv<N, 6, M>(a, s);
+            case 7: return launch_claw_nv<N, 7, M>(a, s);
+            case 8: return launch_claw_nv<N, 8, M>(a, s);
+            default: return cudaErrorInvalidValue;
+            }
+        }
+    }
+
+    template <class M>
+    cudaError_t launch_claw_m(int n, int nv, const ClawArgs &a, cudaStream_t s)
+    {
+        switch (n)
+        {
+        case 2: return launch_claw_n<2, M>(nv, a, s);
+        case 3: return launch_claw_n<3, M>(nv, a, s);
+        case 4: return launch_claw_n<4, M>(nv, a, s);
+        case 5: return launch_claw_n<5, M>(nv, a, s);
+        case 6: return launch_claw_n<6, M>(nv, a, s);
+        case 7: return launch_claw_n<7, M>(nv, a, s);
+        case 8: return launch_claw_n<8, M>(nv, a, s);
+        case 9: return launch_claw_n<9, M>(nv, a, s);
+        default: return cudaErrorInvalidValue;
+        }
+    }
+} // namespace wdg

@@ -1005,10 +1005,25 @@ namespace wdg
 
 #include "stage_ws.cuh"
 #include "stage_ws_batch.cuh"
+#include "claw_kernels.cuh"
 
 namespace wdg
 {
     int ws_chunk_unit(int n) { return kWsConsumers * ws_epw(n); }
+
+    cudaError_t launch_claw(int model, int n, int nv, const ClawArgs &a, cudaStream_t s)
+    {
+        return model == 0 ? launch_claw_m<ClawEuler>(n, nv, a, s) : launch_claw_m<ClawLinear>(n, nv, a, s);
+    }
+    cudaError_t launch_euler_face_flux(int n, int ne, const int *edges, const double *corners, const double *ub,
+                                       double *fb, cudaStream_t s)
+    {
+        if (ne == 0)
+            return cudaSuccess;
+        const long long tot = (long long)n * ne;
+        euler_face_flux_kernel<<<(unsigned)((tot + 127) / 128), 128, 0, s>>>(n, ne, edges, corners, ub, fb);
+        return cudaGetLastError();
+    }
     int ws_slot_bytes(int n, bool fp32, int chunk, bool extra, bool filter)
     {
         const bool staged = extra && (fp32 ? WsStage<float, true>::value : WsStage<double, true>::value);

@@ -81,6 +81,37 @@ namespace wdg
     constexpr int kWsDefaultRing = 2;
     int ws_default_chunk(int n, bool fp32);   // most rounds (<= 4) whose default ring fits 3 CTAs per SM
 
+    // one launch of the fused conservation-law kernels (claw_kernels.cuh)
+    struct ClawArgs
+    {
+        const double *x;      // state the RHS is evaluated at (neighbour traces come from it)
+        double *out;          // CLAW_RHS: dudt; CLAW_DIV: += volume term; RK4: u'; SSPRK3: stage result
+        double *du;           // RK4 register, in place
+        const double *base;   // SSPRK3 stages 1 and 2: u(t)
+        const double *corners;
+        const int4 *fbase;    // partner tables of the wave kernels (3 values per node): /3 gives nodes
+        const uint32_t *fcode;
+        const double *A;      // ClawLinear: A_0, A_1 as a(d, c, k) = A[d + nv (c + nv k)]
+        const double *absA;   // ClawLinear: |n.A| per element side, (nv, nv, 4, nel)
+        unsigned *err;
+        int nel, mode;
+        double rk_a, rk_b, dt;
+    };
+    enum
+    {
+        CLAW_RHS = 0,
+        CLAW_DIV = 1,
+        CLAW_RK4 = 2,
+        CLAW_SSP0 = 3,
+        CLAW_SSP1 = 4,
+        CLAW_SSP2 = 5
+    };
+
+    // model 0: compressible Euler (n_var 4), 1: linear with constant coefficients (n_var 1..8)
+    cudaError_t launch_claw(int model, int n, int nv, const ClawArgs &a, cudaStream_t s);
+    cudaError_t launch_euler_face_flux(int n, int ne, const int *edges, const double *corners, const double *ub,
+                                       double *fb, cudaStream_t s);
+
     // default limit of a bounded device-side wait (a lost copy completion; never reached otherwise)
     constexpr unsigned long long kWaitLimitNs = 2000000000ull;
 

@@ -78,6 +78,12 @@ namespace wdg
 
     extern const double rk4a[5], rk4b[5], rk4c[5];
 
+    // fused conservation-law kernels (claw.cu): launch arguments on a handle's geometry, and
+    // nsteps of RK4 (method 0) or SSPRK3 (method 1) on device array u; bufs: 3 arrays of u's size
+    ClawArgs claw_args(const wdg_wave *w, const double *x, double *out);
+    int claw_steps(wdg_wave *w, int model, int nv, const double *A, const double *absA, double *const *bufs, int method,
+                   double *u, double dt, double *t, int nsteps);
+
     // An FP64 array argument of a C-ABI call: the caller's device pointer, or a staging buffer
     // filled from (and, for outputs, copied back to) the caller's host array.
     struct HostArg

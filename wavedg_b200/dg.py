@@ -805,6 +805,61 @@ class AdvectionSystem:
         return tt.value
 
 
+class EulerSystem:
+    """The compressible Euler system of examples/cl2d.cpp (wdg_euler_create, wdg_claw_*): state
+    u(d, i, j, el) with d = density, x-momentum, y-momentum, energy, gamma = 1.4; DivF2D<true>
+    with the example's flux, EdgeFluxF2D<true> with its local Lax-Friedrichs flux (exterior
+    boundary state = interior state), MassMatrix<true>, on GLL nodes.  FP64."""
+
+    n_var = 4
+
+    def __init__(self, mesh: Mesh2D, basis, device: int = -1):
+        self.mesh, self.n = mesh, _gll_n(basis)
+        h = C.c_void_p()
+        check(lib().wdg_euler_create(mesh._h, self.n, device, C.byref(h)), "wdg_euler_create")
+        self._h = h
+        self.ndof = 4 * self.n * self.n * mesh.n_elem()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _destroy("wdg_claw_destroy", h)
+            self._h = None
+
+    def set_stream(self, stream) -> None:
+        check(lib().wdg_claw_set_stream(self._h, C.c_void_p(getattr(stream, "cuda_stream", stream))))
+
+    def sync(self) -> None:
+        check(lib().wdg_claw_sync(self._h))
+
+    def div(self, u, divF) -> None:
+        """DivF2D<true>::action: divF += (F(u), grad v)."""
+        pu, _ku = _ptr(u, name="u")
+        pd, _kd = _ptr(divF, True, "divF")
+        check(lib().wdg_claw_div(self._h, pu, pd), "DivF2D.action")
+
+    def flux(self, face_type: int, uB, fB) -> None:
+        """EdgeFluxF2D<true>::action on face traces (n, 4, 2, n_edges); fB may be uB."""
+        pu, _ku = _ptr(uB, name="uB")
+        pf, _kf = _ptr(fB, True, "fB")
+        check(lib().wdg_claw_flux(self._h, int(face_type), pu, pf), "EdgeFluxF2D.action")
+
+    def rhs(self, u, dudt) -> None:
+        """The time derivative of examples/cl2d.cpp (approx_quad = true)."""
+        pu, _ku = _ptr(u, name="u")
+        pd, _kd = _ptr(dudt, True, "dudt")
+        check(lib().wdg_claw_rhs(self._h, pu, pd), "rhs")
+
+    def steps(self, u, dt: float, t: float, nsteps: int, method: str = "ssprk3") -> float:
+        """nsteps of ode::SSPRK3 ("ssprk3", the example's stepper) or ode::RungeKutta4 ("rk4")
+        on u in place; returns the new time."""
+        pu, _ku = _ptr(u, True, "u")
+        tt = C.c_double(t)
+        check(lib().wdg_claw_steps(self._h, {"rk4": 0, "ssprk3": 1}[method], pu, float(dt), C.byref(tt),
+                                   int(nsteps)), "steps")
+        return tt.value
+
+
 class Advection(Operator):
     """Advection<true>(n_var, mesh, basis, a, constant_coefficient): du += (A u, grad v) + upwind
     flux over interior edges (wavedg/Advection.hpp:17-142).  Constant symmetric coefficients."""
