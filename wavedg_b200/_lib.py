@@ -12,7 +12,8 @@ import re
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 # WDG_B200_LIB selects another build of the library (e.g. one compiled with different options)
-LIB_PATH = os.environ.get("WDG_B200_LIB") or os.path.join(HERE, "libwdg_b200.so")
+PACKAGE_LIB = os.path.join(HERE, "libwdg_b200.so")
+LIB_PATH = os.environ.get("WDG_B200_LIB") or PACKAGE_LIB
 HEADER = os.path.join(ROOT, "include", "wdg_b200.h")
 
 WDG_OK = 0
@@ -185,6 +186,8 @@ def lib():
                       "(or __graft_entry__.build()).  There is no CPU fallback.")
     L = C.CDLL(LIB_PATH)
     for name, (args, res) in SIGNATURES.items():
+        if LIB_PATH != PACKAGE_LIB and not hasattr(L, name):
+            continue  # another build without this entry point: calling it raises AttributeError
         fn = getattr(L, name)
         fn.argtypes = args
         fn.restype = res

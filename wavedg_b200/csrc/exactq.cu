@@ -12,16 +12,21 @@
 // 1 + (2 (n-1) + 2) / 2.  Face prolongation, the exterior states of the boundary codes and
 // the argument staging are the collocation handle's (an internal wdg_wave, FP64).
 //
-// FP64 only.  This is the accuracy path for callers that set approx_quad = false, not the
-// bandwidth-bound hot path: one CTA per element for the volume term, one thread per edge
-// for the face term, one warp per element for the mass matrix and its inverse (formed at
-// set-up from the block Cholesky factors, applied as dense products).
+// FP64 only.  The accuracy path for callers that set approx_quad = false.  The RHS and every
+// RK4 stage (WaveHoltz periods included) are one fused launch, a warp per element
+// (qfused_kernel: volume term, the four faces through the partner table, forcing, the dense
+// inverse mass matrix formed at set-up from the block Cholesky factors, the stage update);
+// the operator entry points (Div, EdgeFlux, the mass matrix and its inverse) keep component
+// kernels in the reference layouts: one CTA per element for the volume term, one thread per
+// edge for the face term, one warp per element for the dense mass products.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
+#include "wave_bc.cuh"
 #include "wave_impl.hpp"
 
 using namespace wdg;
@@ -35,7 +40,6 @@ struct wdg_waveq
     double *d_nI = nullptr, *d_nB = nullptr; // per edge (n_x, n_y, |E| / 2)
     double *d_M = nullptr, *d_Minv = nullptr; // element mass matrices and their inverses (n^2, n^2, nel)
     double *d_uf = nullptr, *d_uB = nullptr; // face traces
-    double *d_rk = nullptr;                  // RK4: k and the stage derivative (2 ndof)
 };
 
 namespace
@@ -267,30 +271,328 @@ namespace
         }
     }
 
-    __global__ void axpy_kernel(double *y, const double *x, double a, long long n)
+    // ---------------------------------------------------------------- fused RHS / RK4 stage
+    // One warp per element does what rhs_dev's chain of launches does, in one pass over the
+    // element: the Gauss-point volume term of Div<false> (as qdiv_kernel), the four faces of
+    // EdgeFlux<false> / WaveBC (the element's own nodal trace and its neighbour's, read through
+    // the fused kernels' partner table, or the exterior state of the boundary code at the
+    // nodes, both interpolated to the face rule; the closed-form upwind flux of qflux_kernel
+    // with the element's own outward normal, which makes the two elements of an edge add
+    // exactly opposite terms; projected back to the face nodes), the forcing s F, the dense
+    // inverse mass matrix, then the RHS or the RK4 stage update (with the WaveHoltz filter on
+    // the last stage).
+    struct QFusedArgs
     {
-        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-            y[i] += a * x[i];
+        const double *x;      // state the RHS is evaluated at
+        double *out;          // RHS: dudt; RK4: u'
+        double *du;           // RK4 register
+        const double *F;      // forcing (nullable) times fs
+        double fs;
+        double *acc;          // FP64 filter (stage 4, nullable) += acc_c u'
+        double acc_c;
+        const double *corners, *xd, *wd, *Pd, *Dd, *wf, *Pf, *Minv;
+        const int4 *fbase;
+        const uint32_t *fcode;
+        unsigned *err;
+        int n, q, qf, nel, rk; // rk: 0 RHS, 1 RK4 stage (rk_a == 0 on the first)
+        double rk_a, rk_b, dt;
+    };
+    constexpr int kQWarps = 4;
+
+    __host__ __device__ inline int qfused_warp_doubles(int n, int q, int qf)
+    {
+        // su r (3 n^2 each) | Pu (3 n q) | Uq (3 q^2) | Fq (6 q^2) | Df Pg (3 q n each) | T1 (4 n 3) | UF (4 qf 3)
+        return 6 * n * n + 3 * n * q + 9 * q * q + 6 * q * n + 12 * n + 12 * qf;
     }
-    // one low-storage RK4 stage update: k = a k + dt p; u += b k
-    __global__ void rk_stage_kernel(double *u, double *k, const double *p, double a, double b, double dt, bool first,
-                                    long long n)
+
+    // outward unit normal and measure (length / 2) of side s (StraightEdge, wavedg/Edge.hpp:107-122);
+    // side s runs from corner p0 to p1: 0: 0 -> 1, 1: 1 -> 2, 2: 3 -> 2, 3: 0 -> 3
+    __device__ inline void qside(const double *c, int s, double &nx, double &ny, double &meas)
     {
-        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        const int p0 = (s == 0 || s == 3) ? 0 : (s == 1 ? 1 : 3), p1 = (s == 0) ? 1 : (s == 3 ? 3 : 2);
+        const double dx = c[2 * p1] - c[2 * p0], dy = c[2 * p1 + 1] - c[2 * p0 + 1];
+        const double len = sqrt(dx * dx + dy * dy), sgn = (s >= 2) ? -1.0 : 1.0;
+        nx = sgn * dy / len;
+        ny = -sgn * dx / len;
+        meas = 0.5 * len;
+    }
+    // partner walk of a side code (bits 0-1): +3, -3, +3n, -3n values per face node
+    __device__ inline int qstride(int n, uint32_t byte)
+    {
+        const uint32_t c = byte & 3u;
+        return (c == 0) ? 3 : (c == 1) ? -3 : (c == 2) ? 3 * n : -3 * n;
+    }
+
+    __device__ inline int qface_node(int n, int s, int k)
+    {
+        const int i = (s == 0 || s == 2) ? k : (s == 1 ? n - 1 : 0);
+        const int j = (s == 1 || s == 3) ? k : (s == 2 ? n - 1 : 0);
+        return i + n * j;
+    }
+
+    __global__ void __launch_bounds__(32 * kQWarps) qfused_kernel(const QFusedArgs a)
+    {
+        extern __shared__ double qsm[];
+        const int n = a.n, q = a.q, qf = a.qf, nn = n * n, qq = q * q;
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        double *su = qsm + (size_t)warp * qfused_warp_doubles(n, q, qf);
+        double *r = su + 3 * nn, *Pu = r + 3 * nn, *Uq = Pu + 3 * n * q, *Fq = Uq + 3 * qq, *Df = Fq + 6 * qq;
+        double *Pg = Df + 3 * q * n, *T1 = Pg + 3 * q * n, *UF = T1 + 12 * n;
+        const long long limit = 3LL * nn * a.nel;
+        for (int el = blockIdx.x * kQWarps + warp; el < a.nel; el += gridDim.x * kQWarps)
         {
-            const double ki = first ? dt * p[i] : a * k[i] + dt * p[i];
-            k[i] = ki;
-            u[i] += b * ki;
+            const double *ue = a.x + (size_t)3 * nn * el;
+            for (int k = lane; k < 3 * nn; k += 32)
+            {
+                su[k] = ue[k];
+                r[k] = 0.0;
+            }
+            double c[8];
+            for (int k = 0; k < 8; ++k)
+                c[k] = __ldg(a.corners + 8 * (size_t)el + k);
+            const uint32_t codes = __ldg(a.fcode + el);
+            const int4 fb = __ldg(a.fbase + el);
+            __syncwarp();
+            // ---- volume (Div<false>): Pu, U at the points, fluxes, half contractions, back
+            for (int o = lane; o < 3 * n * q; o += 32)
+            {
+                const int l = o % n, d = (o / n) % 3, i = o / (3 * n);
+                double s = 0.0;
+                for (int k = 0; k < n; ++k)
+                    s += a.Pd[i + q * k] * su[d + 3 * (k + n * l)];
+                Pu[o] = s;
+            }
+            __syncwarp();
+            for (int o = lane; o < 3 * qq; o += 32)
+            {
+                const int d = o % 3, i = (o / 3) % q, j = o / (3 * q);
+                double s = 0.0;
+                for (int l = 0; l < n; ++l)
+                    s += a.Pd[j + q * l] * Pu[l + n * (d + 3 * i)];
+                Uq[o] = s;
+            }
+            __syncwarp();
+            for (int o = lane; o < qq; o += 32)
+            {
+                const int i = o % q, j = o / q;
+                double J[4];
+                jac(c, a.xd[i], a.xd[j], J);
+                const double W = a.wd[i] * a.wd[j];
+                const double Xxi = J[0] * W, Yxi = J[1] * W, Xeta = J[2] * W, Yeta = J[3] * W;
+                const double *U = Uq + 3 * o;
+                double *Fo = Fq + 6 * o;
+                Fo[0] = Yeta * U[1] - Xeta * U[2];
+                Fo[1] = -Yxi * U[1] + Xxi * U[2];
+                Fo[2] = Yeta * U[0];
+                Fo[3] = -Yxi * U[0];
+                Fo[4] = -Xeta * U[0];
+                Fo[5] = Xxi * U[0];
+            }
+            __syncwarp();
+            for (int o = lane; o < 3 * q * n; o += 32)
+            {
+                const int j = o % q, d = (o / q) % 3, k = o / (3 * q);
+                double df = 0.0, pg = 0.0;
+                for (int i = 0; i < q; ++i)
+                {
+                    df += a.Dd[i + q * k] * Fq[2 * d + 6 * (i + q * j)];
+                    pg += a.Pd[i + q * k] * Fq[2 * d + 1 + 6 * (i + q * j)];
+                }
+                Df[o] = df;
+                Pg[o] = pg;
+            }
+            // ---- neighbour / exterior nodal traces of the four sides, face-node order: T1(s, k, d)
+            for (int o = lane; o < 4 * n; o += 32)
+            {
+                const int s = o / n, k = o - s * n;
+                const uint32_t byte = (codes >> (8 * s)) & 0xffu;
+                const double *own = su + 3 * qface_node(n, s, k);
+                double *t1 = T1 + 3 * o;
+                if (byte & 0x80u)
+                {
+                    double nx, ny, meas;
+                    qside(c, s, nx, ny, meas);
+                    const double qv[3] = {own[0], own[1], own[2]};
+                    exterior<double>((int)((byte >> 3) & 3u), nx, ny, qv, t1);
+                }
+                else
+                {
+                    const int off = (s == 0) ? fb.x : (s == 1) ? fb.y : (s == 2) ? fb.z : fb.w;
+                    const long long pos = (long long)off + (long long)k * qstride(n, byte);
+                    if (off < 0 || pos < 0 || pos + 3 > limit)
+                    {
+                        atomicOr(a.err, 2u);
+                        t1[0] = own[0];
+                        t1[1] = own[1];
+                        t1[2] = own[2];
+                    }
+                    else
+                    {
+                        t1[0] = __ldg(a.x + pos);
+                        t1[1] = __ldg(a.x + pos + 1);
+                        t1[2] = __ldg(a.x + pos + 2);
+                    }
+                }
+            }
+            __syncwarp();
+            // volume result into r
+            for (int o = lane; o < 3 * nn; o += 32)
+            {
+                const int d = o % 3, k = (o / 3) % n, l = o / (3 * n);
+                double s = 0.0;
+                for (int j = 0; j < q; ++j)
+                    s += a.Pd[j + q * l] * Df[j + q * (d + 3 * k)] + a.Dd[j + q * l] * Pg[j + q * (d + 3 * k)];
+                r[o] = s;
+            }
+            // ---- face points: both traces to the face rule, upwind flux: UF(s, i, d)
+            for (int o = lane; o < 4 * qf; o += 32)
+            {
+                const int s = o / qf, i = o - s * qf;
+                double nx, ny, meas;
+                qside(c, s, nx, ny, meas);
+                double U0[3] = {0.0, 0.0, 0.0}, U1[3] = {0.0, 0.0, 0.0};
+                for (int j = 0; j < n; ++j)
+                {
+                    const double p = a.Pf[i + qf * j];
+                    const double *own = su + 3 * qface_node(n, s, j), *nb = T1 + 3 * (s * n + j);
+                    for (int d = 0; d < 3; ++d)
+                    {
+                        U0[d] += own[d] * p;
+                        U1[d] += nb[d] * p;
+                    }
+                }
+                const double w = a.wf[i] * meas;
+                const double s0 = -0.5 * w * (U0[0] + nx * U0[1] + ny * U0[2]);
+                const double s1 = 0.5 * w * (U1[0] - nx * U1[1] - ny * U1[2]);
+                UF[3 * o] = s0 + s1;
+                UF[3 * o + 1] = nx * (s0 - s1);
+                UF[3 * o + 2] = ny * (s0 - s1);
+            }
+            __syncwarp();
+            // back to the face nodes: sides 0 and 2, then 1 and 3 (corner nodes are shared only
+            // by neighbouring sides)
+            for (int pass = 0; pass < 2; ++pass)
+            {
+                for (int o = lane; o < 2 * n; o += 32)
+                {
+                    const int s = pass + 2 * (o / n), k = o % n;
+                    const int node = qface_node(n, s, k);
+                    for (int d = 0; d < 3; ++d)
+                    {
+                        double f = 0.0;
+                        for (int j = 0; j < qf; ++j)
+                            f += UF[3 * (s * qf + j) + d] * a.Pf[j + qf * k];
+                        r[3 * node + d] += f;
+                    }
+                }
+                __syncwarp();
+            }
+            // ---- forcing, then M^{-1} and the output: lane per row of the element's matrix
+            if (a.F)
+            {
+                for (int o = lane; o < 3 * nn; o += 32)
+                    r[o] += a.fs * __ldg(a.F + (size_t)3 * nn * el + o);
+                __syncwarp();
+            }
+            const double *Me = a.Minv + (size_t)nn * nn * el;
+            for (int row = lane; row < nn; row += 32)
+            {
+                double y[3] = {0.0, 0.0, 0.0};
+                for (int j = 0; j < nn; ++j)
+                {
+                    const double m = __ldg(Me + row + (size_t)nn * j);
+                    y[0] += m * r[3 * j];
+                    y[1] += m * r[3 * j + 1];
+                    y[2] += m * r[3 * j + 2];
+                }
+                const size_t g = (size_t)3 * (nn * (size_t)el + row);
+                for (int d = 0; d < 3; ++d)
+                {
+                    if (!a.rk)
+                    {
+                        a.out[g + d] = y[d];
+                        continue;
+                    }
+                    const double kd = (a.rk_a == 0.0) ? a.dt * y[d] : a.rk_a * a.du[g + d] + a.dt * y[d];
+                    a.du[g + d] = kd;
+                    const double un = su[3 * row + d] + a.rk_b * kd;
+                    a.out[g + d] = un;
+                    if (a.acc)
+                        a.acc[g + d] += a.acc_c * un;
+                }
+            }
+            __syncwarp();
         }
     }
 
-    unsigned grid_for(long long n, int threads) { return (unsigned)std::min<long long>((n + threads - 1) / threads, 148LL * 32); }
 
 
 
     size_t face_count(const wdg_waveq *h, int type)
     {
         return (size_t)h->n * 3 * 2 * (type == 0 ? h->w->nI : h->w->nB);
+    }
+
+    // one launch of the fused kernel on the handle's tables (shared memory above 48 KB is opted
+    // in once per device when the handle is created)
+    int qfused_launch(wdg_waveq *h, QFusedArgs &a)
+    {
+        wdg_wave *w = h->w;
+        a.corners = w->d_corners;
+        a.xd = h->d_xd;
+        a.wd = h->d_wd;
+        a.Pd = h->d_Pd;
+        a.Dd = h->d_Dd;
+        a.wf = h->d_wf;
+        a.Pf = h->d_Pf;
+        a.Minv = h->d_Minv;
+        a.fbase = w->d_fbase;
+        a.fcode = w->d_fcode;
+        a.err = w->d_err;
+        a.n = h->n;
+        a.q = h->nqd;
+        a.qf = h->nqf;
+        a.nel = w->nel;
+        const size_t smem = sizeof(double) * kQWarps * qfused_warp_doubles(h->n, h->nqd, h->nqf);
+        const unsigned blocks = (unsigned)std::max(1, std::min((w->nel + kQWarps - 1) / kQWarps, 148 * 16));
+        qfused_kernel<<<blocks, 32 * kQWarps, smem, w->stream>>>(a);
+        WDG_CUDA(cudaGetLastError());
+        return WDG_OK;
+    }
+
+    // nsteps of ode::RungeKutta4 on device array u (not a rotation buffer), one fused launch per
+    // stage: the rotation u -> B -> C -> B -> C -> u of the wave handle's buffers; with F, the
+    // forcing F s(t) at the stage times; with acc, acc += c_filter[step] u after each step
+    int qfused_rk4(wdg_waveq *h, double *u, double dt, double t, int nsteps, const double *F, double omega,
+                   double *acc, const double *c_filter)
+    {
+        wdg_wave *w = h->w;
+        WDG_TRY(ensure_states(w));
+        double *B = static_cast<double *>(w->d_state[1]), *Cb = static_cast<double *>(w->d_state[2]);
+        QFusedArgs a{};
+        a.du = static_cast<double *>(w->d_du);
+        a.rk = 1;
+        a.dt = dt;
+        a.F = F;
+        for (int step = 0; step < nsteps; ++step)
+        {
+            const double *src = u;
+            for (int st = 0; st < 5; ++st)
+            {
+                double *dst = (st == 4) ? u : ((st % 2 == 0) ? B : Cb);
+                a.x = src;
+                a.out = dst;
+                a.rk_a = rk4a[st];
+                a.rk_b = rk4b[st];
+                a.fs = F ? -std::sin(omega * (t + rk4c[st] * dt)) / omega : 0.0;
+                a.acc = (st == 4) ? acc : nullptr;
+                a.acc_c = (st == 4 && acc) ? c_filter[step] : 0.0;
+                WDG_TRY(qfused_launch(h, a));
+                src = dst;
+            }
+            t += dt;
+        }
+        return WDG_OK;
     }
 
     // ---------------------------------------------------------------- device-side operators
@@ -351,19 +653,15 @@ namespace
         WDG_CUDA(launch_prolong_t(w->geo, 1, h->d_uB, du, w->stream));
         return WDG_OK;
     }
-    // dudt = M^{-1} (A u + B u + s F)
+    // dudt = M^{-1} (A u + B u + s F), one fused launch
     int rhs_dev(wdg_waveq *h, const double *u, double *dudt, const double *F, double s)
     {
-        wdg_wave *w = h->w;
-        WDG_CUDA(cudaMemsetAsync(dudt, 0, sizeof(double) * w->ndof, w->stream));
-        WDG_TRY(wave_dev(h, u, dudt));
-        WDG_TRY(bc_dev(h, u, dudt));
-        if (F)
-        {
-            axpy_kernel<<<grid_for(w->ndof, 256), 256, 0, w->stream>>>(dudt, F, s, w->ndof);
-            WDG_CUDA(cudaGetLastError());
-        }
-        return mass_dev(h, 3, dudt, true);
+        QFusedArgs a{};
+        a.x = u;
+        a.out = dudt;
+        a.F = F;
+        a.fs = s;
+        return qfused_launch(h, a);
     }
 
     typedef int (*Unary)(wdg_waveq *, const double *, double *);
@@ -388,10 +686,7 @@ namespace wdg
     int waveq_prepare(wdg_waveq *h)
     {
         DeviceScope g(h->w->device);
-        WDG_TRY(ensure_states(h->w));
-        if (!h->d_rk)
-            WDG_TRY(device_alloc(&h->d_rk, 2 * (size_t)h->w->ndof));
-        return WDG_OK;
+        return ensure_states(h->w);
     }
 
     // One WaveHoltz period on the exact-quadrature operators, the sequence rk4_run runs on the
@@ -401,24 +696,7 @@ namespace wdg
     int waveq_period(wdg_waveq *h, double *u, double dt, int nt, const double *F, double omega, double *acc,
                      const double *c_filter)
     {
-        wdg_wave *w = h->w;
-        double *k = h->d_rk, *p = h->d_rk + w->ndof;
-        const unsigned gr = grid_for(w->ndof, 256);
-        double t = 0.0;
-        for (int step = 0; step < nt; ++step)
-        {
-            for (int st = 0; st < 5; ++st)
-            {
-                const double s = F ? -std::sin(omega * (t + rk4c[st] * dt)) / omega : 0.0;
-                WDG_TRY(rhs_dev(h, u, p, F, s));
-                rk_stage_kernel<<<gr, 256, 0, w->stream>>>(u, k, p, rk4a[st], rk4b[st], dt, st == 0, w->ndof);
-                WDG_CUDA(cudaGetLastError());
-            }
-            axpy_kernel<<<gr, 256, 0, w->stream>>>(acc, u, c_filter[step], w->ndof);
-            WDG_CUDA(cudaGetLastError());
-            t += dt;
-        }
-        return WDG_OK;
+        return qfused_rk4(h, u, dt, 0.0, nt, F, omega, acc, c_filter);
     }
 
     // P = M^{-1}(A + B) W on the exact operators (WaveHoltz::postprocess's RHS)
@@ -443,6 +721,25 @@ extern "C"
         h->nqf = qface(n_colloc);
         h->nqm = qface(n_colloc);
         DeviceScope g(w->device);
+        {
+            // the fused kernel's shared memory (69.5 KB at n = 9), opted in once per device and
+            // before any period is captured into a graph
+            static std::mutex mu;
+            static uint64_t set = 0;
+            std::lock_guard<std::mutex> lock(mu);
+            if (!(set & (1ull << (w->device & 63))))
+            {
+                const cudaError_t e = cudaFuncSetAttribute(qfused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                           100 * 1024);
+                if (e != cudaSuccess)
+                {
+                    wdg_wave_destroy(w);
+                    delete h;
+                    return cuda_fail(e, "cudaFuncSetAttribute(qfused_kernel)");
+                }
+                set |= 1ull << (w->device & 63);
+            }
+        }
         const int n = n_colloc, c = n * n;
         std::vector<double> x(n), wg(n);
         gauss_lobatto(n, x.data(), wg.data());
@@ -598,7 +895,7 @@ extern "C"
         {
             DeviceScope g(h->w ? h->w->device : 0);
             for (double *p : {h->d_xd, h->d_wd, h->d_Pd, h->d_Dd, h->d_wf, h->d_Pf, h->d_nI, h->d_nB, h->d_M, h->d_Minv, h->d_uf,
-                              h->d_uB, h->d_rk})
+                              h->d_uB})
                 if (p)
                     cudaFree(p);
         }
@@ -703,22 +1000,11 @@ extern "C"
             return fail(WDG_ERR_ARG, "wdg_waveq_rk4_steps: bad arguments");
         DeviceScope g(h->w->device);
         wdg_wave *w = h->w;
-        if (!h->d_rk)
-            WDG_TRY(device_alloc(&h->d_rk, 2 * (size_t)w->ndof));
-        double *k = h->d_rk, *p = h->d_rk + w->ndof;
         HostArg a;
         WDG_TRY(bind_arg(w, 0, u, w->ndof, true, true, a));
-        const unsigned gr = grid_for(w->ndof, 256);
-        for (int step = 0; step < nsteps; ++step)
-        {
-            for (int st = 0; st < 5; ++st)
-            {
-                WDG_TRY(rhs_dev(h, a.dev, p, nullptr, 0.0));
-                rk_stage_kernel<<<gr, 256, 0, w->stream>>>(a.dev, k, p, rk4a[st], rk4b[st], dt, st == 0, w->ndof);
-                WDG_CUDA(cudaGetLastError());
-            }
+        WDG_TRY(qfused_rk4(h, a.dev, dt, *t, nsteps, nullptr, 0.0, nullptr, nullptr));
+        for (int s = 0; s < nsteps; ++s)
             *t += dt; // ode::RungeKutta4::step advances t once per step
-        }
         return finish_args(w, &a, 1);
     }
 }
