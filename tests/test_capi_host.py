@@ -90,6 +90,24 @@ def test_large_mesh_64bit_edge_keys(L):
     assert m.n_edges(0) == 2 * 300 * 299 and m.n_edges(1) == 4 * 300
 
 
+def test_large_scrambled_mesh_edge_tables_equal_the_oracle(L):
+    """Past the int key's range, on a perturbed mesh with scrambled vertex and element numbers
+    (so vertex pairs with large ids meet in every order): the whole interior and boundary edge
+    tables, in the reference's edge order, equal the oracle's (64-bit keys too), element by
+    element and side by side."""
+    import wavedg_b200 as W
+    from oracle import cpu
+    from wavedg_b200 import meshgen as mg
+
+    v, q = mg.perturbed_rect(240, 0.2, seed=17)  # 58081 vertices
+    v, q = mg.scrambled(v, q, seed=18)
+    assert len(v) > 46341  # sqrt(2^31): the reference's int key i + nx j overflows from here
+    m = W.Mesh2D.from_vertices(v, q)
+    o = cpu.Mesh(v, q, "oracle")
+    for t in (0, 1):
+        np.testing.assert_array_equal(m.edges(t), o.edges(t))
+
+
 def test_errors_are_reported(L):
     import wavedg_b200 as W
 
