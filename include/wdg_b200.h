@@ -236,6 +236,11 @@ int wdg_rk4_stage(wdg_wave *wave, int stage, double dt);
  * none) accumulates acc_c * (the new state), the period filter's term of this step. */
 int wdg_rk4_stage_forced(wdg_wave *wave, int stage, double dt, double t, const void *F, double omega, double *acc,
                          double acc_c);
+/* wdg_rk4_stage_forced over elements [el_begin, el_end) only (el_begin a multiple of 4): a
+ * stage split into the elements that read no halo trace and the rest lets the halo exchange
+ * run beside the first part (needs the warp-specialised kernel; WDG_ERR_UNSUPPORTED otherwise) */
+int wdg_rk4_stage_elems(wdg_wave *wave, int stage, double dt, double t, const void *F, double omega, double *acc,
+                        double acc_c, int el_begin, int el_end);
 /* Mesh2D::distribute's element -> rank maps, computed on the host without MPI
  * (source/Mesh2D.cpp:233-382): method 0 recursive coordinate bisection (rcb), 1 reverse
  * Cuthill-McKee blocks (rcm).  e2p: n_elem ranks in [0, n_parts).  The rcb principal axis takes

@@ -81,6 +81,7 @@ SIGNATURES = {
     "wdg_halo_put": ([_v, _i, _ll, _v, _ll], _i),
     "wdg_rk4_stage": ([_v, _i, _d], _i),
     "wdg_rk4_stage_forced": ([_v, _i, _d, _d, _v, _d, _v, _d], _i),
+    "wdg_rk4_stage_elems": ([_v, _i, _d, _d, _v, _d, _v, _d, _i, _i], _i),
     "wdg_mesh_partition": ([_v, _i, _i, _v], _i),
     "wdg_write_raw": ([C.c_char_p, _ll, _v], _i),
     "wdg_read_raw": ([C.c_char_p, _ll, _v], _i),

@@ -169,4 +169,26 @@ extern "C"
         return w->precision == WDG_FP32 ? rk4_stage<float>(w, stage, dt, t, F, omega, acc, acc_c)
                                         : rk4_stage<double>(w, stage, dt, t, F, omega, acc, acc_c);
     }
+
+    int wdg_rk4_stage_elems(wdg_wave *w, int stage, double dt, double t, const void *F, double omega, double *acc,
+                            double acc_c, int el_begin, int el_end)
+    {
+        if (!w || stage < 0 || stage > 4 || (F && !(omega != 0.0)))
+            return fail(WDG_ERR_ARG, "wdg_rk4_stage_elems: stage must be 0..4 and omega nonzero with a forcing");
+        if (el_begin < 0 || el_begin > el_end || el_end > w->nel || (el_begin & 3))
+            return fail(WDG_ERR_ARG, "wdg_rk4_stage_elems: need 0 <= el_begin <= el_end <= n_elem, el_begin a "
+                                     "multiple of 4");
+        if (el_begin == el_end)
+            return WDG_OK;
+        DeviceScope g(w->device);
+        bool dev = true;
+        if (F)
+            WDG_TRY(is_device_ptr(w, F, dev));
+        if (dev && acc)
+            WDG_TRY(is_device_ptr(w, acc, dev));
+        if (!dev)
+            return fail(WDG_ERR_ARG, "wdg_rk4_stage_elems: F and acc must be device arrays");
+        return w->precision == WDG_FP32 ? rk4_stage<float>(w, stage, dt, t, F, omega, acc, acc_c, el_begin, el_end)
+                                        : rk4_stage<double>(w, stage, dt, t, F, omega, acc, acc_c, el_begin, el_end);
+    }
 }

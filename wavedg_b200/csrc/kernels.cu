@@ -1083,10 +1083,14 @@ namespace wdg
     template <typename Real>
     cudaError_t launch_stage(int n, bool rk, const StageArgs<Real> &a, int grid_limit, cudaStream_t s)
     {
+        // a launch over part of the elements exists only in the warp-specialised family
+        const bool partial = a.el_begin != 0 || (a.el_end > 0 && a.el_end != a.nel);
 #define WDG_CASE(NV)                                                                       \
     case NV:                                                                               \
         if (a.family == 2 && rk && a.use_tma && a.tma_out && ws_fits<NV, Real>(a))         \
             return launch_ws_n<NV, Real>(a, grid_limit, s);                                \
+        if (partial)                                                                       \
+            return cudaErrorNotSupported;                                                  \
         if (a.family == 0)                                                                 \
             return rk ? launch_warp_n<NV, Real, true>(a, s) : launch_warp_n<NV, Real, false>(a, s); \
         return rk ? launch_stage_n<NV, Real, true>(a, grid_limit, s)                       \

@@ -52,6 +52,8 @@ namespace wdg
         unsigned long long wait_ns; // limit of every bounded device-side wait (0: kWaitLimitNs)
         int test_skip;        // test hook (family 2): 1 + the number of the chunk every CTA leaves
                               // unloaded, so the waits on it run out; 0 (none) in every other launch
+        int el_begin, el_end; // family 2: the launch updates elements [el_begin, el_end) only
+                              // (el_end 0: nel; el_begin a multiple of 4); other families: all
     };
 
     struct Geometry

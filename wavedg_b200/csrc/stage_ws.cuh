@@ -563,7 +563,8 @@ namespace wdg
     __global__ void __launch_bounds__(kWsThreads, 2) ws_stage_kernel(const StageArgs<Real> a)
     {
         const int C = a.chunk, S = a.ring, G = gridDim.x;
-        const int nchunks = (a.nel + C - 1) / C;
+        const int e0 = a.el_begin, e1 = a.el_end > 0 ? a.el_end : a.nel; // this launch's elements
+        const int nchunks = (e1 - e0 + C - 1) / C;
         const WsLayout L = ws_layout<Real>(N, C, S, WsStage<Real, EXTRA>::value);
 
         extern __shared__ __align__(128) unsigned char smem[];
@@ -610,8 +611,8 @@ namespace wdg
         c.acc_c = a.acc_c;
         auto at = [&](int m)
         {
-            c.el0 = ((int)blockIdx.x + m * G) * C;
-            c.ne = min(C, a.nel - c.el0);
+            c.el0 = e0 + ((int)blockIdx.x + m * G) * C;
+            c.ne = min(C, e1 - c.el0);
         };
         const uint64_t wlim = wait_limit(a.wait_ns);
 
@@ -723,11 +724,14 @@ namespace wdg
             c_grid[extra][slot] = std::max(1, per_sm) * sms;
             c_smem[extra][slot] = smem + 1;
         }
-        const int nchunks = (a.nel + a.chunk - 1) / a.chunk;
+        const int span = (a.el_end > 0 ? a.el_end : a.nel) - a.el_begin;
+        const int nchunks = (span + a.chunk - 1) / a.chunk;
         int grid = c_grid[extra][slot];
         if (grid_limit > 0)
             grid = std::min(grid, grid_limit);
         grid = std::min(grid, nchunks);
+        if (grid < 1)
+            return cudaSuccess; // an empty range
         kern<<<grid, kWsThreads, smem, s>>>(a);
         return cudaGetLastError();
     }

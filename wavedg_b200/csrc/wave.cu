@@ -184,7 +184,8 @@ namespace wdg
     // stage st (0..4) of one RK4 step on the resident buffers, the rotation of rk4_run:
     // reads A, B, C, B, C and writes B, C, B, C, A (A = the resident state)
     template <typename Real>
-    int rk4_stage(wdg_wave *w, int st, double dt, double t, const void *F, double omega, double *acc, double acc_c)
+    int rk4_stage(wdg_wave *w, int st, double dt, double t, const void *F, double omega, double *acc, double acc_c,
+                  int el_begin, int el_end)
     {
         WDG_TRY(ensure_states(w));
         Real *buf[3] = {static_cast<Real *>(w->d_state[0]), static_cast<Real *>(w->d_state[1]),
@@ -212,13 +213,18 @@ namespace wdg
             a.acc = acc;
             a.acc_c = acc_c;
         }
+        a.el_begin = el_begin;
+        a.el_end = el_end;
         cudaError_t e = launch_stage<Real>(w->n, true, a, w->max_ctas, w->stream);
+        if (e == cudaErrorNotSupported)
+            return fail(WDG_ERR_UNSUPPORTED, "rk4 stage over part of the elements: needs the warp-specialised kernel "
+                                             "(wdg_wave_set_kernel 2) with its chunk and ring fitting shared memory");
         if (e != cudaSuccess)
             return cuda_fail(e, "stage kernel launch");
         return WDG_OK;
     }
-    template int rk4_stage<double>(wdg_wave *, int, double, double, const void *, double, double *, double);
-    template int rk4_stage<float>(wdg_wave *, int, double, double, const void *, double, double *, double);
+    template int rk4_stage<double>(wdg_wave *, int, double, double, const void *, double, double *, double, int, int);
+    template int rk4_stage<float>(wdg_wave *, int, double, double, const void *, double, double *, double, int, int);
 } // namespace wdg
 
 namespace

@@ -72,9 +72,11 @@ namespace wdg
     int rk4_run(wdg_wave *w, Real *A, double dt, double &t, int nsteps, const RKExtras &x);
     // stage st of the RK4 step that starts at time t; with F, forcing F * s(t + c_st dt),
     // s(t) = -sin(omega t) / omega; with acc (stage 4 only), the filter acc += acc_c * u_new
+    // el_begin, el_end: update elements [el_begin, el_end) only (el_end 0: all; the
+    // warp-specialised kernel only, el_begin a multiple of 4)
     template <typename Real>
     int rk4_stage(wdg_wave *w, int st, double dt, double t = 0.0, const void *F = nullptr, double omega = 0.0,
-                  double *acc = nullptr, double acc_c = 0.0);
+                  double *acc = nullptr, double acc_c = 0.0, int el_begin = 0, int el_end = 0);
 
     extern const double rk4a[5], rk4b[5], rk4c[5];
 

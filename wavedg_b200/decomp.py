@@ -80,11 +80,18 @@ class Plan:
         nb = np.where(boundary, -1, fb // nd)
         cut = ~boundary & (part[np.maximum(nb, 0)] != part[:, None])
         stride = np.array([3, -3, 3 * n, -3 * n])[(byte & 3).astype(np.int64)]
-        self.local = np.nonzero(part == rank)[0].astype(np.int64)
+        # every rank's local element order, the same on all ranks: the elements that read no
+        # halo trace first, then those with a cut side (a stage can then run its first part
+        # while the halo is in flight)
         g2l = np.full(nel, -1, dtype=np.int64)
+        cut_any = cut.any(axis=1)
         for r in range(self.world):
             ids = np.nonzero(part == r)[0]
-            g2l[ids] = np.arange(len(ids))
+            order = np.concatenate([ids[~cut_any[ids]], ids[cut_any[ids]]])
+            g2l[order] = np.arange(len(order))
+            if r == rank:
+                self.local = order.astype(np.int64)
+                self.n_inner = int(np.count_nonzero(~cut_any[ids]))
         k = np.arange(n)
 
         def slots(r):
@@ -169,6 +176,9 @@ class Domain:
         # device, with no host synchronisation
         self.stream = torch.cuda.current_stream(dev)
         check(lib().wdg_wave_set_stream(h, C.c_void_p(self.stream.cuda_stream)), "Domain stream")
+        # the elements [0, split) read no halo trace (split: a multiple of 4, as the partial
+        # stage launches need)
+        self.split = (p.n_inner // 4) * 4
         self._send_idx = {r: torch.from_numpy(v).to(dev) for r, v in p.send.items()}
         self._send_buf = {r: torch.empty(3 * len(v), dtype=self.dtype, device=dev) for r, v in p.send.items()}
         self._recv_buf = {s: torch.empty(3 * n * cnt, dtype=self.dtype, device=dev) for s, (_, cnt) in p.recv.items()}
@@ -209,15 +219,19 @@ class Domain:
                                  3 * self.n * cnt), "halo put")
 
     def stage(self, stage: int, dt: float, t: float = 0.0, F=None, omega: float = 0.0, acc=None,
-              acc_c: float = 0.0) -> None:
+              acc_c: float = 0.0, part=None) -> None:
         """RK stage `stage` of the step starting at t; optionally the WaveHoltz forcing F (device,
-        the domain's precision) and, at stage 4, the filter acc += acc_c u (device FP64)."""
-        if F is None and acc is None:
+        the domain's precision) and, at stage 4, the filter acc += acc_c u (device FP64).
+        part: None all elements; 0 those that read no halo trace (runs before the halo is
+        filled); 1 the rest."""
+        if part is None and F is None and acc is None:
             check(lib().wdg_rk4_stage(self._h, int(stage), float(dt)), "rk4 stage")
             return
-        check(lib().wdg_rk4_stage_forced(self._h, int(stage), float(dt), float(t),
-                                         None if F is None else C.c_void_p(F.data_ptr()), float(omega),
-                                         None if acc is None else C.c_void_p(acc.data_ptr()), float(acc_c)),
+        b, e = (0, self.ndof // self.plan.nd) if part is None else \
+            ((0, self.split) if part == 0 else (self.split, self.ndof // self.plan.nd))
+        check(lib().wdg_rk4_stage_elems(self._h, int(stage), float(dt), float(t),
+                                        None if F is None else C.c_void_p(F.data_ptr()), float(omega),
+                                        None if acc is None else C.c_void_p(acc.data_ptr()), float(acc_c), b, e),
               "rk4 stage")
 
     def set_state(self, u_local) -> None:
@@ -231,36 +245,62 @@ class Domain:
     def sync(self) -> None:
         check(lib().wdg_wave_sync(self._h))
 
-    def rk4_steps(self, dt: float, nsteps: int, exchange) -> None:
-        """nsteps of ode::RungeKutta4::step; exchange(stage) fills the stage's input halo."""
+    def rk4_steps(self, dt: float, nsteps: int, exchange, overlap: bool = True) -> None:
+        """nsteps of ode::RungeKutta4::step; exchange fills the stage's input halo (with
+        overlap, its start / finish bracket the stage's halo-free part)."""
         for _ in range(nsteps):
             for st in range(5):
-                exchange(st)
-                self.stage(st, dt)
+                stage_all([self], st, exchange, overlap, dt)
+
+
+class Exchange:
+    """A halo exchange in two halves: start(stage) sends and posts the receives, finish(stage)
+    completes them and fills the halos; calling it does both."""
+
+    def __init__(self, start, finish):
+        self.start, self.finish = start, finish
+
+    def __call__(self, stage):
+        self.start(stage)
+        self.finish(stage)
 
 
 def local_exchange(domains):
     """Exchange among Domains of one process (one GPU): device copies.  Every Domain issues its
-    work on its handle's stream, the legacy default stream, so gathers, copies and stages of
-    all domains run in issue order without host synchronisation; a gather buffer is rewritten
-    only by a later gather, issued after the copy that read it."""
+    work on torch's current stream, so gathers, copies and stages of all domains run in issue
+    order without host synchronisation; a gather buffer is rewritten only by a later gather,
+    issued after the copy that read it.  Everything happens in start()."""
 
-    def run(stage):
+    def start(stage):
         for d in domains:
             for r in d.plan.send:
                 domains[r].put(stage, d.rank, d.gather(stage, r))
 
-    return run
+    return Exchange(start, lambda stage: None)
 
 
-def step_all(domains, dt: float, nsteps: int) -> None:
-    """RK4 steps of Domains sharing one process: per stage, exchange then every domain's stage."""
+def stage_all(domains, st: int, exchange, overlap: bool = True, dt: float = 0.0, **kw) -> None:
+    """RK stage st of every domain of this process with its halo exchange: with overlap, the
+    elements that read no halo trace run between the exchange's start and finish."""
+    if overlap and isinstance(exchange, Exchange):
+        exchange.start(st)
+        for d in domains:
+            d.stage(st, dt, part=0, **kw)
+        exchange.finish(st)
+        for d in domains:
+            d.stage(st, dt, part=1, **kw)
+    else:
+        exchange(st)
+        for d in domains:
+            d.stage(st, dt, **kw)
+
+
+def step_all(domains, dt: float, nsteps: int, overlap: bool = True) -> None:
+    """RK4 steps of Domains sharing one process: per stage, the exchange and every domain's stage."""
     ex = local_exchange(domains)
     for _ in range(nsteps):
         for st in range(5):
-            ex(st)
-            for d in domains:
-                d.stage(st, dt)
+            stage_all(domains, st, ex, overlap, dt)
 
 
 def dist_exchange(domain, group=None):
@@ -277,20 +317,25 @@ def dist_exchange(domain, group=None):
     if not on_device:
         host = {s: torch.empty(b.numel(), dtype=b.dtype) for s, b in domain._recv_buf.items()}
 
-    def run(stage):
+    pending = []
+
+    def start(stage):
         ops = []
         for r in sorted(domain.plan.send):
             buf = domain.gather(stage, r)
             ops.append(dist.P2POp(dist.isend, buf if on_device else buf.cpu(), r, group))
         for s in sorted(domain.plan.recv):
             ops.append(dist.P2POp(dist.irecv, domain._recv_buf[s] if on_device else host[s], s, group))
-        if ops:
-            for req in dist.batch_isend_irecv(ops):
-                req.wait()
+        pending[:] = dist.batch_isend_irecv(ops) if ops else []
+
+    def finish(stage):
+        for req in pending:
+            req.wait()
+        pending.clear()
         for s in sorted(domain.plan.recv):
             domain.put(stage, s, domain._recv_buf[s] if on_device else host[s])
 
-    return run
+    return Exchange(start, finish)
 
 
 def dist_allreduce(group=None, device=None):
@@ -355,13 +400,22 @@ def waveholtz_solve(whs, Fs, tol: float, maxit: int, exchange, allreduce, W=None
             wh.d.set_state(w)
             torch.mul(w, 0.5 * wh0.dt * wh0.K(0.0), out=a)
         t = 0.0
+        doms = [wh.d for wh in whs]
         for k in range(1, wh0.nt + 1):
             t1 = t + wh0.dt  # the step's end time, accumulated as ode::RungeKutta4::step does
             c = (0.5 if k == wh0.nt else 1.0) * wh0.dt * wh0.K(t1)
             for st in range(5):
-                exchange(st)
-                for wh, f, a in zip(whs, F, acc):
-                    wh.d.stage(st, wh0.dt, t, f, wh0.omega, a, c)
+                if isinstance(exchange, Exchange):
+                    exchange.start(st)
+                    for d, f, a in zip(doms, F, acc):
+                        d.stage(st, wh0.dt, t, f, wh0.omega, a, c, part=0)
+                    exchange.finish(st)
+                    for d, f, a in zip(doms, F, acc):
+                        d.stage(st, wh0.dt, t, f, wh0.omega, a, c, part=1)
+                else:
+                    exchange(st)
+                    for d, f, a in zip(doms, F, acc):
+                        d.stage(st, wh0.dt, t, f, wh0.omega, a, c)
             t = t1
         sums = [0.0, 0.0]
         for w, a in zip(W, acc):
