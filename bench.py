@@ -374,6 +374,36 @@ def waveholtz_c3(device: int, seed: int = 3) -> dict:
                         "rel_diff_vs_fp64": (Wm - W64).norm().item() / W64.norm().item()}
     out["workload"] = "waveholtz_128x128_P4_omega20_outflow_tol1e-6"
     out["x0"] = [float(x0[0]), float(x0[1])]
+    ref = c3_reference_compare(x0, {"fp64": W64, "fp32_fp64": Wm})
+    if ref is not None:
+        out["vs_cpu_reference"] = ref
+        ref["iterations_equal"] = out["fp64"]["iterations"] == ref["iterations"]
+    return out
+
+
+C3_FIXTURE = os.path.join(ROOT, "tests", "golden", "waveholtz_c3_128x128_P4.npz")
+
+
+def c3_reference_compare(x0, arms) -> dict | None:
+    """Errors of converged iterates against the reference library's own solve of the same
+    problem (the CPU oracle: tests/golden/waveholtz_c3_128x128_P4.npz, written by
+    make_c3_waveholtz.py).  The fixture holds 8192 seeded entries, the 2-norm and four seeded
+    random projections of the reference's W; per arm: the relative 2-norm error over the
+    sampled entries, the largest projection error relative to |W|, and the norm error."""
+    if not os.path.exists(C3_FIXTURE):
+        return None
+    g = np.load(C3_FIXTURE)
+    if not np.array_equal(g["x0"], np.asarray(x0)):
+        return None
+    idx, r, nr = g["sample_index"], g["W_samples"], float(g["W_norm"])
+    out = {"source": "reference library's WaveHoltz solve at this size (compiled from its sources, CPU)",
+           "iterations": int(g["iterations"]), "residual": float(g["residuals"][-1])}
+    for name, W in arms.items():
+        x = W.cpu().numpy()
+        proj = max(abs(np.random.default_rng(int(g["proj_seed"]) + k).standard_normal(x.size) @ x - g["W_proj"][k])
+                   for k in range(int(g["nproj"]))) / nr
+        out[name] = {"rel_err_sampled": float(np.linalg.norm(x[idx] - r) / np.linalg.norm(r)),
+                     "rel_err_projections": float(proj), "rel_err_norm": float(abs(np.linalg.norm(x) - nr) / nr)}
     return out
 
 
