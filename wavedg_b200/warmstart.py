@@ -182,8 +182,9 @@ def make_dataset(fam: Family, count: int, seed: int, tol: float, G: int, net=Non
     grids = t.empty((count, 3, G, G), dtype=t.float32, device="cuda")
     for b0 in range(0, count, fam.nb):
         blk = cs[b0:b0 + fam.nb]
-        pad = fam.nb - len(blk)
-        blk_full = np.concatenate([blk, blk[:pad]]) if pad else blk
+        # a short last block is filled up to the batch size by repeating its problems (their
+        # solutions are not kept twice)
+        blk_full = np.resize(blk, (fam.nb, 2)) if len(blk) < fam.nb else blk
         t0 = time.perf_counter()
         W0 = predict(net, fam, blk_full, scale) if net is not None else None
         W, it32, _, res, st = fam.solve(fam.forcing(blk_full), tol, W0=W0, fp64_finish=False)
