@@ -224,6 +224,91 @@ int main()
         report("WaveHoltzBatch iteration counts", std::abs(res.iterations[0] - ia) + std::abs(res.iterations[1] - ib), 0.5);
     }
 
+    // the nonlinear example's pattern (examples/cl2d.cpp, approx_quad = true): the reference's
+    // DivF2D / EdgeFluxF2D / prolongators / MassMatrix with that example's Euler flux and local
+    // Lax-Friedrichs flux, driven by ode::SSPRK3, against b200::EulerSystem
+    {
+        const int nde = 4 * 25 * mesh.n_elem(), nI = mesh.n_edges(FaceType::INTERIOR),
+                  nB = mesh.n_edges(FaceType::BOUNDARY);
+        auto F = [](const double *, const double *q, double *fg)
+        {
+            const double rho = q[0], uu = q[1] / q[0], vv = q[2] / q[0], E = q[3];
+            const double p = 0.4 * (E - 0.5 * rho * (uu * uu + vv * vv));
+            fg[0] = rho * uu;
+            fg[1] = rho * uu * uu + p;
+            fg[2] = rho * uu * vv;
+            fg[3] = uu * (E + p);
+            fg[4] = rho * vv;
+            fg[5] = rho * uu * vv;
+            fg[6] = rho * vv * vv + p;
+            fg[7] = vv * (E + p);
+        };
+        auto speed = [](const double *q)
+        {
+            const double rho = q[0], uu = q[1] / q[0], vv = q[2] / q[0], E = q[3];
+            const double p = 0.4 * (E - 0.5 * rho * (uu * uu + vv * vv));
+            return std::hypot(uu, vv) + std::sqrt(1.4 * p / rho);
+        };
+        auto llf = [&](const double *x, const double *nrm, const double *qL, const double *qR, double *fh)
+        {
+            double fL[8], fR[8];
+            F(x, qL, fL);
+            F(x, qR, fR);
+            const double c = std::max(speed(qL), speed(qR));
+            for (int d = 0; d < 4; ++d)
+                fh[d] = 0.5 * nrm[0] * (fL[d] + fR[d]) + 0.5 * nrm[1] * (fL[4 + d] + fR[4 + d]) + 0.5 * c * (qL[d] - qR[d]);
+        };
+        DivF2D<true> div(mesh, basis);
+        EdgeFluxF2D<true> fI(mesh, FaceType::INTERIOR, basis), fB(mesh, FaceType::BOUNDARY, basis);
+        auto pI = make_face_prolongator(mesh, basis, FaceType::INTERIOR);
+        auto pB = make_face_prolongator(mesh, basis, FaceType::BOUNDARY);
+        std::vector<double> uI(5 * 4 * 2 * (size_t)nI), uB(5 * 4 * 2 * (size_t)nB);
+        auto dudt = [&](double *out, double, const double *v)
+        {
+            for (int i = 0; i < nde; ++i)
+                out[i] = 0.0;
+            div.action(4, F, v, out);
+            pI->action(4, v, uI.data());
+            fI.action(4, llf, uI.data(), uI.data());
+            for (double &x : uI)
+                x = -x;
+            pI->t(4, uI.data(), out);
+            pB->action(4, v, uB.data());
+            for (int e = 0; e < nB; ++e)
+                for (int d = 0; d < 4; ++d)
+                    for (int i = 0; i < 5; ++i)
+                        uB[i + 5 * (d + 4 * (1 + 2 * (size_t)e))] = uB[i + 5 * (d + 4 * (0 + 2 * (size_t)e))];
+            fB.action(4, llf, uB.data(), uB.data());
+            for (double &x : uB)
+                x = -x;
+            pB->t(4, uB.data(), out);
+            m.inv(4, out);
+        };
+        b200::EulerSystem ge(mesh, basis);
+        std::uniform_real_distribution<double> U01(0.0, 1.0);
+        std::vector<double> q(nde);
+        for (int k = 0; k < nde / 4; ++k)
+        {
+            const double rho = 1.0 + 0.2 * U01(gen), uu = 0.3 * N01(gen), vv = 0.3 * N01(gen), p = 1.0 + 0.2 * U01(gen);
+            q[4 * k] = rho;
+            q[4 * k + 1] = rho * uu;
+            q[4 * k + 2] = rho * vv;
+            q[4 * k + 3] = p / 0.4 + 0.5 * rho * (uu * uu + vv * vv);
+        }
+        std::vector<double> e1(nde), e2(nde);
+        dudt(e1.data(), 0.0, q.data());
+        ge.action(q.data(), e2.data());
+        report("Euler time derivative (cl2d composition)", rel(e2, e1), 1e-12);
+        const double dte = 0.1 * mesh.min_h() / 25.0;
+        std::vector<double> qr = q, qg = q;
+        double tr = 0.0, tg = 0.0;
+        ode::SSPRK3 ssp(nde);
+        for (int s = 0; s < 5; ++s)
+            ssp.step(dte, dudt, tr, qr.data());
+        ge.steps(dte, tg, qg.data(), 5);
+        report("ode::SSPRK3 vs b200::EulerSystem, 5 steps", rel(qg, qr), 1e-11);
+    }
+
     std::printf("%s\n", failures ? "DROP-IN FAILED" : "drop-in ok");
     return failures ? 1 : 0;
 }
