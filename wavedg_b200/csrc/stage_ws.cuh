@@ -344,7 +344,7 @@ namespace wdg
                                                const Real *xtab, const Real *wtab, int cw, int lane)
     {
         using Sh = WsShape<N>;
-        constexpr int NN = Sh::NN, ND = Sh::ND, NF = Sh::NF, EW = Sh::EW;
+        constexpr int ND = Sh::ND, NF = Sh::NF, EW = Sh::EW;
         constexpr bool STG = WsStage<Real, EXTRA>::value;
         const WsSlot o = ws_slot<Real>(N, c.chunk, STG);
         const int flags = c.flags;
