@@ -191,14 +191,20 @@ int wdg_advect_rk4_steps(wdg_advect *adv, double *u, double dt, double *t, int n
  * 1/2 n.(F(uL) + F(uR)) + 1/2 max(|v| + c) (uL - uR) (cl2d.cpp:92-120), MassMatrix<true>. */
 typedef struct wdg_claw wdg_claw;
 int wdg_euler_create(const wdg_mesh *mesh, int n_colloc, int device, wdg_claw **out);
+/* The same system with approx_quad = false, as examples/cl2d.cpp ships: DivF2D<false>
+ * (wavedg/DivF.hpp:262-394) and EdgeFluxF2D<false> (wavedg/EdgeFluxF.hpp:182-254) on their
+ * default 2n-point Gauss-Legendre rules (source/DivF.cpp:59, source/EdgeFluxF.cpp:55), the
+ * face traces interpolated to the face rule, and MassMatrix<false>'s dense inverse.  The
+ * entry points below serve both kinds of handle. */
+int wdg_euler_create_exact(const wdg_mesh *mesh, int n_colloc, int device, wdg_claw **out);
 void wdg_claw_destroy(wdg_claw *claw);
 int wdg_claw_set_stream(wdg_claw *claw, void *cuda_stream);
 int wdg_claw_sync(wdg_claw *claw);
-/* DivF2D<true>::action: divF += (F(u), grad v) */
+/* DivF2D::action: divF += (F(u), grad v) */
 int wdg_claw_div(wdg_claw *claw, const double *u, double *divF);
-/* EdgeFluxF2D<true>::action on face traces uB (n, 4, 2, n_edges(face_type)): fB(side 0) =
- * w_i |E|/2 fh(n, side 0, side 1), fB(side 1) = -fB(side 0), n the outward normal of the
- * edge's first element; fB may be uB */
+/* EdgeFluxF2D::action on nodal face traces uB (n, 4, 2, n_edges(face_type)): fB(side 0) =
+ * sum_i P(i, k) w_i |E|/2 fh(n, side 0, side 1) (P the identity with approx_quad = true),
+ * fB(side 1) = -fB(side 0), n the outward normal of the edge's first element; fB may be uB */
 int wdg_claw_flux(wdg_claw *claw, int face_type, const double *uB, double *fB);
 /* the time derivative of examples/cl2d.cpp:171-220: dudt = M^{-1} (DivF(u) - interior faces -
  * boundary faces with exterior state = interior state), one fused launch */

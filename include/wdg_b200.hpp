@@ -328,11 +328,13 @@ namespace b200
         std::shared_ptr<wdg_whbatch> h_;
     };
 
-    // The compressible Euler system of examples/cl2d.cpp with approx_quad = true (DivF2D<true>,
-    // EdgeFluxF2D<true> with the example's flux and local Lax-Friedrichs numerical flux,
-    // exterior boundary state = interior state, MassMatrix<true>) as one fused operator:
-    // action(u, dudt) overwrites dudt with the example's time derivative.  The flux model is
-    // built into the kernels (a GPU kernel needs its flux at compile time).
+    // The compressible Euler system of examples/cl2d.cpp (DivF2D, EdgeFluxF2D with the example's
+    // flux and local Lax-Friedrichs numerical flux, exterior boundary state = interior state,
+    // MassMatrix) as one fused operator, with the example's approx_quad switch as a template
+    // argument (false, the example's setting: 2n-point Gauss-Legendre rules and the dense
+    // inverse mass matrix): action(u, dudt) overwrites dudt with the example's time derivative.
+    // The flux model is built into the kernels (a GPU kernel needs its flux at compile time).
+    template <bool ApproxQuad = true>
     class EulerSystem : public dg::Operator
     {
     public:
@@ -342,12 +344,13 @@ namespace b200
                 throw std::runtime_error("wdg_b200: the Euler kernels are built for Gauss-Lobatto bases");
             Mesh m(mesh);
             wdg_claw *h = nullptr;
-            check(wdg_euler_create(m.get(), basis->n, device, &h));
+            check(ApproxQuad ? wdg_euler_create(m.get(), basis->n, device, &h)
+                             : wdg_euler_create_exact(m.get(), basis->n, device, &h));
             h_.reset(h, wdg_claw_destroy);
         }
         void action(const double *u, double *dudt) const override { check(wdg_claw_rhs(h_.get(), u, dudt)); }
         void action(int, const double *u, double *dudt) const override { action(u, dudt); }
-        // DivF2D<true>::action: divF += (F(u), grad v)
+        // DivF2D<ApproxQuad>::action: divF += (F(u), grad v)
         void div(const double *u, double *divF) const { check(wdg_claw_div(h_.get(), u, divF)); }
         // ode::SSPRK3::step (the example's stepper) or, with rk4, ode::RungeKutta4::step, nsteps times
         void steps(double dt, double &t, double *u, int nsteps = 1, bool rk4 = false) const

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <random>
+#include <type_traits>
 #include <vector>
 
 #include "wavedg.hpp"
@@ -224,10 +225,13 @@ int main()
         report("WaveHoltzBatch iteration counts", std::abs(res.iterations[0] - ia) + std::abs(res.iterations[1] - ib), 0.5);
     }
 
-    // the nonlinear example's pattern (examples/cl2d.cpp, approx_quad = true): the reference's
-    // DivF2D / EdgeFluxF2D / prolongators / MassMatrix with that example's Euler flux and local
-    // Lax-Friedrichs flux, driven by ode::SSPRK3, against b200::EulerSystem
+    // the nonlinear example's pattern (examples/cl2d.cpp, both settings of approx_quad): the
+    // reference's DivF2D / EdgeFluxF2D / prolongators / MassMatrix with that example's Euler
+    // flux and local Lax-Friedrichs flux, driven by ode::SSPRK3, against b200::EulerSystem
+    auto euler_case = [&](auto approx)
     {
+        constexpr bool AQ = decltype(approx)::value;
+        const char *tag = AQ ? "approx_quad = true" : "approx_quad = false";
         const int nde = 4 * 25 * mesh.n_elem(), nI = mesh.n_edges(FaceType::INTERIOR),
                   nB = mesh.n_edges(FaceType::BOUNDARY);
         auto F = [](const double *, const double *q, double *fg)
@@ -258,8 +262,9 @@ int main()
             for (int d = 0; d < 4; ++d)
                 fh[d] = 0.5 * nrm[0] * (fL[d] + fR[d]) + 0.5 * nrm[1] * (fL[4 + d] + fR[4 + d]) + 0.5 * c * (qL[d] - qR[d]);
         };
-        DivF2D<true> div(mesh, basis);
-        EdgeFluxF2D<true> fI(mesh, FaceType::INTERIOR, basis), fB(mesh, FaceType::BOUNDARY, basis);
+        DivF2D<AQ> div(mesh, basis);
+        EdgeFluxF2D<AQ> fI(mesh, FaceType::INTERIOR, basis), fB(mesh, FaceType::BOUNDARY, basis);
+        MassMatrix<AQ> me(mesh, basis);
         auto pI = make_face_prolongator(mesh, basis, FaceType::INTERIOR);
         auto pB = make_face_prolongator(mesh, basis, FaceType::BOUNDARY);
         std::vector<double> uI(5 * 4 * 2 * (size_t)nI), uB(5 * 4 * 2 * (size_t)nB);
@@ -282,9 +287,9 @@ int main()
             for (double &x : uB)
                 x = -x;
             pB->t(4, uB.data(), out);
-            m.inv(4, out);
+            me.inv(4, out);
         };
-        b200::EulerSystem ge(mesh, basis);
+        b200::EulerSystem<AQ> ge(mesh, basis);
         std::uniform_real_distribution<double> U01(0.0, 1.0);
         std::vector<double> q(nde);
         for (int k = 0; k < nde / 4; ++k)
@@ -298,7 +303,8 @@ int main()
         std::vector<double> e1(nde), e2(nde);
         dudt(e1.data(), 0.0, q.data());
         ge.action(q.data(), e2.data());
-        report("Euler time derivative (cl2d composition)", rel(e2, e1), 1e-12);
+        std::printf("Euler, %s:\n", tag);
+        report("  time derivative (cl2d composition)", rel(e2, e1), 1e-12);
         const double dte = 0.1 * mesh.min_h() / 25.0;
         std::vector<double> qr = q, qg = q;
         double tr = 0.0, tg = 0.0;
@@ -306,8 +312,10 @@ int main()
         for (int s = 0; s < 5; ++s)
             ssp.step(dte, dudt, tr, qr.data());
         ge.steps(dte, tg, qg.data(), 5);
-        report("ode::SSPRK3 vs b200::EulerSystem, 5 steps", rel(qg, qr), 1e-11);
-    }
+        report("  ode::SSPRK3 vs b200::EulerSystem, 5 steps", rel(qg, qr), 1e-11);
+    };
+    euler_case(std::true_type{});
+    euler_case(std::false_type{});
 
     std::printf("%s\n", failures ? "DROP-IN FAILED" : "drop-in ok");
     return failures ? 1 : 0;

@@ -349,6 +349,56 @@ namespace
         }
     };
 
+    // The same composition with approx_quad = false, as examples/cl2d.cpp ships: DivF2D<false>,
+    // EdgeFluxF2D<false> (their default 2n-point rules) and MassMatrix<false>.
+    struct RefOpEQ
+    {
+        static constexpr int nv = 4;
+        const Mesh2D &mesh;
+        const QuadratureRule *basis;
+        const int n, ndof, nI, nB;
+        DivF2D<false> div;
+        EdgeFluxF2D<false> flxI, flxB;
+        std::unique_ptr<FaceProlongator> prolI, prolB;
+        MassMatrix<false> m;
+        mutable std::vector<double> uI, uB;
+
+        RefOpEQ(const Mesh2D &mesh_, int n_colloc)
+            : mesh(mesh_), basis(QuadratureRule::quadrature_rule(n_colloc, QuadratureRule::GaussLobatto)), n(n_colloc),
+              ndof(nv * n_colloc * n_colloc * mesh_.n_elem()), nI(mesh_.n_edges(FaceType::INTERIOR)),
+              nB(mesh_.n_edges(FaceType::BOUNDARY)), div(mesh_, basis), flxI(mesh_, FaceType::INTERIOR, basis),
+              flxB(mesh_, FaceType::BOUNDARY, basis), prolI(make_face_prolongator(mesh_, basis, FaceType::INTERIOR)),
+              prolB(make_face_prolongator(mesh_, basis, FaceType::BOUNDARY)), m(mesh_, basis),
+              uI((size_t)n_colloc * nv * 2 * nI), uB((size_t)n_colloc * nv * 2 * nB)
+        {
+        }
+        void flux(int type, const double *ub, double *fb) const
+        {
+            (type == 0 ? flxI : flxB).action(nv, euler_llf, ub, fb);
+        }
+        void rhs(const double *u, double *dudt) const
+        {
+            for (int i = 0; i < ndof; ++i)
+                dudt[i] = 0.0;
+            div.action(nv, euler_flux, u, dudt);
+            prolI->action(nv, u, uI.data());
+            flxI.action(nv, euler_llf, uI.data(), uI.data());
+            for (double &x : uI)
+                x *= -1;
+            prolI->t(nv, uI.data(), dudt);
+            prolB->action(nv, u, uB.data());
+            for (int e = 0; e < nB; ++e)
+                for (int d = 0; d < nv; ++d)
+                    for (int i = 0; i < n; ++i)
+                        uB[i + n * (d + nv * (1 + 2 * (size_t)e))] = uB[i + n * (d + nv * (0 + 2 * (size_t)e))];
+            flxB.action(nv, euler_llf, uB.data(), uB.data());
+            for (double &x : uB)
+                x *= -1;
+            prolB->t(nv, uB.data(), dudt);
+            m.inv(nv, dudt);
+        }
+    };
+
     // WaveHoltz restated over RefOp so that the composed boundary operator can
     // be used (the reference class hard-wires WaveBC).  Loop structure, time
     // accumulation and filter weights follow source/WaveHoltz.cpp:5-145; with
@@ -618,6 +668,33 @@ extern "C"
     void ref_ope_steps(void *o, int method, double dt, int nsteps, double *t, double *u)
     {
         RefOpE *op = static_cast<RefOpE *>(o);
+        auto f = [op](double *dudt, const double, const double *v) { op->rhs(v, dudt); };
+        if (method == 0)
+        {
+            ode::RungeKutta4 rk(op->ndof);
+            for (int s = 0; s < nsteps; ++s)
+                rk.step(dt, f, *t, u);
+        }
+        else
+        {
+            ode::SSPRK3 rk(op->ndof);
+            for (int s = 0; s < nsteps; ++s)
+                rk.step(dt, f, *t, u);
+        }
+    }
+
+    // ---- compressible Euler with approx_quad = false (examples/cl2d.cpp as shipped) ----
+    void *ref_opeq_create(void *m, int n_colloc) { return new RefOpEQ(static_cast<RefMesh *>(m)->mesh, n_colloc); }
+    void ref_opeq_destroy(void *o) { delete static_cast<RefOpEQ *>(o); }
+    void ref_opeq_div(void *o, const double *u, double *du)
+    {
+        static_cast<RefOpEQ *>(o)->div.action(RefOpEQ::nv, euler_flux, u, du);
+    }
+    void ref_opeq_flux(void *o, int type, const double *ub, double *fb) { static_cast<RefOpEQ *>(o)->flux(type, ub, fb); }
+    void ref_opeq_rhs(void *o, const double *u, double *du) { static_cast<RefOpEQ *>(o)->rhs(u, du); }
+    void ref_opeq_steps(void *o, int method, double dt, int nsteps, double *t, double *u)
+    {
+        RefOpEQ *op = static_cast<RefOpEQ *>(o);
         auto f = [op](double *dudt, const double, const double *v) { op->rhs(v, dudt); };
         if (method == 0)
         {

@@ -244,6 +244,35 @@ def euler_fixture(name, v, q, m, n, seed):
     np.savez_compressed(os.path.join(HERE, f"euler_{name}_n{n}.npz"), **out)
 
 
+def euler_exact_fixture(name, v, q, m, n, seed):
+    """The Euler operators with approx_quad = false (examples/cl2d.cpp as shipped): DivF2D<false>,
+    EdgeFluxF2D<false> on the prolonged traces (boundary: exterior = interior), the time
+    derivative with MassMatrix<false>, 3 RK4 and 3 SSPRK3 steps."""
+    rng = np.random.default_rng(seed)
+    op = cpu.OpEQ(m, n)
+    prol = cpu.OpE(m, n)  # the Lobatto prolongators are the same for both rules
+    u = euler_state(op.ndof, rng)
+    out = dict(verts=v, quads=q, n=n, u=u)
+    r = rng.standard_normal(op.ndof)
+    out["div_in"] = r.copy()
+    op.div(u, r)
+    out["div"] = r
+    for k in (0, 1):
+        ub = prol.prolong(k, u)
+        if k == 1:
+            ub = ub.reshape(-1, 2, 4 * n)
+            ub[:, 1] = ub[:, 0]
+            ub = ub.reshape(-1)
+        out[f"flux{k}_in"] = ub
+        out[f"flux{k}"] = op.flux(k, ub)
+    out["rhs"] = op.rhs(u)
+    dt = 0.1 * m.min_h() / (n * n)
+    out["dt"] = dt
+    out["rk4_3"], _ = op.steps(u, dt, 3, "rk4")
+    out["ssprk3_3"], _ = op.steps(u, dt, 3, "ssprk3")
+    np.savez_compressed(os.path.join(HERE, f"eulerq_{name}_n{n}.npz"), **out)
+
+
 def reference_meshes():
     """The reference's mesh files, copied unchanged into tests/golden/meshes/<name>/ (data, read
     by Mesh2D::from_file, source/Mesh2D.cpp:94-128); per mesh the connectivity the reference's
@@ -278,6 +307,10 @@ def main():
         v = np.loadtxt(os.path.join(g, "coordinates.txt")).reshape(-1, 2)
         q = np.loadtxt(os.path.join(g, "elements.txt"), dtype=np.int32).reshape(-1, 4)
         euler_fixture("fileSquare", v, q, cpu.Mesh(v, q, KIND), 3, 4999)
+        qcases = {"scrambled6": [4], "lshape3": [3]}
+        for seed, (name, v, q) in enumerate(meshes()):
+            for n in qcases.get(name, []):
+                euler_exact_fixture(name, v, q, cpu.Mesh(v, q, KIND), n, 4500 + 100 * seed + n)
         print("Euler fixtures written to", HERE)
         return
     if "--reference-meshes" in sys.argv:

@@ -1,8 +1,10 @@
 """The nonlinear conservation-law path (the compressible Euler system of examples/cl2d.cpp)
-against the reference library compiled from its sources (tests/golden/euler_*.npz, written by
-make_golden.py --euler: DivF2D<true>, EdgeFluxF2D<true> with the example's local Lax-Friedrichs
-flux, the example's time derivative, ode::RungeKutta4 and ode::SSPRK3), and the fused
-advection path against the Advection fixtures.
+against the reference library compiled from its sources (written by make_golden.py --euler:
+tests/golden/euler_*.npz with approx_quad = true, DivF2D<true> and EdgeFluxF2D<true>;
+tests/golden/eulerq_*.npz with approx_quad = false, as the example ships, DivF2D<false>,
+EdgeFluxF2D<false> and MassMatrix<false>; both with the example's local Lax-Friedrichs flux,
+its time derivative, ode::RungeKutta4 and ode::SSPRK3), and the fused advection path against
+the Advection fixtures.
 
 Bars: 1e-12 relative (2-norm) per operator and RHS; 1e-11 after three RK4 or SSPRK3 steps.
 """
@@ -19,12 +21,25 @@ def _system(g):
 
     mesh = W.Mesh2D.from_vertices(g["verts"], g["quads"])
     basis = W.QuadratureRule.quadrature_rule(int(g["n"]), W.QuadratureRule.GaussLobatto)
-    return W, mesh, W.EulerSystem(mesh, basis)
+    return W, mesh, W.EulerSystem(mesh, basis, approx_quad=not fname_exact(g))
 
 
-@pytest.mark.parametrize("fname", golden_files("euler_"))
+def fname_exact(g):
+    return bool(g.get("exact", False))
+
+
+EULER_FILES = golden_files("euler_") + golden_files("eulerq_")
+
+
+def _load(fname):
+    g = dict(golden(fname))
+    g["exact"] = fname.startswith("eulerq_")
+    return g
+
+
+@pytest.mark.parametrize("fname", EULER_FILES)
 def test_euler_operators_match_the_reference(gpu_lib, fname):
-    g = golden(fname)
+    g = _load(fname)
     W, mesh, s = _system(g)
     u = g["u"]
     d = g["div_in"].copy()
@@ -44,12 +59,12 @@ def test_euler_operators_match_the_reference(gpu_lib, fname):
     assert e < 1e-12
 
 
-@pytest.mark.parametrize("fname", golden_files("euler_"))
+@pytest.mark.parametrize("fname", EULER_FILES)
 @pytest.mark.parametrize("method", ["rk4", "ssprk3"])
 def test_euler_steps_match_the_reference(gpu_lib, fname, method):
     import torch
 
-    g = golden(fname)
+    g = _load(fname)
     W, mesh, s = _system(g)
     want = g["rk4_3" if method == "rk4" else "ssprk3_3"]
     u = g["u"].copy()

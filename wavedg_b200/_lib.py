@@ -68,6 +68,7 @@ SIGNATURES = {
     "wdg_advect_rhs": ([_v, _v, _v], _i),
     "wdg_advect_rk4_steps": ([_v, _v, _d, _v, _i], _i),
     "wdg_euler_create": ([_v, _i, _i, _vp], _i),
+    "wdg_euler_create_exact": ([_v, _i, _i, _vp], _i),
     "wdg_claw_destroy": ([_v], None),
     "wdg_claw_set_stream": ([_v, _v], _i),
     "wdg_claw_sync": ([_v], _i),

@@ -42,17 +42,12 @@ struct wdg_waveq
     double *d_uf = nullptr, *d_uB = nullptr; // face traces
 };
 
-namespace
+namespace wdg
 {
-    constexpr int kMaxQ = 16;
-
-    int qdiv(int n) { return 1 + ((n - 2) + (n - 1) + 1) / 2; }
-    int qface(int n) { return 1 + (2 * (n - 1) + 2) / 2; }
-
     // D(i, j) = phi_j'(xq_i) for the Lagrange basis on the nodes x, by the barycentric
     // derivative formula: at a node the diagonal form, elsewhere the quotient form
     // (lagrange_basis_deriv, source/lagrange_interpolation.cpp:33-50, 96-139)
-    void deriv_at(int n, const double *x, int nq, const double *xq, double *D)
+    void lagrange_deriv_at(int n, const double *x, int nq, const double *xq, double *D)
     {
         std::vector<double> lw(n), B((size_t)nq * n);
         for (int i = 0; i < n; ++i)
@@ -95,6 +90,16 @@ namespace
                 D[i + (size_t)nq * j] = A / S;
             }
     }
+
+    const double *waveq_minv(const wdg_waveq *h) { return h->d_Minv; }
+} // namespace wdg
+
+namespace
+{
+    constexpr int kMaxQ = 16;
+
+    int qdiv(int n) { return 1 + ((n - 2) + (n - 1) + 1) / 2; }
+    int qface(int n) { return 1 + (2 * (n - 1) + 2) / 2; }
 
     // QuadElement::jacobian (source/Element.cpp:21-27): J = (x_xi, y_xi, x_eta, y_eta)
     __host__ __device__ inline void jac(const double *c, double xi, double eta, double J[4])
@@ -747,7 +752,7 @@ extern "C"
         std::vector<double> xd(h->nqd), wd(h->nqd), Pd((size_t)h->nqd * n), Dd((size_t)h->nqd * n);
         gauss_legendre(h->nqd, xd.data(), wd.data());
         interp_matrix(n, x.data(), h->nqd, xd.data(), Pd.data());
-        deriv_at(n, x.data(), h->nqd, xd.data(), Dd.data());
+        lagrange_deriv_at(n, x.data(), h->nqd, xd.data(), Dd.data());
         // face rule
         std::vector<double> xf(h->nqf), wf(h->nqf), Pf((size_t)h->nqf * n);
         gauss_legendre(h->nqf, xf.data(), wf.data());

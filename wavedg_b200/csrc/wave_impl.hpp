@@ -82,6 +82,11 @@ namespace wdg
 
     // fused conservation-law kernels (claw.cu): launch arguments on a handle's geometry, and
     // nsteps of RK4 (method 0) or SSPRK3 (method 1) on device array u; bufs: 3 arrays of u's size
+    // D(i, j) = phi_j'(xq_i) of the Lagrange basis on nodes x at points xq (barycentric, the
+    // reference's lagrange_basis_deriv); the element inverse mass matrices of an exact handle
+    void lagrange_deriv_at(int n, const double *x, int nq, const double *xq, double *D);
+    const double *waveq_minv(const wdg_waveq *h);
+
     ClawArgs claw_args(const wdg_wave *w, const double *x, double *out);
     int claw_steps(wdg_wave *w, int model, int nv, const double *A, const double *absA, double *const *bufs, int method,
                    double *u, double dt, double *t, int nsteps);

@@ -806,17 +806,20 @@ class AdvectionSystem:
 
 
 class EulerSystem:
-    """The compressible Euler system of examples/cl2d.cpp (wdg_euler_create, wdg_claw_*): state
-    u(d, i, j, el) with d = density, x-momentum, y-momentum, energy, gamma = 1.4; DivF2D<true>
-    with the example's flux, EdgeFluxF2D<true> with its local Lax-Friedrichs flux (exterior
-    boundary state = interior state), MassMatrix<true>, on GLL nodes.  FP64."""
+    """The compressible Euler system of examples/cl2d.cpp (wdg_euler_create[_exact], wdg_claw_*):
+    state u(d, i, j, el) with d = density, x-momentum, y-momentum, energy, gamma = 1.4; DivF2D
+    with the example's flux, EdgeFluxF2D with its local Lax-Friedrichs flux (exterior boundary
+    state = interior state) and MassMatrix on GLL nodes, with the example's approx_quad switch:
+    True for the collocation rule, False (as the example ships) for the 2n-point Gauss-Legendre
+    rules and the dense inverse mass matrix.  FP64."""
 
     n_var = 4
 
-    def __init__(self, mesh: Mesh2D, basis, device: int = -1):
-        self.mesh, self.n = mesh, _gll_n(basis)
+    def __init__(self, mesh: Mesh2D, basis, device: int = -1, approx_quad: bool = True):
+        self.mesh, self.n, self.approx_quad = mesh, _gll_n(basis), bool(approx_quad)
+        name = "wdg_euler_create" if self.approx_quad else "wdg_euler_create_exact"
         h = C.c_void_p()
-        check(lib().wdg_euler_create(mesh._h, self.n, device, C.byref(h)), "wdg_euler_create")
+        check(getattr(lib(), name)(mesh._h, self.n, device, C.byref(h)), name)
         self._h = h
         self.ndof = 4 * self.n * self.n * mesh.n_elem()
 
@@ -833,19 +836,19 @@ class EulerSystem:
         check(lib().wdg_claw_sync(self._h))
 
     def div(self, u, divF) -> None:
-        """DivF2D<true>::action: divF += (F(u), grad v)."""
+        """DivF2D::action: divF += (F(u), grad v)."""
         pu, _ku = _ptr(u, name="u")
         pd, _kd = _ptr(divF, True, "divF")
         check(lib().wdg_claw_div(self._h, pu, pd), "DivF2D.action")
 
     def flux(self, face_type: int, uB, fB) -> None:
-        """EdgeFluxF2D<true>::action on face traces (n, 4, 2, n_edges); fB may be uB."""
+        """EdgeFluxF2D::action on nodal face traces (n, 4, 2, n_edges); fB may be uB."""
         pu, _ku = _ptr(uB, name="uB")
         pf, _kf = _ptr(fB, True, "fB")
         check(lib().wdg_claw_flux(self._h, int(face_type), pu, pf), "EdgeFluxF2D.action")
 
     def rhs(self, u, dudt) -> None:
-        """The time derivative of examples/cl2d.cpp (approx_quad = true)."""
+        """The time derivative of examples/cl2d.cpp."""
         pu, _ku = _ptr(u, name="u")
         pd, _kd = _ptr(dudt, True, "dudt")
         check(lib().wdg_claw_rhs(self._h, pu, pd), "rhs")
