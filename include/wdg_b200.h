@@ -183,6 +183,28 @@ int wdg_advect_bc_action(wdg_advect *adv, const double *u, double *du); /* Advec
 int wdg_advect_rhs(wdg_advect *adv, const double *u, double *dudt);
 int wdg_advect_rk4_steps(wdg_advect *adv, double *u, double dt, double *t, int nsteps);
 
+/* ---- linear advection with a spatially varying coefficient ---- */
+/* Advection<AQ> and AdvectionHomogeneousBC<AQ> with constant_coefficient = false
+ * (wavedg/Advection.hpp:59-273) and MassMatrix<AQ> on a GLL basis: a is the host array
+ * a(k, l, comp, i, j, el) = a[k + n_var (l + n_var (comp + 2 (i + n (j + n el))))], A^comp_{k,l}
+ * at node (i, j) of element el (the reference's layout); approx_quad selects Div<true> /
+ * EdgeFlux<true> (1) or Div<false> / EdgeFlux<false> on their default Gauss-Legendre rules with
+ * MassMatrix<false> (0, the setting of examples/advec2d.cpp).  The flux matrices come from an
+ * eigen-decomposition of n.A at every face point: n_var = 1, or n.A symmetric (n_var <= 8;
+ * WDG_ERR_UNSUPPORTED otherwise).  FP64. */
+typedef struct wdg_vadvect wdg_vadvect;
+int wdg_vadvect_create(const wdg_mesh *mesh, int n_colloc, int n_var, const double *a, int approx_quad, int device,
+                       wdg_vadvect **out);
+void wdg_vadvect_destroy(wdg_vadvect *adv);
+int wdg_vadvect_set_stream(wdg_vadvect *adv, void *cuda_stream);
+int wdg_vadvect_sync(wdg_vadvect *adv);
+int wdg_vadvect_action(wdg_vadvect *adv, const double *u, double *du);    /* Advection::action, du += */
+int wdg_vadvect_bc_action(wdg_vadvect *adv, const double *u, double *du); /* AdvectionHomogeneousBC::action, du += */
+/* dudt = M^{-1} (Advection + AdvectionHomogeneousBC) u, and nsteps of ode::RungeKutta4 (method 0)
+ * or ode::SSPRK3 (method 1, the stepper of examples/advec2d.cpp) on u in place */
+int wdg_vadvect_rhs(wdg_vadvect *adv, const double *u, double *dudt);
+int wdg_vadvect_steps(wdg_vadvect *adv, int method, double *u, double dt, double *t, int nsteps);
+
 /* ---- nonlinear conservation law: the compressible Euler system of examples/cl2d.cpp ---- */
 /* State u(d, i, j, el), d = density, x-momentum, y-momentum, energy; gamma = 1.4; FP64.
  * The operators of the example with approx_quad = true on GLL nodes: DivF2D<true>

@@ -60,6 +60,12 @@ _SIGS = {
     "opa_bc_action": ([_v, _dp, _dp], None),
     "opa_rhs": ([_v, _dp, _dp], None),
     "opa_rk4": ([_v, _d, _i, C.POINTER(C.c_double), _dp], None),
+    "opv_create": ([_v, _i, _i, _dp, _i], _v),
+    "opv_destroy": ([_v], None),
+    "opv_action": ([_v, _dp, _dp], None),
+    "opv_bc_action": ([_v, _dp, _dp], None),
+    "opv_rhs": ([_v, _dp, _dp], None),
+    "opv_steps": ([_v, _i, _d, _i, C.POINTER(C.c_double), _dp], None),
     "ope_create": ([_v, _i], _v),
     "ope_destroy": ([_v], None),
     "ope_div": ([_v, _dp, _dp], None),
@@ -122,8 +128,8 @@ def lib(kind: str = "oracle"):
     for name, (args, res) in _SIGS.items():
         fn = getattr(L, prefix + name, None)
         if fn is None:
-            if kind == "oracle" and name.startswith("opeq_"):
-                continue  # the approx_quad = false Euler operators exist in the reference harness only
+            if kind == "oracle" and name.startswith(("opeq_", "opv_")):
+                continue  # operators that only the reference harness carries
             raise AttributeError(f"{path}: missing {prefix + name}")
         fn.argtypes = args
         fn.restype = res
@@ -429,6 +435,41 @@ class OpEQ(OpE):
         u = _f64(u).copy()
         tt = C.c_double(t)
         self.L.opeq_steps(self.h, {"rk4": 0, "ssprk3": 1}[method], dt, nsteps, C.byref(tt), u)
+        return u, tt.value
+
+
+class OpV:
+    """Advection<AQ> + AdvectionHomogeneousBC<AQ> + MassMatrix<AQ> with a spatially varying
+    coefficient a(n_var, n_var, 2, n, n, n_elem) (constant_coefficient = false), GLL basis;
+    the reference harness only."""
+
+    def __init__(self, mesh: Mesh, n: int, nv: int, a, approx_quad: bool):
+        self.L, self.mesh, self.n, self.nv = mesh.L, mesh, n, nv
+        self.a = _f64(a).reshape(-1)
+        assert self.a.size == 2 * nv * nv * n * n * mesh.n_elem
+        self.h = self.L.opv_create(mesh.h, n, nv, self.a, int(bool(approx_quad)))
+        self.ndof = nv * n * n * mesh.n_elem
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.opv_destroy(self.h)
+            self.h = None
+
+    def action(self, u, du):
+        self.L.opv_action(self.h, _f64(u), du)
+
+    def bc_action(self, u, du):
+        self.L.opv_bc_action(self.h, _f64(u), du)
+
+    def rhs(self, u):
+        du = np.zeros(self.ndof)
+        self.L.opv_rhs(self.h, _f64(u), du)
+        return du
+
+    def steps(self, u, dt, nsteps, method="rk4", t=0.0):
+        u = _f64(u).copy()
+        tt = C.c_double(t)
+        self.L.opv_steps(self.h, {"rk4": 0, "ssprk3": 1}[method], dt, nsteps, C.byref(tt), u)
         return u, tt.value
 
 

@@ -265,6 +265,47 @@ namespace
         }
     };
 
+    // Advection<AQ> and AdvectionHomogeneousBC<AQ> with a spatially varying coefficient
+    // a(n_var, n_var, 2, n, n, n_elem) (constant_coefficient = false, wavedg/Advection.hpp:59-273)
+    // and MassMatrix<AQ>, on a GLL basis
+    struct RefOpVBase
+    {
+        int nv = 0, ndof = 0;
+        virtual ~RefOpVBase() = default;
+        virtual void action(const double *u, double *du) const = 0;
+        virtual void bc_action(const double *u, double *du) const = 0;
+        virtual void inv(double *du) const = 0;
+        void rhs(const double *u, double *du) const
+        {
+            for (int i = 0; i < ndof; ++i)
+                du[i] = 0.0;
+            action(u, du);
+            bc_action(u, du);
+            inv(du);
+        }
+    };
+    template <bool AQ>
+    struct RefOpV : RefOpVBase
+    {
+        const QuadratureRule *basis;
+        std::vector<double> a;
+        Advection<AQ> adv;
+        AdvectionHomogeneousBC<AQ> bc;
+        MassMatrix<AQ> m;
+
+        RefOpV(const Mesh2D &mesh, int n_colloc, int nv_, const double *a_)
+            : basis(QuadratureRule::quadrature_rule(n_colloc, QuadratureRule::GaussLobatto)),
+              a(a_, a_ + (size_t)2 * nv_ * nv_ * n_colloc * n_colloc * mesh.n_elem()),
+              adv(nv_, mesh, basis, a.data(), false), bc(nv_, mesh, basis, a.data(), false), m(mesh, basis)
+        {
+            nv = nv_;
+            ndof = nv_ * n_colloc * n_colloc * mesh.n_elem();
+        }
+        void action(const double *u, double *du) const override { adv.action(u, du); }
+        void bc_action(const double *u, double *du) const override { bc.action(u, du); }
+        void inv(double *du) const override { m.inv(nv, du); }
+    };
+
     // The compressible Euler system of examples/cl2d.cpp (gamma = 1.4): its physical flux,
     // wave speed and local Lax-Friedrichs numerical flux, as that example defines them
     // (cl2d.cpp:67-126), for the reference's nonlinear operators below.
@@ -668,6 +709,36 @@ extern "C"
     void ref_ope_steps(void *o, int method, double dt, int nsteps, double *t, double *u)
     {
         RefOpE *op = static_cast<RefOpE *>(o);
+        auto f = [op](double *dudt, const double, const double *v) { op->rhs(v, dudt); };
+        if (method == 0)
+        {
+            ode::RungeKutta4 rk(op->ndof);
+            for (int s = 0; s < nsteps; ++s)
+                rk.step(dt, f, *t, u);
+        }
+        else
+        {
+            ode::SSPRK3 rk(op->ndof);
+            for (int s = 0; s < nsteps; ++s)
+                rk.step(dt, f, *t, u);
+        }
+    }
+
+    // ---- Advection with a spatially varying coefficient ----
+    void *ref_opv_create(void *m, int n_colloc, int nv, const double *a, int approx)
+    {
+        const Mesh2D &mesh = static_cast<RefMesh *>(m)->mesh;
+        if (approx)
+            return static_cast<RefOpVBase *>(new RefOpV<true>(mesh, n_colloc, nv, a));
+        return static_cast<RefOpVBase *>(new RefOpV<false>(mesh, n_colloc, nv, a));
+    }
+    void ref_opv_destroy(void *o) { delete static_cast<RefOpVBase *>(o); }
+    void ref_opv_action(void *o, const double *u, double *du) { static_cast<RefOpVBase *>(o)->action(u, du); }
+    void ref_opv_bc_action(void *o, const double *u, double *du) { static_cast<RefOpVBase *>(o)->bc_action(u, du); }
+    void ref_opv_rhs(void *o, const double *u, double *du) { static_cast<RefOpVBase *>(o)->rhs(u, du); }
+    void ref_opv_steps(void *o, int method, double dt, int nsteps, double *t, double *u)
+    {
+        RefOpVBase *op = static_cast<RefOpVBase *>(o);
         auto f = [op](double *dudt, const double, const double *v) { op->rhs(v, dudt); };
         if (method == 0)
         {

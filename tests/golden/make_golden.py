@@ -1,7 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the reference library.
 
     make -C oracle ref          # compiles the reference (needs its sources)
-    python tests/golden/make_golden.py [--exact-quadrature-only | --advection-only | --reference-meshes | --euler]
+    python tests/golden/make_golden.py [--exact-quadrature-only | --advection-only | --reference-meshes | --euler | --vadvection]
 
 Every output array is produced by the reference waveDG code compiled from its
 own sources (oracle/_ref/libwdgref.so, driven through oracle/ref_harness.cpp).
@@ -176,6 +176,62 @@ def advection_fixture(name, v, q, m, n, nv, seed):
     np.savez_compressed(os.path.join(HERE, f"adv_{name}_n{n}_v{nv}.npz"), **out)
 
 
+def node_coordinates(v, q, n):
+    """Physical coordinates (x, y) of the GLL nodes, shape (n_elem, n, n) each, node (i, j) at
+    [el, j, i]: the bilinear map of the corners (QuadElement::physical_coordinates)."""
+    xs = np.asarray(cpu.basis(n, KIND)[0])
+    c = np.asarray(v)[np.asarray(q)]  # (nel, 4, 2)
+    xi, eta = xs[None, None, :], xs[None, :, None]
+    out = []
+    for k in range(2):
+        out.append(0.25 * ((1 - xi) * (1 - eta) * c[:, 0, k][:, None, None] + (1 + xi) * (1 - eta) * c[:, 1, k][:, None, None]
+                           + (1 + xi) * (1 + eta) * c[:, 2, k][:, None, None] + (1 - xi) * (1 + eta) * c[:, 3, k][:, None, None]))
+    return out
+
+
+def variable_coefficient(v, q, n, nv):
+    """a(n_var, n_var, 2, n, n, n_elem) from a smooth field at the nodes: n_var = 1 the rotating
+    velocity r (y, -x) of examples/advec2d.cpp's coefficient(); n_var > 1 symmetric matrices
+    varying in space."""
+    x, y = node_coordinates(v, q, n)  # (nel, n, n), [el, j, i]
+    nel = x.shape[0]
+    a = np.zeros((nel, n, n, 2, nv, nv))  # C order of the reverse of (k, l, comp, i, j, el)
+    if nv == 1:
+        r = np.hypot(x, y)
+        a[..., 0, 0, 0] = r * y
+        a[..., 1, 0, 0] = -r * x
+    else:
+        for k in range(nv):
+            for l in range(k, nv):
+                c0 = (1.0 + 0.3 * x + 0.1 * k) if k == l else 0.2 * np.sin(x + 2 * y + k + l)
+                c1 = (-0.5 + 0.2 * y * x - 0.1 * l) if k == l else 0.3 * np.cos(2 * x - y + k * l)
+                a[..., 0, l, k] = a[..., 0, k, l] = c0
+                a[..., 1, l, k] = a[..., 1, k, l] = c1
+    return a.reshape(-1)
+
+
+def vadvection_fixture(name, v, q, m, n, nv, approx, seed):
+    """Advection<AQ> + AdvectionHomogeneousBC<AQ> with a spatially varying coefficient
+    (constant_coefficient = false), MassMatrix<AQ>; actions, RHS, 3 steps of RK4 and SSPRK3."""
+    rng = np.random.default_rng(seed)
+    a = variable_coefficient(v, q, n, nv)
+    op = cpu.OpV(m, n, nv, a, approx)
+    u = rng.standard_normal(op.ndof)
+    out = dict(verts=v, quads=q, n=n, nv=nv, approx=int(approx), a=a, u=u)
+    for nm in ("action", "bc_action"):
+        r = rng.standard_normal(op.ndof)
+        out[f"{nm}_in"] = r.copy()
+        getattr(op, nm)(u, r)
+        out[nm] = r
+    out["rhs"] = op.rhs(u)
+    dt = 0.1 * m.min_h() / n ** 2
+    out["dt"] = dt
+    out["rk4_3"], _ = op.steps(u, dt, 3, "rk4")
+    out["ssprk3_3"], _ = op.steps(u, dt, 3, "ssprk3")
+    tag = "aq" if approx else "ex"
+    np.savez_compressed(os.path.join(HERE, f"vadv_{name}_n{n}_v{nv}_{tag}.npz"), **out)
+
+
 def opq_fixture(name, v, q, m, n, seed):
     """approx_quad = false: Div<false>, EdgeFlux<false> (interior and boundary), WaveEquation,
     the composed boundary operator over EdgeFlux<false>, MassMatrix<false>, RHS, 5 RK4 steps."""
@@ -312,6 +368,15 @@ def main():
             for n in qcases.get(name, []):
                 euler_exact_fixture(name, v, q, cpu.Mesh(v, q, KIND), n, 4500 + 100 * seed + n)
         print("Euler fixtures written to", HERE)
+        return
+    if "--vadvection" in sys.argv:
+        vcases = {"scrambled6": [(4, 1), (5, 2)], "lshape3": [(3, 1), (4, 3)]}
+        for seed, (name, v, q) in enumerate(meshes()):
+            for n, nv in vcases.get(name, []):
+                for approx in (True, False):
+                    vadvection_fixture(name, v, q, cpu.Mesh(v, q, KIND), n, nv, approx,
+                                       6000 + 100 * seed + 10 * n + nv + 5 * approx)
+        print("variable-coefficient advection fixtures written to", HERE)
         return
     if "--reference-meshes" in sys.argv:
         reference_meshes()

@@ -248,3 +248,21 @@ def test_reference_exact_euler_fixtures_reproduce(fname):
     np.testing.assert_array_equal(op.rhs(g["u"]), g["rhs"])
     np.testing.assert_array_equal(op.steps(g["u"], float(g["dt"]), 3, "rk4")[0], g["rk4_3"])
     np.testing.assert_array_equal(op.steps(g["u"], float(g["dt"]), 3, "ssprk3")[0], g["ssprk3_3"])
+
+
+@pytest.mark.parametrize("fname", golden_files("vadv_"))
+def test_reference_variable_advection_fixtures_reproduce(fname):
+    """The variable-coefficient advection fixtures (Advection<AQ>, AdvectionHomogeneousBC<AQ>
+    with constant_coefficient = false, MassMatrix<AQ>) are what the compiled reference computes
+    on their inputs; the GPU tests compare the CUDA path with them directly."""
+    require_reference_build()
+    g = golden(fname)
+    op = cpu.OpV(cpu.Mesh(g["verts"], g["quads"], "reference"), int(g["n"]), int(g["nv"]), g["a"],
+                 bool(int(g["approx"])))
+    for nm in ("action", "bc_action"):
+        r = g[f"{nm}_in"].copy()
+        getattr(op, nm)(g["u"], r)
+        np.testing.assert_array_equal(r, g[nm])
+    np.testing.assert_array_equal(op.rhs(g["u"]), g["rhs"])
+    np.testing.assert_array_equal(op.steps(g["u"], float(g["dt"]), 3, "rk4")[0], g["rk4_3"])
+    np.testing.assert_array_equal(op.steps(g["u"], float(g["dt"]), 3, "ssprk3")[0], g["ssprk3_3"])

@@ -38,6 +38,58 @@ struct wdg_advect
     double *d_rk = nullptr;             // RK4: the two rotation buffers and the register
 };
 
+namespace wdg
+{
+    // symmetric m x m eigen-decomposition, cyclic Jacobi: A = R diag(e) R^T (column-major)
+    void jacobi_eig(int m, const double *A_, double *R, double *e)
+    {
+        double A[kJacobiMax * kJacobiMax];
+        std::memcpy(A, A_, sizeof(double) * m * m);
+        for (int i = 0; i < m * m; ++i)
+            R[i] = (i % (m + 1) == 0) ? 1.0 : 0.0;
+        for (int sweep = 0; sweep < 100; ++sweep)
+        {
+            double off = 0.0;
+            for (int p = 0; p < m; ++p)
+                for (int q = p + 1; q < m; ++q)
+                    off += A[p + m * q] * A[p + m * q];
+            if (off < 1e-300)
+                break;
+            for (int p = 0; p < m; ++p)
+                for (int q = p + 1; q < m; ++q)
+                {
+                    const double apq = A[p + m * q];
+                    if (apq == 0.0)
+                        continue;
+                    const double theta = (A[q + m * q] - A[p + m * p]) / (2.0 * apq);
+                    const double t = (theta >= 0 ? 1.0 : -1.0) / (std::abs(theta) + std::sqrt(theta * theta + 1.0));
+                    const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+                    for (int k = 0; k < m; ++k)
+                    {
+                        const double akp = A[k + m * p], akq = A[k + m * q];
+                        A[k + m * p] = c * akp - sn * akq;
+                        A[k + m * q] = sn * akp + c * akq;
+                    }
+                    for (int k = 0; k < m; ++k)
+                    {
+                        const double apk = A[p + m * k], aqk = A[q + m * k];
+                        A[p + m * k] = c * apk - sn * aqk;
+                        A[q + m * k] = sn * apk + c * aqk;
+                    }
+                    for (int k = 0; k < m; ++k)
+                    {
+                        const double rkp = R[k + m * p], rkq = R[k + m * q];
+                        R[k + m * p] = c * rkp - sn * rkq;
+                        R[k + m * q] = sn * rkp + c * rkq;
+                    }
+                }
+        }
+        for (int i = 0; i < m; ++i)
+            e[i] = A[i + m * i];
+    }
+
+} // namespace wdg
+
 namespace
 {
     constexpr int kMaxVar = 8;
@@ -188,54 +240,6 @@ namespace
             fb[i + n * (d + nv * (0 + 2 * (size_t)e))] = out[d];
             fb[i + n * (d + nv * (1 + 2 * (size_t)e))] = -out[d];
         }
-    }
-
-    // symmetric m x m eigen-decomposition, cyclic Jacobi: A = R diag(e) R^T (column-major)
-    void jacobi_eig(int m, const double *A_, double *R, double *e)
-    {
-        double A[kMaxVar * kMaxVar];
-        std::memcpy(A, A_, sizeof(double) * m * m);
-        for (int i = 0; i < m * m; ++i)
-            R[i] = (i % (m + 1) == 0) ? 1.0 : 0.0;
-        for (int sweep = 0; sweep < 100; ++sweep)
-        {
-            double off = 0.0;
-            for (int p = 0; p < m; ++p)
-                for (int q = p + 1; q < m; ++q)
-                    off += A[p + m * q] * A[p + m * q];
-            if (off < 1e-300)
-                break;
-            for (int p = 0; p < m; ++p)
-                for (int q = p + 1; q < m; ++q)
-                {
-                    const double apq = A[p + m * q];
-                    if (apq == 0.0)
-                        continue;
-                    const double theta = (A[q + m * q] - A[p + m * p]) / (2.0 * apq);
-                    const double t = (theta >= 0 ? 1.0 : -1.0) / (std::abs(theta) + std::sqrt(theta * theta + 1.0));
-                    const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
-                    for (int k = 0; k < m; ++k)
-                    {
-                        const double akp = A[k + m * p], akq = A[k + m * q];
-                        A[k + m * p] = c * akp - sn * akq;
-                        A[k + m * q] = sn * akp + c * akq;
-                    }
-                    for (int k = 0; k < m; ++k)
-                    {
-                        const double apk = A[p + m * k], aqk = A[q + m * k];
-                        A[p + m * k] = c * apk - sn * aqk;
-                        A[q + m * k] = sn * apk + c * aqk;
-                    }
-                    for (int k = 0; k < m; ++k)
-                    {
-                        const double rkp = R[k + m * p], rkq = R[k + m * q];
-                        R[k + m * p] = c * rkp - sn * rkq;
-                        R[k + m * q] = sn * rkp + c * rkq;
-                    }
-                }
-        }
-        for (int i = 0; i < m; ++i)
-            e[i] = A[i + m * i];
     }
 
     // per edge: |E|/2 Fs(c, d) for both sides, Fs = R diag(-lambda/2 -+ |lambda|/2) R^T of n . A

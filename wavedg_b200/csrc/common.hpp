@@ -41,6 +41,16 @@ namespace wdg
     constexpr int kSideFrom[4] = {0, 1, 3, 0};
     constexpr int kSideTo[4] = {1, 2, 2, 3};
 
+    // QuadElement::jacobian (source/Element.cpp:21-27) of the bilinear map of the corners
+    // c = (x0, y0, ..., x3, y3) at (xi, eta): J = (x_xi, y_xi, x_eta, y_eta)
+    __host__ __device__ inline void quad_jacobian(const double *c, double xi, double eta, double J[4])
+    {
+        J[0] = 0.25 * ((1.0 - eta) * (c[2] - c[0]) + (1.0 + eta) * (c[4] - c[6]));
+        J[1] = 0.25 * ((1.0 - eta) * (c[3] - c[1]) + (1.0 + eta) * (c[5] - c[7]));
+        J[2] = 0.25 * ((1.0 - xi) * (c[6] - c[0]) + (1.0 + xi) * (c[4] - c[2]));
+        J[3] = 0.25 * ((1.0 - xi) * (c[7] - c[1]) + (1.0 + xi) * (c[5] - c[3]));
+    }
+
     struct EdgeRec
     {
         int el0, s0, el1, s1, delta;

@@ -86,6 +86,10 @@ namespace wdg
     // reference's lagrange_basis_deriv); the element inverse mass matrices of an exact handle
     void lagrange_deriv_at(int n, const double *x, int nq, const double *xq, double *D);
     const double *waveq_minv(const wdg_waveq *h);
+    // symmetric m x m (m <= kJacobiMax) eigen-decomposition by cyclic Jacobi rotations:
+    // A = R diag(e) R^T, column-major
+    constexpr int kJacobiMax = 8;
+    void jacobi_eig(int m, const double *A, double *R, double *e);
 
     ClawArgs claw_args(const wdg_wave *w, const double *x, double *out);
     int claw_steps(wdg_wave *w, int model, int nv, const double *A, const double *absA, double *const *bufs, int method,

@@ -805,6 +805,62 @@ class AdvectionSystem:
         return tt.value
 
 
+class VariableAdvectionSystem:
+    """Linear advection with a spatially varying coefficient (wdg_vadvect_*): Advection<AQ>,
+    AdvectionHomogeneousBC<AQ> (constant_coefficient = false) and MassMatrix<AQ> for n_var
+    variables on a GLL basis; a in the reference's (n_var, n_var, 2, n, n, n_elem) layout
+    (a host array); approx_quad False selects the Gauss-Legendre rules of Div<false> /
+    EdgeFlux<false> and the dense mass matrix, as examples/advec2d.cpp does.  One variable, or
+    symmetric coefficient matrices.  FP64."""
+
+    def __init__(self, n_var: int, mesh: Mesh2D, basis, a, approx_quad: bool = True, device: int = -1):
+        self.n_var, self.mesh, self.n = int(n_var), mesh, _gll_n(basis)
+        self.approx_quad = bool(approx_quad)
+        av = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+        if av.size != 2 * self.n_var ** 2 * self.n ** 2 * mesh.n_elem():
+            raise WdgError(_lib.WDG_ERR_ARG, "a must hold 2 n_var^2 n^2 n_elem coefficients")
+        h = C.c_void_p()
+        check(lib().wdg_vadvect_create(mesh._h, self.n, self.n_var, C.c_void_p(av.ctypes.data),
+                                       int(self.approx_quad), device, C.byref(h)), "wdg_vadvect_create")
+        self._h = h
+        self.ndof = self.n_var * self.n * self.n * mesh.n_elem()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _destroy("wdg_vadvect_destroy", h)
+            self._h = None
+
+    def _call(self, fn, u, du, what):
+        pu, _ku = _ptr(u, name="u")
+        pd, _kd = _ptr(du, True, "du")
+        check(getattr(lib(), fn)(self._h, pu, pd), what)
+
+    def set_stream(self, stream) -> None:
+        check(lib().wdg_vadvect_set_stream(self._h, C.c_void_p(getattr(stream, "cuda_stream", stream))))
+
+    def sync(self) -> None:
+        check(lib().wdg_vadvect_sync(self._h))
+
+    def action(self, u, du) -> None:
+        self._call("wdg_vadvect_action", u, du, "Advection.action")
+
+    def bc_action(self, u, du) -> None:
+        self._call("wdg_vadvect_bc_action", u, du, "AdvectionHomogeneousBC.action")
+
+    def rhs(self, u, dudt) -> None:
+        self._call("wdg_vadvect_rhs", u, dudt, "rhs")
+
+    def steps(self, u, dt: float, t: float, nsteps: int, method: str = "ssprk3") -> float:
+        """nsteps of ode::SSPRK3 ("ssprk3", examples/advec2d.cpp's stepper) or ode::RungeKutta4
+        ("rk4") on u in place; returns the new time."""
+        pu, _ku = _ptr(u, True, "u")
+        tt = C.c_double(t)
+        check(lib().wdg_vadvect_steps(self._h, {"rk4": 0, "ssprk3": 1}[method], pu, float(dt), C.byref(tt),
+                                      int(nsteps)), "steps")
+        return tt.value
+
+
 class EulerSystem:
     """The compressible Euler system of examples/cl2d.cpp (wdg_euler_create[_exact], wdg_claw_*):
     state u(d, i, j, el) with d = density, x-momentum, y-momentum, energy, gamma = 1.4; DivF2D
@@ -863,30 +919,34 @@ class EulerSystem:
         return tt.value
 
 
+def _advection_system(n_var, mesh, basis, a, constant_coefficient, quad, approx_quad):
+    if quad is not None:
+        raise WdgError(_lib.WDG_ERR_UNSUPPORTED, "advection is built for the default quadrature rules")
+    if not constant_coefficient:
+        return VariableAdvectionSystem(n_var, mesh, basis, a, approx_quad)
+    _require_approx(approx_quad)
+    return AdvectionSystem(n_var, mesh, basis, a)
+
+
 class Advection(Operator):
-    """Advection<true>(n_var, mesh, basis, a, constant_coefficient): du += (A u, grad v) + upwind
-    flux over interior edges (wavedg/Advection.hpp:17-142).  Constant symmetric coefficients."""
+    """Advection<AQ>(n_var, mesh, basis, a, constant_coefficient): du += (A u, grad v) + upwind
+    flux over interior edges (wavedg/Advection.hpp:17-142).  Constant symmetric coefficients
+    (approx_quad = True), or a spatially varying coefficient with either quadrature."""
 
     def __init__(self, n_var: int, mesh: Mesh2D, basis, a, constant_coefficient: bool = True, quad=None,
                  approx_quad: bool = True):
-        _require_approx(approx_quad)
-        if not constant_coefficient or quad is not None:
-            raise WdgError(_lib.WDG_ERR_UNSUPPORTED, "advection is built for constant coefficients and the GLL rule")
-        self.sys = AdvectionSystem(n_var, mesh, basis, a)
+        self.sys = _advection_system(n_var, mesh, basis, a, constant_coefficient, quad, approx_quad)
 
     def action(self, *args) -> None:
         self.sys.action(args[-2], args[-1])
 
 
 class AdvectionHomogeneousBC(Operator):
-    """AdvectionHomogeneousBC<true>: du += boundary flux with u = 0 outside (wavedg/Advection.hpp:144-273)."""
+    """AdvectionHomogeneousBC<AQ>: du += boundary flux with u = 0 outside (wavedg/Advection.hpp:144-273)."""
 
     def __init__(self, n_var: int, mesh: Mesh2D, basis, a, constant_coefficient: bool = True, quad=None,
                  approx_quad: bool = True):
-        _require_approx(approx_quad)
-        if not constant_coefficient or quad is not None:
-            raise WdgError(_lib.WDG_ERR_UNSUPPORTED, "advection is built for constant coefficients and the GLL rule")
-        self.sys = AdvectionSystem(n_var, mesh, basis, a)
+        self.sys = _advection_system(n_var, mesh, basis, a, constant_coefficient, quad, approx_quad)
 
     def action(self, *args) -> None:
         self.sys.bc_action(args[-2], args[-1])
