@@ -185,7 +185,8 @@ int wdg_advect_rk4_steps(wdg_advect *adv, double *u, double dt, double *t, int n
 
 /* ---- linear advection with a spatially varying coefficient ---- */
 /* Advection<AQ> and AdvectionHomogeneousBC<AQ> with constant_coefficient = false
- * (wavedg/Advection.hpp:59-273) and MassMatrix<AQ> on a GLL basis: a is the host array
+ * (wavedg/Advection.hpp:59-273) and MassMatrix<AQ> on a basis of basis_type (Gauss-Lobatto, or
+ * Gauss-Legendre as examples/advec2d.cpp uses, with LegendreFaceProlongator's traces): a is the host array
  * a(k, l, comp, i, j, el) = a[k + n_var (l + n_var (comp + 2 (i + n (j + n el))))], A^comp_{k,l}
  * at node (i, j) of element el (the reference's layout); approx_quad selects Div<true> /
  * EdgeFlux<true> (1) or Div<false> / EdgeFlux<false> on their default Gauss-Legendre rules with
@@ -193,8 +194,10 @@ int wdg_advect_rk4_steps(wdg_advect *adv, double *u, double dt, double *t, int n
  * eigen-decomposition of n.A at every face point: n_var = 1, or n.A symmetric (n_var <= 8;
  * WDG_ERR_UNSUPPORTED otherwise).  FP64. */
 typedef struct wdg_vadvect wdg_vadvect;
-int wdg_vadvect_create(const wdg_mesh *mesh, int n_colloc, int n_var, const double *a, int approx_quad, int device,
-                       wdg_vadvect **out);
+#define WDG_GAUSS_LEGENDRE 0 /* QuadratureRule::GaussLegendre (wavedg/QuadratureRule.hpp:26-30) */
+#define WDG_GAUSS_LOBATTO 1  /* QuadratureRule::GaussLobatto */
+int wdg_vadvect_create(const wdg_mesh *mesh, int n_colloc, int basis_type, int n_var, const double *a,
+                       int approx_quad, int device, wdg_vadvect **out);
 void wdg_vadvect_destroy(wdg_vadvect *adv);
 int wdg_vadvect_set_stream(wdg_vadvect *adv, void *cuda_stream);
 int wdg_vadvect_sync(wdg_vadvect *adv);

@@ -60,7 +60,7 @@ _SIGS = {
     "opa_bc_action": ([_v, _dp, _dp], None),
     "opa_rhs": ([_v, _dp, _dp], None),
     "opa_rk4": ([_v, _d, _i, C.POINTER(C.c_double), _dp], None),
-    "opv_create": ([_v, _i, _i, _dp, _i], _v),
+    "opv_create": ([_v, _i, _i, _dp, _i, _i], _v),
     "opv_destroy": ([_v], None),
     "opv_action": ([_v, _dp, _dp], None),
     "opv_bc_action": ([_v, _dp, _dp], None),
@@ -440,14 +440,14 @@ class OpEQ(OpE):
 
 class OpV:
     """Advection<AQ> + AdvectionHomogeneousBC<AQ> + MassMatrix<AQ> with a spatially varying
-    coefficient a(n_var, n_var, 2, n, n, n_elem) (constant_coefficient = false), GLL basis;
-    the reference harness only."""
+    coefficient a(n_var, n_var, 2, n, n, n_elem) (constant_coefficient = false) on a Gauss-Lobatto
+    (basis_type 1) or Gauss-Legendre (0) basis; the reference harness only."""
 
-    def __init__(self, mesh: Mesh, n: int, nv: int, a, approx_quad: bool):
+    def __init__(self, mesh: Mesh, n: int, nv: int, a, approx_quad: bool, basis_type: int = 1):
         self.L, self.mesh, self.n, self.nv = mesh.L, mesh, n, nv
         self.a = _f64(a).reshape(-1)
         assert self.a.size == 2 * nv * nv * n * n * mesh.n_elem
-        self.h = self.L.opv_create(mesh.h, n, nv, self.a, int(bool(approx_quad)))
+        self.h = self.L.opv_create(mesh.h, n, nv, self.a, int(bool(approx_quad)), int(basis_type))
         self.ndof = nv * n * n * mesh.n_elem
 
     def __del__(self):

@@ -267,7 +267,7 @@ namespace
 
     // Advection<AQ> and AdvectionHomogeneousBC<AQ> with a spatially varying coefficient
     // a(n_var, n_var, 2, n, n, n_elem) (constant_coefficient = false, wavedg/Advection.hpp:59-273)
-    // and MassMatrix<AQ>, on a GLL basis
+    // and MassMatrix<AQ>, on a Gauss-Lobatto or Gauss-Legendre basis
     struct RefOpVBase
     {
         int nv = 0, ndof = 0;
@@ -293,8 +293,8 @@ namespace
         AdvectionHomogeneousBC<AQ> bc;
         MassMatrix<AQ> m;
 
-        RefOpV(const Mesh2D &mesh, int n_colloc, int nv_, const double *a_)
-            : basis(QuadratureRule::quadrature_rule(n_colloc, QuadratureRule::GaussLobatto)),
+        RefOpV(const Mesh2D &mesh, int n_colloc, int nv_, const double *a_, QuadratureRule::QuadratureType type)
+            : basis(QuadratureRule::quadrature_rule(n_colloc, type)),
               a(a_, a_ + (size_t)2 * nv_ * nv_ * n_colloc * n_colloc * mesh.n_elem()),
               adv(nv_, mesh, basis, a.data(), false), bc(nv_, mesh, basis, a.data(), false), m(mesh, basis)
         {
@@ -725,12 +725,14 @@ extern "C"
     }
 
     // ---- Advection with a spatially varying coefficient ----
-    void *ref_opv_create(void *m, int n_colloc, int nv, const double *a, int approx)
+    // basis_type: 0 Gauss-Legendre, 1 Gauss-Lobatto (QuadratureRule::QuadratureType's order)
+    void *ref_opv_create(void *m, int n_colloc, int nv, const double *a, int approx, int basis_type)
     {
         const Mesh2D &mesh = static_cast<RefMesh *>(m)->mesh;
+        const auto type = basis_type == 0 ? QuadratureRule::GaussLegendre : QuadratureRule::GaussLobatto;
         if (approx)
-            return static_cast<RefOpVBase *>(new RefOpV<true>(mesh, n_colloc, nv, a));
-        return static_cast<RefOpVBase *>(new RefOpV<false>(mesh, n_colloc, nv, a));
+            return static_cast<RefOpVBase *>(new RefOpV<true>(mesh, n_colloc, nv, a, type));
+        return static_cast<RefOpVBase *>(new RefOpV<false>(mesh, n_colloc, nv, a, type));
     }
     void ref_opv_destroy(void *o) { delete static_cast<RefOpVBase *>(o); }
     void ref_opv_action(void *o, const double *u, double *du) { static_cast<RefOpVBase *>(o)->action(u, du); }

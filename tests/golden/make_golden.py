@@ -176,10 +176,11 @@ def advection_fixture(name, v, q, m, n, nv, seed):
     np.savez_compressed(os.path.join(HERE, f"adv_{name}_n{n}_v{nv}.npz"), **out)
 
 
-def node_coordinates(v, q, n):
-    """Physical coordinates (x, y) of the GLL nodes, shape (n_elem, n, n) each, node (i, j) at
-    [el, j, i]: the bilinear map of the corners (QuadElement::physical_coordinates)."""
-    xs = np.asarray(cpu.basis(n, KIND)[0])
+def node_coordinates(v, q, n, legendre=False):
+    """Physical coordinates (x, y) of the basis nodes (GLL, or Gauss-Legendre), shape
+    (n_elem, n, n) each, node (i, j) at [el, j, i]: the bilinear map of the corners
+    (QuadElement::physical_coordinates)."""
+    xs = np.polynomial.legendre.leggauss(n)[0] if legendre else np.asarray(cpu.basis(n, KIND)[0])
     c = np.asarray(v)[np.asarray(q)]  # (nel, 4, 2)
     xi, eta = xs[None, None, :], xs[None, :, None]
     out = []
@@ -189,11 +190,11 @@ def node_coordinates(v, q, n):
     return out
 
 
-def variable_coefficient(v, q, n, nv):
+def variable_coefficient(v, q, n, nv, legendre=False):
     """a(n_var, n_var, 2, n, n, n_elem) from a smooth field at the nodes: n_var = 1 the rotating
     velocity r (y, -x) of examples/advec2d.cpp's coefficient(); n_var > 1 symmetric matrices
     varying in space."""
-    x, y = node_coordinates(v, q, n)  # (nel, n, n), [el, j, i]
+    x, y = node_coordinates(v, q, n, legendre)  # (nel, n, n), [el, j, i]
     nel = x.shape[0]
     a = np.zeros((nel, n, n, 2, nv, nv))  # C order of the reverse of (k, l, comp, i, j, el)
     if nv == 1:
@@ -210,14 +211,15 @@ def variable_coefficient(v, q, n, nv):
     return a.reshape(-1)
 
 
-def vadvection_fixture(name, v, q, m, n, nv, approx, seed):
+def vadvection_fixture(name, v, q, m, n, nv, approx, seed, legendre=False):
     """Advection<AQ> + AdvectionHomogeneousBC<AQ> with a spatially varying coefficient
-    (constant_coefficient = false), MassMatrix<AQ>; actions, RHS, 3 steps of RK4 and SSPRK3."""
+    (constant_coefficient = false), MassMatrix<AQ>, on a Gauss-Lobatto or (legendre) a
+    Gauss-Legendre basis; actions, RHS, 3 steps of RK4 and SSPRK3."""
     rng = np.random.default_rng(seed)
-    a = variable_coefficient(v, q, n, nv)
-    op = cpu.OpV(m, n, nv, a, approx)
+    a = variable_coefficient(v, q, n, nv, legendre)
+    op = cpu.OpV(m, n, nv, a, approx, 0 if legendre else 1)
     u = rng.standard_normal(op.ndof)
-    out = dict(verts=v, quads=q, n=n, nv=nv, approx=int(approx), a=a, u=u)
+    out = dict(verts=v, quads=q, n=n, nv=nv, approx=int(approx), basis_type=0 if legendre else 1, a=a, u=u)
     for nm in ("action", "bc_action"):
         r = rng.standard_normal(op.ndof)
         out[f"{nm}_in"] = r.copy()
@@ -228,7 +230,7 @@ def vadvection_fixture(name, v, q, m, n, nv, approx, seed):
     out["dt"] = dt
     out["rk4_3"], _ = op.steps(u, dt, 3, "rk4")
     out["ssprk3_3"], _ = op.steps(u, dt, 3, "ssprk3")
-    tag = "aq" if approx else "ex"
+    tag = ("aq" if approx else "ex") + ("_gl" if legendre else "")
     np.savez_compressed(os.path.join(HERE, f"vadv_{name}_n{n}_v{nv}_{tag}.npz"), **out)
 
 
@@ -376,6 +378,13 @@ def main():
                 for approx in (True, False):
                     vadvection_fixture(name, v, q, cpu.Mesh(v, q, KIND), n, nv, approx,
                                        6000 + 100 * seed + 10 * n + nv + 5 * approx)
+        # Gauss-Legendre bases (examples/advec2d.cpp: n = 5, n_var = 1, approx_quad = false)
+        gcases = {"scrambled6": [(5, 1), (3, 2)], "lshape3": [(4, 1)]}
+        for seed, (name, v, q) in enumerate(meshes()):
+            for n, nv in gcases.get(name, []):
+                for approx in (True, False):
+                    vadvection_fixture(name, v, q, cpu.Mesh(v, q, KIND), n, nv, approx,
+                                       6500 + 100 * seed + 10 * n + nv + 5 * approx, legendre=True)
         print("variable-coefficient advection fixtures written to", HERE)
         return
     if "--reference-meshes" in sys.argv:

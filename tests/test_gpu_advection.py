@@ -78,8 +78,9 @@ def test_variable_coefficient_advection_matches_reference(gpu_lib, fname):
     """Advection<AQ> / AdvectionHomogeneousBC<AQ> with constant_coefficient = false
     (tests/golden/vadv_*.npz: the compiled reference's outputs for n_var = 1 with the rotating
     velocity of examples/advec2d.cpp and n_var = 2, 3 with symmetric matrices varying in
-    space; approx_quad true (_aq) and false (_ex)): the actions and the RHS to 1e-12, three
-    RK4 and SSPRK3 steps to 1e-11, host and device arrays alike."""
+    space; approx_quad true (_aq) and false (_ex); Gauss-Lobatto bases, and Gauss-Legendre
+    (_gl) as examples/advec2d.cpp uses): the actions and the RHS to 1e-12, three RK4 and
+    SSPRK3 steps to 1e-11, host and device arrays alike."""
     import torch
 
     import wavedg_b200 as W
@@ -87,7 +88,7 @@ def test_variable_coefficient_advection_matches_reference(gpu_lib, fname):
     g = golden(fname)
     mesh = W.Mesh2D.from_vertices(g["verts"], g["quads"])
     n, nv, approx = int(g["n"]), int(g["nv"]), bool(int(g["approx"]))
-    basis = W.QuadratureRule.quadrature_rule(n, W.QuadratureRule.GaussLobatto)
+    basis = W.QuadratureRule.quadrature_rule(n, int(g["basis_type"]))
     u = g["u"]
     r = g["action_in"].copy()
     W.Advection(nv, mesh, basis, g["a"], False, approx_quad=approx).action(u, r)

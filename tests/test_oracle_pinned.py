@@ -258,7 +258,7 @@ def test_reference_variable_advection_fixtures_reproduce(fname):
     require_reference_build()
     g = golden(fname)
     op = cpu.OpV(cpu.Mesh(g["verts"], g["quads"], "reference"), int(g["n"]), int(g["nv"]), g["a"],
-                 bool(int(g["approx"])))
+                 bool(int(g["approx"])), int(g["basis_type"]))
     for nm in ("action", "bc_action"):
         r = g[f"{nm}_in"].copy()
         getattr(op, nm)(g["u"], r)

@@ -92,6 +92,86 @@ namespace wdg
     }
 
     const double *waveq_minv(const wdg_waveq *h) { return h->d_Minv; }
+
+    // MassMatrix<false> (source/MassMatrix.cpp:84-227) on the basis with nodes x: the element
+    // mass matrices M(i, j) = sum_p w_p det J_p phi_i phi_j on the qm x qm Gauss-Legendre rule
+    // (lower triangle, Cholesky in place; chol, linalg.cpp:5-30) and their inverses, solved
+    // column by column (solve_chol, linalg.cpp:32-66); (n^2, n^2, nel) each
+    int exact_mass(const wdg_mesh &mesh, int n, const double *x, int qm, std::vector<double> &Mf,
+                   std::vector<double> &Mi)
+    {
+        const int c = n * n, q2 = qm * qm;
+        std::vector<double> xm(qm), wm(qm), Bm((size_t)qm * n), L((size_t)c * c, 0.0), detJ(q2);
+        Mf.assign((size_t)c * c * mesh.nel, 0.0);
+        Mi.assign((size_t)c * c * mesh.nel, 0.0);
+        gauss_legendre(qm, xm.data(), wm.data());
+        interp_matrix(n, x, qm, xm.data(), Bm.data());
+        int st = WDG_OK;
+        for (int el = 0; el < mesh.nel && st == WDG_OK; ++el)
+        {
+            const double *cr = &mesh.corners[8 * (size_t)el];
+            for (int p = 0; p < q2; ++p)
+            {
+                double J[4];
+                quad_jacobian(cr, xm[p % qm], xm[p / qm], J);
+                detJ[p] = J[0] * J[3] - J[2] * J[1];
+            }
+            double *M = L.data();
+            std::fill(L.begin(), L.end(), 0.0);
+            for (int j = 0; j < c; ++j)
+                for (int i = j; i < c; ++i)
+                {
+                    double mij = 0.0;
+                    for (int p = 0; p < q2; ++p)
+                    {
+                        const double bi = Bm[p % qm + qm * (i % n)] * Bm[p / qm + qm * (i / n)];
+                        const double bj = Bm[p % qm + qm * (j % n)] * Bm[p / qm + qm * (j / n)];
+                        mij += bi * bj * detJ[p] * wm[p % qm] * wm[p / qm];
+                    }
+                    M[i + c * j] = mij;
+                    Mf[(size_t)c * c * el + i + c * j] = mij;
+                    Mf[(size_t)c * c * el + j + c * i] = mij;
+                }
+            for (int k = 0; k < c && st == WDG_OK; ++k)
+            {
+                for (int j = k + 1; j < c; ++j)
+                {
+                    const double sc = M[j + c * k] / M[k + c * k];
+                    for (int i = j; i < c; ++i)
+                        M[i + c * j] -= sc * M[i + c * k];
+                }
+                if (!(M[k + c * k] > 0.0))
+                    st = fail(WDG_ERR_ARG, "an element mass matrix is not positive definite");
+                else
+                {
+                    const double sc = 1.0 / std::sqrt(M[k + c * k]);
+                    for (int i = k; i < c; ++i)
+                        M[i + c * k] *= sc;
+                }
+            }
+            // M^{-1} column by column: solve_chol on the unit vectors (linalg.cpp:32-66)
+            for (int col = 0; col < c && st == WDG_OK; ++col)
+            {
+                double *X = &Mi[(size_t)c * c * el + (size_t)c * col];
+                for (int i = 0; i < c; ++i)
+                    X[i] = (i == col) ? 1.0 : 0.0;
+                for (int j = 0; j < c; ++j)
+                {
+                    X[j] /= M[j + c * j];
+                    for (int i = j + 1; i < c; ++i)
+                        X[i] -= M[i + c * j] * X[j];
+                }
+                for (int j = c - 1; j >= 0; --j)
+                {
+                    X[j] /= M[j + c * j];
+                    for (int i = 0; i < j; ++i)
+                        X[i] -= M[j + c * i] * X[j];
+                }
+            }
+        }
+        return st;
+    }
+
 } // namespace wdg
 
 namespace
@@ -775,75 +855,8 @@ extern "C"
             return nr;
         };
         const std::vector<double> nI = normals(mesh->interior), nB = normals(mesh->boundary);
-        // element mass matrices on the nqm x nqm rule (lower triangle), Cholesky in place
-        const int qm = h->nqm, q2 = qm * qm;
-        std::vector<double> xm(qm), wm(qm), Bm((size_t)qm * n), L((size_t)c * c, 0.0), detJ(q2);
-        std::vector<double> Mf((size_t)c * c * w->nel), Mi((size_t)c * c * w->nel);
-        gauss_legendre(qm, xm.data(), wm.data());
-        interp_matrix(n, x.data(), qm, xm.data(), Bm.data());
-        int st = WDG_OK;
-        for (int el = 0; el < w->nel && st == WDG_OK; ++el)
-        {
-            const double *cr = &mesh->corners[8 * (size_t)el];
-            for (int p = 0; p < q2; ++p)
-            {
-                double J[4];
-                jac(cr, xm[p % qm], xm[p / qm], J);
-                detJ[p] = J[0] * J[3] - J[2] * J[1];
-            }
-            double *M = L.data();
-            std::fill(L.begin(), L.end(), 0.0);
-            for (int j = 0; j < c; ++j)
-                for (int i = j; i < c; ++i)
-                {
-                    double mij = 0.0;
-                    for (int p = 0; p < q2; ++p)
-                    {
-                        const double bi = Bm[p % qm + qm * (i % n)] * Bm[p / qm + qm * (i / n)];
-                        const double bj = Bm[p % qm + qm * (j % n)] * Bm[p / qm + qm * (j / n)];
-                        mij += bi * bj * detJ[p] * wm[p % qm] * wm[p / qm];
-                    }
-                    M[i + c * j] = mij;
-                    Mf[(size_t)c * c * el + i + c * j] = mij;
-                    Mf[(size_t)c * c * el + j + c * i] = mij;
-                }
-            for (int k = 0; k < c && st == WDG_OK; ++k)
-            {
-                for (int j = k + 1; j < c; ++j)
-                {
-                    const double sc = M[j + c * k] / M[k + c * k];
-                    for (int i = j; i < c; ++i)
-                        M[i + c * j] -= sc * M[i + c * k];
-                }
-                if (!(M[k + c * k] > 0.0))
-                    st = fail(WDG_ERR_ARG, "wdg_waveq_create: an element mass matrix is not positive definite");
-                else
-                {
-                    const double sc = 1.0 / std::sqrt(M[k + c * k]);
-                    for (int i = k; i < c; ++i)
-                        M[i + c * k] *= sc;
-                }
-            }
-            // M^{-1} column by column: solve_chol on the unit vectors (linalg.cpp:32-66)
-            for (int col = 0; col < c && st == WDG_OK; ++col)
-            {
-                double *X = &Mi[(size_t)c * c * el + (size_t)c * col];
-                for (int i = 0; i < c; ++i)
-                    X[i] = (i == col) ? 1.0 : 0.0;
-                for (int j = 0; j < c; ++j)
-                {
-                    X[j] /= M[j + c * j];
-                    for (int i = j + 1; i < c; ++i)
-                        X[i] -= M[i + c * j] * X[j];
-                }
-                for (int j = c - 1; j >= 0; --j)
-                {
-                    X[j] /= M[j + c * j];
-                    for (int i = 0; i < j; ++i)
-                        X[i] -= M[j + c * i] * X[j];
-                }
-            }
-        }
+        std::vector<double> Mf, Mi;
+        int st = exact_mass(*mesh, n, x.data(), h->nqm, Mf, Mi);
         auto chk = [&](int r)
         {
             if (st == WDG_OK)

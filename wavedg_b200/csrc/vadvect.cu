@@ -1,7 +1,7 @@
 // C-ABI: linear advection with a spatially varying coefficient, Advection<AQ> and
 // AdvectionHomogeneousBC<AQ> with constant_coefficient = false (wavedg/Advection.hpp:59-273), on
-// GLL bases with either quadrature, MassMatrix<AQ>, as one fused kernel per operator
-// application, RHS or time-stepping stage.
+// Gauss-Lobatto or Gauss-Legendre bases with either quadrature, MassMatrix<AQ>, as one fused
+// kernel per operator application, RHS or time-stepping stage.
 //
 // The reference turns the coefficient and the geometry into operator tables once, at
 // construction; this handle does the same on the host, with the same arithmetic:
@@ -19,8 +19,10 @@
 // The kernel (one warp per element, the element staged in shared memory) forms u at the volume
 // points, the flux sum_c op(comp, c, d) u_c and its D / P contractions back to the nodes
 // (div_2d_c and div_2d_q, source/Div.cpp:131-180, 469-589); per side the own trace and the
-// neighbour's (partner table of the collocation handle) at the face points, the two matrices,
-// back with P^T (flux_action_2d_c / _q, source/EdgeFlux.cpp:289-320, 553-624); then adds the
+// neighbour's at the face points (Lobatto: nodal values, through the partner table of the
+// collocation handle; Legendre: the interpolation of LegendreFaceProlongator along the lines of
+// nodes normal to the side), the two matrices, back with P^T (flux_action_2d_c / _q,
+// source/EdgeFlux.cpp:289-320, 553-624) and onto the nodes (the prolongator's transpose); then adds the
 // result (the operators' action), or applies M^{-1} and writes the RHS or an RK4 / SSPRK3 stage.
 // The flux matrices need a real eigen-decomposition of n.A: one variable, or symmetric
 // coefficient matrices (cyclic Jacobi), are built.  FP64.
@@ -38,12 +40,13 @@ using namespace wdg;
 struct wdg_vadvect
 {
     wdg_wave *w = nullptr;      // geometry, partner tables, argument staging
-    wdg_waveq *exact = nullptr; // approx_quad = false: owns w, and MassMatrix<false>'s inverse
     int n = 0, nv = 0, Q = 0, Qf = 0;
-    bool approx = true;
+    bool approx = true, legendre = false;
     double *d_Pv = nullptr, *d_Dv = nullptr, *d_Pf = nullptr;  // the rules' matrices (Q x n, Qf x n)
-    double *d_xg = nullptr, *d_wg = nullptr;                   // GLL nodes and weights
-    double *d_op = nullptr, *d_G = nullptr;                                   // volume and face tables
+    double *d_xg = nullptr, *d_wg = nullptr, *d_e = nullptr;   // basis nodes, weights, phi(-1)
+    double *d_op = nullptr, *d_G = nullptr;                    // volume and face tables
+    double *d_Minv = nullptr;                                  // approx_quad = false: MassMatrix<false>^{-1}
+    int *d_nb = nullptr; // Gauss-Legendre: per side (neighbour element * 4 + its side) * 2 + reversed, -1 boundary
     double *d_buf[3] = {nullptr, nullptr, nullptr};
 };
 
@@ -58,14 +61,16 @@ namespace
     struct VArgs
     {
         ClawArgs c; // state, output, stage coefficients, geometry, partner table, error word
-        const double *op, *G, *Pv, *Dv, *Pf, *xg, *wg, *Minv;
-        int n, nv, Q, Qf, approx;
+        const double *op, *G, *Pv, *Dv, *Pf, *xg, *wg, *e, *Minv;
+        const int *nb;
+        int n, nv, Q, Qf, approx, legendre;
     };
 
     __host__ __device__ inline int va_warp_doubles(int n, int nv, int Q, int Qf)
     {
-        // su r (nv n^2 each) | Pu (nv n Q) | Uq (nv Q^2) | Fq (2 nv Q^2) | Df Pg (nv Q n each) | T1 (4 n nv) | UF (4 Qf nv)
-        return 2 * nv * n * n + nv * n * Q + 3 * nv * Q * Q + 2 * nv * Q * n + 4 * n * nv + 4 * Qf * nv;
+        // su r (nv n^2 each) | Pu (nv n Q) | Uq (nv Q^2) | Fq (2 nv Q^2) | Df Pg (nv Q n each) | T0 T1 (4 n nv each)
+        // | UF (4 Qf nv)
+        return 2 * nv * n * n + nv * n * Q + 3 * nv * Q * Q + 2 * nv * Q * n + 8 * n * nv + 4 * Qf * nv;
     }
 
     __device__ inline int va_node(int n, int s, int k)
@@ -73,6 +78,15 @@ namespace
         const int i = (s == 0 || s == 2) ? k : (s == 1 ? n - 1 : 0);
         const int j = (s == 1 || s == 3) ? k : (s == 2 ? n - 1 : 0);
         return i + n * j;
+    }
+
+    // LegendreFaceProlongator's node map (source/FaceProlongator.cpp:716-737): the node at
+    // distance k from side s at position i along it
+    __device__ inline int va_line(int n, int s, int i, int k)
+    {
+        const int x = (s == 0 || s == 2) ? i : (s == 1 ? n - 1 - k : k);
+        const int y = (s == 1 || s == 3) ? i : (s == 2 ? n - 1 - k : k);
+        return x + n * y;
     }
 
     __global__ void vadv_kernel(const VArgs A, int warps)
@@ -84,7 +98,9 @@ namespace
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
         double *su = vsm + (size_t)warp * va_warp_doubles(n, nv, Q, Qf);
         double *r = su + nv * nn, *Pu = r + nv * nn, *Uq = Pu + nv * n * Q, *Fq = Uq + nv * QQ;
-        double *Df = Fq + 2 * nv * QQ, *Pg = Df + nv * Q * n, *T1 = Pg + nv * Q * n, *UF = T1 + 4 * n * nv;
+        double *Df = Fq + 2 * nv * QQ, *Pg = Df + nv * Q * n, *T0 = Pg + nv * Q * n, *T1 = T0 + 4 * n * nv;
+        double *UF = T1 + 4 * n * nv;
+        const bool leg = A.legendre != 0;
         const long long limit = (long long)nn * a.nel;
         const bool vol = a.mode != VA_BC;
         for (int el = blockIdx.x * warps + warp; el < a.nel; el += gridDim.x * warps)
@@ -189,16 +205,46 @@ namespace
                 const bool bnd = ((codes >> (8 * s)) & 0x80u) != 0;
                 return a.mode == VA_ACT ? !bnd : (a.mode == VA_BC ? bnd : true);
             };
-            // neighbour nodal traces T1(s, k, c) on interior sides
+            // the element's own traces T0(s, k, c) and its neighbours' T1(s, k, c) on the sides this
+            // call adds (interior sides; 0 on the boundary): GLL nodal values through the partner
+            // table, Gauss-Legendre sum_k phi_k(-1) u(line node k) (legendre_action_2d,
+            // source/FaceProlongator.cpp:806-834)
             for (int o = lane; o < 4 * n; o += 32)
             {
                 const int s = o / n, k = o - s * n;
                 const uint32_t byte = (codes >> (8 * s)) & 0xffu;
-                double *t1 = T1 + nv * o;
-                if ((byte & 0x80u) || !wanted(s))
+                double *t0 = T0 + nv * o, *t1 = T1 + nv * o;
+                for (int d = 0; d < nv; ++d)
                 {
+                    double v = 0.0;
+                    if (leg)
+                        for (int m = 0; m < n; ++m)
+                            v += su[d + nv * va_line(n, s, k, m)] * A.e[m];
+                    else
+                        v = su[d + nv * va_node(n, s, k)];
+                    t0[d] = v;
+                    t1[d] = 0.0;
+                }
+                if ((byte & 0x80u) || !wanted(s))
+                    continue;
+                if (leg)
+                {
+                    const int code = __ldg(A.nb + 4 * (size_t)el + s);
+                    const long long ne = code >> 3; // neighbour element
+                    const int ns = (code >> 1) & 3, kk = (code & 1) ? n - 1 - k : k;
+                    if (code < 0 || ne >= a.nel)
+                    {
+                        atomicOr(a.err, 2u);
+                        continue;
+                    }
+                    const double *xn = a.x + (size_t)nv * nn * ne;
                     for (int d = 0; d < nv; ++d)
-                        t1[d] = 0.0;
+                    {
+                        double v = 0.0;
+                        for (int m = 0; m < n; ++m)
+                            v += __ldg(xn + d + nv * va_line(n, ns, kk, m)) * A.e[m];
+                        t1[d] = v;
+                    }
                     continue;
                 }
                 const int off = (s == 0) ? fb.x : (s == 1) ? fb.y : (s == 2) ? fb.z : fb.w;
@@ -206,11 +252,7 @@ namespace
                 const int stride = (sc == 0) ? 1 : (sc == 1) ? -1 : (sc == 2) ? n : -n; // in nodes
                 const long long pn = (long long)(off / 3) + (long long)k * stride;
                 if (off < 0 || pn < 0 || pn >= limit)
-                {
                     atomicOr(a.err, 2u);
-                    for (int d = 0; d < nv; ++d)
-                        t1[d] = 0.0;
-                }
                 else
                     for (int d = 0; d < nv; ++d)
                         t1[d] = __ldg(a.x + (size_t)nv * pn + d);
@@ -236,7 +278,7 @@ namespace
                         for (int j = 0; j < n; ++j)
                         {
                             const double p = A.Pf[q + Qf * j];
-                            so += su[cc + nv * va_node(n, s, j)] * p;
+                            so += T0[cc + nv * (s * n + j)] * p;
                             sn += T1[cc + nv * (s * n + j)] * p;
                         }
                         Uo[cc] = so;
@@ -244,7 +286,7 @@ namespace
                     }
                     else
                     {
-                        Uo[cc] = su[cc + nv * va_node(n, s, q)];
+                        Uo[cc] = T0[cc + nv * (s * n + q)];
                         Un[cc] = T1[cc + nv * (s * n + q)];
                     }
                 }
@@ -258,32 +300,54 @@ namespace
                 }
             }
             __syncwarp();
-            // back to the face nodes, added: sides 0 and 2, then 1 and 3 (corners are shared by
-            // neighbouring sides only)
-            for (int pass = 0; pass < 2; ++pass)
+            // back to the face positions (P^T with approx_quad = false) into T0, then added to the
+            // nodes: GLL at the face nodes, sides 0 and 2, then 1 and 3 (corners are shared by
+            // neighbouring sides only); Gauss-Legendre along the lines, phi_k(-1) times the face
+            // value, one side at a time (legendre_transpose_2d)
+            for (int o = lane; o < 4 * n; o += 32)
             {
-                for (int o = lane; o < 2 * n; o += 32)
+                const int s = o / n, k = o - s * n;
+                for (int d = 0; d < nv; ++d)
                 {
-                    const int s = pass + 2 * (o / n), k = o % n;
-                    if (!wanted(s))
-                        continue;
-                    const int node = va_node(n, s, k);
-                    for (int d = 0; d < nv; ++d)
+                    double f = 0.0;
+                    if (wanted(s))
                     {
-                        double f;
                         if (ex)
-                        {
-                            f = 0.0;
                             for (int q = 0; q < Qf; ++q)
                                 f += UF[nv * (s * Qf + q) + d] * A.Pf[q + Qf * k];
-                        }
                         else
                             f = UF[nv * (s * Qf + k) + d];
-                        r[nv * node + d] += f;
                     }
+                    T0[nv * o + d] = f;
                 }
-                __syncwarp();
             }
+            __syncwarp();
+            if (leg)
+                for (int s = 0; s < 4; ++s)
+                {
+                    if (wanted(s))
+                        for (int o = lane; o < nn; o += 32)
+                        {
+                            const int i = o % n, k = o / n, node = va_line(n, s, i, k);
+                            for (int d = 0; d < nv; ++d)
+                                r[nv * node + d] += T0[nv * (s * n + i) + d] * A.e[k];
+                        }
+                    __syncwarp();
+                }
+            else
+                for (int pass = 0; pass < 2; ++pass)
+                {
+                    for (int o = lane; o < 2 * n; o += 32)
+                    {
+                        const int s = pass + 2 * (o / n), k = o % n;
+                        if (!wanted(s))
+                            continue;
+                        const int node = va_node(n, s, k);
+                        for (int d = 0; d < nv; ++d)
+                            r[nv * node + d] += T0[nv * (s * n + k) + d];
+                    }
+                    __syncwarp();
+                }
             if (a.mode == VA_ACT || a.mode == VA_BC)
             {
                 for (int o = lane; o < nv * nn; o += 32)
@@ -309,7 +373,7 @@ namespace
                 }
                 else
                 {
-                    // MassMatrix<true>: w_i w_j det J at the node
+                    // MassMatrix<true>: w_i w_j det J at the basis node
                     const int i = row % n, j = row / n;
                     const double xi = A.xg[i], eta = A.xg[j];
                     const double Xx = 0.25 * ((1.0 - eta) * (c[2] - c[0]) + (1.0 + eta) * (c[4] - c[6]));
@@ -452,14 +516,32 @@ namespace
     // source/EdgeFlux.cpp:140-190, or setup_flux_2d_q, :430-494, per edge in the edge's order,
     // the coefficient traces as LobattoFaceProlongator lays them out); G(t, c, d, q, s, el),
     // t = 0 the element's own trace, 1 its neighbour's
-    int face_table(const wdg_mesh &mesh, int n, int nv, int Qf, bool approx, const double *a,
-                   const std::vector<double> &wg, const std::vector<double> &wf, const std::vector<double> &Pf,
-                   std::vector<double> &G)
+    int line_of(int n, int s, int i, int k)
+    {
+        const int x = (s == 0 || s == 2) ? i : (s == 1 ? n - 1 - k : k);
+        const int y = (s == 1 || s == 3) ? i : (s == 2 ? n - 1 - k : k);
+        return x + n * y;
+    }
+
+    int face_table(const wdg_mesh &mesh, int n, int nv, int Qf, bool approx, bool legendre, const double *a,
+                   const std::vector<double> &e, const std::vector<double> &wg, const std::vector<double> &wf,
+                   const std::vector<double> &Pf, std::vector<double> &G)
     {
         const int v2 = nv * nv, nn = n * n;
         G.assign((size_t)2 * v2 * Qf * 4 * mesh.nel, 0.0);
         auto A = [&](int flat, int comp, int node, int el)
         { return a[flat + v2 * (comp + 2 * (node + (size_t)nn * el))]; };
+        // the coefficient's trace at position j of side s of element el (Lobatto: the face node;
+        // Legendre: sum_k phi_k(-1) a(line node k), legendre_action_2d)
+        auto trace = [&](int flat, int comp, int s, int j, int el)
+        {
+            if (!legendre)
+                return A(flat, comp, node_of(n, s, j), el);
+            double v = 0.0;
+            for (int k = 0; k < n; ++k)
+                v += A(flat, comp, line_of(n, s, j, k), el) * e[k];
+            return v;
+        };
         std::vector<double> F((size_t)2 * v2 * Qf), nA(v2), At((size_t)2 * v2 * n);
         for (int type = 0; type < 2; ++type)
         {
@@ -481,9 +563,9 @@ namespace
                             {
                                 double v = 0.0;
                                 if (s == 0)
-                                    v = A(f, comp, node_of(n, E.s0, j), E.el0);
+                                    v = trace(f, comp, E.s0, j, E.el0);
                                 else if (type == 0)
-                                    v = A(f, comp, node_of(n, E.s1, E.delta < 0 ? n - 1 - j : j), E.el1);
+                                    v = trace(f, comp, E.s1, E.delta < 0 ? n - 1 - j : j, E.el1);
                                 At[f + v2 * (comp + 2 * (size_t)j)] = v;
                             }
                     for (int q = 0; q < Qf; ++q)
@@ -573,12 +655,15 @@ namespace
         A.Pf = h->d_Pf;
         A.xg = h->d_xg;
         A.wg = h->d_wg;
-        A.Minv = h->exact ? waveq_minv(h->exact) : nullptr;
+        A.e = h->d_e;
+        A.nb = h->d_nb;
+        A.Minv = h->d_Minv;
         A.n = h->n;
         A.nv = h->nv;
         A.Q = h->Q;
         A.Qf = h->Qf;
         A.approx = h->approx ? 1 : 0;
+        A.legendre = h->legendre ? 1 : 0;
         const int warps = va_warps(h);
         const size_t smem = sizeof(double) * (size_t)va_warp_doubles(h->n, h->nv, h->Q, h->Qf) * warps;
         const unsigned blocks = (unsigned)std::max(1, std::min((c.nel + warps - 1) / warps, 148 * 16));
@@ -605,8 +690,8 @@ namespace
 
 extern "C"
 {
-    int wdg_vadvect_create(const wdg_mesh *mesh, int n_colloc, int n_var, const double *a, int approx_quad, int device,
-                           wdg_vadvect **out)
+    int wdg_vadvect_create(const wdg_mesh *mesh, int n_colloc, int basis_type, int n_var, const double *a,
+                           int approx_quad, int device, wdg_vadvect **out)
     {
         if (!mesh || !a || !out)
             return fail(WDG_ERR_ARG, "wdg_vadvect_create: null argument");
@@ -615,15 +700,22 @@ extern "C"
             return fail(WDG_ERR_UNSUPPORTED, "wdg_vadvect_create: n_var must be 1..8");
         if (n_colloc < kMinN || n_colloc > kMaxN)
             return fail(WDG_ERR_UNSUPPORTED, "wdg_vadvect_create: n_colloc must be 2..9");
+        if (basis_type != WDG_GAUSS_LEGENDRE && basis_type != WDG_GAUSS_LOBATTO)
+            return fail(WDG_ERR_ARG, "wdg_vadvect_create: basis_type must be WDG_GAUSS_LEGENDRE or WDG_GAUSS_LOBATTO");
         const int n = n_colloc, nv = n_var;
-        const bool approx = approx_quad != 0;
+        const bool approx = approx_quad != 0, legendre = basis_type == WDG_GAUSS_LEGENDRE;
         // default rules: Div<false> p = (n-2) + (n-1) + 1 + (n-1) (source/Div.cpp:313-330),
         // EdgeFlux<false> p = 2 (n-1) + 2 + (n-1) (source/EdgeFlux.cpp:496-512); exact to 2 (1 + p/2) - 1
         const int Q = approx ? n : 1 + ((n - 2) + (n - 1) + 1 + (n - 1)) / 2;
         const int Qf = approx ? n : 1 + (2 * (n - 1) + 2 + (n - 1)) / 2;
         std::vector<double> xg(n), wg(n), xv(Q), wv(Q), xf(Qf), wf(Qf), P((size_t)Q * n), D((size_t)Q * n),
-            Pf((size_t)Qf * n), op, G;
-        gauss_lobatto(n, xg.data(), wg.data());
+            Pf((size_t)Qf * n), e(n), op, G, Mf, Mi;
+        if (legendre)
+            gauss_legendre(n, xg.data(), wg.data());
+        else
+            gauss_lobatto(n, xg.data(), wg.data());
+        const double minus1 = -1.0;
+        interp_matrix(n, xg.data(), 1, &minus1, e.data()); // phi_k(-1)
         if (approx)
         {
             xv = xg;
@@ -640,7 +732,21 @@ extern "C"
         lagrange_deriv_at(n, xg.data(), Q, xv.data(), D.data());
         interp_matrix(n, xg.data(), Qf, xf.data(), Pf.data());
         volume_table(*mesh, n, nv, Q, approx, a, xg, wg, xv, wv, P, op);
-        WDG_TRY(face_table(*mesh, n, nv, Qf, approx, a, wg, wf, Pf, G));
+        WDG_TRY(face_table(*mesh, n, nv, Qf, approx, legendre, a, e, wg, wf, Pf, G));
+        if (!approx)
+            WDG_TRY(exact_mass(*mesh, n, xg.data(), 1 + (2 * (n - 1) + 2) / 2, Mf, Mi));
+        // Legendre: each side's neighbour and its side, and whether the edge runs against it
+        std::vector<int> nb;
+        if (legendre)
+        {
+            nb.assign(4 * (size_t)mesh->nel, -1);
+            for (const EdgeRec &E : mesh->interior)
+            {
+                const int rev = E.delta < 0 ? 1 : 0;
+                nb[4 * (size_t)E.el0 + E.s0] = ((E.el1 * 4 + E.s1) << 1) | rev;
+                nb[4 * (size_t)E.el1 + E.s1] = ((E.el0 * 4 + E.s0) << 1) | rev;
+            }
+        }
 
         wdg_vadvect *h = new wdg_vadvect;
         h->n = n;
@@ -648,15 +754,8 @@ extern "C"
         h->Q = Q;
         h->Qf = Qf;
         h->approx = approx;
-        int st = WDG_OK;
-        if (approx)
-            st = wdg_wave_create(mesh, n, nullptr, WDG_FP64, device, &h->w);
-        else
-        {
-            st = wdg_waveq_create(mesh, n, nullptr, device, &h->exact);
-            if (st == WDG_OK)
-                st = wdg_waveq_wave(h->exact, &h->w);
-        }
+        h->legendre = legendre;
+        int st = wdg_wave_create(mesh, n, nullptr, WDG_FP64, device, &h->w);
         if (st != WDG_OK)
         {
             wdg_vadvect_destroy(h);
@@ -675,6 +774,15 @@ extern "C"
         chk(upload(wg, &h->d_wg));
         chk(upload(op, &h->d_op));
         chk(upload(G, &h->d_G));
+        chk(upload(e, &h->d_e));
+        if (!approx)
+            chk(upload(Mi, &h->d_Minv));
+        if (legendre)
+        {
+            chk(device_alloc(&h->d_nb, nb.size()));
+            if (st == WDG_OK)
+                chk(device_put(h->d_nb, nb));
+        }
         if (st == WDG_OK)
         {
             static std::mutex mu;
@@ -707,14 +815,14 @@ extern "C"
         if (h->w)
         {
             DeviceScope g(h->w->device);
-            for (double *p : {h->d_Pv, h->d_Dv, h->d_Pf, h->d_xg, h->d_wg, h->d_op, h->d_G, h->d_buf[0], h->d_buf[1],
-                              h->d_buf[2]})
+            for (double *p : {h->d_Pv, h->d_Dv, h->d_Pf, h->d_xg, h->d_wg, h->d_e, h->d_op, h->d_G, h->d_Minv,
+                              h->d_buf[0], h->d_buf[1], h->d_buf[2]})
                 if (p)
                     cudaFree(p);
+            if (h->d_nb)
+                cudaFree(h->d_nb);
         }
-        if (h->exact)
-            wdg_waveq_destroy(h->exact); // owns w
-        else if (h->w)
+        if (h->w)
             wdg_wave_destroy(h->w);
         delete h;
     }

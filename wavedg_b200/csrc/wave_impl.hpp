@@ -86,6 +86,10 @@ namespace wdg
     // reference's lagrange_basis_deriv); the element inverse mass matrices of an exact handle
     void lagrange_deriv_at(int n, const double *x, int nq, const double *xq, double *D);
     const double *waveq_minv(const wdg_waveq *h);
+    // MassMatrix<false>'s element matrices and inverses for the basis with nodes x on the
+    // qm x qm Gauss-Legendre rule, (n^2, n^2, nel) each
+    int exact_mass(const wdg_mesh &mesh, int n, const double *x, int qm, std::vector<double> &Mf,
+                   std::vector<double> &Mi);
     // symmetric m x m (m <= kJacobiMax) eigen-decomposition by cyclic Jacobi rotations:
     // A = R diag(e) R^T, column-major
     constexpr int kJacobiMax = 8;

@@ -808,19 +808,24 @@ class AdvectionSystem:
 class VariableAdvectionSystem:
     """Linear advection with a spatially varying coefficient (wdg_vadvect_*): Advection<AQ>,
     AdvectionHomogeneousBC<AQ> (constant_coefficient = false) and MassMatrix<AQ> for n_var
-    variables on a GLL basis; a in the reference's (n_var, n_var, 2, n, n, n_elem) layout
-    (a host array); approx_quad False selects the Gauss-Legendre rules of Div<false> /
-    EdgeFlux<false> and the dense mass matrix, as examples/advec2d.cpp does.  One variable, or
-    symmetric coefficient matrices.  FP64."""
+    variables on a Gauss-Lobatto or Gauss-Legendre basis (a QuadratureRule; an int means
+    Gauss-Lobatto); a in the reference's (n_var, n_var, 2, n, n, n_elem) layout (a host array);
+    approx_quad False selects the Gauss-Legendre rules of Div<false> / EdgeFlux<false> and the
+    dense mass matrix.  examples/advec2d.cpp uses a Gauss-Legendre basis with approx_quad False.
+    One variable, or symmetric coefficient matrices.  FP64."""
 
     def __init__(self, n_var: int, mesh: Mesh2D, basis, a, approx_quad: bool = True, device: int = -1):
-        self.n_var, self.mesh, self.n = int(n_var), mesh, _gll_n(basis)
+        if isinstance(basis, QuadratureRule):
+            self.n, self.basis_type = basis.n, basis.type
+        else:
+            self.n, self.basis_type = int(basis), QuadratureRule.GaussLobatto
+        self.n_var, self.mesh = int(n_var), mesh
         self.approx_quad = bool(approx_quad)
         av = np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
         if av.size != 2 * self.n_var ** 2 * self.n ** 2 * mesh.n_elem():
             raise WdgError(_lib.WDG_ERR_ARG, "a must hold 2 n_var^2 n^2 n_elem coefficients")
         h = C.c_void_p()
-        check(lib().wdg_vadvect_create(mesh._h, self.n, self.n_var, C.c_void_p(av.ctypes.data),
+        check(lib().wdg_vadvect_create(mesh._h, self.n, int(self.basis_type), self.n_var, C.c_void_p(av.ctypes.data),
                                        int(self.approx_quad), device, C.byref(h)), "wdg_vadvect_create")
         self._h = h
         self.ndof = self.n_var * self.n * self.n * mesh.n_elem()
