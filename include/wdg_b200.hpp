@@ -361,6 +361,89 @@ namespace b200
     private:
         std::shared_ptr<wdg_claw> h_;
     };
+
+    // Linear advection (wavedg/Advection.hpp:17-273) on the GPU for any coefficient, basis and
+    // quadrature of the reference's Advection<ApproxQuad>: a spatially varying coefficient
+    // a(n_var, n_var, 2, n, n, n_elem), or a constant one (n_var, n_var, 2) spread to the
+    // nodes.  n.A must be scalar or symmetric.  The handle behind these classes holds the
+    // operator tables the reference builds at construction.
+    inline std::shared_ptr<wdg_vadvect> make_advection(int n_var, const dg::Mesh2D &mesh, const dg::QuadratureRule *basis,
+                                                       const double *a, bool constant_coefficient, bool approx_quad,
+                                                       int device)
+    {
+        const int n = basis->n, nel = mesh.n_elem(), per = 2 * n_var * n_var;
+        std::vector<double> spread;
+        if (constant_coefficient)
+        {
+            spread.resize((size_t)per * n * n * nel);
+            for (size_t p = 0; p < (size_t)n * n * nel; ++p)
+                for (int k = 0; k < per; ++k)
+                    spread[(size_t)per * p + k] = a[k];
+            a = spread.data();
+        }
+        const int type = basis->type == dg::QuadratureRule::GaussLegendre ? WDG_GAUSS_LEGENDRE : WDG_GAUSS_LOBATTO;
+        Mesh m(mesh);
+        wdg_vadvect *h = nullptr;
+        check(wdg_vadvect_create(m.get(), n, type, n_var, a, approx_quad ? 1 : 0, device, &h));
+        return std::shared_ptr<wdg_vadvect>(h, wdg_vadvect_destroy);
+    }
+
+    template <bool ApproxQuad>
+    class Advection : public dg::Operator
+    {
+    public:
+        Advection(int n_var, const dg::Mesh2D &mesh, const dg::QuadratureRule *basis, const double *a,
+                  bool constant_coefficient, int device = -1)
+            : h_(make_advection(n_var, mesh, basis, a, constant_coefficient, ApproxQuad, device))
+        {
+        }
+        // du += (A u, grad v) - interior fluxes
+        void action(const double *u, double *du) const override { check(wdg_vadvect_action(h_.get(), u, du)); }
+        void action(int, const double *u, double *du) const override { action(u, du); }
+
+    private:
+        std::shared_ptr<wdg_vadvect> h_;
+    };
+
+    template <bool ApproxQuad>
+    class AdvectionHomogeneousBC : public dg::Operator
+    {
+    public:
+        AdvectionHomogeneousBC(int n_var, const dg::Mesh2D &mesh, const dg::QuadratureRule *basis, const double *a,
+                               bool constant_coefficient, int device = -1)
+            : h_(make_advection(n_var, mesh, basis, a, constant_coefficient, ApproxQuad, device))
+        {
+        }
+        // du += boundary fluxes with u = 0 outside the domain
+        void action(const double *u, double *du) const override { check(wdg_vadvect_bc_action(h_.get(), u, du)); }
+        void action(int, const double *u, double *du) const override { action(u, du); }
+
+    private:
+        std::shared_ptr<wdg_vadvect> h_;
+    };
+
+    // The time derivative of examples/advec2d.cpp as one operator: action(u, dudt) overwrites
+    // dudt with M^{-1} (Advection + AdvectionHomogeneousBC) u; steps() runs ode::SSPRK3 (the
+    // example's stepper) or ode::RungeKutta4 with one fused launch per stage.
+    template <bool ApproxQuad>
+    class AdvectionSystem : public dg::Operator
+    {
+    public:
+        AdvectionSystem(int n_var, const dg::Mesh2D &mesh, const dg::QuadratureRule *basis, const double *a,
+                        bool constant_coefficient, int device = -1)
+            : h_(make_advection(n_var, mesh, basis, a, constant_coefficient, ApproxQuad, device))
+        {
+        }
+        void action(const double *u, double *dudt) const override { check(wdg_vadvect_rhs(h_.get(), u, dudt)); }
+        void action(int, const double *u, double *dudt) const override { action(u, dudt); }
+        void steps(double dt, double &t, double *u, int nsteps = 1, bool rk4 = false) const
+        {
+            check(wdg_vadvect_steps(h_.get(), rk4 ? 0 : 1, u, dt, &t, nsteps));
+        }
+
+    private:
+        std::shared_ptr<wdg_vadvect> h_;
+    };
 } // namespace b200
 } // namespace dg
 

@@ -317,6 +317,65 @@ int main()
     euler_case(std::true_type{});
     euler_case(std::false_type{});
 
+    // examples/advec2d.cpp as shipped: a Gauss-Legendre basis, approx_quad = false, the rotating
+    // coefficient c = r (y, -x) projected by LinearFunctional2D and MassMatrix<false>::inv, and
+    // ode::SSPRK3 on M^{-1} (Advection + AdvectionHomogeneousBC), against b200::Advection,
+    // b200::AdvectionHomogeneousBC and b200::AdvectionSystem
+    {
+        auto gl = QuadratureRule::quadrature_rule(5, QuadratureRule::GaussLegendre);
+        Mesh2D amesh = perturbed_mesh(8, 11);
+        const int nd = 25 * amesh.n_elem();
+        MassMatrix<false> am(amesh, gl);
+        LinearFunctional2D LF(amesh, gl);
+        std::vector<double> c(2 * (size_t)nd);
+        auto coefficient = [](const double x[2], double cc[2])
+        {
+            const double r = std::hypot(x[0], x[1]);
+            cc[0] = r * x[1];
+            cc[1] = -r * x[0];
+        };
+        LF.action(2, coefficient, c.data());
+        am.inv(2, c.data());
+        Advection<false> adv(1, amesh, gl, c.data(), false);
+        AdvectionHomogeneousBC<false> abc(1, amesh, gl, c.data(), false);
+        auto dudt = [&](double *out, double, const double *v)
+        {
+            for (int i = 0; i < nd; ++i)
+                out[i] = 0.0;
+            adv.action(v, out);
+            abc.action(v, out);
+            am.inv(1, out);
+        };
+        b200::Advection<false> gadv(1, amesh, gl, c.data(), false);
+        b200::AdvectionHomogeneousBC<false> gbc(1, amesh, gl, c.data(), false);
+        b200::AdvectionSystem<false> gsys(1, amesh, gl, c.data(), false);
+        std::vector<double> u(nd), r1(nd), r2(nd);
+        for (double &x : u)
+            x = N01(gen);
+        for (int i = 0; i < nd; ++i)
+            r1[i] = r2[i] = N01(gen);
+        adv.action(u.data(), r1.data());
+        gadv.action(u.data(), r2.data());
+        std::printf("advection, Gauss-Legendre basis, approx_quad = false:\n");
+        report("  Advection::action", rel(r2, r1), 1e-12);
+        for (int i = 0; i < nd; ++i)
+            r1[i] = r2[i] = N01(gen);
+        abc.action(u.data(), r1.data());
+        gbc.action(u.data(), r2.data());
+        report("  AdvectionHomogeneousBC::action", rel(r2, r1), 1e-12);
+        dudt(r1.data(), 0.0, u.data());
+        gsys.action(u.data(), r2.data());
+        report("  time derivative (advec2d composition)", rel(r2, r1), 1e-12);
+        const double dta = 1.0 / 25.0 / M_SQRT2 * amesh.min_h();
+        std::vector<double> ur = u, ug = u;
+        double tr = 0.0, tg = 0.0;
+        ode::SSPRK3 ssp(nd);
+        for (int s = 0; s < 5; ++s)
+            ssp.step(dta, dudt, tr, ur.data());
+        gsys.steps(dta, tg, ug.data(), 5);
+        report("  ode::SSPRK3 vs b200::AdvectionSystem, 5 steps", rel(ug, ur), 1e-11);
+    }
+
     std::printf("%s\n", failures ? "DROP-IN FAILED" : "drop-in ok");
     return failures ? 1 : 0;
 }

@@ -155,8 +155,8 @@ def test_argument_errors_before_any_device_work(L):
         W.AdvectionSystem(2, mesh, basis, np.zeros(5))
     with pytest.raises(W.WdgError, match="n_elem coefficients"):
         W.Advection(1, mesh, basis, [1.0, 0.0], constant_coefficient=False)
-    with pytest.raises(W.WdgError, match="approx_quad=True only"):
-        W.Advection(1, mesh, basis, [1.0, 0.0], approx_quad=False)
+    with pytest.raises(W.WdgError, match="2 n_var"):
+        W.Advection(1, mesh, basis, [1.0, 0.0, 3.0], approx_quad=False)
     # a spatially varying coefficient whose n.A is not symmetric: refused at set-up, on the host
     a = np.zeros((mesh.n_elem(), 4, 4, 2, 2, 2))
     a[..., 0, 0, 1] = 1.0  # A_0 = [[0, 0], [1, 0]]

@@ -113,3 +113,23 @@ def test_variable_coefficient_advection_matches_reference(gpu_lib, fname):
         s.sync()
         np.testing.assert_array_equal(vd.cpu().numpy(), v)
 
+
+
+@pytest.mark.parametrize("fname", golden_files("adv_"))
+def test_constant_coefficient_through_the_table_path(gpu_lib, fname):
+    """A constant coefficient spread to the nodes through the variable-coefficient kernel gives
+    the reference's constant-coefficient Advection<true> results (the route the mirror classes
+    take for exact quadrature and Gauss-Legendre bases)."""
+    import wavedg_b200 as W
+
+    g = golden(fname)
+    mesh = W.Mesh2D.from_vertices(g["verts"], g["quads"])
+    n, nv = int(g["n"]), int(g["nv"])
+    basis = W.QuadratureRule.quadrature_rule(n, W.QuadratureRule.GaussLobatto)
+    s = W.VariableAdvectionSystem(nv, mesh, basis, np.tile(g["a"], n * n * mesh.n_elem()), True)
+    r = np.zeros_like(g["u"])
+    s.rhs(g["u"], r)
+    assert rel(r, g["rhs"]) < TOL
+    r = g["action_in"].copy()
+    s.action(g["u"], r)
+    assert rel(r, g["action"]) < TOL

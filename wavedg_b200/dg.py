@@ -925,12 +925,21 @@ class EulerSystem:
 
 
 def _advection_system(n_var, mesh, basis, a, constant_coefficient, quad, approx_quad):
+    """The fused constant-coefficient path for GLL bases with approx_quad; every other case
+    (a varying coefficient, exact quadrature, a Gauss-Legendre basis) through the table-driven
+    path, a constant coefficient spread to the nodes."""
     if quad is not None:
         raise WdgError(_lib.WDG_ERR_UNSUPPORTED, "advection is built for the default quadrature rules")
-    if not constant_coefficient:
-        return VariableAdvectionSystem(n_var, mesh, basis, a, approx_quad)
-    _require_approx(approx_quad)
-    return AdvectionSystem(n_var, mesh, basis, a)
+    legendre = isinstance(basis, QuadratureRule) and basis.type == QuadratureRule.GaussLegendre
+    if constant_coefficient and approx_quad and not legendre:
+        return AdvectionSystem(n_var, mesh, basis, a)
+    if constant_coefficient:
+        n = basis.n if isinstance(basis, QuadratureRule) else int(basis)
+        av = np.asarray(a, dtype=np.float64).reshape(-1)
+        if av.size != 2 * int(n_var) ** 2:
+            raise WdgError(_lib.WDG_ERR_ARG, "a must hold 2 n_var^2 coefficients")
+        a = np.tile(av, n * n * mesh.n_elem())
+    return VariableAdvectionSystem(n_var, mesh, basis, a, approx_quad)
 
 
 class Advection(Operator):
