@@ -687,6 +687,68 @@ def advection(device: int, n_el: int = 256, P: int = 4, nv: int = 2, reps: int =
             op.rhs(uh)
             out["cpu_reference_ms_per_rhs"] = (time.perf_counter() - t0) * 1e3
             out["cpu_reference"] = "the reference's Advection / AdvectionHomogeneousBC / MassMatrix<true>, 1 thread"
+    out["advec2d"] = advection_variable(device, n_el, P, reps, cpu_leg)
+    return out
+
+
+def _rhs_ms(s, u, du, reps):
+    import torch
+
+    for _ in range(3):
+        s.rhs(u, du)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        s.rhs(u, du)
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def advection_variable(device: int, n_el: int, P: int, reps: int, cpu_leg: bool) -> dict:
+    """examples/advec2d.cpp's operators: one variable, the rotating coefficient r (y, -x) at the
+    nodes of a Gauss-Legendre basis, approx_quad = false (Div<false>, EdgeFlux<false>,
+    MassMatrix<false>): one fused RHS on a perturbed n_el x n_el mesh.  Algorithmic bytes: u in,
+    dudt out, the volume and face tables and the dense inverse mass matrix per element."""
+    import torch
+
+    import wavedg_b200 as W
+    from wavedg_b200 import meshgen as mg
+
+    v, q = mg.perturbed_rect(n_el, 0.2, seed=1)
+    mesh = W.Mesh2D.from_vertices(v, q)
+    n = P + 1
+    basis = W.QuadratureRule.quadrature_rule(n, W.QuadratureRule.GaussLegendre)
+    xg = np.polynomial.legendre.leggauss(n)[0]
+    c = np.asarray(v)[np.asarray(q)]
+    xi, eta = xg[None, None, :], xg[None, :, None]
+    xy = [0.25 * ((1 - xi) * (1 - eta) * c[:, 0, k][:, None, None] + (1 + xi) * (1 - eta) * c[:, 1, k][:, None, None]
+                  + (1 + xi) * (1 + eta) * c[:, 2, k][:, None, None] + (1 - xi) * (1 + eta) * c[:, 3, k][:, None, None])
+          for k in range(2)]
+    r = np.hypot(xy[0], xy[1])
+    a = np.stack([r * xy[1], -r * xy[0]], axis=-1).reshape(-1)  # a(0, 0, comp, i, j, el)
+    s = W.VariableAdvectionSystem(1, mesh, basis, a, approx_quad=False, device=device)
+    u = torch.from_numpy(np.random.default_rng(2).standard_normal(s.ndof)).cuda()
+    du = torch.empty_like(u)
+    ms = _rhs_ms(s, u, du, reps)
+    nel = mesh.n_elem()
+    Q, Qf = 1 + (3 * n - 3) // 2, 1 + (3 * n - 1) // 2
+    byts = 16 * s.ndof + 8 * nel * (2 * Q * Q + 8 * Qf + n ** 4) + 64 * nel
+    peak, _ = peak_hbm()
+    out = {"workload": f"rhs_advec2d_nvar1_gauss_legendre_exact_{n_el}x{n_el}_P{P}_perturbed", "values": s.ndof,
+           "ms_per_rhs": ms, "values_per_s": s.ndof / (ms / 1e3), "bytes_per_rhs": byts,
+           "achieved_gbs": byts / (ms / 1e3) / 1e9, "frac": byts / (ms / 1e3) / 1e9 / peak,
+           "kernel": "vadv_kernel (one fused launch per RHS)"}
+    if cpu_leg:
+        kind, cpu = _ref_lib()
+        if kind == "reference":
+            op = cpu.OpV(cpu.Mesh(v, q, "reference"), n, 1, a, False, 0)
+            uh = u.cpu().numpy()
+            t0 = time.perf_counter()
+            op.rhs(uh)
+            out["cpu_reference_ms_per_rhs"] = (time.perf_counter() - t0) * 1e3
+            out["cpu_reference"] = "the reference's Advection<false> / AdvectionHomogeneousBC<false> / MassMatrix<false>, 1 thread"
     return out
 
 
@@ -747,6 +809,21 @@ def euler(device: int, n_el: int = 256, P: int = 4, reps: int = 20, cpu_leg: boo
             op.rhs(U)
             out["cpu_reference_ms_per_rhs"] = (time.perf_counter() - t0) * 1e3
             out["cpu_reference"] = "the reference's DivF2D / EdgeFluxF2D / MassMatrix<true> with the example's fluxes, 1 thread"
+    # approx_quad = false, as the example ships: 2n-point rules and the dense inverse mass matrix
+    sq = W.EulerSystem(mesh, basis, device=device, approx_quad=False)
+    msq = _rhs_ms(sq, u, du, reps)
+    byq = byts + 8 * nel * n ** 4
+    out["exact"] = {"workload": f"rhs_euler_exact_{n_el}x{n_el}_P{P}_perturbed", "ms_per_rhs": msq,
+                    "values_per_s": s.ndof / (msq / 1e3), "bytes_per_rhs": byq,
+                    "achieved_gbs": byq / (msq / 1e3) / 1e9, "frac": byq / (msq / 1e3) / 1e9 / peak,
+                    "kernel": "qeuler_kernel (one fused launch per RHS / stage)"}
+    if cpu_leg:
+        kind, cpu = _ref_lib()
+        if kind == "reference":
+            opq = cpu.OpEQ(cpu.Mesh(v, q, "reference"), n)
+            t0 = time.perf_counter()
+            opq.rhs(U)
+            out["exact"]["cpu_reference_ms_per_rhs"] = (time.perf_counter() - t0) * 1e3
     return out
 
 
