@@ -28,7 +28,7 @@ def _setup(precision):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-@pytest.mark.parametrize("world,kind", [(3, "blocks"), (4, "random")])
+@pytest.mark.parametrize("world,kind", [(3, "blocks"), (3, "rcb"), (4, "random")])
 def test_decomposed_steps_match_undivided(gpu_lib, precision, world, kind):
     from wavedg_b200 import decomp
 
@@ -38,11 +38,15 @@ def test_decomposed_steps_match_undivided(gpu_lib, precision, world, kind):
     ref = u0.copy()
     whole.rk4_steps(ref, dt, 0.0, nsteps)
     nel = mesh.n_elem()
-    part = decomp.partition(nel, world) if kind == "blocks" else \
-        np.random.default_rng(9).integers(0, world, size=nel).astype(np.int32)
+    if kind == "blocks":  # contiguous element ids: spatially scattered on this scrambled mesh
+        part = decomp.partition(nel, world)
+    elif kind == "rcb":
+        part = decomp.partition_mesh(mesh, world, "rcb")
+    else:
+        part = np.random.default_rng(9).integers(0, world, size=nel).astype(np.int32)
     doms = [decomp.Domain(mesh, basis, bc, part, r, precision=precision) for r in range(world)]
     assert all(d.halo > 0 for d in doms)
-    if kind == "blocks":  # block partitions have elements that read no halo trace
+    if kind == "rcb":  # coordinate bisection leaves elements that read no halo trace
         assert all(d.split > 0 for d in doms)
     for overlap in (True, False):
         for d in doms:
