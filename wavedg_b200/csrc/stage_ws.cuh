@@ -49,25 +49,6 @@ namespace wdg
 
     int ws_epw(int n) { return 32 / n; }
 
-    // Layout of a consumer warp's column-pass scratch: the sums of node (i, j), field f of the
-    // warp-round's element e at e * ss + 3 i + rs * j + f.  The column pass writes with lanes
-    // across (e, i) and the row pass reads with lanes across (e, j); the padded row stride rs
-    // and element stride ss (chosen per n and word size by counting, for the lane split
-    // e = lane / n, the distinct words per shared-memory bank in each access) make both
-    // patterns free of bank conflicts where the split allows it (8-byte words: n = 3, 7, 9
-    // keep a few).
-    struct WsScratch
-    {
-        int rs, ss;
-    };
-    template <typename Real>
-    __host__ __device__ constexpr WsScratch ws_scratch(int n)
-    {
-        constexpr int r8[10] = {0, 0, 7, 13, 13, 19, 19, 23, 25, 31}, s8[10] = {0, 0, 14, 39, 52, 95, 114, 161, 200, 279};
-        constexpr int r4[10] = {0, 0, 7, 9, 13, 15, 19, 21, 25, 29}, s4[10] = {0, 0, 14, 27, 52, 75, 114, 152, 200, 261};
-        return sizeof(Real) == 8 ? WsScratch{r8[n], s8[n]} : WsScratch{r4[n], s4[n]};
-    }
-
     // shared-memory layout (bytes), identical on host and device:
     //   [2 S mbarriers | pad to 128][x (n), w (n) | pad to 128][S slots][consumer scratch]
     //   slot    = u (C, 3 n^2) | du (C, 3 n^2) | halo (C, 4 n, 3) | corners (C, 8 doubles) | fcode (C, u32)
@@ -143,7 +124,6 @@ namespace wdg
         r1 = r[1];
         r2 = r[2];
     }
-
 
     // One chunk of one RK stage as both roles see it (the single-solve kernel fills it from
     // its launch arguments, the batched kernel from its solve table).
@@ -344,7 +324,7 @@ namespace wdg
                                                const Real *xtab, const Real *wtab, int cw, int lane)
     {
         using Sh = WsShape<N>;
-        constexpr int ND = Sh::ND, NF = Sh::NF, EW = Sh::EW;
+        constexpr int NN = Sh::NN, ND = Sh::ND, NF = Sh::NF, EW = Sh::EW;
         constexpr bool STG = WsStage<Real, EXTRA>::value;
         const WsSlot o = ws_slot<Real>(N, c.chunk, STG);
         const int flags = c.flags;
@@ -371,8 +351,7 @@ namespace wdg
                 uint32_t codes = 0;
                 const Real *halo_e = halo + le * NF * 3;
                 Real *ue = us + le * ND;
-                constexpr WsScratch SC = ws_scratch<Real>(N);
-                Real *rc = Rc + el_l * SC.ss; // this element's column-pass sums (WsScratch layout)
+                Real *rc = Rc + el_l * NN * 3; // this element's column-pass sums, (node, field)
                 if (act)
                 {
                     const double2 *c2 = reinterpret_cast<const double2 *>(cs + 8 * le);
@@ -424,7 +403,7 @@ namespace wdg
 #pragma unroll
                     for (int j = 0; j < N; ++j)
                     {
-                        Real *o = rc + 3 * i + SC.rs * j;
+                        Real *o = rc + 3 * (i + N * j);
                         o[0] = sp[j];
                         o[1] = su[j];
                         o[2] = sv[j];
@@ -490,7 +469,7 @@ namespace wdg
 #pragma unroll
                     for (int i = 0; i < N; ++i)
                     {
-                        const Real *cr = rc + 3 * i + SC.rs * j;
+                        const Real *cr = rc + 3 * (i + N * j);
                         Real r0 = ap[i] + cr[0], r1 = au[i] + cr[1], r2 = av[i] + cr[2];
                         const size_t g = (size_t)(c.el0 + le) * ND + 3 * (i + N * j);
                         if (EXTRA && (flags & F_FORCE))
@@ -569,12 +548,12 @@ namespace wdg
     __host__ __device__ inline WsLayout ws_layout(int n, int chunk, int stages, bool staged)
     {
         WsLayout L;
-        const int ew = 32 / n;
+        const int nn = n * n, ew = 32 / n;
         L.slot = ws_slot<Real>(n, chunk, staged).bytes;
         L.tab = 128;
         L.slots = (L.tab + 2 * n * (int)sizeof(Real) + 127) & ~127;
         L.scratch = L.slots + stages * L.slot;
-        L.warp_scratch = ((ew * ws_scratch<Real>(n).ss * (int)sizeof(Real)) + 15) & ~15;
+        L.warp_scratch = ((ew * 3 * nn * (int)sizeof(Real)) + 15) & ~15;
         L.total = L.scratch + kWsConsumers * L.warp_scratch;
         return L;
     }
@@ -681,7 +660,7 @@ namespace wdg
         }
 
         // ---------------------------------------------------------------- consumers
-        Real *Rc = reinterpret_cast<Real *>(smem + L.scratch + warp * L.warp_scratch); // column sums (WsScratch)
+        Real *Rc = reinterpret_cast<Real *>(smem + L.scratch + warp * L.warp_scratch); // [EW][NN][3] column sums
         for (int m = 0; m < M; ++m)
         {
             const int q = m % S;
