@@ -337,15 +337,24 @@ namespace
                 dzb[i] = __float2bfloat16(v);
         }
     }
-    // db[c] (+)= sum_{b, p} dz[b, c, p]: one block per channel, fixed summation order
-    __global__ void bias_grad_kernel(const float *dz, float *db, int Bn, int Cn, long long P, int accumulate)
+    // db[c] (+)= sum_{b, p} dz[b, c, p] in a fixed summation order, in two launches so that the
+    // whole GPU reads dz: block (c, slice) sums its slice of every sample's plane into part,
+    // then one thread per channel adds the slices in order
+    constexpr int kBiasSlices = 64;
+    __global__ void bias_grad_partial_kernel(const float *__restrict__ dz, float *__restrict__ part, int Bn, int Cn,
+                                             long long P)
     {
         __shared__ float red[256];
-        const int c = blockIdx.x;
+        const int c = blockIdx.x, sl = blockIdx.y;
+        const long long chunk = (P + gridDim.y - 1) / gridDim.y;
+        const long long p0 = sl * chunk, p1 = (p0 + chunk < P) ? p0 + chunk : P;
         float s = 0.f;
         for (int b = 0; b < Bn; ++b)
-            for (long long p = threadIdx.x; p < P; p += blockDim.x)
-                s += dz[((long long)b * Cn + c) * P + p];
+        {
+            const float *row = dz + ((long long)b * Cn + c) * P;
+            for (long long p = p0 + threadIdx.x; p < p1; p += blockDim.x)
+                s += row[p];
+        }
         red[threadIdx.x] = s;
         __syncthreads();
         for (int h = blockDim.x / 2; h > 0; h >>= 1)
@@ -355,7 +364,17 @@ namespace
             __syncthreads();
         }
         if (threadIdx.x == 0)
-            db[c] = accumulate ? db[c] + red[0] : red[0];
+            part[(long long)c * gridDim.y + sl] = red[0];
+    }
+    __global__ void bias_grad_final_kernel(const float *__restrict__ part, float *db, int Cn, int S, int accumulate)
+    {
+        const int c = blockIdx.x * blockDim.x + threadIdx.x;
+        if (c >= Cn)
+            return;
+        float s = 0.f;
+        for (int k = 0; k < S; ++k)
+            s += part[(long long)c * S + k];
+        db[c] = accumulate ? db[c] + s : s;
     }
     __global__ void f32_to_bf16_kernel(const float *x, bf16 *y, long long n)
     {
@@ -598,7 +617,16 @@ extern "C"
     }
     int wdg_fno_bias_grad(const float *dz, float *db, int B, int C, long long P, int accumulate, void *stream)
     {
-        bias_grad_kernel<<<C, 256, 0, st(stream)>>>(dz, db, B, C, P, accumulate);
+        if (B < 1 || C < 1 || P < 1)
+            return wdg::fail(WDG_ERR_ARG, "wdg_fno_bias_grad: empty shape");
+        // the slices' partial sums in stream-ordered scratch
+        float *part = nullptr;
+        const cudaError_t e = cudaMallocAsync(reinterpret_cast<void **>(&part), sizeof(float) * C * kBiasSlices, st(stream));
+        if (e != cudaSuccess)
+            return wdg::cuda_fail(e, "cudaMallocAsync (wdg_fno_bias_grad)");
+        bias_grad_partial_kernel<<<dim3(C, kBiasSlices), 256, 0, st(stream)>>>(dz, part, B, C, P);
+        bias_grad_final_kernel<<<(C + 127) / 128, 128, 0, st(stream)>>>(part, db, C, kBiasSlices, accumulate);
+        cudaFreeAsync(part, st(stream));
         return done("wdg_fno_bias_grad");
     }
     int wdg_fno_to_bf16(const float *x, void *y, long long n, void *stream)
