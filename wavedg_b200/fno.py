@@ -276,3 +276,64 @@ class NodalGrid:
         check(_fn("wdg_fno_grid_to_nodes")(_p(g.contiguous()), _p(u), self.ne, self.n, _p(self.x), self.G,
                                            float(scale), C.c_void_p(t.cuda.current_stream().cuda_stream)))
         return u
+
+
+def step_profile(grid: int = 512, width: int = 32, modes: int = 16, layers: int = 4, hidden: int = 64,
+                 train_batch: int = 4, predict_batch: int = 8, warmup: int = 3) -> dict:
+    """Time one training step (forward, MSE, backward, Adam) and one prediction after `warmup`
+    rounds of both, on seeded inputs, and list every GEMM of the timed pair in launch order with
+    its shape and algorithmic bytes (BF16 operands read once; the FP32 result written, and read
+    again where beta = 1 or split-K accumulates).  The command to run under a launch-list
+    profiler: python -m wavedg_b200.fno --step-profile."""
+    import torch
+
+    net = FNO(grid=grid, width=width, modes=modes, layers=layers, hidden=hidden, seed=0)
+    rng = np.random.default_rng(0)
+    tgt = torch.from_numpy(rng.standard_normal((train_batch, 3, grid, grid))).to("cuda", torch.float32)
+    log = []
+    gemm = net._gemm
+
+    def logged(A, B, Cm, M, N, K, lda, ldb, ldc, sA=0, sB=0, sC=0, batch=1, tA=0, tB=0, alpha=1.0, beta=0.0,
+               ksplit=0):
+        rw = 2 if (beta != 0.0 or ksplit) else 1
+        log.append(dict(M=M, N=N, K=K, batch=batch, tA=tA, tB=tB, beta=beta, ksplit=ksplit,
+                        bytes=2 * batch * (M * K + K * N) + 4 * (batch if sC else 1) * M * N * rw,
+                        flops=2.0 * M * N * K * batch))
+        return gemm(A, B, Cm, M, N, K, lda, ldb, ldc, sA, sB, sC, batch, tA, tB, alpha, beta, ksplit)
+
+    net._gemm = logged
+
+    def train_step():
+        x = inputs(grid, rng.uniform(-0.5, 0.5, (train_batch, 2)), 0.05, 1.0)
+        y = net.forward(x, keep=True)
+        _, dy = net.mse(y, tgt)
+        net.backward(dy)
+        net.adam_step(lr=1e-3)
+
+    def predict():
+        return net.forward(inputs(grid, rng.uniform(-0.5, 0.5, (predict_batch, 2)), 0.05, 1.0))
+
+    for _ in range(warmup):
+        train_step()
+        predict()
+    torch.cuda.synchronize()
+    log.clear()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record()
+    train_step()
+    e1.record()
+    n_train = len(log)
+    predict()
+    e2.record()
+    torch.cuda.synchronize()
+    return {"train_step_ms": e0.elapsed_time(e1), "predict_ms": e1.elapsed_time(e2),
+            "train_gemms": log[:n_train], "predict_gemms": log[n_train:]}
+
+
+if __name__ == "__main__":
+    import json
+    import sys
+
+    if "--step-profile" not in sys.argv:
+        raise SystemExit("usage: python -m wavedg_b200.fno --step-profile")
+    print(json.dumps(step_profile()), flush=True)
