@@ -69,3 +69,22 @@ def test_grid_and_node_symmetries_agree():
         a = ws.sym_grid(torch.from_numpy(sample(u)), k).numpy()
         b = sample(ws.sym_nodes(u, NE, N, k))
         assert np.array_equal(a, b), k
+
+
+def test_shipped_weights_record_their_training():
+    """The network the bench's learned warm start loads: the shipped shape (4 Fourier layers,
+    32 channels, 16 modes, hidden 64, 512 grid), trained on 2000 generated solutions of the
+    128 x 128, P = 4, omega = 20 family, with every spectral tensor stored as float16 and a
+    power-of-two scale."""
+    import json
+
+    path = ws.PACKAGED_WEIGHTS
+    z = np.load(path)
+    meta = json.loads(str(z["__meta__"]))
+    assert meta["fno"] == {"layers": 4, "width": 32, "modes": 16, "hidden": 64}
+    assert meta["grid"] == 512 and meta["family"] == "waveholtz_128x128_P4_omega20_outflow"
+    assert meta["data"]["solutions"] == 2000 and meta["data"]["symmetries"] == 8
+    assert meta["final_rel_rms_error"] < 1e-2
+    spectral = [k for k in z.files if k.startswith("R") and not k.endswith(".exp2")]
+    assert spectral and all(z[k].dtype == np.float16 and k + ".exp2" in z.files for k in spectral)
+    assert float(z["__scale__"]) > 0
