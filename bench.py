@@ -296,9 +296,12 @@ def run_ours(args, rank, world, local_rank):
         companion("decomposition", decomposition, local_rank)
     if want("waveholtz_config4") and wh_ok:
         # last: its FP32 phase gets what is left of the run's time budget (0: no limit), keeping
-        # about three minutes for its FP64 finish and the plain-FP64 periods
+        # about three minutes for its FP64 finish and the plain-FP64 periods.  All 64 solves
+        # take about 21 minutes on one B200, more than a default run's budget: with a budget the
+        # leg solves the first 32 problems of the same seeded draw (about 7 minutes)
         left = args.budget - (time.perf_counter() - T_START) - 180.0 if args.budget > 0 else 1e9
-        companion("waveholtz_config4", waveholtz_config4, local_rank, deadline=max(60.0, left))
+        count = 64 if args.budget <= 0 or left > 1500.0 else 32
+        companion("waveholtz_config4", waveholtz_config4, local_rank, deadline=max(60.0, left), count=count)
 
 
     if dist is not None:
@@ -457,7 +460,8 @@ def waveholtz_config4(device: int, count: int = 64, seed: int = 4, deadline: flo
               from the iterate with the |pi0| measured before, so nothing is repeated); it stops
               at `deadline` seconds, and the record then says which solves were unfinished.
     plain     plain FP64 WaveHoltz, one solve at a time, is timed as one period of every solve
-              (WaveHoltz::S after a warm-up period) times the periods a plain solve of it runs:
+              (the faster of two WaveHoltz::S calls after a warm-up period) times the periods a
+              plain solve of it runs:
               its iterations + 1 (the pi0 period), the iterations being those the batch needed
               (FP32 + FP64 iterations; the same fixed-point map).  The rule is checked on the two
               solves with the fewest DOF-steps per period, solved in full.
@@ -540,11 +544,14 @@ def waveholtz_config4(device: int, count: int = 64, seed: int = 4, deadline: flo
         wh = W.WaveHoltz(oms[i], meshes[i], bases[i], bcs[i], True, system=s64[i])
         w = torch.zeros_like(Fs[i])
         wh.pi0(w, Fs[i])  # warm-up: records the period's graph
-        torch.cuda.synchronize()
-        ts = time.perf_counter()
-        wh.S(w)
-        torch.cuda.synchronize()
-        per[i] = time.perf_counter() - ts
+        best = float("inf")
+        for _ in range(2):
+            torch.cuda.synchronize()
+            ts = time.perf_counter()
+            wh.S(w)
+            torch.cuda.synchronize()
+            best = min(best, time.perf_counter() - ts)
+        per[i] = best
         del wh, w
     plain_iters = it32 + it64
     t_plain_est = per * (plain_iters + 1)
@@ -565,6 +572,7 @@ def waveholtz_config4(device: int, count: int = 64, seed: int = 4, deadline: flo
     done = int(np.sum((st64 == 0) & (r64 < 1e-6)))
     return {"workload": f"waveholtz_batch_{count}_solves_n64-256_P3-6_omega10-40_1-4src_tol1e-6",
             "solves": count, "total_dof": int(ndof.sum()), "seed": seed,
+            "draw": f"the first {count} problems of the seeded draw (seed {seed}) whose first 64 are the stated batch",
             "per_solve": [{"n": p[0], "P": p[1], "omega": round(p[2], 4), "sources": len(p[4]), "ndof": int(ndof[i]),
                            "nt": int(nt[i]), "fp32_iterations": int(it32[i]), "fp64_iterations": int(it64[i]),
                            "residual": float(r64[i]), "plain_period_s": float(per[i])}
