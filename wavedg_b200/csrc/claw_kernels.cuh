@@ -34,13 +34,24 @@ namespace wdg
 
     constexpr int kClawWarps = 4;
 
+    // resident CTAs per SM the register budget is set for (the kernel is latency-bound: more
+    // resident warps hide more of each warp's load -> compute -> store chain); degrees above 4
+    // keep the compiler's own budget (their unrolled contractions would spill)
+    template <int N, int NV>
+    constexpr int claw_min_blocks()
+    {
+        return N > 5 ? 1 : NV <= 2 ? 6 : NV == 3 ? 5 : NV <= 6 ? 4 : 3;
+    }
+
     template <int N, int NV, class M>
-    __global__ void __launch_bounds__(32 * kClawWarps) claw_kernel(const ClawArgs a)
+    __global__ void __launch_bounds__(32 * kClawWarps, claw_min_blocks<N, NV>()) claw_kernel(const ClawArgs a)
     {
         constexpr int NN = N * N, ND = NV * NN;
         extern __shared__ double csm[];
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        double *q = csm + (size_t)warp * 3 * ND, *Fs = q + ND, *Gs = Fs + ND;
+        // per warp: the element's values, the two contravariant fluxes, and the neighbour traces
+        // T(s, k, d) of its interior sides
+        double *q = csm + (size_t)warp * (3 * ND + 4 * N * NV), *Fs = q + ND, *Gs = Fs + ND, *T = Gs + ND;
         const long long limit = (long long)a.nel * NN; // nodes a neighbour index may name
         for (int el = blockIdx.x * kClawWarps + warp; el < a.nel; el += gridDim.x * kClawWarps)
         {
@@ -53,6 +64,24 @@ namespace wdg
                 c[k] = __ldg(a.corners + 8 * (size_t)el + k);
             const uint32_t codes = __ldg(a.fcode + el);
             const int4 fb = __ldg(a.fbase + el);
+            // the neighbour traces of the interior sides, copied asynchronously (cp.async) while
+            // the volume term is formed; an index outside the state is reported and not read
+            for (int o = lane; o < 4 * N; o += 32)
+            {
+                const int s = o / N, k = o - s * N;
+                const uint32_t byte = (codes >> (8 * s)) & 0xffu;
+                if (byte & 0x80u)
+                    continue;
+                const int off = (s == 0) ? fb.x : (s == 1) ? fb.y : (s == 2) ? fb.z : fb.w;
+                const long long pn = (long long)(off / 3) + (long long)k * (partner_stride<N>(byte) / 3);
+                if (off < 0 || pn < 0 || pn >= limit)
+                    atomicOr(a.err, 2u);
+                else
+#pragma unroll
+                    for (int d = 0; d < NV; ++d)
+                        cp_async<8>(T + NV * o + d, a.x + (size_t)NV * pn + d);
+            }
+            cp_async_commit();
             __syncwarp();
             // volume: contravariant fluxes per node
             for (int node = lane; node < NN; node += 32)
@@ -76,6 +105,7 @@ namespace wdg
                     Gs[NV * node + d] = -(Yx * W) * f[d] + (Xx * W) * g[d];
                 }
             }
+            cp_async_wait<0>();
             __syncwarp();
             for (int node = lane; node < NN; node += 32)
             {
@@ -120,19 +150,10 @@ namespace wdg
                     {
                         const int off = (s == 0) ? fb.x : (s == 1) ? fb.y : (s == 2) ? fb.z : fb.w;
                         const long long pn = (long long)(off / 3) + (long long)k * (partner_stride<N>(byte) / 3);
-                        if (off < 0 || pn < 0 || pn >= limit)
-                        {
-                            atomicOr(a.err, 2u);
+                        const bool bad = off < 0 || pn < 0 || pn >= limit; // reported by the gather
 #pragma unroll
-                            for (int d = 0; d < NV; ++d)
-                                ext[d] = qq[d];
-                        }
-                        else
-                        {
-#pragma unroll
-                            for (int d = 0; d < NV; ++d)
-                                ext[d] = __ldg(a.x + (size_t)NV * pn + d);
-                        }
+                        for (int d = 0; d < NV; ++d)
+                            ext[d] = bad ? qq[d] : T[NV * (s * N + k) + d];
                     }
                     double nx, ny, meas, fh[NV];
                     claw_side(c, s, nx, ny, meas);
@@ -223,7 +244,10 @@ namespace wdg
     }
 
     // shared memory of one CTA of claw_kernel
-    inline size_t claw_smem(int n, int nv) { return sizeof(double) * 3 * (size_t)nv * n * n * kClawWarps; }
+    inline size_t claw_smem(int n, int nv)
+    {
+        return sizeof(double) * ((size_t)3 * nv * n * n + (size_t)4 * n * nv) * kClawWarps;
+    }
 
     template <int N, int NV, class M>
     cudaError_t launch_claw_nv(const ClawArgs &a, cudaStream_t s)
