@@ -33,6 +33,8 @@ namespace wdg
     }
 
     constexpr int kClawWarps = 4;
+    // doubles of a CTA's shared copy of the basis table (D, nodes, weights), kept even
+    __host__ __device__ constexpr int claw_tab_doubles(int n) { return (n * n + 2 * n + 1) & ~1; }
 
     // resident CTAs per SM the register budget is set for (the kernel is latency-bound: more
     // resident warps hide more of each warp's load -> compute -> store chain); degrees above 4
@@ -49,9 +51,21 @@ namespace wdg
         constexpr int NN = N * N, ND = NV * NN;
         extern __shared__ double csm[];
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        // the basis table (D, nodes, weights) in shared memory: the lanes of a warp read
+        // different entries, which the constant cache would serve one address at a time
+        double *sD = csm, *sx = sD + NN, *sw = sx + N;
+        for (int k = threadIdx.x; k < NN; k += blockDim.x)
+            sD[k] = Tab<double>::D(N, k);
+        for (int k = threadIdx.x; k < N; k += blockDim.x)
+        {
+            sx[k] = Tab<double>::x(N, k);
+            sw[k] = Tab<double>::w(N, k);
+        }
+        __syncthreads();
         // per warp: the element's values, the two contravariant fluxes, and the neighbour traces
         // T(s, k, d) of its interior sides
-        double *q = csm + (size_t)warp * (3 * ND + 4 * N * NV), *Fs = q + ND, *Gs = Fs + ND, *T = Gs + ND;
+        double *q = csm + claw_tab_doubles(N) + (size_t)warp * (3 * ND + 4 * N * NV), *Fs = q + ND, *Gs = Fs + ND,
+               *T = Gs + ND;
         const long long limit = (long long)a.nel * NN; // nodes a neighbour index may name
         for (int el = blockIdx.x * kClawWarps + warp; el < a.nel; el += gridDim.x * kClawWarps)
         {
@@ -87,12 +101,12 @@ namespace wdg
             for (int node = lane; node < NN; node += 32)
             {
                 const int i = node % N, j = node / N;
-                const double xi = Tab<double>::x(N, i), eta = Tab<double>::x(N, j);
+                const double xi = sx[i], eta = sx[j];
                 const double Xx = 0.25 * ((1.0 - eta) * (c[2] - c[0]) + (1.0 + eta) * (c[4] - c[6]));
                 const double Yx = 0.25 * ((1.0 - eta) * (c[3] - c[1]) + (1.0 + eta) * (c[5] - c[7]));
                 const double Xe = 0.25 * ((1.0 - xi) * (c[6] - c[0]) + (1.0 + xi) * (c[4] - c[2]));
                 const double Ye = 0.25 * ((1.0 - xi) * (c[7] - c[1]) + (1.0 + xi) * (c[5] - c[3]));
-                const double W = Tab<double>::w(N, i) * Tab<double>::w(N, j);
+                const double W = sw[i] * sw[j];
                 double qq[NV], f[NV], g[NV];
 #pragma unroll
                 for (int d = 0; d < NV; ++d)
@@ -117,8 +131,8 @@ namespace wdg
                     double s = 0.0;
 #pragma unroll
                     for (int l = 0; l < N; ++l)
-                        s += Tab<double>::D(N, l + N * i) * Fs[NV * (l + N * j) + d] +
-                             Tab<double>::D(N, l + N * j) * Gs[NV * (i + N * l) + d];
+                        s += sD[l + N * i] * Fs[NV * (l + N * j) + d] +
+                             sD[l + N * j] * Gs[NV * (i + N * l) + d];
                     r[d] = s;
                 }
                 const size_t g0 = (size_t)el * ND + (size_t)NV * node;
@@ -158,19 +172,19 @@ namespace wdg
                     double nx, ny, meas, fh[NV];
                     claw_side(c, s, nx, ny, meas);
                     M::template numflux<NV>(a, el, s, nx, ny, qq, ext, fh);
-                    const double wk = Tab<double>::w(N, k) * meas;
+                    const double wk = sw[k] * meas;
 #pragma unroll
                     for (int d = 0; d < NV; ++d)
                         r[d] -= wk * fh[d];
                 }
                 // M^{-1}: w_i w_j det J (MassMatrix<true>)
                 {
-                    const double xi = Tab<double>::x(N, i), eta = Tab<double>::x(N, j);
+                    const double xi = sx[i], eta = sx[j];
                     const double Xx = 0.25 * ((1.0 - eta) * (c[2] - c[0]) + (1.0 + eta) * (c[4] - c[6]));
                     const double Yx = 0.25 * ((1.0 - eta) * (c[3] - c[1]) + (1.0 + eta) * (c[5] - c[7]));
                     const double Xe = 0.25 * ((1.0 - xi) * (c[6] - c[0]) + (1.0 + xi) * (c[4] - c[2]));
                     const double Ye = 0.25 * ((1.0 - xi) * (c[7] - c[1]) + (1.0 + xi) * (c[5] - c[3]));
-                    const double m = Tab<double>::w(N, i) * Tab<double>::w(N, j) * (Xx * Ye - Yx * Xe);
+                    const double m = sw[i] * sw[j] * (Xx * Ye - Yx * Xe);
 #pragma unroll
                     for (int d = 0; d < NV; ++d)
                         r[d] /= m;
@@ -246,7 +260,7 @@ namespace wdg
     // shared memory of one CTA of claw_kernel
     inline size_t claw_smem(int n, int nv)
     {
-        return sizeof(double) * ((size_t)3 * nv * n * n + (size_t)4 * n * nv) * kClawWarps;
+        return sizeof(double) * (claw_tab_doubles(n) + ((size_t)3 * nv * n * n + (size_t)4 * n * nv) * kClawWarps);
     }
 
     template <int N, int NV, class M>
