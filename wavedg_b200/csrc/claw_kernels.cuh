@@ -35,6 +35,11 @@ namespace wdg
     constexpr int kClawWarps = 4;
     // doubles of a CTA's shared copy of the basis table (D, nodes, weights), kept even
     __host__ __device__ constexpr int claw_tab_doubles(int n) { return (n * n + 2 * n + 1) & ~1; }
+    // doubles of one warp's staging: values, two fluxes, neighbour traces, masses, side geometry
+    __host__ __device__ constexpr int claw_warp_doubles(int n, int nv)
+    {
+        return (3 * nv * n * n + 4 * n * nv + n * n + 12 + 1) & ~1;
+    }
 
     // resident CTAs per SM the register budget is set for (the kernel is latency-bound: more
     // resident warps hide more of each warp's load -> compute -> store chain); degrees above 4
@@ -62,10 +67,11 @@ namespace wdg
             sw[k] = Tab<double>::w(N, k);
         }
         __syncthreads();
-        // per warp: the element's values, the two contravariant fluxes, and the neighbour traces
-        // T(s, k, d) of its interior sides
-        double *q = csm + claw_tab_doubles(N) + (size_t)warp * (3 * ND + 4 * N * NV), *Fs = q + ND, *Gs = Fs + ND,
-               *T = Gs + ND;
+        // per warp: the element's values, the two contravariant fluxes, the neighbour traces
+        // T(s, k, d) of its interior sides, the mass w_i w_j det J per node and (n_x, n_y, |E|/2)
+        // per side
+        double *q = csm + claw_tab_doubles(N) + (size_t)warp * claw_warp_doubles(N, NV), *Fs = q + ND, *Gs = Fs + ND,
+               *T = Gs + ND, *mj = T + 4 * N * NV, *sn = mj + NN;
         const long long limit = (long long)a.nel * NN; // nodes a neighbour index may name
         for (int el = blockIdx.x * kClawWarps + warp; el < a.nel; el += gridDim.x * kClawWarps)
         {
@@ -96,6 +102,21 @@ namespace wdg
                         cp_async<8>(T + NV * o + d, a.x + (size_t)NV * pn + d);
             }
             cp_async_commit();
+            if (lane < 4)
+            {
+                // one side per lane, each with a compile-time side index (keeps c in registers)
+                double nx = 0.0, ny = 0.0, meas = 0.0;
+                switch (lane)
+                {
+                case 0: claw_side(c, 0, nx, ny, meas); break;
+                case 1: claw_side(c, 1, nx, ny, meas); break;
+                case 2: claw_side(c, 2, nx, ny, meas); break;
+                default: claw_side(c, 3, nx, ny, meas); break;
+                }
+                sn[3 * lane] = nx;
+                sn[3 * lane + 1] = ny;
+                sn[3 * lane + 2] = meas;
+            }
             __syncwarp();
             // volume: contravariant fluxes per node
             for (int node = lane; node < NN; node += 32)
@@ -107,6 +128,7 @@ namespace wdg
                 const double Xe = 0.25 * ((1.0 - xi) * (c[6] - c[0]) + (1.0 + xi) * (c[4] - c[2]));
                 const double Ye = 0.25 * ((1.0 - xi) * (c[7] - c[1]) + (1.0 + xi) * (c[5] - c[3]));
                 const double W = sw[i] * sw[j];
+                mj[node] = W * (Xx * Ye - Yx * Xe); // MassMatrix<true>: w_i w_j det J
                 double qq[NV], f[NV], g[NV];
 #pragma unroll
                 for (int d = 0; d < NV; ++d)
@@ -169,22 +191,17 @@ namespace wdg
                         for (int d = 0; d < NV; ++d)
                             ext[d] = bad ? qq[d] : T[NV * (s * N + k) + d];
                     }
-                    double nx, ny, meas, fh[NV];
-                    claw_side(c, s, nx, ny, meas);
+                    const double nx = sn[3 * s], ny = sn[3 * s + 1], meas = sn[3 * s + 2];
+                    double fh[NV];
                     M::template numflux<NV>(a, el, s, nx, ny, qq, ext, fh);
                     const double wk = sw[k] * meas;
 #pragma unroll
                     for (int d = 0; d < NV; ++d)
                         r[d] -= wk * fh[d];
                 }
-                // M^{-1}: w_i w_j det J (MassMatrix<true>)
+                // M^{-1}: w_i w_j det J (MassMatrix<true>), formed with the volume term
                 {
-                    const double xi = sx[i], eta = sx[j];
-                    const double Xx = 0.25 * ((1.0 - eta) * (c[2] - c[0]) + (1.0 + eta) * (c[4] - c[6]));
-                    const double Yx = 0.25 * ((1.0 - eta) * (c[3] - c[1]) + (1.0 + eta) * (c[5] - c[7]));
-                    const double Xe = 0.25 * ((1.0 - xi) * (c[6] - c[0]) + (1.0 + xi) * (c[4] - c[2]));
-                    const double Ye = 0.25 * ((1.0 - xi) * (c[7] - c[1]) + (1.0 + xi) * (c[5] - c[3]));
-                    const double m = sw[i] * sw[j] * (Xx * Ye - Yx * Xe);
+                    const double m = mj[node];
 #pragma unroll
                     for (int d = 0; d < NV; ++d)
                         r[d] /= m;
@@ -260,7 +277,7 @@ namespace wdg
     // shared memory of one CTA of claw_kernel
     inline size_t claw_smem(int n, int nv)
     {
-        return sizeof(double) * (claw_tab_doubles(n) + ((size_t)3 * nv * n * n + (size_t)4 * n * nv) * kClawWarps);
+        return sizeof(double) * (claw_tab_doubles(n) + (size_t)claw_warp_doubles(n, nv) * kClawWarps);
     }
 
     template <int N, int NV, class M>
