@@ -386,8 +386,10 @@ namespace
 
     __host__ __device__ inline int qfused_warp_doubles(int n, int q, int qf)
     {
-        // su r (3 n^2 each) | Pu (3 n q) | Uq (3 q^2) | Fq (6 q^2) | Df Pg (3 q n each) | T1 (4 n 3) | UF (4 qf 3)
-        return 6 * n * n + 3 * n * q + 9 * q * q + 6 * q * n + 12 * n + 12 * qf;
+        // su r (3 n^2 each) | Pu (3 n q) | Uq (3 q^2) | Fq (7 q^2: six fluxes per point at an odd
+        // stride, which spreads a warp's accesses over the shared-memory banks) | Df Pg (3 q n
+        // each) | T1 (4 n 3) | UF (4 qf 3)
+        return 6 * n * n + 3 * n * q + 10 * q * q + 6 * q * n + 12 * n + 12 * qf;
     }
 
     // outward unit normal and measure (length / 2) of side s (StraightEdge, wavedg/Edge.hpp:107-122);
@@ -421,7 +423,7 @@ namespace
         const int n = a.n, q = a.q, qf = a.qf, nn = n * n, qq = q * q;
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
         double *su = qsm + (size_t)warp * qfused_warp_doubles(n, q, qf);
-        double *r = su + 3 * nn, *Pu = r + 3 * nn, *Uq = Pu + 3 * n * q, *Fq = Uq + 3 * qq, *Df = Fq + 6 * qq;
+        double *r = su + 3 * nn, *Pu = r + 3 * nn, *Uq = Pu + 3 * n * q, *Fq = Uq + 3 * qq, *Df = Fq + 7 * qq;
         double *Pg = Df + 3 * q * n, *T1 = Pg + 3 * q * n, *UF = T1 + 12 * n;
         const long long limit = 3LL * nn * a.nel;
         for (int el = blockIdx.x * kQWarps + warp; el < a.nel; el += gridDim.x * kQWarps)
@@ -465,7 +467,7 @@ namespace
                 const double W = a.wd[i] * a.wd[j];
                 const double Xxi = J[0] * W, Yxi = J[1] * W, Xeta = J[2] * W, Yeta = J[3] * W;
                 const double *U = Uq + 3 * o;
-                double *Fo = Fq + 6 * o;
+                double *Fo = Fq + 7 * o;
                 Fo[0] = Yeta * U[1] - Xeta * U[2];
                 Fo[1] = -Yxi * U[1] + Xxi * U[2];
                 Fo[2] = Yeta * U[0];
@@ -480,8 +482,8 @@ namespace
                 double df = 0.0, pg = 0.0;
                 for (int i = 0; i < q; ++i)
                 {
-                    df += a.Dd[i + q * k] * Fq[2 * d + 6 * (i + q * j)];
-                    pg += a.Pd[i + q * k] * Fq[2 * d + 1 + 6 * (i + q * j)];
+                    df += a.Dd[i + q * k] * Fq[2 * d + 7 * (i + q * j)];
+                    pg += a.Pd[i + q * k] * Fq[2 * d + 1 + 7 * (i + q * j)];
                 }
                 Df[o] = df;
                 Pg[o] = pg;
@@ -807,7 +809,7 @@ extern "C"
         h->nqm = qface(n_colloc);
         DeviceScope g(w->device);
         {
-            // the fused kernel's shared memory (69.5 KB at n = 9), opted in once per device and
+            // the fused kernel's shared memory (70.4 KiB at n = 9), opted in once per device and
             // before any period is captured into a graph
             static std::mutex mu;
             static uint64_t set = 0;
