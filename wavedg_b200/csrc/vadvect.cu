@@ -6,9 +6,9 @@
 // The reference turns the coefficient and the geometry into operator tables once, at
 // construction; this handle does the same on the host, with the same arithmetic:
 //   volume  op(comp, c, d, p, el), the contravariant coefficient times the weights at volume
-//           point p: the GLL nodes with approx_quad = true (Div<true>, source/Div.cpp:6-54), the
-//           Gauss-Legendre rule of Div<false> otherwise, the nodal coefficient interpolated to
-//           it first (op_2d, source/Div.cpp:239-361);
+//           point p: the basis nodes with approx_quad = true (Div<true>, source/Div.cpp:6-54),
+//           the Gauss-Legendre rule of Div<false> otherwise, the nodal coefficient interpolated
+//           to it first (op_2d, source/Div.cpp:239-361);
 //   faces   per element side and face point, in the element's own order, the two n_var x n_var
 //           matrices that multiply the element's own and its neighbour's trace: w |E|/2 Fs with
 //           Fs = R diag(-lambda/2 -+ |lambda|/2) R^T of n.A, A the face trace of each side's
@@ -22,8 +22,9 @@
 // neighbour's at the face points (Lobatto: nodal values, through the partner table of the
 // collocation handle; Legendre: the interpolation of LegendreFaceProlongator along the lines of
 // nodes normal to the side), the two matrices, back with P^T (flux_action_2d_c / _q,
-// source/EdgeFlux.cpp:289-320, 553-624) and onto the nodes (the prolongator's transpose); then adds the
-// result (the operators' action), or applies M^{-1} and writes the RHS or an RK4 / SSPRK3 stage.
+// source/EdgeFlux.cpp:289-320, 553-624) and onto the nodes (the prolongator's transpose);
+// then adds the result (the operators' action), or applies M^{-1} and writes the RHS or an
+// RK4 / SSPRK3 stage.
 // The flux matrices need a real eigen-decomposition of n.A: one variable, or symmetric
 // coefficient matrices (cyclic Jacobi), are built.  FP64.
 #include <cuda_runtime.h>
