@@ -208,6 +208,24 @@ int wdg_vadvect_bc_action(wdg_vadvect *adv, const double *u, double *du); /* Adv
 int wdg_vadvect_rhs(wdg_vadvect *adv, const double *u, double *dudt);
 int wdg_vadvect_steps(wdg_vadvect *adv, int method, double *u, double dt, double *t, int nsteps);
 
+/* ---- set-up operators on either basis type ---- */
+/* MassMatrix<AQ> (source/MassMatrix.cpp:6-227; approx_quad 1: diag(w_i w_j det J), 0: the exact
+ * element matrices on the (n + 1)-point rule) and LinearFunctional2D (wavedg/LinearFunctional.hpp:
+ * 61-202, its default n-point Gauss-Legendre rule) on a basis of basis_type, FP64: what
+ * examples/advec2d.cpp uses to project its coefficient, c = M^{-1} (f, phi), on a
+ * Gauss-Legendre basis. */
+typedef struct wdg_massmatrix wdg_massmatrix;
+int wdg_massmatrix_create(const wdg_mesh *mesh, int n_colloc, int basis_type, int approx_quad, int device,
+                          wdg_massmatrix **out);
+void wdg_massmatrix_destroy(wdg_massmatrix *m);
+int wdg_massmatrix_set_stream(wdg_massmatrix *m, void *cuda_stream);
+int wdg_massmatrix_action(wdg_massmatrix *m, int n_var, const double *x, double *y); /* y = M x (y may be x) */
+int wdg_massmatrix_inv(wdg_massmatrix *m, int n_var, double *x);                     /* x = M^{-1} x */
+/* the points the load vector samples f at: (x, y) of point k + n (l + n el), host array (2, n, n, nel) */
+int wdg_massmatrix_points(const wdg_massmatrix *m, double *xy);
+/* F(d, i, j, el) = (f_d, phi_ij) from fq(d, point), f at those points (host); F host or device */
+int wdg_massmatrix_load(wdg_massmatrix *m, int n_var, const double *fq, double *F);
+
 /* ---- nonlinear conservation law: the compressible Euler system of examples/cl2d.cpp ---- */
 /* State u(d, i, j, el), d = density, x-momentum, y-momentum, energy; gamma = 1.4; FP64.
  * The operators of the example with approx_quad = true on GLL nodes: DivF2D<true>

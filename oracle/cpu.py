@@ -60,6 +60,12 @@ _SIGS = {
     "opa_bc_action": ([_v, _dp, _dp], None),
     "opa_rhs": ([_v, _dp, _dp], None),
     "opa_rk4": ([_v, _d, _i, C.POINTER(C.c_double), _dp], None),
+    "mb_create": ([_v, _i, _i, _i], _v),
+    "mb_destroy": ([_v], None),
+    "mb_action": ([_v, _i, _dp, _dp], None),
+    "mb_inv": ([_v, _i, _dp], None),
+    "mb_points": ([_v, _dp], None),
+    "mb_load": ([_v, _i, _dp, _dp], None),
     "opv_create": ([_v, _i, _i, _dp, _i, _i], _v),
     "opv_destroy": ([_v], None),
     "opv_action": ([_v, _dp, _dp], None),
@@ -128,7 +134,7 @@ def lib(kind: str = "oracle"):
     for name, (args, res) in _SIGS.items():
         fn = getattr(L, prefix + name, None)
         if fn is None:
-            if kind == "oracle" and name.startswith(("opeq_", "opv_")):
+            if kind == "oracle" and name.startswith(("opeq_", "opv_", "mb_")):
                 continue  # operators that only the reference harness carries
             raise AttributeError(f"{path}: missing {prefix + name}")
         fn.argtypes = args
@@ -436,6 +442,41 @@ class OpEQ(OpE):
         tt = C.c_double(t)
         self.L.opeq_steps(self.h, {"rk4": 0, "ssprk3": 1}[method], dt, nsteps, C.byref(tt), u)
         return u, tt.value
+
+
+class MassB:
+    """MassMatrix<AQ> and LinearFunctional2D on a Gauss-Lobatto (basis_type 1) or
+    Gauss-Legendre (0) basis; the reference harness only."""
+
+    def __init__(self, mesh: Mesh, n: int, basis_type: int, approx_quad: bool):
+        self.L, self.mesh, self.n = mesh.L, mesh, n
+        self.h = self.L.mb_create(mesh.h, n, int(basis_type), int(bool(approx_quad)))
+        self.npts = n * n * mesh.n_elem
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.mb_destroy(self.h)
+            self.h = None
+
+    def action(self, nv, x):
+        y = np.zeros_like(_f64(x))
+        self.L.mb_action(self.h, nv, _f64(x), y)
+        return y
+
+    def inv(self, nv, x):
+        y = _f64(x).copy()
+        self.L.mb_inv(self.h, nv, y)
+        return y
+
+    def points(self):
+        xy = np.zeros(2 * self.npts)
+        self.L.mb_points(self.h, xy)
+        return xy
+
+    def load(self, nv, fq):
+        F = np.zeros(nv * self.npts)
+        self.L.mb_load(self.h, nv, _f64(fq), F)
+        return F
 
 
 class OpV:

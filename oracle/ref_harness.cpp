@@ -756,6 +756,77 @@ extern "C"
         }
     }
 
+    // ---- MassMatrix<AQ> and LinearFunctional2D on a basis of either type ----
+    struct RefMassB
+    {
+        const QuadratureRule *basis;
+        bool approx;
+        std::unique_ptr<MassMatrix<true>> mt;
+        std::unique_ptr<MassMatrix<false>> mf;
+        LinearFunctional2D lf;
+        int nel;
+        RefMassB(const Mesh2D &mesh, int n, QuadratureRule::QuadratureType type, bool approx_)
+            : basis(QuadratureRule::quadrature_rule(n, type)), approx(approx_), lf(mesh, basis), nel(mesh.n_elem())
+        {
+            if (approx)
+                mt = std::make_unique<MassMatrix<true>>(mesh, basis);
+            else
+                mf = std::make_unique<MassMatrix<false>>(mesh, basis);
+        }
+    };
+    // basis_type: 0 Gauss-Legendre, 1 Gauss-Lobatto
+    void *ref_mb_create(void *m, int n_colloc, int basis_type, int approx)
+    {
+        return new RefMassB(static_cast<RefMesh *>(m)->mesh, n_colloc,
+                            basis_type == 0 ? QuadratureRule::GaussLegendre : QuadratureRule::GaussLobatto, approx != 0);
+    }
+    void ref_mb_destroy(void *o) { delete static_cast<RefMassB *>(o); }
+    void ref_mb_action(void *o, int nv, const double *x, double *y)
+    {
+        RefMassB *b = static_cast<RefMassB *>(o);
+        if (b->approx)
+            b->mt->action(nv, x, y);
+        else
+            b->mf->action(nv, x, y);
+    }
+    void ref_mb_inv(void *o, int nv, double *x)
+    {
+        RefMassB *b = static_cast<RefMassB *>(o);
+        if (b->approx)
+            b->mt->inv(nv, x);
+        else
+            b->mf->inv(nv, x);
+    }
+    // the points at which LinearFunctional2D::action evaluates f, in its call order
+    // (x, y per point; point k + n (l + n el) of its default n-point rule)
+    void ref_mb_points(void *o, double *xy)
+    {
+        RefMassB *b = static_cast<RefMassB *>(o);
+        long long p = 0;
+        std::vector<double> F((size_t)b->basis->n * b->basis->n * b->nel);
+        auto f = [&](const double *x, double *out)
+        {
+            xy[2 * p] = x[0];
+            xy[2 * p + 1] = x[1];
+            ++p;
+            out[0] = 0.0;
+        };
+        b->lf.action(1, f, F.data());
+    }
+    // LinearFunctional2D::action with f given by its values fq(d, point) at those points
+    void ref_mb_load(void *o, int nv, const double *fq, double *F)
+    {
+        RefMassB *b = static_cast<RefMassB *>(o);
+        long long p = 0;
+        auto f = [&](const double *, double *out)
+        {
+            for (int d = 0; d < nv; ++d)
+                out[d] = fq[(size_t)nv * p + d];
+            ++p;
+        };
+        b->lf.action(nv, f, F);
+    }
+
     // ---- compressible Euler with approx_quad = false (examples/cl2d.cpp as shipped) ----
     void *ref_opeq_create(void *m, int n_colloc) { return new RefOpEQ(static_cast<RefMesh *>(m)->mesh, n_colloc); }
     void ref_opeq_destroy(void *o) { delete static_cast<RefOpEQ *>(o); }

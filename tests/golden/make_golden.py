@@ -234,6 +234,25 @@ def vadvection_fixture(name, v, q, m, n, nv, approx, seed, legendre=False):
     np.savez_compressed(os.path.join(HERE, f"vadv_{name}_n{n}_v{nv}_{tag}.npz"), **out)
 
 
+def mass_basis_fixture(name, v, q, m, n, legendre, approx, seed):
+    """MassMatrix<AQ> (action, inverse) and LinearFunctional2D on a Gauss-Legendre or
+    Gauss-Lobatto basis: the load of examples/advec2d.cpp's coefficient r (y, -x) and its
+    projection M^{-1} (f, phi), as that example forms it."""
+    rng = np.random.default_rng(seed)
+    bt = 0 if legendre else 1
+    mb = cpu.MassB(m, n, bt, approx)
+    x = rng.standard_normal(2 * mb.npts)
+    pts = mb.points()
+    px, py = pts[0::2], pts[1::2]
+    r = np.hypot(px, py)
+    fq = np.stack([r * py, -r * px], axis=1).reshape(-1)  # (d, point)
+    F = mb.load(2, fq)
+    out = dict(verts=v, quads=q, n=n, basis_type=bt, approx=int(approx), x=x, action=mb.action(2, x),
+               inv=mb.inv(2, x), points=pts, fq=fq, load=F, projection=mb.inv(2, F))
+    tag = ("gl" if legendre else "gll") + ("_aq" if approx else "_ex")
+    np.savez_compressed(os.path.join(HERE, f"massb_{name}_n{n}_{tag}.npz"), **out)
+
+
 def opq_fixture(name, v, q, m, n, seed):
     """approx_quad = false: Div<false>, EdgeFlux<false> (interior and boundary), WaveEquation,
     the composed boundary operator over EdgeFlux<false>, MassMatrix<false>, RHS, 5 RK4 steps."""
@@ -385,7 +404,14 @@ def main():
                 for approx in (True, False):
                     vadvection_fixture(name, v, q, cpu.Mesh(v, q, KIND), n, nv, approx,
                                        6500 + 100 * seed + 10 * n + nv + 5 * approx, legendre=True)
-        print("variable-coefficient advection fixtures written to", HERE)
+        mcases = {"scrambled6": [5, 3], "lshape3": [4]}
+        for seed, (name, v, q) in enumerate(meshes()):
+            for n in mcases.get(name, []):
+                for legendre in (True, False):
+                    for approx in (True, False):
+                        mass_basis_fixture(name, v, q, cpu.Mesh(v, q, KIND), n, legendre, approx,
+                                           6800 + 100 * seed + 10 * n + 2 * legendre + approx)
+        print("variable-coefficient advection and mass / load-vector fixtures written to", HERE)
         return
     if "--reference-meshes" in sys.argv:
         reference_meshes()

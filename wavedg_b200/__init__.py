@@ -14,6 +14,7 @@ from .dg import (  # noqa: F401
     EdgeFlux,
     EulerSystem,
     VariableAdvectionSystem,
+    BasisMassMatrix,
     FaceProlongator,
     FaceType,
     LinearFunctional2D,
@@ -35,7 +36,7 @@ from .dg import (  # noqa: F401
 )
 
 __all__ = [
-    "Advection", "AdvectionHomogeneousBC", "AdvectionSystem", "read_file", "to_file", "Discretisation", "Div", "ExactDiscretisation", "EdgeFlux", "EulerSystem", "VariableAdvectionSystem",
+    "Advection", "AdvectionHomogeneousBC", "AdvectionSystem", "read_file", "to_file", "Discretisation", "Div", "ExactDiscretisation", "EdgeFlux", "EulerSystem", "VariableAdvectionSystem", "BasisMassMatrix",
     "FaceProlongator", "FaceType", "LinearFunctional2D", "MassMatrix",
     "Mesh2D", "Operator", "QuadratureRule", "RungeKutta4", "WaveBC", "WaveEquation", "WaveHoltz", "WaveHoltzBatch", "WaveSystem",
     "WdgError", "WDG_FP32", "WDG_FP64", "error", "lib", "make_face_prolongator", "norm",

@@ -67,6 +67,13 @@ SIGNATURES = {
     "wdg_advect_bc_action": ([_v, _v, _v], _i),
     "wdg_advect_rhs": ([_v, _v, _v], _i),
     "wdg_advect_rk4_steps": ([_v, _v, _d, _v, _i], _i),
+    "wdg_massmatrix_create": ([_v, _i, _i, _i, _i, _vp], _i),
+    "wdg_massmatrix_destroy": ([_v], None),
+    "wdg_massmatrix_set_stream": ([_v, _v], _i),
+    "wdg_massmatrix_action": ([_v, _i, _v, _v], _i),
+    "wdg_massmatrix_inv": ([_v, _i, _v], _i),
+    "wdg_massmatrix_points": ([_v, _v], _i),
+    "wdg_massmatrix_load": ([_v, _i, _v, _v], _i),
     "wdg_vadvect_create": ([_v, _i, _i, _i, _v, _i, _i, _vp], _i),
     "wdg_vadvect_destroy": ([_v], None),
     "wdg_vadvect_set_stream": ([_v, _v], _i),

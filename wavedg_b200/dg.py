@@ -556,17 +556,73 @@ class EdgeFlux(Operator):
         check(lib().wdg_edge_flux(self.disc._h, self.face_type, pu, pf), "EdgeFlux.action")
 
 
+class BasisMassMatrix:
+    """MassMatrix<AQ> and LinearFunctional2D on a basis of either type (wdg_massmatrix_*): the
+    set-up operators for Gauss-Legendre bases (examples/advec2d.cpp)."""
+
+    def __init__(self, mesh: Mesh2D, basis, approx_quad: bool = True, device: int = -1):
+        n, bt = (basis.n, basis.type) if isinstance(basis, QuadratureRule) else (int(basis), QuadratureRule.GaussLobatto)
+        self.mesh, self.n = mesh, n
+        h = C.c_void_p()
+        check(lib().wdg_massmatrix_create(mesh._h, n, int(bt), int(bool(approx_quad)), device, C.byref(h)),
+              "wdg_massmatrix_create")
+        self._h = h
+        self.npts = n * n * mesh.n_elem()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _destroy("wdg_massmatrix_destroy", h)
+            self._h = None
+
+    def action(self, n_var, x, y) -> None:
+        px, _kx = _ptr(x, name="x")
+        py, _ky = _ptr(y, True, "y")
+        check(lib().wdg_massmatrix_action(self._h, int(n_var), px, py), "MassMatrix.action")
+
+    def inv(self, n_var, x) -> None:
+        px, _kx = _ptr(x, True, "x")
+        check(lib().wdg_massmatrix_inv(self._h, int(n_var), px), "MassMatrix.inv")
+
+    def points(self) -> np.ndarray:
+        """(npts, 2): where LinearFunctional2D samples f (its default n-point rule)."""
+        xy = np.zeros(2 * self.npts)
+        check(lib().wdg_massmatrix_points(self._h, C.c_void_p(xy.ctypes.data)), "points")
+        return xy.reshape(-1, 2)
+
+    def load(self, n_var, fq, F) -> None:
+        fq = np.ascontiguousarray(fq, dtype=np.float64).reshape(-1)
+        if fq.size != int(n_var) * self.npts:
+            raise WdgError(_lib.WDG_ERR_ARG, "fq must hold n_var values per point")
+        pF, _kF = _ptr(F, True, "F")
+        check(lib().wdg_massmatrix_load(self._h, int(n_var), C.c_void_p(fq.ctypes.data), pF),
+              "LinearFunctional2D.action")
+
+
+def _legendre(basis) -> bool:
+    return isinstance(basis, QuadratureRule) and basis.type == QuadratureRule.GaussLegendre
+
+
 class MassMatrix:
     """MassMatrix<true>: diagonal w_i w_j detJ (source/MassMatrix.cpp:6-82); with
-    approx_quad=False MassMatrix<false>: block Cholesky of the exact element mass matrices."""
+    approx_quad=False MassMatrix<false>: block Cholesky of the exact element mass matrices.
+    Gauss-Legendre bases through BasisMassMatrix."""
 
     def __init__(self, mesh: Mesh2D, basis, quad=None, approx_quad: bool = True):
         self.exact = not approx_quad
+        self.basis_mm = None
+        if _legendre(basis):
+            if quad is not None:
+                raise WdgError(_lib.WDG_ERR_UNSUPPORTED, "only the default rules are built for Gauss-Legendre bases")
+            self.basis_mm = BasisMassMatrix(mesh, basis, approx_quad)
+            return
         self.disc = (ExactDiscretisation(mesh, _gll_n(basis), quad=quad) if self.exact
                      else Discretisation(mesh, _gll_n(basis)))
 
     def action(self, *args) -> None:
         n_var, x, y = (args if len(args) == 3 else (1, *args))
+        if self.basis_mm is not None:
+            return self.basis_mm.action(n_var, x, y)
         if self.exact:
             return self.disc.mass_action(n_var, x, y)
         px, _kx = _ptr(x, name="x")
@@ -575,6 +631,8 @@ class MassMatrix:
 
     def inv(self, *args) -> None:
         n_var, x = (args if len(args) == 2 else (1, *args))
+        if self.basis_mm is not None:
+            return self.basis_mm.inv(n_var, x)
         if self.exact:
             return self.disc.mass_inv(n_var, x)
         px, _kx = _ptr(x, True, "x")
@@ -592,15 +650,25 @@ class WaveSystem(Discretisation):
 
 
 class LinearFunctional2D:
-    """(f, phi) with the n-point Gauss-Legendre rule (wavedg/LinearFunctional.hpp:136-202)."""
+    """(f, phi) with the n-point Gauss-Legendre rule (wavedg/LinearFunctional.hpp:136-202), on a
+    Gauss-Lobatto or Gauss-Legendre basis."""
 
     def __init__(self, mesh: Mesh2D, basis, quad=None):
-        if quad is not None and quad.n != _gll_n(basis):
+        self.basis_mm = None
+        n = basis.n if isinstance(basis, QuadratureRule) else int(basis)
+        if quad is not None and quad.n != n:
             raise WdgError(_lib.WDG_ERR_UNSUPPORTED, "only the default n-point quadrature is built")
+        if _legendre(basis):
+            self.basis_mm = BasisMassMatrix(mesh, basis, True)
+            return
         self.disc = Discretisation(mesh, _gll_n(basis))
 
     def action(self, n_var: int, f, F) -> None:
         """f(x, y) -> array (n_var, npts) (vectorised over quadrature points)."""
+        if self.basis_mm is not None:
+            xy = self.basis_mm.points()
+            vals = np.asarray(f(xy[:, 0], xy[:, 1]), dtype=np.float64).reshape(n_var, -1)
+            return self.basis_mm.load(n_var, np.ascontiguousarray(vals.T), F)
         xy = self.disc.quad_points().reshape(-1, 2)
         vals = np.asarray(f(xy[:, 0], xy[:, 1]), dtype=np.float64).reshape(n_var, -1)
         fq = np.ascontiguousarray(vals.T)
