@@ -172,3 +172,11 @@ def test_argument_errors_before_any_device_work(L):
     assert L.wdg_advect_create(mesh._h, 4, 9, C.c_void_p(np.zeros(162).ctypes.data), 0, C.byref(h)) == \
         W._lib.WDG_ERR_UNSUPPORTED
     assert L.wdg_mesh_partner_table(mesh._h, 1, None, None, None) == W._lib.WDG_ERR_ARG
+    # the Gauss-Legendre set-up and variable-coefficient handles check basis type and degree
+    # before any device work
+    a = np.zeros(2 * 16 * mesh.n_elem())
+    assert L.wdg_massmatrix_create(mesh._h, 4, 7, 1, 0, C.byref(h)) == W._lib.WDG_ERR_ARG
+    assert L.wdg_massmatrix_create(mesh._h, 12, 0, 1, 0, C.byref(h)) == W._lib.WDG_ERR_UNSUPPORTED
+    assert L.wdg_vadvect_create(mesh._h, 4, 7, 1, C.c_void_p(a.ctypes.data), 1, 0, C.byref(h)) == W._lib.WDG_ERR_ARG
+    assert L.wdg_vadvect_create(mesh._h, 4, 0, 9, C.c_void_p(a.ctypes.data), 1, 0, C.byref(h)) == \
+        W._lib.WDG_ERR_UNSUPPORTED
